@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 covariance path (one JSON line on rank 0).
+
+Workload (default): the medium synthetic scene - 200 cameras on a sphere cap,
+50k points, 2+Poisson(5) observations per point (~350k), 9-parameter
+cameras, FP64 Jacobian, TAYLOR_EXPANSION with three fixed points; the dense
+Schur complement is 1800 x 1800. One step = one full covariance solve
+(ingest -> J^T J blocks -> Schur complement -> inverse -> Taylor series ->
+camera and point covariances).
+
+  value : solves/s with the Jacobian resident in HBM (unc_compute_device),
+          L2 flushed (256 MB write) before every step, CUDA events on the
+          launching stream, max over ranks.
+  e2e   : solves/s through the public host API (unc_compute) from pinned
+          host buffers, H2D of the Jacobian and D2H of all outputs inside.
+  --impl reference : the CPU restatement of the reference algorithm (the
+          reference itself cannot be built here) on all host cores, including
+          its O(points x observations) per-point scan.
+
+Multi-GPU: the path does not shard (one dense Schur inverse per scene), so
+N GPUs run N independent replicas (scaling "weak"); value = N*K / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "medium": "medium scene: 200 cams (sphere cap r=20), 50k pts (4x4x2 box), 2+Poisson(5) obs/pt, "
+              "N=9C=1800, TAYLOR_EXPANSION",
+    "small": "small scene: 10 cams (ring r=10), 500 pts, 2+Poisson(4) obs/pt, N=90, TAYLOR_EXPANSION",
+    "large": "large scene: 2000 cams (3-loop trajectory), 500k pts, 2+Poisson(5) obs/pt, N=18000, "
+             "TAYLOR_EXPANSION",
+}
+METRIC = "covariance solve throughput (1 / solve time)"
+UNIT = "solves/s"
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="medium")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _traffic_from_profile(workload: str):
+    """DRAM bytes per Taylor-product launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"gemm_f64_{workload}.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+def _fp64_peak_tflops(torch, dev):
+    """cuBLAS DGEMM 8192^3, best of 5 (FP64 has no entry in the measured peaks file)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def run_reference(a):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from uncertaintyte_b200 import scenes
+    jac = scenes.synthetic_jacobian(a.workload, seed=0)
+    cores = os.cpu_count() or 1
+    faithful = a.workload != "large"
+    for _ in range(a.warmup):
+        oracle.compute(jac, threads=cores, faithful_point_scan=faithful)
+    t = 0.0
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        oracle.compute(jac, threads=cores, faithful_point_scan=faithful)
+        t += time.perf_counter() - t0
+    v = a.steps / t
+    sample = (f"{a.steps} full solves of the {a.workload} scene"
+              + (" with the reference's O(points x obs) point scan" if faithful else ""))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * t / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, no public dataset)",
+            "config": {"workload": WORKLOADS[a.workload], "threads": cores},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+
+    from uncertaintyte_b200 import native, scenes
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        dist.init_process_group("nccl", device_id=dev, timeout=__import__("datetime").timedelta(seconds=300))
+
+    jac = scenes.synthetic_jacobian(a.workload, seed=rank)
+    opts = native.make_options(jac, precision=a.precision)
+    d_rows = torch.from_numpy(jac.rows).to(dev)
+    d_cols = torch.from_numpy(jac.cols).to(dev)
+    d_vals = torch.from_numpy(jac.values).to(dev)
+    d_cam = torch.zeros(jac.num_cams * 45, dtype=torch.float64, device=dev)
+    d_pt = torch.zeros(jac.num_points * 6, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ctx = native.Context(local)
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+
+    def step():
+        return native.compute_covariances_device(ctx, opts, jac.num_rows, jac.num_cols,
+                                                 d_rows.data_ptr(), d_cols.data_ptr(),
+                                                 d_vals.data_ptr(), d_cam.data_ptr(),
+                                                 d_pt.data_ptr(), sptr)
+
+    for _ in range(max(a.warmup, 0)):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+
+    ctx.set_profiling(True)
+    ctx.profile(reset=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = native.kernel_launches()
+    evs = []
+    stats = None
+    for _ in range(a.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        stats = step()
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    launches = native.kernel_launches() - launches0
+    clk = clocks.stop()
+    ctx.set_profiling(False)
+    n_prod, prod_s, prod_flops = ctx.profile(reset=True)
+    t_local = sum(e0.elapsed_time(e1) for e0, e1 in evs) * 1e-3
+    t = torch.tensor([t_local], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_max = float(t.item())
+    value = ws * a.steps / t_max
+
+    # end to end through the public host API, pinned host buffers
+    e2e_steps = a.e2e_steps or max(3, a.steps // 2)
+    pinned = [torch.from_numpy(jac.rows).pin_memory(), torch.from_numpy(jac.cols).pin_memory(),
+              torch.from_numpy(jac.values).pin_memory(),
+              torch.zeros(jac.num_cams * 45, dtype=torch.float64).pin_memory(),
+              torch.zeros(jac.num_points * 6, dtype=torch.float64).pin_memory()]
+    h_rows, h_cols, h_vals, h_cam, h_pt = (t.numpy() for t in pinned)
+    import ctypes as C
+    L = native.lib()
+
+    def e2e_step():
+        st = native.UncStatistic()
+        rc = L.unc_compute(ctx.handle, C.byref(opts), jac.num_rows, jac.num_cols, h_rows.ctypes.data,
+                           h_cols.ctypes.data, h_vals.ctypes.data, h_cam.ctypes.data,
+                           h_pt.ctypes.data, C.byref(st))
+        native._check(rc)
+
+    e2e_step()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    te = 0.0
+    for _ in range(e2e_steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        te += time.perf_counter() - t0
+    te_t = torch.tensor([te], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(te_t, op=dist.ReduceOp.MAX)
+    e2e_value = ws * e2e_steps / float(te_t.item())
+    h2d = h_rows.nbytes + h_cols.nbytes + h_vals.nbytes
+    d2h = h_cam.nbytes + h_pt.nbytes
+
+    # roofline of the dominant kernel (the N x N x N FP64 Taylor product)
+    roof = None
+    if rank == 0:
+        peak = _fp64_peak_tflops(torch, dev)
+        achieved = prod_flops / prod_s / 1e12 if prod_s > 0 else None
+        traffic = _traffic_from_profile(a.workload)
+        roof = {"bound": "tensor", "kernel": "k_gemm_f64 (Taylor-series product, DMMA m8n8k4)",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak if achieved else None, "traffic": traffic,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in "
+                               "MEASURED_PEAKS.json)",
+                "launches_timed": n_prod, "flops_per_launch": prod_flops / max(n_prod, 1)}
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        cores = os.cpu_count() or 1
+        faithful = a.workload != "large"
+        t0 = time.perf_counter()
+        oracle.compute(jac, threads=cores, faithful_point_scan=faithful)
+        tc = time.perf_counter() - t0
+        cpu = {"value": 1.0 / tc, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"1 full solve of the {a.workload} scene (CPU restatement of the reference, "
+                         f"OpenMP + OpenBLAS{', O(points x obs) point scan' if faithful else ''})"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": 1e3 * t_max / a.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "mixed",
+                "data": "synthetic (seeded generator with the configuration's shapes; no public dataset)",
+                "config": {"workload": WORKLOADS[a.workload], "precision": a.precision,
+                           "l2": "flushed by a 256 MB write before every step",
+                           "parallelism": f"replicas x{ws}", "te_iterations": stats["te_iterations"]},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": int(d2h)},
+                "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+                "stage_seconds": {k: stats[k] for k in ("time_create_j", "time_fix_j", "time_norm_j",
+                                                        "time_multiply_jj", "time_compose_z",
+                                                        "time_inv_z", "time_te", "time_pts_unc",
+                                                        "time_all")}}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = _args()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

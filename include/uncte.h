@@ -1,0 +1,142 @@
+/*
+ * uncte.h - C ABI of the B200 (sm_100a) covariance-propagation library
+ * (libuncte.so). Plain C types only: pointers, sizes and status codes.
+ *
+ * Each entry point names the uncertaintyTE interface it replaces (paths are
+ * relative to the uncertaintyTE source tree). The C++ drop-in header
+ * include/uncertainty.h forwards to these functions.
+ *
+ * Layout contract (same as the reference): the Jacobian is a Ceres CRS
+ * matrix whose columns are [9*numCams camera params | 3*numPoints point
+ * params]; every observation is two consecutive rows of 12 entries (9 camera
+ * columns then 3 point columns, ascending). Outputs are caller-allocated:
+ * cam_unc[numCams*45] (row-major upper triangle of each 9x9 block) and
+ * pt_unc[numPoints*6] (00,01,02,11,12,22 of each 3x3 block).
+ *
+ * All functions are synchronous with respect to the host unless the name
+ * ends in _async. Errors are returned, never exit()ed.
+ */
+#ifndef UNCTE_H
+#define UNCTE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define UNC_OK 0
+#define UNC_ERR_INVALID_ARG (-1)   /* null pointer, negative size, inconsistent options */
+#define UNC_ERR_LAYOUT (-2)        /* Jacobian is not in the 2-row x 12-entry observation layout */
+#define UNC_ERR_NO_FIXED_POINTS (-3) /* TAYLOR_EXPANSION needs three fixed points */
+#define UNC_ERR_CUDA (-4)          /* CUDA runtime error (message: unc_last_error) */
+#define UNC_ERR_OUT_OF_MEMORY (-5) /* device allocation failed / request above the HBM budget */
+#define UNC_ERR_SINGULAR (-6)      /* non-positive pivot or non-finite value in the dense inverse */
+#define UNC_ERR_UNSUPPORTED (-7)   /* option combination not implemented (message: unc_last_error) */
+#define UNC_ERR_TOO_LARGE (-8)     /* size above a documented limit */
+
+/* algorithm selector, same values as include/uncertainty.h:11-13 */
+#define UNC_SVD_QR_ITERATION 0
+#define UNC_SVD_DEVIDE_AND_CONQUER 1
+#define UNC_TAYLOR_EXPANSION 2
+
+/* precision of the dense Taylor-series products */
+#define UNC_PRECISION_FP64 0  /* plain FP64 (DMMA) products: the parity path */
+#define UNC_PRECISION_MIXED 1 /* tensor-core split products + FP64 refinement */
+
+typedef struct unc_context unc_context;
+
+/* Mirrors cov::Options (src/uncertaintyTE/uncertainty.h:52-71) as plain C. */
+typedef struct {
+    int algorithm;      /* UNC_SVD_QR_ITERATION / UNC_SVD_DEVIDE_AND_CONQUER / UNC_TAYLOR_EXPANSION */
+    double epsilon;     /* SVD: singular-value threshold when svd_remove_n == -1 */
+    double lambda;      /* TE regulariser, -1 = automatic 10^(-1.2653 log10 N - 2.9415) */
+    int num_cams, cam_params, num_points, num_obs;
+    int svd_remove_n;   /* SVD: number of smallest singular values dropped (-1 = use epsilon) */
+    int max_iter_te;    /* unused by the reference (-1); kept for layout parity */
+    int pts2fix[3];     /* fixed point ids (TE); only the first two are sorted, as the reference does */
+    int has_pts2fix;    /* 0 = no fixed points given */
+    int precision;      /* UNC_PRECISION_FP64 or UNC_PRECISION_MIXED */
+} unc_options;
+
+/* Mirrors cov::Statistic (src/uncertaintyTE/uncertainty.h:73-82). Times are
+ * true seconds measured with CUDA events (the reference prints ms/100). */
+typedef struct {
+    double time_create_j, time_fix_j, time_norm_j, time_multiply_jj, time_split_jj, time_inv_v,
+        time_compose_z, time_inv_z, time_te, time_pts_unc, time_all;
+    double lambda;
+    int fixed_pts[3];
+    int te_iterations;        /* == cycle_change.size() in the reference */
+    double cycle_change[20];
+    long long device_bytes;   /* device workspace used by the call */
+} unc_statistic;
+
+/* Fill *opt with the reference's defaults: TAYLOR_EXPANSION, epsilon 1e-10,
+ * lambda -1, svd_remove_n -1, max_iter_te -1, 9 camera parameters
+ * (cov::Options::Options(numCams, camParams, numPoints, numObs),
+ * src/uncertaintyTE/uncertainty.h:62-63). */
+void unc_options_init(unc_options* opt, int num_cams, int cam_params, int num_points, int num_obs);
+
+/* A context owns a CUDA device, a stream and a growable device workspace
+ * that is reused across calls. Not thread-safe: one context per thread. */
+int unc_context_create(int device, unc_context** ctx);
+int unc_context_destroy(unc_context* ctx);
+
+/* computeCovariances(options, statistic, jacobian, camUnc, ptUnc)
+ * (src/uncertaintyTE/compute.h:92-97, compute.cpp:458-540).
+ * Host pointers in and out; ctx may be NULL (a temporary context on device 0
+ * is created and destroyed). stat may be NULL. */
+int unc_compute(unc_context* ctx, const unc_options* opt, int num_rows, int num_cols,
+                const int* rows, const int* cols, const double* values, double* cam_unc,
+                double* pt_unc, unc_statistic* stat);
+
+/* Same computation with every array already in device memory (inputs
+ * resident in HBM). stream: a cudaStream_t or NULL for the context's stream.
+ * pt_unc follows the reference's zeroing rule (compute.cpp:511): entries
+ * [0, 6*(numPoints-3)) are cleared and fixed points beyond that keep their
+ * previous contents. Returns after the results are written. */
+int unc_compute_device(unc_context* ctx, const unc_options* opt, int num_rows, int num_cols,
+                       const int* d_rows, const int* d_cols, const double* d_values,
+                       double* d_cam_unc, double* d_pt_unc, unc_statistic* stat, void* stream);
+
+/* Profiling of the dense Taylor-series products: when enabled, every
+ * N x N x N product of the Taylor loop is bracketed by CUDA events on the
+ * stream it runs on. unc_context_profile returns the number of products, their
+ * summed device time (s) and their algorithmic flops (2 N^3 each) since the
+ * last reset. */
+int unc_context_set_profiling(unc_context* ctx, int enable);
+int unc_context_profile(unc_context* ctx, long long* launches, double* seconds, double* flops,
+                        int reset);
+
+/* Device bytes unc_compute_device would use for this problem (admission). */
+long long unc_workspace_bytes(const unc_options* opt, int num_rows, int num_cols);
+
+/* SDM::inv (src/uncertaintyTE/ScaledDenseMatrix.cpp:232-279) for a
+ * symmetric positive-definite n x n matrix in device memory (column-major,
+ * leading dimension lda >= n, lda even): inverted in place by blocked
+ * Gauss-Jordan elimination on the GPU. Scratch is allocated per call. */
+int unc_dense_inverse_device(double* d_A, int n, int lda, void* stream);
+
+/* SSM J^T J (trn() then operator*, ScaledSparseMatrix.cpp:384-388,517-539)
+ * computed by the GPU block-assembly kernels and returned as host CRS in the
+ * reference's pattern. Observations may have 12-entry rows (camera + point)
+ * or 9-entry rows (camera only). First call with out_cols == NULL returns
+ * the nnz in *nnz; the second call fills out_rows (num_cols+1), out_cols,
+ * out_vals. num_cams/cam_params describe the camera column block. */
+int unc_jtj_crs(int num_rows, int num_cols, const int* rows, const int* cols, const double* values,
+                int num_cams, int cam_params, long long* nnz, int* out_rows, int* out_cols,
+                double* out_vals);
+
+/* Human-readable name of a status code, and the last error message of the
+ * calling thread (empty when none). */
+const char* unc_status_string(int status);
+const char* unc_last_error(void);
+
+/* Number of this library's kernels launched since load (diagnostics). */
+long long unc_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UNCTE_H */

@@ -1,0 +1,773 @@
+/*
+ * uncte_oracle.cpp - CPU FP64 restatement of uncertaintyTE's covariance path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA product path and the
+ * timed CPU baseline. It is never linked into the product library.
+ *
+ * Every function cites the reference lines (paths relative to the
+ * uncertaintyTE source tree) that it restates. The reference could not be
+ * compiled here (Ceres, Eigen and MAGMA are absent), so dense LAPACK/BLAS
+ * calls go to the OpenBLAS bundled with scipy (same routines the reference
+ * calls through MAGMA's lapackf77_/blasf77_ wrappers), and the Eigen sparse
+ * product / complete-orthogonal-decomposition pseudo-inverse are restated
+ * here (structural sparse product; Householder QR pseudo-inverse).
+ *
+ * Reference quirks reproduced on purpose:
+ *   - camera output is (iZ(j,k) + iZ(k,j)/2)*d_j*d_k, i.e. 1.5x  (compute.cpp:176,178)
+ *   - point propagation uses block-diagonal camera covariance     (compute.cpp:422-441)
+ *   - all rows of fixed points are deleted                         (compute.cpp:337-366)
+ *   - only pts[0..1] are sorted                                    (compute.cpp:285)
+ *   - factorial() is 32-bit int and wraps from 13! on              (compute.cpp:57-62,146)
+ *   - only the first 6*(P-3) point outputs are zeroed              (compute.cpp:511)
+ */
+#include "uncte_oracle.h"
+
+#include <algorithm>
+#include <cfloat>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+extern "C" {
+void scipy_dgemm_(const char*, const char*, const int*, const int*, const int*, const double*,
+                  const double*, const int*, const double*, const int*, const double*, double*,
+                  const int*);
+void scipy_dgetrf_(const int*, const int*, double*, const int*, int*, int*);
+void scipy_dgetri_(const int*, double*, const int*, const int*, double*, const int*, int*);
+void scipy_dgesvd_(const char*, const char*, const int*, const int*, double*, const int*, double*,
+                   double*, const int*, double*, const int*, double*, const int*, int*);
+void scipy_dgesdd_(const char*, const int*, const int*, double*, const int*, double*, double*,
+                   const int*, double*, const int*, double*, const int*, int*, int*);
+void scipy_openblas_set_num_threads(int);
+int scipy_openblas_get_num_threads(void);
+}
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+double secs(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double>(b - a).count();
+}
+
+struct Crs {
+    int nr = 0, nc = 0;
+    std::vector<int> row, col;
+    std::vector<double> val;
+    long nnz() const { return row.empty() ? 0 : row[nr]; }
+};
+
+/* ---------------- sparse helpers (ScaledSparseMatrix.cpp) ---------------- */
+
+/* trn(): ScaledSparseMatrix.cpp:384-388 (Eigen transpose; columns ascend). */
+Crs transpose(const Crs& A) {
+    Crs T;
+    T.nr = A.nc;
+    T.nc = A.nr;
+    T.row.assign(T.nr + 1, 0);
+    for (long k = 0; k < A.nnz(); ++k) T.row[A.col[k] + 1]++;
+    for (int i = 0; i < T.nr; ++i) T.row[i + 1] += T.row[i];
+    T.col.resize(A.nnz());
+    T.val.resize(A.nnz());
+    std::vector<int> fill(T.row.begin(), T.row.end() - 1);
+    for (int r = 0; r < A.nr; ++r)
+        for (int k = A.row[r]; k < A.row[r + 1]; ++k) {
+            int p = fill[A.col[k]]++;
+            T.col[p] = r;
+            T.val[p] = A.val[k];
+        }
+    return T;
+}
+
+/* operator*= -> sparseMultEigen: ScaledSparseMatrix.cpp:459-465,517-539.
+ * Structural product (explicit zeros kept), columns ascending per row. The
+ * reference's row/column rescale around the product only changes rounding. */
+Crs multiply(const Crs& A, const Crs& B) {
+    Crs C;
+    C.nr = A.nr;
+    C.nc = B.nc;
+    C.row.assign(C.nr + 1, 0);
+    std::vector<std::vector<int>> rc(C.nr);
+    std::vector<std::vector<double>> rv(C.nr);
+#pragma omp parallel
+    {
+        std::vector<double> acc(B.nc, 0.0);
+        std::vector<int> mark(B.nc, -1);
+        std::vector<int> cols;
+#pragma omp for schedule(dynamic, 64)
+        for (int i = 0; i < A.nr; ++i) {
+            cols.clear();
+            for (int ka = A.row[i]; ka < A.row[i + 1]; ++ka) {
+                int k = A.col[ka];
+                double a = A.val[ka];
+                for (int kb = B.row[k]; kb < B.row[k + 1]; ++kb) {
+                    int j = B.col[kb];
+                    if (mark[j] != i) {
+                        mark[j] = i;
+                        acc[j] = 0.0;
+                        cols.push_back(j);
+                    }
+                    acc[j] += a * B.val[kb];
+                }
+            }
+            std::sort(cols.begin(), cols.end());
+            rc[i] = cols;
+            rv[i].resize(cols.size());
+            for (size_t t = 0; t < cols.size(); ++t) rv[i][t] = acc[cols[t]];
+        }
+    }
+    for (int i = 0; i < C.nr; ++i) C.row[i + 1] = C.row[i] + (int)rc[i].size();
+    C.col.resize(C.row[C.nr]);
+    C.val.resize(C.row[C.nr]);
+    for (int i = 0; i < C.nr; ++i) {
+        std::copy(rc[i].begin(), rc[i].end(), C.col.begin() + C.row[i]);
+        std::copy(rv[i].begin(), rv[i].end(), C.val.begin() + C.row[i]);
+    }
+    return C;
+}
+
+/* splitTo3Blocks: ScaledSparseMatrix.cpp:238-299. A = [0,bx)x[0,by),
+ * B = [0,bx)x[by,nc), C = [bx,nr)x[by,nc); the lower-left block is dropped. */
+void split3(const Crs& M, int bx, int by, Crs& A, Crs& B, Crs& C) {
+    auto init = [](Crs& X, int nr, int nc) {
+        X.nr = nr;
+        X.nc = nc;
+        X.row.assign(nr + 1, 0);
+        X.col.clear();
+        X.val.clear();
+    };
+    init(A, bx, by);
+    init(B, bx, M.nc - by);
+    init(C, M.nr - bx, M.nc - by);
+    for (int i = 0; i < M.nr; ++i) {
+        for (int k = M.row[i]; k < M.row[i + 1]; ++k) {
+            int j = M.col[k];
+            if (i < bx && j < by) {
+                A.col.push_back(j);
+                A.val.push_back(M.val[k]);
+            } else if (i < bx && j >= by) {
+                B.col.push_back(j - by);
+                B.val.push_back(M.val[k]);
+            } else if (i >= bx && j >= by) {
+                C.col.push_back(j - by);
+                C.val.push_back(M.val[k]);
+            }
+        }
+        if (i < bx) {
+            A.row[i + 1] = (int)A.col.size();
+            B.row[i + 1] = (int)B.col.size();
+        } else {
+            C.row[i + 1 - bx] = (int)C.col.size();
+        }
+    }
+}
+
+/* inv3x3blockSymmDiag: ScaledSparseMatrix.cpp:210-230. Closed-form inverse of
+ * each symmetric 3x3 block stored as 9 consecutive CRS values. */
+Crs inv3x3_blocks(const Crs& V) {
+    Crs R = V;
+    const double* v = V.val.data();
+    for (long i = 0; i + 8 < V.nnz(); i += 9) {
+        const double a = v[i], b = v[i + 1], c = v[i + 2], e = v[i + 4], f = v[i + 5], k = v[i + 8];
+        double div = a * e * k - a * f * f - b * b * k + 2 * b * c * f - c * c * e;
+        double* o = R.val.data() + i;
+        o[0] = (e * k - f * f) / div;
+        o[1] = (-b * k + c * f) / div;
+        o[2] = (b * f - c * e) / div;
+        o[3] = o[1];
+        o[4] = (a * k - c * c) / div;
+        o[5] = (-a * f + b * c) / div;
+        o[6] = o[2];
+        o[7] = o[5];
+        o[8] = (a * e - b * b) / div;
+    }
+    return R;
+}
+
+/* addSSM(-1, B) then SDM(sZ): ScaledSparseMatrix.cpp:554-641 and
+ * ScaledDenseMatrix.cpp:54-66. Dense column-major A - B. */
+void dense_sub(const Crs& A, const Crs& B, double* Z) {
+    const int n = A.nr;
+    std::fill(Z, Z + (size_t)n * A.nc, 0.0);
+    for (int i = 0; i < n; ++i) {
+        for (int k = A.row[i]; k < A.row[i + 1]; ++k) Z[i + (size_t)A.col[k] * n] += A.val[k];
+        for (int k = B.row[i]; k < B.row[i + 1]; ++k) Z[i + (size_t)B.col[k] * n] -= B.val[k];
+    }
+}
+
+/* ---------------- dense helpers (ScaledDenseMatrix.cpp) ---------------- */
+
+void gemm_nn(int n, const double* A, const double* B, double* C) {
+    const double one = 1.0, zero = 0.0;
+    scipy_dgemm_("N", "N", &n, &n, &n, &one, A, &n, B, &n, &zero, C, &n);
+}
+
+/* absMax: ScaledDenseMatrix.cpp:207-216 (starts from DBL_MIN). */
+double abs_max(size_t n, const double* A) {
+    double m = DBL_MIN;
+#pragma omp parallel for reduction(max : m)
+    for (size_t i = 0; i < n; ++i) m = std::max(m, std::fabs(A[i]));
+    return m;
+}
+
+/* factorial: compute.cpp:57-62. 32-bit signed recursion; wraps from 13! on
+ * (two's-complement, what the reference binary computes). */
+int32_t factorial_i32(int n) {
+    uint32_t f = 1;
+    for (int i = 2; i <= n; ++i) f = f * (uint32_t)i;
+    return (int32_t)f;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_set_threads(int threads) {
+    if (threads > 0) {
+#ifdef _OPENMP
+        omp_set_num_threads(threads);
+#endif
+        scipy_openblas_set_num_threads(threads);
+    }
+    return scipy_openblas_get_num_threads();
+}
+
+/* ScaledDenseMatrix::inv: ScaledDenseMatrix.cpp:232-279 (with scaleMat LEFT then
+ * RIGHT, :150-204). */
+int oracle_dense_inv(int n, double* A) {
+    std::vector<double> sL(n, 0.0), sR(n, 0.0);
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < n; ++r) sL[r] += A[r + (size_t)c * n] * A[r + (size_t)c * n];
+    for (int r = 0; r < n; ++r) sL[r] = std::sqrt(sL[r]);
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < n; ++r) A[r + (size_t)c * n] *= 1 / sL[r];
+    for (int c = 0; c < n; ++c) {
+        double s = 0;
+        for (int r = 0; r < n; ++r) s += A[r + (size_t)c * n] * A[r + (size_t)c * n];
+        sR[c] = std::sqrt(s);
+    }
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < n; ++r) A[r + (size_t)c * n] *= 1 / sR[c];
+
+    std::vector<int> ipiv(n);
+    int info = 0, info2 = 0;
+    scipy_dgetrf_(&n, &n, A, &n, ipiv.data(), &info);
+    int lwork = -1;
+    double wq = 0;
+    scipy_dgetri_(&n, A, &n, ipiv.data(), &wq, &lwork, &info2);
+    lwork = std::max(1, (int)wq);
+    std::vector<double> work(lwork);
+    scipy_dgetri_(&n, A, &n, ipiv.data(), work.data(), &lwork, &info2);
+    if (info == 0) info = info2;
+
+    for (int i = 0; i < n; ++i) sL[i] = 1 / sL[i];
+    for (int i = 0; i < n; ++i) sR[i] = 1 / sR[i];
+    /* element (row j, col i) *= sL[i] * sR[j]  (ScaledDenseMatrix.cpp:270-273) */
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) A[j + (size_t)i * n] *= sL[i] * sR[j];
+    return info;
+}
+
+/* teInverse: compute.cpp:121-166 (iZupdate :64-71, operator*= :314-353). */
+int oracle_te_inverse(int n, double* Z, double lambda, oracle_stats* st) {
+    auto t0 = Clock::now();
+    for (int i = 0; i < n; ++i) Z[i + (size_t)i * n] += lambda;
+    int info = oracle_dense_inv(n, Z);
+    auto t1 = Clock::now();
+    const size_t nn = (size_t)n * n;
+    std::vector<double> X(Z, Z + nn), add(nn), tmp(nn);
+    gemm_nn(n, X.data(), X.data(), add.data());
+    double old_change = DBL_MAX;
+    int iters = 0;
+    for (int i = 1; i < 20; ++i) {
+        double k = std::pow(lambda, i) / factorial_i32(i - 1);
+        double change = std::fabs(k * abs_max(nn, add.data()));
+        if (change < 1e-5 || change > old_change) break;
+        old_change = change;
+        if (st && iters < 20) st->cycle_change[iters] = change;
+        iters++;
+#pragma omp parallel for
+        for (size_t e = 0; e < nn; ++e) Z[e] = Z[e] + k * add[e];
+        gemm_nn(n, add.data(), X.data(), tmp.data());
+        add.swap(tmp);
+    }
+    auto t2 = Clock::now();
+    if (st) {
+        st->te_iterations = iters;
+        st->lambda = lambda;
+        st->lu_info = info;
+        st->t_inv_z = secs(t0, t1);
+        st->t_te = secs(t1, t2);
+    }
+    return info;
+}
+
+long oracle_jtj(int nrows, int ncols, const int* rows, const int* cols, const double* vals,
+                int* out_rows, int* out_cols, double* out_vals) {
+    Crs J;
+    J.nr = nrows;
+    J.nc = ncols;
+    J.row.assign(rows, rows + nrows + 1);
+    J.col.assign(cols, cols + rows[nrows]);
+    J.val.assign(vals, vals + rows[nrows]);
+    Crs M = multiply(transpose(J), J);
+    if (out_cols) {
+        std::copy(M.row.begin(), M.row.end(), out_rows);
+        std::copy(M.col.begin(), M.col.end(), out_cols);
+        std::copy(M.val.begin(), M.val.end(), out_vals);
+    }
+    return M.nnz();
+}
+
+}  // extern "C"
+
+namespace {
+
+/* fixPts: compute.cpp:283-368. Deletes the 9 columns of the fixed points and
+ * every row that loses its point entries, renumbers the remaining columns and
+ * rebuilds rowptr as i*(camParams+3). */
+void fix_points(Crs& J, int pts[3], int num_cams, int cam_params, oracle_stats* st) {
+    std::sort(pts, pts + 2); /* sorts only the first two ids (compute.cpp:285) */
+    if (st) {
+        st->fixed_pts[0] = pts[0];
+        st->fixed_pts[1] = pts[1];
+        st->fixed_pts[2] = pts[2];
+    }
+    int rem[9];
+    const int cam_off = num_cams * cam_params;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) rem[i * 3 + j] = cam_off + pts[i] * 3 + j;
+    std::vector<int> newid(J.nc, 0);
+    for (int i = 0; i < 9; ++i) newid[rem[i]] = -1;
+    int off = 0;
+    for (int i = 0; i < J.nc; ++i) {
+        off += newid[i];
+        newid[i] = i + off;
+    }
+    std::vector<int> rws{0}, cs, cs2;
+    std::vector<double> vs, vs2;
+    for (int i = 0; i < J.nr; ++i) {
+        for (int k = J.row[i]; k < J.row[i + 1]; ++k) {
+            bool use = true;
+            for (int r = 0; r < 9; ++r)
+                if (J.col[k] == rem[r]) use = false;
+            if (use) {
+                cs.push_back(newid[J.col[k]]);
+                vs.push_back(J.val[k]);
+            }
+        }
+        rws.push_back((int)cs.size());
+    }
+    /* "remove redundant cameras": rows that lost their 3 point entries */
+    const int per_row = cam_params + 3;
+    std::vector<char> use_cols;
+    int err_off = 0;
+    for (size_t i = 1; i < rws.size(); ++i) {
+        bool use = true;
+        if (rws[i] != (int)i * per_row - err_off) {
+            err_off += 3;
+            use = false;
+        } else {
+            use_cols.push_back(1);
+            use_cols.push_back(1);
+            use_cols.push_back(1);
+        }
+        for (int j = 0; j < cam_params; ++j) use_cols.push_back(use ? 1 : 0);
+    }
+    for (size_t i = 0; i < cs.size(); ++i)
+        if (i < use_cols.size() && use_cols[i]) {
+            cs2.push_back(cs[i]);
+            vs2.push_back(vs[i]);
+        }
+    const int nr = (int)cs2.size() / per_row + 1;
+    J.nr = nr - 1;
+    J.nc = J.nc - 9;
+    J.row.resize(nr);
+    for (int i = 0; i < nr; ++i) J.row[i] = i * per_row;
+    J.col = cs2;
+    J.val = vs2;
+}
+
+/* Householder-QR pseudo-inverse of a tall m x 3 matrix (column-major), the
+ * full-rank case of Eigen's completeOrthogonalDecomposition().pseudoInverse()
+ * used at compute.cpp:524. Rank-deficient input falls back to the normal-
+ * equation pseudo-inverse through a symmetric 3x3 eigen-decomposition.
+ * out: 3 x m, column-major. */
+void sym3_eig(const double S[9], double w[3], double V[9]);
+
+void pinv_tall3(int m, const double* A, double* P) {
+    std::vector<double> R(A, A + (size_t)m * 3);
+    std::vector<double> vs((size_t)m * 3, 0.0);
+    double tau[3];
+    double rmax = 0;
+    for (int j = 0; j < 3 && j < m; ++j) {
+        double nrm = 0;
+        for (int i = j; i < m; ++i) nrm += R[i + (size_t)j * m] * R[i + (size_t)j * m];
+        nrm = std::sqrt(nrm);
+        double alpha = R[j + (size_t)j * m] >= 0 ? -nrm : nrm;
+        double* v = vs.data() + (size_t)j * m;
+        for (int i = 0; i < m; ++i) v[i] = 0;
+        for (int i = j; i < m; ++i) v[i] = R[i + (size_t)j * m];
+        v[j] -= alpha;
+        double vn = 0;
+        for (int i = j; i < m; ++i) vn += v[i] * v[i];
+        tau[j] = vn > 0 ? 2.0 / vn : 0.0;
+        for (int c = j; c < 3; ++c) {
+            double d = 0;
+            for (int i = j; i < m; ++i) d += v[i] * R[i + (size_t)c * m];
+            d *= tau[j];
+            for (int i = j; i < m; ++i) R[i + (size_t)c * m] -= d * v[i];
+        }
+        rmax = std::max(rmax, std::fabs(R[j + (size_t)j * m]));
+    }
+    bool full = m >= 3;
+    for (int j = 0; j < 3 && full; ++j)
+        if (std::fabs(R[j + (size_t)j * m]) <= rmax * DBL_EPSILON * 3) full = false;
+    if (full) {
+        /* P = R^{-1} Q^T: apply the reflectors to the identity rows */
+        double Ri[9] = {0};
+        for (int c = 0; c < 3; ++c) {
+            double e[3] = {0, 0, 0};
+            e[c] = 1;
+            for (int r = 2; r >= 0; --r) {
+                double s = e[r];
+                for (int k = r + 1; k < 3; ++k) s -= R[r + (size_t)k * m] * Ri[k + 3 * c];
+                Ri[r + 3 * c] = s / R[r + (size_t)r * m];
+            }
+        }
+        /* Q^T = H3 H2 H1 applied to I_m; P = Ri * (Q^T)[0:3, :] */
+        std::vector<double> QT((size_t)m * 3, 0.0); /* first 3 columns of Q, m x 3 */
+        for (int c = 0; c < 3; ++c) {
+            std::vector<double> q(m, 0.0);
+            q[c] = 1;
+            for (int j = 2; j >= 0; --j) {
+                const double* v = vs.data() + (size_t)j * m;
+                double d = 0;
+                for (int i = j; i < m; ++i) d += v[i] * q[i];
+                d *= tau[j];
+                for (int i = j; i < m; ++i) q[i] -= d * v[i];
+            }
+            for (int i = 0; i < m; ++i) QT[i + (size_t)c * m] = q[i];
+        }
+        for (int r = 0; r < 3; ++r)
+            for (int i = 0; i < m; ++i) {
+                double s = 0;
+                for (int k = 0; k < 3; ++k) s += Ri[r + 3 * k] * QT[i + (size_t)k * m];
+                P[r + (size_t)i * 3] = s;
+            }
+        return;
+    }
+    /* rank-deficient: P = (A^T A)^+ A^T */
+    double S[9] = {0};
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            double s = 0;
+            for (int i = 0; i < m; ++i) s += A[i + (size_t)a * m] * A[i + (size_t)b * m];
+            S[a + 3 * b] = s;
+        }
+    double w[3], V[9];
+    sym3_eig(S, w, V);
+    double wmax = std::max(std::fabs(w[0]), std::max(std::fabs(w[1]), std::fabs(w[2])));
+    double Sp[9] = {0};
+    for (int k = 0; k < 3; ++k) {
+        if (w[k] <= wmax * DBL_EPSILON * 3 * 3 || w[k] <= 0) continue;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) Sp[a + 3 * b] += V[a + 3 * k] * V[b + 3 * k] / w[k];
+    }
+    for (int r = 0; r < 3; ++r)
+        for (int i = 0; i < m; ++i) {
+            double s = 0;
+            for (int k = 0; k < 3; ++k) s += Sp[r + 3 * k] * A[i + (size_t)k * m];
+            P[r + (size_t)i * 3] = s;
+        }
+}
+
+/* cyclic Jacobi eigen-decomposition of a symmetric 3x3 (column-major) */
+void sym3_eig(const double S[9], double w[3], double V[9]) {
+    double a[9];
+    std::copy(S, S + 9, a);
+    for (int i = 0; i < 9; ++i) V[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 50; ++sweep) {
+        double off = std::fabs(a[3]) + std::fabs(a[6]) + std::fabs(a[7]);
+        if (off == 0) break;
+        for (int p = 0; p < 2; ++p)
+            for (int q = p + 1; q < 3; ++q) {
+                double apq = a[p + 3 * q];
+                if (apq == 0) continue;
+                double app = a[p + 3 * p], aqq = a[q + 3 * q];
+                double theta = (aqq - app) / (2 * apq);
+                double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1));
+                double c = 1 / std::sqrt(t * t + 1), s = t * c;
+                for (int k = 0; k < 3; ++k) {
+                    double akp = a[k + 3 * p], akq = a[k + 3 * q];
+                    a[k + 3 * p] = c * akp - s * akq;
+                    a[k + 3 * q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    double apk = a[p + 3 * k], aqk = a[q + 3 * k];
+                    a[p + 3 * k] = c * apk - s * aqk;
+                    a[q + 3 * k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    double vkp = V[k + 3 * p], vkq = V[k + 3 * q];
+                    V[k + 3 * p] = c * vkp - s * vkq;
+                    V[k + 3 * q] = s * vkp + c * vkq;
+                }
+            }
+    }
+    for (int k = 0; k < 3; ++k) w[k] = a[k + 3 * k];
+}
+
+/* removeScaleJ4Z: compute.cpp:168-183 (the a + b/2 precedence quirk kept). */
+void camera_output(const double* iZ, int N, const double* d, int num_cams, int cp, double* cam) {
+    int l = -1;
+    for (int i = 0; i < num_cams; ++i) {
+        int st = i * cp;
+        for (int j = st; j < st + cp; ++j)
+            for (int k = j; k < st + cp; ++k) {
+                double v = iZ[j + (size_t)k * N] + iZ[k + (size_t)j * N] / 2;
+                cam[++l] = d ? v * d[j] * d[k] : v;
+            }
+    }
+}
+
+/* Point propagation: compute.cpp:370-455 and the loop at :517-527. */
+void point_output(const oracle_options* opt, const Crs& J, const double* iZ, int N,
+                  const double* scale, const int fixed[3], double* out) {
+    const int cp = opt->cam_params, np = cp + 3, cam_off = opt->num_cams * cp;
+    const int nobs = J.nr / 2, npts = opt->num_points - 3;
+    std::vector<std::vector<int>> obs_of(npts), cams_of(npts);
+    for (int i = 0; i < nobs; ++i) { /* findCams2Point :370-380 */
+        int pt = (J.col[(size_t)i * 2 * np + cp] - cam_off) / 3;
+        int cam = J.col[(size_t)i * 2 * np] / cp;
+        cams_of[pt].push_back(cam);
+        obs_of[pt].push_back(i);
+    }
+    const bool scan = opt->faithful_point_scan != 0;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int p = 0; p < npts; ++p) {
+        const std::vector<int>& cams = cams_of[p];
+        const int n = (int)cams.size(), m = 2 * n, nb = (cp + 2) * n;
+        std::vector<double> A((size_t)m * 3, 0.0), B((size_t)m * nb, 0.0), sA(3), sB(nb);
+        /* composeCams2PointJacobian :382-420 */
+        auto fill = [&](int i, int t) {
+            size_t k = (size_t)i * 2 * np;
+            for (int j = 0; j < cp; ++j) {
+                B[(t * 2 + 0) + (size_t)(t * (cp + 2) + j) * m] = J.val[k + j];
+                B[(t * 2 + 1) + (size_t)(t * (cp + 2) + j) * m] = J.val[k + j + np];
+                sB[t * (cp + 2) + j] = 1 / scale[J.col[k + j]];
+            }
+            B[(t * 2 + 0) + (size_t)(t * (cp + 2) + cp + 0) * m] = -1;
+            B[(t * 2 + 1) + (size_t)(t * (cp + 2) + cp + 1) * m] = -1;
+            sB[t * (cp + 2) + cp + 0] = 1;
+            sB[t * (cp + 2) + cp + 1] = 1;
+            for (int j = 0; j < 3; ++j) {
+                A[(t * 2 + 0) + (size_t)j * m] = J.val[k + cp + j];
+                A[(t * 2 + 1) + (size_t)j * m] = J.val[k + cp + j + np];
+                sA[j] = 1 / scale[J.col[k + cp + j]];
+            }
+        };
+        int t = 0;
+        if (scan) {
+            for (int i = 0; i < nobs; ++i) {
+                size_t k = (size_t)i * 2 * np;
+                if (p == (J.col[k + cp] - cam_off) / 3) fill(i, t++);
+            }
+        } else {
+            for (int i : obs_of[p]) fill(i, t++);
+        }
+        for (int j = 0; j < 3; ++j)
+            for (int r = 0; r < m; ++r) A[r + (size_t)j * m] *= sA[j];
+        for (int j = 0; j < nb; ++j)
+            for (int r = 0; r < m; ++r) B[r + (size_t)j * m] *= sB[j];
+        /* composeCamCovariances :422-441 (unscaled, without the 1.5x) */
+        std::vector<double> Sig((size_t)nb * nb, 0.0);
+        for (int i = 0; i < n; ++i) {
+            int so = i * (cp + 2), zo = cams[i] * cp;
+            for (int a = 0; a < cp; ++a)
+                for (int b = 0; b < cp; ++b)
+                    Sig[(so + a) + (size_t)(so + b) * nb] =
+                        iZ[(zo + a) + (size_t)(zo + b) * N] * scale[zo + a] * scale[zo + b];
+            Sig[(so + cp) + (size_t)(so + cp) * nb] = 1;
+            Sig[(so + cp + 1) + (size_t)(so + cp + 1) * nb] = 1;
+        }
+        std::vector<double> P((size_t)3 * m);
+        if (m > 0) pinv_tall3(m, A.data(), P.data());
+        /* Sigma_pt = (pinvA*B) * Sigma * (B^T * pinvA^T) */
+        std::vector<double> PB((size_t)3 * nb, 0.0), PBS((size_t)3 * nb, 0.0);
+        for (int j = 0; j < nb; ++j)
+            for (int r = 0; r < m; ++r) {
+                double b = B[r + (size_t)j * m];
+                if (b == 0) continue;
+                for (int a = 0; a < 3; ++a) PB[a + (size_t)j * 3] += P[a + (size_t)r * 3] * b;
+            }
+        for (int j = 0; j < nb; ++j)
+            for (int k = 0; k < nb; ++k) {
+                double s = Sig[k + (size_t)j * nb];
+                if (s == 0) continue;
+                for (int a = 0; a < 3; ++a) PBS[a + (size_t)j * 3] += PB[a + (size_t)k * 3] * s;
+            }
+        double S[9] = {0};
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) {
+                double s = 0;
+                for (int j = 0; j < nb; ++j) s += PBS[a + (size_t)j * 3] * PB[b + (size_t)j * 3];
+                S[a + 3 * b] = s;
+            }
+        /* fillPtUnc2OutArray :443-455 (index shift past the fixed points) */
+        int id = p;
+        for (int i = 0; i < 3; ++i)
+            if (id >= fixed[i]) id++;
+        double* o = out + (size_t)id * 6;
+        o[0] = S[0];
+        o[1] = S[3];
+        o[2] = S[6];
+        o[3] = S[4];
+        o[4] = S[7];
+        o[5] = S[8];
+    }
+}
+
+}  // namespace
+
+extern "C" int oracle_compute(const oracle_options* opt, int nrows, int ncols, const int* rows,
+                              const int* cols, const double* vals, double* cam_unc, double* pt_unc,
+                              oracle_stats* st, double* dbg_Z, double* dbg_iZ, double* dbg_d) {
+    if (!opt || !rows || !cols || !vals || !cam_unc || !pt_unc) return -1;
+    if (opt->cam_params <= 0 || opt->num_cams <= 0 || opt->num_points < 0) return -1;
+    if (opt->threads > 0) oracle_set_threads(opt->threads);
+    oracle_stats local{};
+    if (!st) st = &local;
+    auto t_all0 = Clock::now();
+    Crs J;
+    J.nr = nrows;
+    J.nc = ncols;
+    J.row.assign(rows, rows + nrows + 1);
+    J.col.assign(cols, cols + rows[nrows]);
+    J.val.assign(vals, vals + rows[nrows]);
+    const int cp = opt->cam_params;
+    const int Ncams = opt->num_cams * cp;
+    const int Npar = Ncams + opt->num_points * 3;
+
+    if (opt->algorithm == 0 || opt->algorithm == 1) {
+        /* svdInverse: compute.cpp:185-249 on the dense, unscaled, unfixed J^T J */
+        auto t0 = Clock::now();
+        Crs M = multiply(transpose(J), J);
+        const int N = Npar;
+        std::vector<double> Z((size_t)N * N, 0.0), U((size_t)N * N), Vt((size_t)N * N), sv(N);
+        for (int i = 0; i < M.nr; ++i)
+            for (int k = M.row[i]; k < M.row[i + 1]; ++k) Z[i + (size_t)M.col[k] * N] = M.val[k];
+        int info = 0;
+        if (opt->algorithm == 0) {
+            int lwork = -1;
+            double wq;
+            scipy_dgesvd_("A", "A", &N, &N, Z.data(), &N, sv.data(), U.data(), &N, Vt.data(), &N, &wq,
+                          &lwork, &info);
+            lwork = (int)wq;
+            std::vector<double> work(lwork);
+            scipy_dgesvd_("A", "A", &N, &N, Z.data(), &N, sv.data(), U.data(), &N, Vt.data(), &N,
+                          work.data(), &lwork, &info);
+        } else {
+            int lwork = -1;
+            double wq;
+            std::vector<int> iwork(8 * (size_t)N);
+            scipy_dgesdd_("A", &N, &N, Z.data(), &N, sv.data(), U.data(), &N, Vt.data(), &N, &wq,
+                          &lwork, iwork.data(), &info);
+            lwork = (int)wq;
+            std::vector<double> work(lwork);
+            scipy_dgesdd_("A", &N, &N, Z.data(), &N, sv.data(), U.data(), &N, Vt.data(), &N,
+                          work.data(), &lwork, iwork.data(), &info);
+        }
+        st->lu_info = info;
+        double eps = opt->epsilon < 0 ? 1e-10 : opt->epsilon;
+#pragma omp parallel for
+        for (int i = 0; i < N; ++i) {
+            double f;
+            if (opt->svd_remove_n != -1)
+                f = i < (N - opt->svd_remove_n) ? 1 / sv[i] : 0;
+            else
+                f = sv[i] > eps ? 1 / sv[i] : 0;
+            for (int j = 0; j < N; ++j) U[(size_t)i * N + j] *= f;
+        }
+        gemm_nn(N, U.data(), Vt.data(), Z.data());
+        auto t1 = Clock::now();
+        st->t_inv_z = secs(t0, t1);
+        camera_output(Z.data(), N, nullptr, opt->num_cams, cp, cam_unc);
+        /* The reference's point stage dereferences a NULL scale vector in this
+         * mode (compute.cpp:402,413). The oracle defines the point output as the
+         * 3x3 diagonal point blocks of the same pseudo-inverse (upper triangle). */
+        for (int p = 0; p < opt->num_points; ++p) {
+            size_t b = (size_t)Ncams + 3 * (size_t)p;
+            double* o = pt_unc + (size_t)p * 6;
+            o[0] = Z[b + b * N];
+            o[1] = Z[b + (b + 1) * N];
+            o[2] = Z[b + (b + 2) * N];
+            o[3] = Z[(b + 1) + (b + 1) * N];
+            o[4] = Z[(b + 1) + (b + 2) * N];
+            o[5] = Z[(b + 2) + (b + 2) * N];
+        }
+        st->t_all = secs(t_all0, Clock::now());
+        return 0;
+    }
+    if (opt->algorithm != 2) return -1;
+    if (!opt->has_pts2fix) return -2; /* the TE path needs 3 fixed points (compute.cpp:446,517) */
+
+    /* TAYLOR_EXPANSION: compute.cpp:497-513 */
+    auto t0 = Clock::now();
+    int pts[3] = {opt->pts2fix[0], opt->pts2fix[1], opt->pts2fix[2]};
+    fix_points(J, pts, opt->num_cams, cp, st);
+    auto t1 = Clock::now();
+    st->t_fix = secs(t0, t1);
+
+    /* composeZ: compute.cpp:73-118 */
+    std::vector<double> s(J.nc, 0.0);
+    for (long k = 0; k < J.nnz(); ++k) s[J.col[k]] += J.val[k] * J.val[k];
+    for (int c = 0; c < J.nc; ++c) s[c] = std::sqrt(s[c]);
+    for (long k = 0; k < J.nnz(); ++k)
+        if (s[J.col[k]] != 0) J.val[k] *= 1 / s[J.col[k]];
+    std::vector<double> d(J.nc);
+    for (int c = 0; c < J.nc; ++c) d[c] = 1 / (1.0 * s[c]);
+    auto t2 = Clock::now();
+    st->t_norm = secs(t1, t2);
+
+    Crs M = multiply(transpose(J), J);
+    auto t3 = Clock::now();
+    st->t_jtj = secs(t2, t3);
+    Crs U, W, V;
+    split3(M, Ncams, Ncams, U, W, V);
+    auto t4 = Clock::now();
+    st->t_split = secs(t3, t4);
+    Crs iV = inv3x3_blocks(V);
+    auto t5 = Clock::now();
+    st->t_invv = secs(t4, t5);
+    Crs Y = multiply(W, iV);
+    Crs YWt = multiply(Y, transpose(W));
+    const int N = Ncams;
+    std::vector<double> Z((size_t)N * N);
+    dense_sub(U, YWt, Z.data());
+    auto t6 = Clock::now();
+    st->t_compose_z = secs(t5, t6);
+    if (dbg_Z) std::copy(Z.begin(), Z.end(), dbg_Z);
+    if (dbg_d) std::copy(d.begin(), d.begin() + N, dbg_d);
+
+    /* teInverse: compute.cpp:121-166 */
+    double lambda = opt->lambda;
+    if (lambda == -1) lambda = std::pow(10, -1.2653 * std::log10(N) - 2.9415);
+    oracle_te_inverse(N, Z.data(), lambda, st);
+    if (dbg_iZ) std::copy(Z.begin(), Z.end(), dbg_iZ);
+
+    auto t7 = Clock::now();
+    camera_output(Z.data(), N, d.data(), opt->num_cams, cp, cam_unc);
+    if (opt->num_points > 3) std::memset(pt_unc, 0, 6 * (size_t)(opt->num_points - 3) * sizeof(double));
+    auto t8 = Clock::now();
+    st->t_cams = secs(t7, t8);
+    point_output(opt, J, Z.data(), N, d.data(), st->fixed_pts, pt_unc);
+    auto t9 = Clock::now();
+    st->t_pts = secs(t8, t9);
+    st->t_all = secs(t_all0, t9);
+    return 0;
+}

@@ -1,0 +1,171 @@
+"""CUDA path vs the CPU oracle and the reference's goldens (needs a B200).
+
+Tolerances (relative Frobenius error per camera 9x9 / point 3x3 block):
+  * vs the reference's golden output.cov: 1e-5 (the file prints 6 digits)
+  * FP64 GPU vs the FP64 oracle: FP64_TOL below. Both are FP64 but the dense
+    inverse takes different routes (GPU: Jacobi-equilibrated Gauss-Jordan;
+    oracle: row/column-equilibrated LU as the reference), so the difference is
+    bounded by cond(Z + lambda*I) * eps.
+  * structure (J^T J pattern, iteration count, fixed points) bit-exact.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import block_rel_err, golden, golden_jacobian
+from uncertaintyte_b200 import native, scenes
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-7
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = native.Context(0)
+    yield c
+    c.close()
+
+
+def _parity(jac, ctx, tol=FP64_TOL, **kw):
+    cam, pt, st = native.compute_covariances(jac, ctx)
+    ref = oracle.compute(jac, threads=8, **kw)
+    ost = ref["stats"]
+    assert st["te_iterations"] == ost.te_iterations
+    assert st["fixed_pts"] == list(ost.fixed_pts)
+    np.testing.assert_allclose(st["cycle_change"], list(ost.cycle_change[: ost.te_iterations]), rtol=1e-6)
+    assert st["lambda"] == ost.lam
+    ec = block_rel_err(cam, ref["cam"], 45)
+    ep = block_rel_err(pt, ref["pt"], 6)
+    print(f"cams {ec:.3e} points {ep:.3e} iters {st['te_iterations']}")
+    assert ec < tol and ep < tol
+    return cam, pt, st, ref
+
+
+def test_daliborka_golden(ctx):
+    jac = golden_jacobian("daliborka")
+    g = golden("daliborka")
+    cam, pt, st = native.compute_covariances(jac, ctx)
+    assert st["te_iterations"] == 14
+    np.testing.assert_allclose(st["cycle_change"], g["gold_cycle_change"], rtol=1e-5)
+    assert abs(st["lambda"] - g["gold_lambda"]) < 1e-5 * g["gold_lambda"]
+    assert st["fixed_pts"] == list(g["gold_fixed"])
+    assert block_rel_err(cam, g["gold_cam"], 45) < 1e-5
+    assert block_rel_err(pt, g["gold_pt"], 6) < 1e-5
+
+
+def test_daliborka_vs_oracle(ctx):
+    _parity(golden_jacobian("daliborka"), ctx)
+
+
+def test_cube_vs_oracle_and_tail_rule(ctx):
+    """01_Cube fixes points 11, 12, 14 of 15: slots < 6*(P-3) are zeroed, fixed
+    points beyond keep the caller's values (compute.cpp:511)."""
+    jac = golden_jacobian("cube")
+    sentinel = np.full(jac.num_points * 6, 7.0)
+    cam, pt, st = native.compute_covariances(jac, ctx, pt_init=sentinel)
+    ref = oracle.compute(jac, threads=8, pt_init=sentinel)
+    pt = pt.reshape(-1, 6)
+    assert np.all(pt[11] == 0)
+    assert np.all(pt[12] == 7.0) and np.all(pt[14] == 7.0)
+    np.testing.assert_array_equal(ref["pt"].reshape(-1, 6)[[11, 12, 14]], pt[[11, 12, 14]])
+    assert block_rel_err(cam, ref["cam"], 45) < FP64_TOL
+    assert block_rel_err(pt, ref["pt"], 6) < FP64_TOL
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_small_scene_vs_oracle(ctx, seed):
+    _parity(scenes.synthetic_jacobian("small", seed=seed), ctx)
+
+
+def test_medium_scene_vs_oracle(ctx):
+    """The benchmark's workload (200 cameras, 50k points, N = 1800)."""
+    _parity(scenes.synthetic_jacobian("medium", seed=0), ctx)
+
+
+def test_repeatable(ctx):
+    jac = scenes.synthetic_jacobian("small", seed=4)
+    a = native.compute_covariances(jac, ctx)
+    b = native.compute_covariances(jac, ctx)
+    assert block_rel_err(a[0], b[0], 45) < 1e-12
+    assert block_rel_err(a[1], b[1], 6) < 1e-12
+
+
+def test_layout_error(ctx):
+    jac = scenes.synthetic_jacobian("tiny", seed=0)
+    jac.cols = jac.cols.copy()
+    jac.cols[24 * 5 + 3] += 1  # breaks observation 5's camera columns
+    with pytest.raises(native.UncError) as e:
+        native.compute_covariances(jac, ctx)
+    assert e.value.status == -2
+
+
+def test_single_observation_point_is_singular(ctx):
+    """A point seen once has a singular 3x3 block; the reference divides by a
+    zero determinant (ScaledSparseMatrix.cpp:219) and propagates NaN. The GPU
+    path reports UNC_ERR_SINGULAR instead."""
+    sc = scenes.make_scene("tiny", seed=1)
+    fix = scenes.farthest_triple(sc.points)
+    victim = next(p for p in range(len(sc.points)) if p not in fix)
+    idx = np.where(sc.obs_pt == victim)[0]
+    keep = np.ones(len(sc.obs_pt), bool)
+    keep[idx[1:]] = False
+    sc = scenes.Scene(sc.cams, sc.points, sc.obs_cam[keep], sc.obs_pt[keep])
+    jac = scenes.scene_jacobian(sc)
+    with pytest.raises(native.UncError) as e:
+        native.compute_covariances(jac, ctx)
+    assert e.value.status == -6
+
+
+def test_jtj_golden_pattern_and_values():
+    d = golden("multipl_01")
+    nr, nc = (int(x) for x in d["in_dims"])
+    r, c, v = native.jtj_crs(nr, nc, d["in_rows"], d["in_cols"], d["in_vals"], num_cams=10)
+    np.testing.assert_array_equal(r, d["out_rows"])
+    np.testing.assert_array_equal(c, d["out_cols"])
+    np.testing.assert_allclose(v, d["out_vals"], rtol=1e-10, atol=0)
+
+
+def test_jtj_matches_oracle_on_daliborka():
+    jac = golden_jacobian("daliborka")
+    r, c, v = native.jtj_crs(jac.num_rows, jac.num_cols, jac.rows, jac.cols, jac.values, jac.num_cams)
+    ro, co, vo = oracle.jtj(jac.num_rows, jac.num_cols, jac.rows, jac.cols, jac.values)
+    np.testing.assert_array_equal(r, ro)
+    np.testing.assert_array_equal(c, co)
+    np.testing.assert_allclose(v, vo, rtol=1e-12, atol=1e-12 * np.abs(vo).max())
+
+
+def _dense_inverse_gpu(A):
+    import torch
+    n = A.shape[0]
+    lda = (n + 7) & ~7
+    buf = torch.zeros((n, lda), dtype=torch.float64, device="cuda")  # row i of buf = column i
+    buf[:, :n] = torch.from_numpy(np.asfortranarray(A).T.copy())
+    native.dense_inverse_device(buf.data_ptr(), n, lda)
+    torch.cuda.synchronize()
+    return buf[:, :n].cpu().numpy().T
+
+
+def test_dense_inverse_golden_spd():
+    d = golden("inv_sparse_01")  # symmetric positive definite, cond 9.9e5
+    Ai = _dense_inverse_gpu(d["A"])
+    assert np.max(np.abs(Ai - d["Ainv"])) / np.max(np.abs(d["Ainv"])) < 1e-9
+
+
+def test_dense_inverse_random_spd_sizes():
+    rng = np.random.default_rng(0)
+    for n in (1, 7, 64, 65, 130, 700):
+        Q = rng.standard_normal((n, n))
+        A = Q @ Q.T + n * np.eye(n)
+        Ai = _dense_inverse_gpu(A)
+        ref = np.linalg.inv(A)
+        assert np.max(np.abs(Ai - ref)) / np.max(np.abs(ref)) < 1e-11, n
+
+
+def test_dense_inverse_rejects_indefinite():
+    A = np.diag([1.0, -2.0, 3.0])
+    with pytest.raises(native.UncError) as e:
+        _dense_inverse_gpu(A)
+    assert e.value.status == -6

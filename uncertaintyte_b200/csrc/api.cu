@@ -1,0 +1,644 @@
+// api.cu - C ABI of libuncte.so: validation, workspace planning and the
+// orchestration of the covariance pipeline on one CUDA stream.
+//
+// Replaces computeCovariances (compute.cpp:458-540). Host code; every
+// arithmetic step runs in the kernels of assembly.cu / dense.cu / points.cu.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/uncte.h"
+#include "internal.h"
+
+namespace unc {
+thread_local std::string g_last_error;
+long long g_launches = 0;
+}  // namespace unc
+
+using namespace unc;
+
+struct unc_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    cudaEvent_t ev[12] = {};
+    // profiling of the Taylor-series products
+    bool prof = false;
+    std::vector<cudaEvent_t> pev;
+    long long prof_launches = 0;
+    double prof_seconds = 0, prof_flops = 0;
+};
+
+namespace {
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) {                                                                  \
+            g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);                    \
+            return e_ == cudaErrorMemoryAllocation ? UNC_ERR_OUT_OF_MEMORY : UNC_ERR_CUDA;        \
+        }                                                                                         \
+    } while (0)
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+// Bump allocator over one device allocation; every piece 256-byte aligned.
+struct Carver {
+    char* base;
+    size_t off = 0;
+    template <class T>
+    T* take(size_t n) {
+        off = (off + 255) & ~size_t(255);
+        T* p = reinterpret_cast<T*>(base ? base + off : nullptr);
+        off += n * sizeof(T);
+        return p;
+    }
+};
+
+struct Plan {
+    int C, P, nobs, N, ld;
+};
+
+struct Buffers {
+    int *rows, *cols;
+    double* vals;
+    double *cam_out, *pt_out;
+    SceneDev s;
+    double *Z, *iZ, *add, *tmp, *e, *gjws, *sig;
+    unsigned long long* amax;
+};
+
+// Lay out the workspace; with base == nullptr only the size is computed.
+size_t carve(char* base, const Plan& pl, bool host_io, long long nnz, int nrows, Buffers& b) {
+    Carver c{base};
+    memset(&b, 0, sizeof(b));
+    if (host_io) {
+        b.rows = c.take<int>((size_t)nrows + 1);
+        b.cols = c.take<int>((size_t)nnz);
+        b.vals = c.take<double>((size_t)nnz);
+        b.cam_out = c.take<double>((size_t)pl.C * 45);
+        b.pt_out = c.take<double>((size_t)pl.P * 6);
+    }
+    SceneDev& s = b.s;
+    s.obs_cam = c.take<int>(pl.nobs);
+    s.obs_pt = c.take<int>(pl.nobs);
+    s.cam_ptr = c.take<int>((size_t)pl.C + 1);
+    s.cam_obs = c.take<int>(pl.nobs);
+    s.pt_ptr = c.take<int>((size_t)pl.P + 1);
+    s.pt_obs = c.take<int>(pl.nobs);
+    s.cursor = c.take<int>((size_t)pl.C + pl.P + 1);
+    s.scan_tmp = c.take<int>(scan_tmp_ints(std::max(pl.C, pl.P)));
+    s.s_cam = c.take<double>((size_t)pl.C * 9);
+    s.s_pt = c.take<double>((size_t)pl.P * 3);
+    s.Vraw = c.take<double>((size_t)pl.P * 6);
+    s.iVs = c.take<double>((size_t)pl.P * 6);
+    s.Ws = c.take<double>((size_t)pl.nobs * 27);
+    s.Ys = c.take<double>((size_t)pl.nobs * 27);
+    s.err = c.take<int>(4);
+    b.amax = c.take<unsigned long long>(4);
+    const size_t nn = (size_t)pl.ld * pl.N;
+    b.Z = c.take<double>(nn);
+    b.iZ = c.take<double>(nn);
+    b.add = c.take<double>(nn);
+    b.tmp = c.take<double>(nn);
+    b.e = c.take<double>(pl.N);
+    b.gjws = c.take<double>(gj_workspace_doubles(pl.N));
+    b.sig = c.take<double>((size_t)pl.C * 81);
+    return c.off + 256;
+}
+
+int ensure_ws(unc_context* ctx, size_t bytes) {
+    if (ctx->ws_bytes >= bytes) return UNC_OK;
+    if (ctx->ws) cudaFree(ctx->ws);
+    ctx->ws = nullptr;
+    ctx->ws_bytes = 0;
+    CK(cudaMalloc(&ctx->ws, bytes));
+    ctx->ws_bytes = bytes;
+    return UNC_OK;
+}
+
+int check_options(const unc_options* o, int num_rows, int num_cols) {
+    if (!o) return fail(UNC_ERR_INVALID_ARG, "options is NULL");
+    if (o->num_cams <= 0 || o->num_points < 0 || num_rows < 0 || (num_rows & 1))
+        return fail(UNC_ERR_INVALID_ARG, "invalid sizes (num_cams > 0, num_points >= 0, even num_rows)");
+    if (o->cam_params != kCamParams)
+        return fail(UNC_ERR_UNSUPPORTED, "only 9 camera parameters are supported");
+    if ((long long)num_cols != 9LL * o->num_cams + 3LL * o->num_points)
+        return fail(UNC_ERR_INVALID_ARG, "num_cols != 9*num_cams + 3*num_points");
+    if (o->algorithm != UNC_TAYLOR_EXPANSION)
+        return fail(UNC_ERR_UNSUPPORTED, "SVD algorithms are not implemented in this build");
+    if (!o->has_pts2fix) return fail(UNC_ERR_NO_FIXED_POINTS, "TAYLOR_EXPANSION needs three fixed points");
+    for (int i = 0; i < 3; ++i)
+        if (o->pts2fix[i] < 0 || o->pts2fix[i] >= o->num_points)
+            return fail(UNC_ERR_INVALID_ARG, "fixed point id out of range");
+    if (o->precision != UNC_PRECISION_FP64)
+        return fail(UNC_ERR_UNSUPPORTED, "mixed precision is not implemented in this build");
+    if (9LL * o->num_cams > 46000) return fail(UNC_ERR_TOO_LARGE, "9*num_cams above 46000");
+    return UNC_OK;
+}
+
+// factorial() of compute.cpp:57-62: 32-bit signed, wraps from 13! on.
+int32_t factorial_i32(int n) {
+    uint32_t f = 1;
+    for (int i = 2; i <= n; ++i) f *= (uint32_t)i;
+    return (int32_t)f;
+}
+
+float ev_s(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms * 1e-3f;
+}
+
+// The pipeline (all device pointers). rows/cols/vals: the Jacobian.
+int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long nnz, const int* rows,
+                 const int* cols, const double* vals, double* cam_out, double* pt_out, Buffers& b,
+                 const Plan& pl, unc_statistic* st, cudaStream_t sm) {
+    SceneDev& s = b.s;
+    s.nnz = (long)nnz;
+    s.num_cams = pl.C;
+    s.num_points = pl.P;
+    s.num_obs = pl.nobs;
+    s.rows = rows;
+    s.cols = cols;
+    s.J = vals;
+    int fx[3] = {o->pts2fix[0], o->pts2fix[1], o->pts2fix[2]};
+    std::sort(fx, fx + 2);  // the reference sorts only the first two ids (compute.cpp:285)
+    s.has_fix = 1;
+    for (int i = 0; i < 3; ++i) s.fix[i] = fx[i];
+    const int N = pl.N, ld = pl.ld;
+    cudaEvent_t* ev = ctx->ev;
+
+    CK(cudaEventRecord(ev[0], sm));
+    CK(cudaMemsetAsync(s.err, 0, 16, sm));
+    launch_validate_obs(s, sm);
+    CK(cudaEventRecord(ev[1], sm));
+    launch_build_index(s, sm);
+    CK(cudaEventRecord(ev[2], sm));
+    // zero the dense buffers once (padding rows must stay finite for the GEMM loads)
+    CK(cudaMemsetAsync(b.Z, 0, (size_t)((char*)(b.tmp + (size_t)ld * N) - (char*)b.Z), sm));
+    launch_camera_blocks(s, b.Z, ld, sm);
+    launch_point_blocks(s, sm);
+    CK(cudaEventRecord(ev[3], sm));
+    launch_obs_blocks(s, sm);
+    CK(cudaEventRecord(ev[4], sm));
+    launch_schur(s, b.Z, ld, sm);
+    launch_mirror_upper(b.Z, N, ld, sm);
+    CK(cudaEventRecord(ev[5], sm));
+
+    double lambda = o->lambda;
+    if (lambda == -1) lambda = pow(10, -1.2653 * log10((double)N) - 2.9415);  // compute.cpp:124-125
+    launch_shift_equilibrate(b.Z, N, ld, lambda, b.e, s.err, sm);
+    gj_inverse(b.Z, N, ld, b.gjws, s.err, sm);
+    launch_unequilibrate(b.Z, N, ld, b.e, b.iZ, sm);  // X in Z, iZ = X
+    CK(cudaEventRecord(ev[6], sm));
+
+    // Taylor expansion (compute.cpp:141-160): iZ = X + sum lambda^i/(i-1)! X^(i+1)
+    const double* X = b.Z;
+    double* add = b.add;
+    double* tmp = b.tmp;
+    size_t npev = 0;
+    auto prof_mark = [&]() -> int {
+        if (!ctx->prof) return UNC_OK;
+        if (npev == ctx->pev.size()) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            ctx->pev.push_back(e);
+        }
+        CK(cudaEventRecord(ctx->pev[npev++], sm));
+        return UNC_OK;
+    };
+    CK(cudaMemsetAsync(b.amax, 0, 8, sm));
+    if (int r = prof_mark()) return r;
+    gemm_f64(N, N, N, 1.0, X, ld, X, ld, 0.0, add, ld, b.amax, sm);
+    if (int r = prof_mark()) return r;
+    double old_change = DBL_MAX;
+    int iters = 0;
+    unsigned long long amax_bits = 0;
+    for (int i = 1; i < 20; ++i) {
+        CK(cudaMemcpyAsync(&amax_bits, b.amax, 8, cudaMemcpyDeviceToHost, sm));
+        CK(cudaStreamSynchronize(sm));
+        double amax;
+        memcpy(&amax, &amax_bits, 8);
+        amax = std::max(amax, DBL_MIN);  // absMax starts at DBL_MIN (ScaledDenseMatrix.cpp:208)
+        double k = pow(lambda, i) / factorial_i32(i - 1);
+        double change = fabs(k * amax);
+        if (change < 1e-5 || change > old_change) break;
+        old_change = change;
+        if (st) st->cycle_change[iters] = change;
+        iters++;
+        launch_axpy(b.iZ, add, k, N, ld, sm);
+        CK(cudaMemsetAsync(b.amax, 0, 8, sm));
+        if (int r = prof_mark()) return r;
+        gemm_f64(N, N, N, 1.0, add, ld, X, ld, 0.0, tmp, ld, b.amax, sm);
+        if (int r = prof_mark()) return r;
+        std::swap(add, tmp);
+    }
+    CK(cudaEventRecord(ev[7], sm));
+
+    launch_camera_output(b.iZ, ld, s.s_cam, pl.C, cam_out, b.sig, sm);
+    if (pl.P > 3) CK(cudaMemsetAsync(pt_out, 0, sizeof(double) * 6 * ((size_t)pl.P - 3), sm));
+    launch_point_cov(s, b.sig, pt_out, sm);
+    CK(cudaEventRecord(ev[8], sm));
+
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, s.err, sizeof(int), cudaMemcpyDeviceToHost, sm));
+    CK(cudaStreamSynchronize(sm));
+    CK(cudaGetLastError());
+    for (size_t i = 0; i + 1 < npev; i += 2) {
+        ctx->prof_seconds += ev_s(ctx->pev[i], ctx->pev[i + 1]);
+        ctx->prof_launches += 1;
+        ctx->prof_flops += 2.0 * (double)N * N * N;
+    }
+    if (st) {
+        st->lambda = lambda;
+        for (int i = 0; i < 3; ++i) st->fixed_pts[i] = fx[i];
+        st->te_iterations = iters;
+        st->time_create_j = ev_s(ev[0], ev[1]);
+        st->time_fix_j = ev_s(ev[1], ev[2]);
+        st->time_norm_j = ev_s(ev[2], ev[3]);
+        st->time_multiply_jj = ev_s(ev[3], ev[4]);
+        st->time_split_jj = 0;
+        st->time_inv_v = 0;
+        st->time_compose_z = ev_s(ev[4], ev[5]);
+        st->time_inv_z = ev_s(ev[5], ev[6]);
+        st->time_te = ev_s(ev[6], ev[7]);
+        st->time_pts_unc = ev_s(ev[7], ev[8]);
+        st->time_all = ev_s(ev[0], ev[8]);
+    }
+    if (err & ERRBIT_LAYOUT)
+        return fail(UNC_ERR_LAYOUT, "Jacobian rows are not in the 2 x (9 camera + 3 point) observation layout");
+    if (err & (ERRBIT_SINGULAR | ERRBIT_NONFINITE))
+        return fail(UNC_ERR_SINGULAR, "non-positive pivot or non-finite value while inverting Z + lambda*I");
+    {
+        double amax;
+        memcpy(&amax, &amax_bits, 8);
+        if (!(amax <= DBL_MAX)) return fail(UNC_ERR_SINGULAR, "non-finite Taylor-series power");
+    }
+    return UNC_OK;
+}
+
+Plan make_plan(const unc_options* o, int num_rows) {
+    Plan pl;
+    pl.C = o->num_cams;
+    pl.P = o->num_points;
+    pl.nobs = num_rows / 2;
+    pl.N = 9 * pl.C;
+    pl.ld = ld_of(pl.N);
+    return pl;
+}
+
+}  // namespace
+
+extern "C" {
+
+void unc_options_init(unc_options* o, int num_cams, int cam_params, int num_points, int num_obs) {
+    if (!o) return;
+    memset(o, 0, sizeof(*o));
+    o->algorithm = UNC_TAYLOR_EXPANSION;
+    o->epsilon = 1e-10;
+    o->lambda = -1;
+    o->num_cams = num_cams;
+    o->cam_params = cam_params;
+    o->num_points = num_points;
+    o->num_obs = num_obs;
+    o->svd_remove_n = -1;
+    o->max_iter_te = -1;
+    o->precision = UNC_PRECISION_FP64;
+}
+
+int unc_context_create(int device, unc_context** out) {
+    if (!out) return fail(UNC_ERR_INVALID_ARG, "ctx is NULL");
+    *out = nullptr;
+    unc_context* c = new unc_context();
+    c->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    for (int i = 0; i < 12 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
+    if (e != cudaSuccess) {
+        g_last_error = std::string("context creation: ") + cudaGetErrorString(e);
+        delete c;
+        return UNC_ERR_CUDA;
+    }
+    *out = c;
+    return UNC_OK;
+}
+
+int unc_context_set_profiling(unc_context* c, int enable) {
+    if (!c) return fail(UNC_ERR_INVALID_ARG, "ctx is NULL");
+    c->prof = enable != 0;
+    return UNC_OK;
+}
+
+int unc_context_profile(unc_context* c, long long* launches, double* seconds, double* flops, int reset) {
+    if (!c) return fail(UNC_ERR_INVALID_ARG, "ctx is NULL");
+    if (launches) *launches = c->prof_launches;
+    if (seconds) *seconds = c->prof_seconds;
+    if (flops) *flops = c->prof_flops;
+    if (reset) {
+        c->prof_launches = 0;
+        c->prof_seconds = 0;
+        c->prof_flops = 0;
+    }
+    return UNC_OK;
+}
+
+int unc_context_destroy(unc_context* c) {
+    if (!c) return UNC_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (cudaEvent_t e : c->pev) cudaEventDestroy(e);
+    if (c->ws) cudaFree(c->ws);
+    for (int i = 0; i < 12; ++i)
+        if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return UNC_OK;
+}
+
+long long unc_workspace_bytes(const unc_options* o, int num_rows, int num_cols) {
+    if (!o || num_rows < 0) return -1;
+    (void)num_cols;
+    Plan pl = make_plan(o, num_rows);
+    Buffers b;
+    return (long long)carve(nullptr, pl, false, 0, num_rows, b);
+}
+
+int unc_compute_device(unc_context* ctx, const unc_options* o, int num_rows, int num_cols,
+                       const int* d_rows, const int* d_cols, const double* d_values,
+                       double* d_cam_unc, double* d_pt_unc, unc_statistic* st, void* stream) {
+    g_last_error.clear();
+    if (!ctx) return fail(UNC_ERR_INVALID_ARG, "unc_compute_device needs a context");
+    int rc = check_options(o, num_rows, num_cols);
+    if (rc) return rc;
+    if (!d_rows || !d_cols || !d_values || !d_cam_unc || !d_pt_unc)
+        return fail(UNC_ERR_INVALID_ARG, "null device pointer");
+    if (((uintptr_t)d_cols & 15) || ((uintptr_t)d_values & 15))
+        return fail(UNC_ERR_INVALID_ARG, "cols/values must be 16-byte aligned");
+    CK(cudaSetDevice(ctx->device));
+    Plan pl = make_plan(o, num_rows);
+    Buffers b;
+    size_t bytes = carve(nullptr, pl, false, 0, num_rows, b);
+    rc = ensure_ws(ctx, bytes);
+    if (rc) return rc;
+    carve((char*)ctx->ws, pl, false, 0, num_rows, b);
+    if (st) {
+        memset(st, 0, sizeof(*st));
+        st->device_bytes = (long long)bytes;
+    }
+    cudaStream_t sm = stream ? (cudaStream_t)stream : ctx->stream;
+    // the arrays are trusted to hold the reference layout's 24 entries per observation
+    return run_pipeline(ctx, o, num_rows, 24LL * pl.nobs, d_rows, d_cols, d_values, d_cam_unc, d_pt_unc,
+                        b, pl, st, sm);
+}
+
+int unc_compute(unc_context* ctx, const unc_options* o, int num_rows, int num_cols, const int* rows,
+                const int* cols, const double* values, double* cam_unc, double* pt_unc,
+                unc_statistic* st) {
+    g_last_error.clear();
+    int rc = check_options(o, num_rows, num_cols);
+    if (rc) return rc;
+    if (!rows || !cols || !values || !cam_unc || !pt_unc) return fail(UNC_ERR_INVALID_ARG, "null pointer");
+    unc_context* own = nullptr;
+    if (!ctx) {
+        rc = unc_context_create(0, &own);
+        if (rc) return rc;
+        ctx = own;
+    }
+    struct Guard {
+        unc_context* c;
+        ~Guard() { unc_context_destroy(c); }
+    } guard{own};
+    const long long nnz = rows[num_rows];
+    if (nnz < 0 || rows[0] != 0) return fail(UNC_ERR_INVALID_ARG, "rowptr must start at 0 and end at nnz >= 0");
+    CK(cudaSetDevice(ctx->device));
+    Plan pl = make_plan(o, num_rows);
+    Buffers b;
+    size_t bytes = carve(nullptr, pl, true, nnz, num_rows, b);
+    rc = ensure_ws(ctx, bytes);
+    if (rc) return rc;
+    carve((char*)ctx->ws, pl, true, nnz, num_rows, b);
+    if (st) {
+        memset(st, 0, sizeof(*st));
+        st->device_bytes = (long long)bytes;
+    }
+    cudaStream_t sm = ctx->stream;
+    CK(cudaMemcpyAsync(b.rows, rows, sizeof(int) * ((size_t)num_rows + 1), cudaMemcpyHostToDevice, sm));
+    CK(cudaMemcpyAsync(b.cols, cols, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, sm));
+    CK(cudaMemcpyAsync(b.vals, values, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice, sm));
+    rc = run_pipeline(ctx, o, num_rows, nnz, b.rows, b.cols, b.vals, b.cam_out, b.pt_out, b, pl, st, sm);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(cam_unc, b.cam_out, sizeof(double) * 45 * (size_t)pl.C, cudaMemcpyDeviceToHost, sm));
+    // Points: slots [0, 6(P-3)) are written (zeroed or computed); of the last
+    // three points only the non-fixed ones are written (compute.cpp:511,526).
+    size_t head = pl.P > 3 ? (size_t)(pl.P - 3) : 0;
+    if (head) CK(cudaMemcpyAsync(pt_unc, b.pt_out, sizeof(double) * 6 * head, cudaMemcpyDeviceToHost, sm));
+    for (int p = (int)head; p < pl.P; ++p) {
+        if (p == b.s.fix[0] || p == b.s.fix[1] || p == b.s.fix[2]) continue;
+        CK(cudaMemcpyAsync(pt_unc + 6L * p, b.pt_out + 6L * p, sizeof(double) * 6, cudaMemcpyDeviceToHost, sm));
+    }
+    CK(cudaStreamSynchronize(sm));
+    return UNC_OK;
+}
+
+int unc_dense_inverse_device(double* d_A, int n, int lda, void* stream) {
+    g_last_error.clear();
+    if (!d_A || n <= 0 || lda < n || (lda & 1)) return fail(UNC_ERR_INVALID_ARG, "bad matrix arguments");
+    cudaStream_t sm = (cudaStream_t)stream;
+    size_t wsd = gj_workspace_doubles(n) + (size_t)n + 64;
+    double* ws = nullptr;
+    int* err = nullptr;
+    CK(cudaMalloc(&ws, wsd * sizeof(double) + 256));
+    err = reinterpret_cast<int*>(ws + wsd);
+    double* e = ws + gj_workspace_doubles(n);
+    int h_err = 0;
+    cudaError_t ce = cudaMemsetAsync(err, 0, sizeof(int), sm);
+    if (ce == cudaSuccess) {
+        launch_shift_equilibrate(d_A, n, lda, 0.0, e, err, sm);
+        gj_inverse(d_A, n, lda, ws, err, sm);
+        launch_unequilibrate(d_A, n, lda, e, nullptr, sm);
+        ce = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, sm);
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(sm);
+    cudaFree(ws);
+    if (ce != cudaSuccess) return fail(UNC_ERR_CUDA, cudaGetErrorString(ce));
+    if (h_err & (ERRBIT_SINGULAR | ERRBIT_NONFINITE)) return fail(UNC_ERR_SINGULAR, "matrix is not positive definite");
+    return UNC_OK;
+}
+
+int unc_jtj_crs(int num_rows, int num_cols, const int* rows, const int* cols, const double* values,
+                int num_cams, int cam_params, long long* nnz_out, int* out_rows, int* out_cols,
+                double* out_vals) {
+    g_last_error.clear();
+    if (!rows || !cols || !values || !nnz_out || num_rows < 0 || (num_rows & 1) || num_cams <= 0)
+        return fail(UNC_ERR_INVALID_ARG, "bad arguments");
+    if (cam_params != kCamParams) return fail(UNC_ERR_UNSUPPORTED, "only 9 camera parameters are supported");
+    const int C = num_cams, cam_off = 9 * C;
+    if (num_cols < cam_off || (num_cols - cam_off) % 3) return fail(UNC_ERR_INVALID_ARG, "bad num_cols");
+    const int P = (num_cols - cam_off) / 3;
+    const int nobs = num_rows / 2;
+    const long long nnz = rows[num_rows];
+    if (rows[0] != 0) return fail(UNC_ERR_INVALID_ARG, "rowptr must start at 0");
+    for (int i = 0; i < num_rows; ++i)
+        if (rows[i + 1] < rows[i] || rows[i + 1] > nnz) return fail(UNC_ERR_INVALID_ARG, "rowptr not monotone");
+    // device buffers
+    int *d_rows = nullptr, *d_cols = nullptr;
+    double *d_vals = nullptr, *d_J = nullptr, *d_U = nullptr, *d_W = nullptr;
+    SceneDev s{};
+    s.num_cams = C;
+    s.num_points = P;
+    s.num_obs = nobs;
+    std::vector<void*> owned;
+    auto dal = [&](void** p, size_t bytes) {
+        cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+        if (e == cudaSuccess) owned.push_back(*p);
+        return e;
+    };
+    struct Free {
+        std::vector<void*>& v;
+        ~Free() {
+            for (void* p : v) cudaFree(p);
+        }
+    } fr{owned};
+    cudaStream_t sm = nullptr;
+    CK(dal((void**)&d_rows, sizeof(int) * ((size_t)num_rows + 1)));
+    CK(dal((void**)&d_cols, sizeof(int) * (size_t)nnz));
+    CK(dal((void**)&d_vals, sizeof(double) * (size_t)nnz));
+    CK(dal((void**)&d_J, sizeof(double) * 24 * (size_t)nobs));
+    CK(dal((void**)&s.obs_cam, sizeof(int) * (size_t)nobs));
+    CK(dal((void**)&s.obs_pt, sizeof(int) * (size_t)nobs));
+    CK(dal((void**)&s.cam_ptr, sizeof(int) * ((size_t)C + 1)));
+    CK(dal((void**)&s.cam_obs, sizeof(int) * (size_t)nobs));
+    CK(dal((void**)&s.pt_ptr, sizeof(int) * ((size_t)P + 1)));
+    CK(dal((void**)&s.pt_obs, sizeof(int) * (size_t)nobs));
+    CK(dal((void**)&s.cursor, sizeof(int) * ((size_t)C + P + 1)));
+    CK(dal((void**)&s.scan_tmp, sizeof(int) * scan_tmp_ints(std::max(C, P))));
+    CK(dal((void**)&s.s_pt, sizeof(double) * 3 * (size_t)P));
+    CK(dal((void**)&s.Vraw, sizeof(double) * 6 * (size_t)P));
+    CK(dal((void**)&s.iVs, sizeof(double) * 6 * (size_t)P));
+    CK(dal((void**)&s.err, sizeof(int) * 4));
+    CK(dal((void**)&d_U, sizeof(double) * 81 * (size_t)C));
+    CK(dal((void**)&d_W, sizeof(double) * 27 * (size_t)nobs));
+    s.J = d_J;
+    CK(cudaMemcpy(d_rows, rows, sizeof(int) * ((size_t)num_rows + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_cols, cols, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_vals, values, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice));
+    CK(cudaMemset(s.err, 0, 16));
+    launch_repack_generic(nobs, cam_off, d_rows, d_cols, d_vals, d_J, s.obs_cam, s.obs_pt, s.err, sm);
+    launch_build_index(s, sm);
+    launch_point_blocks(s, sm);
+    launch_unscaled_blocks(s, d_U, d_W, sm);
+    CK(cudaDeviceSynchronize());
+    int err = 0;
+    CK(cudaMemcpy(&err, s.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err & ERRBIT_LAYOUT) return fail(UNC_ERR_LAYOUT, "rows must have 12 (camera + point) or 9 (camera) entries");
+    std::vector<double> U(81 * (size_t)C), W(27 * (size_t)nobs), V(6 * (size_t)P);
+    std::vector<int> ocam(nobs), opt(nobs);
+    CK(cudaMemcpy(U.data(), d_U, sizeof(double) * U.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(W.data(), d_W, sizeof(double) * W.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(V.data(), s.Vraw, sizeof(double) * V.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ocam.data(), s.obs_cam, sizeof(int) * nobs, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(opt.data(), s.obs_pt, sizeof(int) * nobs, cudaMemcpyDeviceToHost));
+    // Pattern of J^T J from the block structure: camera rows hold their own
+    // 9x9 block then one 3-wide block per observed point; point rows hold one
+    // 9-wide block per observing camera then their own 3x3 block.
+    std::vector<char> cam_seen(C, 0);
+    std::vector<std::vector<std::pair<int, int>>> cam_pts(C), pt_cams(P);  // (other id, obs)
+    for (int o = 0; o < nobs; ++o) {
+        if (ocam[o] < 0) continue;
+        cam_seen[ocam[o]] = 1;
+        if (opt[o] >= 0) {
+            cam_pts[ocam[o]].push_back({opt[o], o});
+            pt_cams[opt[o]].push_back({ocam[o], o});
+        }
+    }
+    for (auto& v : cam_pts) std::sort(v.begin(), v.end());
+    for (auto& v : pt_cams) std::sort(v.begin(), v.end());
+    std::vector<int> orow(num_cols + 1, 0), ocol;
+    std::vector<double> oval;
+    for (int c = 0; c < C; ++c)
+        for (int j = 0; j < 9; ++j) {
+            if (cam_seen[c])
+                for (int k = 0; k < 9; ++k) {
+                    ocol.push_back(9 * c + k);
+                    oval.push_back(U[81L * c + 9 * j + k]);
+                }
+            auto& lst = cam_pts[c];
+            for (size_t a = 0; a < lst.size();) {
+                size_t e = a;
+                double sum[3] = {0, 0, 0};
+                while (e < lst.size() && lst[e].first == lst[a].first) {
+                    for (int k = 0; k < 3; ++k) sum[k] += W[27L * lst[e].second + 3 * j + k];
+                    ++e;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    ocol.push_back(cam_off + 3 * lst[a].first + k);
+                    oval.push_back(sum[k]);
+                }
+                a = e;
+            }
+            orow[9 * c + j + 1] = (int)ocol.size();
+        }
+    for (int p = 0; p < P; ++p)
+        for (int k = 0; k < 3; ++k) {
+            auto& lst = pt_cams[p];
+            for (size_t a = 0; a < lst.size();) {
+                size_t e = a;
+                double sum[9] = {0};
+                while (e < lst.size() && lst[e].first == lst[a].first) {
+                    for (int j = 0; j < 9; ++j) sum[j] += W[27L * lst[e].second + 3 * j + k];
+                    ++e;
+                }
+                for (int j = 0; j < 9; ++j) {
+                    ocol.push_back(9 * lst[a].first + j);
+                    oval.push_back(sum[j]);
+                }
+                a = e;
+            }
+            if (!lst.empty()) {
+                const double* v = V.data() + 6L * p;
+                const double full[3][3] = {{v[0], v[1], v[2]}, {v[1], v[3], v[4]}, {v[2], v[4], v[5]}};
+                for (int q = 0; q < 3; ++q) {
+                    ocol.push_back(cam_off + 3 * p + q);
+                    oval.push_back(full[k][q]);
+                }
+            }
+            orow[cam_off + 3 * p + k + 1] = (int)ocol.size();
+        }
+    *nnz_out = (long long)ocol.size();
+    if (out_cols) {
+        if (!out_rows || !out_vals) return fail(UNC_ERR_INVALID_ARG, "null output arrays");
+        std::copy(orow.begin(), orow.end(), out_rows);
+        std::copy(ocol.begin(), ocol.end(), out_cols);
+        std::copy(oval.begin(), oval.end(), out_vals);
+    }
+    return UNC_OK;
+}
+
+const char* unc_status_string(int s) {
+    switch (s) {
+        case UNC_OK: return "UNC_OK";
+        case UNC_ERR_INVALID_ARG: return "UNC_ERR_INVALID_ARG";
+        case UNC_ERR_LAYOUT: return "UNC_ERR_LAYOUT";
+        case UNC_ERR_NO_FIXED_POINTS: return "UNC_ERR_NO_FIXED_POINTS";
+        case UNC_ERR_CUDA: return "UNC_ERR_CUDA";
+        case UNC_ERR_OUT_OF_MEMORY: return "UNC_ERR_OUT_OF_MEMORY";
+        case UNC_ERR_SINGULAR: return "UNC_ERR_SINGULAR";
+        case UNC_ERR_UNSUPPORTED: return "UNC_ERR_UNSUPPORTED";
+        case UNC_ERR_TOO_LARGE: return "UNC_ERR_TOO_LARGE";
+        default: return "UNC_ERR_UNKNOWN";
+    }
+}
+
+const char* unc_last_error(void) { return g_last_error.c_str(); }
+
+long long unc_kernel_launches(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+}  // extern "C"

@@ -1,0 +1,95 @@
+// internal.h - shared declarations of the uncertaintyTE B200 kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+namespace unc {
+
+// Device-side error bits (accumulated with atomicOr into a device int).
+enum : int {
+    ERRBIT_LAYOUT = 1,      // observation rows not 12 entries / columns out of range
+    ERRBIT_SINGULAR = 2,    // non-positive or non-finite pivot
+    ERRBIT_NONFINITE = 4,   // NaN / Inf produced
+    ERRBIT_SORT_CAP = 8,    // a segment was too long to sort (order left nondeterministic)
+};
+
+constexpr int kCamParams = 9;
+constexpr int kObsVals = 24;  // one observation = 2 rows x (9 camera + 3 point) values
+
+// Round a leading dimension up so every column starts 64-byte aligned.
+inline int ld_of(int n) { return (n + 7) & ~7; }
+
+extern thread_local std::string g_last_error;
+extern long long g_launches;
+inline void count_launch(int n = 1) { __atomic_add_fetch(&g_launches, n, __ATOMIC_RELAXED); }
+
+// ---------------- assembly.cu ----------------
+struct SceneDev {
+    int num_cams, num_points, num_obs;  // num_obs = num_rows / 2
+    long nnz;                           // entries of cols / values
+    int fix[3];
+    int has_fix;
+    const int* rows;      // CRS rowptr
+    const int* cols;      // CRS column ids
+    const double* J;      // observation blocks, 24 doubles each: [row0: c0..c8 p0..p2 | row1: ...]
+    int* obs_cam;         // per observation camera id (-1 = dropped)
+    int* obs_pt;          // per observation point id (-1 = dropped: fixed point or no point)
+    int* cam_ptr;         // num_cams + 1
+    int* cam_obs;         // observation ids grouped by camera (ascending within a camera)
+    int* pt_ptr;          // num_points + 1
+    int* pt_obs;          // observation ids grouped by point (ascending within a point)
+    int* cursor;          // scratch: max(num_cams, num_points) + 1 ints
+    int* scan_tmp;        // scratch for the scan
+    double* s_cam;        // 9*num_cams column norms of J (camera columns)
+    double* s_pt;         // 3*num_points column norms (point columns)
+    double* Vraw;         // 6*num_points upper triangle of the unscaled point block J_p^T J_p
+    double* iVs;          // 6*num_points upper triangle of the inverse of the scaled point block
+    double* Ws;           // 27*num_obs scaled W_o = (J_c^T J_p)/(s s), 9x3 row-major
+    double* Ys;           // 27*num_obs Y_o = W_o * iV_p, 9x3 row-major
+    int* err;             // device error bits
+};
+
+void launch_validate_obs(const SceneDev& s, cudaStream_t st);
+void launch_build_index(SceneDev& s, cudaStream_t st);
+// U blocks (scaled) written to the diagonal blocks of Z (ldz), column norms.
+void launch_camera_blocks(const SceneDev& s, double* Z, int ldz, cudaStream_t st);
+void launch_point_blocks(const SceneDev& s, cudaStream_t st);
+void launch_obs_blocks(const SceneDev& s, cudaStream_t st);
+// Z(c,c') -= sum_p Y_o W_o'^T (upper camera-block triangle), then mirror.
+void launch_schur(const SceneDev& s, double* Z, int ldz, cudaStream_t st);
+void launch_mirror_upper(double* Z, int n, int ldz, cudaStream_t st);
+// Generic 9/12-entry-row repack for the J^T J export (camera-only rows allowed).
+void launch_repack_generic(int num_obs, int cam_off, const int* rows, const int* cols,
+                           const double* vals, double* J, int* obs_cam, int* obs_pt, int* err,
+                           cudaStream_t st);
+void launch_unscaled_blocks(const SceneDev& s, double* U, double* W, cudaStream_t st);
+void exclusive_scan(const int* in, int* out, int n, int* tmp, cudaStream_t st);
+size_t scan_tmp_ints(int n);
+
+// ---------------- dense.cu ----------------
+// C = alpha*A*B + beta*C, column-major, FP64 on DMMA. If amax != nullptr the
+// epilogue folds max|C| into *amax (bit pattern of a non-negative double).
+void gemm_f64(int M, int N, int K, double alpha, const double* A, int lda, const double* B,
+              int ldb, double beta, double* C, int ldc, unsigned long long* amax, cudaStream_t st);
+// In-place inverse of an SPD matrix by blocked Gauss-Jordan (no pivoting).
+// ws: workspace of gj_workspace_doubles(n) doubles. Sets ERRBIT_SINGULAR in err.
+size_t gj_workspace_doubles(int n);
+void gj_inverse(double* A, int n, int lda, double* ws, int* err, cudaStream_t st);
+// A <- A + lambda*I and symmetric Jacobi equilibration: A_s = E A E, E = diag(A_ii)^-1/2.
+void launch_shift_equilibrate(double* A, int n, int lda, double lambda, double* e, int* err,
+                              cudaStream_t st);
+// X <- E X E (undo equilibration), also copies into Y if Y != nullptr.
+void launch_unequilibrate(double* X, int n, int lda, const double* e, double* Y, cudaStream_t st);
+// Y <- Y + k*X  (N x N, column-major)
+void launch_axpy(double* Y, const double* X, double k, int n, int ld, cudaStream_t st);
+void launch_zero(double* p, size_t n, cudaStream_t st);
+// Camera output (a+b/2 quirk) and the unscaled 9x9 camera covariance blocks.
+void launch_camera_output(const double* iZ, int ldz, const double* s_cam, int num_cams,
+                          double* cam_unc, double* sig, cudaStream_t st);
+
+// ---------------- points.cu ----------------
+void launch_point_cov(const SceneDev& s, const double* sig, double* pt_unc, cudaStream_t st);
+
+}  // namespace unc

@@ -1,0 +1,234 @@
+"""ctypes binding of libuncte.so (the C ABI in include/uncte.h).
+
+The product path is the CUDA library; there is no CPU fallback. Importing
+this module without the built library raises ImportError, and every call
+returns the library's status as an UncError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from .jacob import Jacobian
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libuncte.so")
+
+UNC_OK = 0
+TAYLOR_EXPANSION = 2
+SVD_QR_ITERATION = 0
+SVD_DEVIDE_AND_CONQUER = 1
+PRECISION = {"fp64": 0, "mixed": 1}
+
+
+class UncError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class UncOptions(C.Structure):
+    _fields_ = [
+        ("algorithm", C.c_int),
+        ("epsilon", C.c_double),
+        ("lam", C.c_double),
+        ("num_cams", C.c_int),
+        ("cam_params", C.c_int),
+        ("num_points", C.c_int),
+        ("num_obs", C.c_int),
+        ("svd_remove_n", C.c_int),
+        ("max_iter_te", C.c_int),
+        ("pts2fix", C.c_int * 3),
+        ("has_pts2fix", C.c_int),
+        ("precision", C.c_int),
+    ]
+
+
+class UncStatistic(C.Structure):
+    _fields_ = [
+        ("time_create_j", C.c_double),
+        ("time_fix_j", C.c_double),
+        ("time_norm_j", C.c_double),
+        ("time_multiply_jj", C.c_double),
+        ("time_split_jj", C.c_double),
+        ("time_inv_v", C.c_double),
+        ("time_compose_z", C.c_double),
+        ("time_inv_z", C.c_double),
+        ("time_te", C.c_double),
+        ("time_pts_unc", C.c_double),
+        ("time_all", C.c_double),
+        ("lam", C.c_double),
+        ("fixed_pts", C.c_int * 3),
+        ("te_iterations", C.c_int),
+        ("cycle_change", C.c_double * 20),
+        ("device_bytes", C.c_longlong),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("fixed_pts", "cycle_change", "lam")}
+        d["lambda"] = self.lam
+        d["fixed_pts"] = list(self.fixed_pts)
+        d["cycle_change"] = list(self.cycle_change[: self.te_iterations])
+        return d
+
+
+# every symbol declared in include/uncte.h
+EXPORTS = ("unc_options_init", "unc_context_create", "unc_context_destroy", "unc_compute",
+           "unc_context_set_profiling", "unc_context_profile",
+           "unc_compute_device", "unc_workspace_bytes", "unc_dense_inverse_device", "unc_jtj_crs",
+           "unc_status_string", "unc_last_error", "unc_kernel_launches")
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C uncertaintyte_b200/csrc` "
+                          "(or __graft_entry__.build())")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    vp = C.c_void_p
+    L.unc_options_init.argtypes = [P(UncOptions), C.c_int, C.c_int, C.c_int, C.c_int]
+    L.unc_options_init.restype = None
+    L.unc_context_create.argtypes = [C.c_int, P(vp)]
+    L.unc_context_destroy.argtypes = [vp]
+    L.unc_compute.argtypes = [vp, P(UncOptions), C.c_int, C.c_int, vp, vp, vp, vp, vp, P(UncStatistic)]
+    L.unc_compute_device.argtypes = [vp, P(UncOptions), C.c_int, C.c_int, vp, vp, vp, vp, vp,
+                                     P(UncStatistic), vp]
+    L.unc_context_set_profiling.argtypes = [vp, C.c_int]
+    L.unc_context_profile.argtypes = [vp, P(C.c_longlong), P(C.c_double), P(C.c_double), C.c_int]
+    L.unc_workspace_bytes.argtypes = [P(UncOptions), C.c_int, C.c_int]
+    L.unc_workspace_bytes.restype = C.c_longlong
+    L.unc_dense_inverse_device.argtypes = [vp, C.c_int, C.c_int, vp]
+    L.unc_jtj_crs.argtypes = [C.c_int, C.c_int, vp, vp, vp, C.c_int, C.c_int, P(C.c_longlong), vp,
+                              vp, vp]
+    L.unc_status_string.argtypes = [C.c_int]
+    L.unc_status_string.restype = C.c_char_p
+    L.unc_last_error.restype = C.c_char_p
+    L.unc_kernel_launches.restype = C.c_longlong
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != UNC_OK:
+        L = lib()
+        raise UncError(rc, f"{L.unc_status_string(rc).decode()}: {L.unc_last_error().decode()}")
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def make_options(jac: Jacobian, algorithm: Optional[int] = None, precision: str = "fp64",
+                 lam: Optional[float] = None) -> UncOptions:
+    o = UncOptions()
+    lib().unc_options_init(C.byref(o), jac.num_cams, jac.cam_params, jac.num_points, jac.num_obs)
+    o.algorithm = jac.algorithm if algorithm is None else algorithm
+    o.epsilon = jac.epsilon
+    o.lam = jac.lam if lam is None else lam
+    o.svd_remove_n = jac.svd_remove_n
+    if jac.pts2fix is not None:
+        o.pts2fix[:] = [int(x) for x in jac.pts2fix]
+        o.has_pts2fix = 1
+    o.precision = PRECISION[precision]
+    return o
+
+
+class Context:
+    """Owns a CUDA stream and a device workspace reused across calls."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        _check(lib().unc_context_create(device, C.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().unc_context_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_profiling(self, enable: bool = True):
+        _check(lib().unc_context_set_profiling(self._h, int(enable)))
+
+    def profile(self, reset: bool = True):
+        """(launches, seconds, flops) of the Taylor-series products since the last reset."""
+        n, s, f = C.c_longlong(), C.c_double(), C.c_double()
+        _check(lib().unc_context_profile(self._h, C.byref(n), C.byref(s), C.byref(f), int(reset)))
+        return n.value, s.value, f.value
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def compute_covariances(jac: Jacobian, ctx: Optional[Context] = None, algorithm: Optional[int] = None,
+                        precision: str = "fp64", cam_init=None, pt_init=None):
+    """computeCovariances on host arrays: returns (cam (C*45,), pt (P*6,), stats dict)."""
+    o = make_options(jac, algorithm, precision)
+    cam = np.zeros(jac.num_cams * 45) if cam_init is None else np.array(cam_init, dtype=np.float64)
+    pt = np.zeros(jac.num_points * 6) if pt_init is None else np.array(pt_init, dtype=np.float64)
+    rows = np.ascontiguousarray(jac.rows, dtype=np.int32)
+    cols = np.ascontiguousarray(jac.cols, dtype=np.int32)
+    vals = np.ascontiguousarray(jac.values, dtype=np.float64)
+    st = UncStatistic()
+    _check(lib().unc_compute(ctx.handle if ctx else None, C.byref(o), jac.num_rows, jac.num_cols,
+                             _ptr(rows), _ptr(cols), _ptr(vals), _ptr(cam), _ptr(pt), C.byref(st)))
+    return cam, pt, st.as_dict()
+
+
+def compute_covariances_device(ctx: Context, opts: UncOptions, num_rows: int, num_cols: int,
+                               d_rows: int, d_cols: int, d_vals: int, d_cam: int, d_pt: int,
+                               stream: int = 0) -> dict:
+    """Device-pointer form (inputs resident in HBM); pointers are integers."""
+    st = UncStatistic()
+    _check(lib().unc_compute_device(ctx.handle, C.byref(opts), num_rows, num_cols, d_rows, d_cols,
+                                    d_vals, d_cam, d_pt, C.byref(st), stream or None))
+    return st.as_dict()
+
+
+def workspace_bytes(jac: Jacobian) -> int:
+    o = make_options(jac)
+    return int(lib().unc_workspace_bytes(C.byref(o), jac.num_rows, jac.num_cols))
+
+
+def dense_inverse_device(d_ptr: int, n: int, lda: int, stream: int = 0) -> None:
+    _check(lib().unc_dense_inverse_device(d_ptr, n, lda, stream or None))
+
+
+def jtj_crs(num_rows: int, num_cols: int, rows, cols, vals, num_cams: int, cam_params: int = 9):
+    """GPU J^T J in the reference's CRS pattern: (rowptr, cols, vals)."""
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    cols = np.ascontiguousarray(cols, dtype=np.int32)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    nnz = C.c_longlong(0)
+    L = lib()
+    _check(L.unc_jtj_crs(num_rows, num_cols, _ptr(rows), _ptr(cols), _ptr(vals), num_cams, cam_params,
+                         C.byref(nnz), None, None, None))
+    orow = np.zeros(num_cols + 1, np.int32)
+    ocol = np.zeros(nnz.value, np.int32)
+    oval = np.zeros(nnz.value)
+    _check(L.unc_jtj_crs(num_rows, num_cols, _ptr(rows), _ptr(cols), _ptr(vals), num_cams, cam_params,
+                         C.byref(nnz), _ptr(orow), _ptr(ocol), _ptr(oval)))
+    return orow, ocol, oval
+
+
+def kernel_launches() -> int:
+    return int(lib().unc_kernel_launches())
