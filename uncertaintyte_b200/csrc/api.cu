@@ -25,6 +25,8 @@ struct unc_context {
     cudaStream_t stream = nullptr;
     void* ws = nullptr;
     size_t ws_bytes = 0;
+    void* tup = nullptr;  // Schur pair tuples (sized at run time)
+    size_t tup_bytes = 0;
     cudaEvent_t ev[12] = {};
     // profiling of the Taylor-series products
     bool prof = false;
@@ -101,6 +103,8 @@ size_t carve(char* base, const Plan& pl, bool host_io, long long nnz, int nrows,
     s.iVs = c.take<double>((size_t)pl.P * 6);
     s.Ws = c.take<double>((size_t)pl.nobs * 27);
     s.Ys = c.take<double>((size_t)pl.nobs * 27);
+    s.deg = c.take<int>(pl.nobs);
+    s.tup_off = c.take<int>((size_t)pl.nobs + 1);
     s.err = c.take<int>(4);
     b.amax = c.take<unsigned long long>(4);
     const size_t nn = (size_t)pl.ld * pl.N;
@@ -109,7 +113,7 @@ size_t carve(char* base, const Plan& pl, bool host_io, long long nnz, int nrows,
     b.add = c.take<double>(nn);
     b.tmp = c.take<double>(nn);
     b.e = c.take<double>(pl.N);
-    b.gjws = c.take<double>(gj_workspace_doubles(pl.N));
+    b.gjws = c.take<double>(chol_small_doubles(pl.N));
     b.sig = c.take<double>((size_t)pl.C * 81);
     return c.off + 256;
 }
@@ -188,7 +192,23 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     launch_point_blocks(s, sm);
     CK(cudaEventRecord(ev[3], sm));
     launch_obs_blocks(s, sm);
+    launch_schur_offsets(s, sm);
+    int ntup = 0;
+    CK(cudaMemcpyAsync(&ntup, s.tup_off + pl.nobs, sizeof(int), cudaMemcpyDeviceToHost, sm));
     CK(cudaEventRecord(ev[4], sm));
+    CK(cudaStreamSynchronize(sm));
+    if (ntup < 0) return fail(UNC_ERR_TOO_LARGE, "more than 2^31 Schur pair terms");
+    if (ctx->tup_bytes < (size_t)ntup * sizeof(int4) + 16) {
+        if (ctx->tup) cudaFree(ctx->tup);
+        ctx->tup = nullptr;
+        ctx->tup_bytes = 0;
+        size_t want = (size_t)ntup * sizeof(int4) + 16;
+        want += want / 4;  // headroom for the next scene
+        CK(cudaMalloc(&ctx->tup, want));
+        ctx->tup_bytes = want;
+    }
+    s.tup = reinterpret_cast<int4*>(ctx->tup);
+    launch_schur_tuples(s, sm);
     launch_schur(s, b.Z, ld, sm);
     launch_mirror_upper(b.Z, N, ld, sm);
     CK(cudaEventRecord(ev[5], sm));
@@ -196,7 +216,7 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     double lambda = o->lambda;
     if (lambda == -1) lambda = pow(10, -1.2653 * log10((double)N) - 2.9415);  // compute.cpp:124-125
     launch_shift_equilibrate(b.Z, N, ld, lambda, b.e, s.err, sm);
-    gj_inverse(b.Z, N, ld, b.gjws, s.err, sm);
+    chol_inverse(b.Z, N, ld, b.iZ, b.add, b.tmp, b.gjws, s.err, sm);
     launch_unequilibrate(b.Z, N, ld, b.e, b.iZ, sm);  // X in Z, iZ = X
     CK(cudaEventRecord(ev[6], sm));
 
@@ -356,6 +376,7 @@ int unc_context_destroy(unc_context* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (cudaEvent_t e : c->pev) cudaEventDestroy(e);
     if (c->ws) cudaFree(c->ws);
+    if (c->tup) cudaFree(c->tup);
     for (int i = 0; i < 12; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -452,17 +473,18 @@ int unc_dense_inverse_device(double* d_A, int n, int lda, void* stream) {
     g_last_error.clear();
     if (!d_A || n <= 0 || lda < n || (lda & 1)) return fail(UNC_ERR_INVALID_ARG, "bad matrix arguments");
     cudaStream_t sm = (cudaStream_t)stream;
-    size_t wsd = gj_workspace_doubles(n) + (size_t)n + 64;
+    const size_t mat = (size_t)lda * n;
+    const size_t wsd = 3 * mat + chol_small_doubles(n) + (size_t)n + 64;
     double* ws = nullptr;
-    int* err = nullptr;
     CK(cudaMalloc(&ws, wsd * sizeof(double) + 256));
-    err = reinterpret_cast<int*>(ws + wsd);
-    double* e = ws + gj_workspace_doubles(n);
+    double *T = ws, *W = ws + mat, *Tt = ws + 2 * mat, *small = ws + 3 * mat;
+    double* e = small + chol_small_doubles(n);
+    int* err = reinterpret_cast<int*>(ws + wsd);
     int h_err = 0;
-    cudaError_t ce = cudaMemsetAsync(err, 0, sizeof(int), sm);
+    cudaError_t ce = cudaMemsetAsync(ws, 0, wsd * sizeof(double) + 256, sm);
     if (ce == cudaSuccess) {
         launch_shift_equilibrate(d_A, n, lda, 0.0, e, err, sm);
-        gj_inverse(d_A, n, lda, ws, err, sm);
+        chol_inverse(d_A, n, lda, T, W, Tt, small, err, sm);
         launch_unequilibrate(d_A, n, lda, e, nullptr, sm);
         ce = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, sm);
     }

@@ -365,12 +365,12 @@ __global__ void __launch_bounds__(128) k_camera_blocks(int num_cams, const doubl
 #pragma unroll
     for (int j = 0; j < 9; ++j) s[j] = sqrt(acc[ut9(j, j)]);
     if (lane < 9 && s_cam) s_cam[9 * cam + lane] = s[lane];
-    // lanes 0..44 write one upper-triangle value each (and its mirror)
+    // 45 upper-triangle values over 32 lanes: lane l writes t = l and t = l + 32
 #pragma unroll
     for (int j = 0; j < 9; ++j)
 #pragma unroll
         for (int k = j; k < 9; ++k) {
-            if (lane == ut9(j, k)) {
+            if (lane == ut9(j, k) || lane + 32 == ut9(j, k)) {
                 double v = acc[ut9(j, k)];
                 if (kScaled) {
                     // J <- J * diag(1/s) skipping s == 0 (ScaledSparseMatrix.cpp:352-356)
@@ -488,39 +488,152 @@ void launch_obs_blocks(const SceneDev& s, cudaStream_t st) {
     count_launch();
 }
 
-// One warp per point: Z(c_a, c_b) -= Y_a W_b^T over ordered observation pairs
-// with c_a <= c_b (upper camera-block triangle; inside a diagonal block only
-// the upper element triangle). Element-major lane mapping keeps the FP64
-// atomics of a warp on consecutive rows of one column.
-__global__ void __launch_bounds__(256) k_schur(int num_points, const int* __restrict__ pt_ptr,
-                                               const int* __restrict__ pt_obs,
-                                               const int* __restrict__ obs_cam,
-                                               const double* __restrict__ Ws,
-                                               const double* __restrict__ Ys, double* Z, long ldz) {
-    int p = blockIdx.x * 8 + (threadIdx.x >> 5);
-    int lane = threadIdx.x & 31;
-    if (p >= num_points) return;
-    int b = pt_ptr[p], n = pt_ptr[p + 1] - b;
-    if (n == 0) return;
-    const int items = n * n * 81;
-    for (int it = lane; it < items; it += 32) {
-        int pair = it / 81, el = it - pair * 81;
-        int ia = pair / n, ib = pair - ia * n;
-        int oa = pt_obs[b + ia], ob = pt_obs[b + ib];
-        int ca = obs_cam[oa], cb = obs_cam[ob];
-        int col = el / 9, row = el - col * 9;  // element (row, col) of the 9x9 block
-        if (ca > cb || (ca == cb && row > col)) continue;
-        const double* y = Ys + 27L * oa + 3 * row;
-        const double* w = Ws + 27L * ob + 3 * col;
-        double v = y[0] * w[0] + y[1] * w[1] + y[2] * w[2];
-        atomicAdd(Z + (9L * ca + row) + (9L * cb + col) * ldz, -v);
+// Deterministic Schur scatter, in two kernels.
+//
+// k_pair_tuples: for every entry i of the camera-grouped observation list
+// (observation o of camera c, point p) write the tuples (o, o2, camera(o2))
+// for all observations o2 of p, at offsets from one exclusive scan of the
+// point degrees. The result lists, camera by camera, every (o, o2) pair that
+// contributes Y_o W_o2^T to the block row of c, in a fixed order.
+//
+// k_schur_rows: one CTA owns the block row of camera c (columns of cameras
+// [c0, c0 + kSchurChunk)) and accumulates it in shared memory:
+//   Z(c, c') -= sum over points p seen by c and c' of Y_o W_o'^T,  c' >= c.
+// Four thread groups split the target cameras (c' mod 4); inside a group
+// thread e < 81 owns element (row, col) = (e % 9, e / 9) of every 9x9 block,
+// so each output element receives its terms in one fixed order: bitwise
+// repeatable results. Z is written once (upper block triangle; inside the
+// diagonal block only row <= col) and mirrored afterwards.
+constexpr int kSchurChunk = 200;  // cameras per column chunk: 9 x 1800 doubles = 129.6 KB smem
+constexpr int kSchurSmem = 9 * 9 * kSchurChunk * (int)sizeof(double);
+constexpr int kSchurGroups = 4;
+
+__global__ void k_point_degree(int n, const int* __restrict__ cam_obs, const int* __restrict__ obs_pt,
+                               const int* __restrict__ pt_ptr, const int* __restrict__ n_valid,
+                               int* __restrict__ deg) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (i >= *n_valid) {  // entries past the kept observations
+        deg[i] = 0;
+        return;
+    }
+    int p = obs_pt[cam_obs[i]];
+    deg[i] = pt_ptr[p + 1] - pt_ptr[p];
+}
+
+__global__ void k_pair_tuples(int n, const int* __restrict__ cam_obs, const int* __restrict__ obs_pt,
+                              const int* __restrict__ pt_ptr, const int* __restrict__ pt_obs,
+                              const int* __restrict__ obs_cam, const int* __restrict__ off,
+                              const int* __restrict__ n_valid, int4* __restrict__ tup) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || i >= *n_valid) return;
+    int o = cam_obs[i], p = obs_pt[o];
+    long long t = off[i];
+    for (int k = pt_ptr[p]; k < pt_ptr[p + 1]; ++k, ++t) {
+        int o2 = pt_obs[k];
+        tup[t] = make_int4(o, o2, obs_cam[o2], 0);
     }
 }
 
+__global__ void __launch_bounds__(96 * kSchurGroups) k_schur_rows(int num_cams,
+                                                                  const int* __restrict__ cam_ptr,
+                                                                  const int* __restrict__ off,
+                                                                  const int4* __restrict__ tup,
+                                                                  const double* __restrict__ Ws,
+                                                                  const double* __restrict__ Ys,
+                                                                  double* Z, long ldz) {
+    extern __shared__ double acc[];  // acc[row * (9 * kSchurChunk) + (c' - c0) * 9 + col]
+    const int c = blockIdx.x;
+    const int c0 = blockIdx.y * kSchurChunk;
+    const int cn = min(kSchurChunk, num_cams - c0);
+    if (c0 + cn <= c) return;  // chunk entirely left of the diagonal
+    const int W9 = 9 * kSchurChunk;
+    for (int i = threadIdx.x; i < 9 * W9; i += blockDim.x) acc[i] = 0.0;
+    __syncthreads();
+    const int g = threadIdx.x / 96, e = threadIdx.x % 96;
+    const int row = e % 9, col = e / 9;
+    const int lo = max(c, c0), hi = c0 + cn;
+    if (e < 81) {
+        const long long t0 = off[cam_ptr[c]], t1 = off[cam_ptr[c + 1]];  // tuples of camera c
+        long long t = t0;
+        for (; t + 4 <= t1; t += 4) {
+            int4 q[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) q[u] = __ldg(tup + t + u);
+            double v[4];
+            bool take[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                take[u] = q[u].z >= lo && q[u].z < hi && (q[u].z & (kSchurGroups - 1)) == g;
+                v[u] = 0.0;
+                if (take[u]) {
+                    const double* y = Ys + 27L * q[u].x + 3 * row;
+                    const double* w = Ws + 27L * q[u].y + 3 * col;
+                    v[u] = __ldg(y) * __ldg(w) + __ldg(y + 1) * __ldg(w + 1) + __ldg(y + 2) * __ldg(w + 2);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (take[u]) acc[row * W9 + (q[u].z - c0) * 9 + col] += v[u];
+        }
+        for (; t < t1; ++t) {
+            int4 q = __ldg(tup + t);
+            if (q.z >= lo && q.z < hi && (q.z & (kSchurGroups - 1)) == g) {
+                const double* y = Ys + 27L * q.x + 3 * row;
+                const double* w = Ws + 27L * q.y + 3 * col;
+                acc[row * W9 + (q.z - c0) * 9 + col] +=
+                    __ldg(y) * __ldg(w) + __ldg(y + 1) * __ldg(w + 1) + __ldg(y + 2) * __ldg(w + 2);
+            }
+        }
+    }
+    __syncthreads();
+    // write: column-major Z, 9 consecutive rows per column
+    const int ncols = 9 * (hi - lo);
+    for (int idx = threadIdx.x; idx < 9 * ncols; idx += blockDim.x) {
+        const int r = idx % 9, q = idx / 9;
+        const int cc = lo + q / 9, cl = q % 9;
+        const double v = acc[r * W9 + (cc - c0) * 9 + cl];
+        double* z = Z + (9L * c + r) + (9L * cc + cl) * ldz;
+        if (cc == c) {
+            if (r <= cl) *z -= v;  // diagonal block holds U (scaled) already
+        } else {
+            *z = -v;
+        }
+    }
+}
+
+// Degrees and offsets of the tuple list; returns nothing, the total is
+// tup_off[num_obs] (read back by the caller to size the tuple buffer).
+void launch_schur_offsets(const SceneDev& s, cudaStream_t st) {
+    const int n = s.num_obs;
+    if (n == 0) {
+        cudaMemsetAsync(s.tup_off, 0, sizeof(int), st);
+        return;
+    }
+    k_point_degree<<<(n + 255) / 256, 256, 0, st>>>(n, s.cam_obs, s.obs_pt, s.pt_ptr, s.cam_ptr + s.num_cams,
+                                                    s.deg);
+    count_launch();
+    exclusive_scan(s.deg, s.tup_off, n, s.scan_tmp, st);
+}
+
+void launch_schur_tuples(const SceneDev& s, cudaStream_t st) {
+    const int n = s.num_obs;
+    if (n == 0) return;
+    k_pair_tuples<<<(n + 255) / 256, 256, 0, st>>>(n, s.cam_obs, s.obs_pt, s.pt_ptr, s.pt_obs, s.obs_cam,
+                                                   s.tup_off, s.cam_ptr + s.num_cams, s.tup);
+    count_launch();
+}
+
 void launch_schur(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
-    if (s.num_points == 0) return;
-    k_schur<<<(s.num_points + 7) / 8, 256, 0, st>>>(s.num_points, s.pt_ptr, s.pt_obs, s.obs_cam,
-                                                    s.Ws, s.Ys, Z, ldz);
+    if (s.num_cams == 0) return;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_schur_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kSchurSmem);
+        attr = true;
+    }
+    dim3 grid(s.num_cams, (s.num_cams + kSchurChunk - 1) / kSchurChunk);
+    k_schur_rows<<<grid, 96 * kSchurGroups, kSchurSmem, st>>>(s.num_cams, s.cam_ptr, s.tup_off, s.tup,
+                                                              s.Ws, s.Ys, Z, ldz);
     count_launch();
 }
 
@@ -576,7 +689,7 @@ __global__ void __launch_bounds__(128) k_camera_blocks_raw(int num_cams, const d
     for (int j = 0; j < 9; ++j)
 #pragma unroll
         for (int k = j; k < 9; ++k)
-            if (lane == ut9(j, k)) {
+            if (lane == ut9(j, k) || lane + 32 == ut9(j, k)) {
                 U[81L * cam + 9 * j + k] = acc[ut9(j, k)];
                 U[81L * cam + 9 * k + j] = acc[ut9(j, k)];
             }

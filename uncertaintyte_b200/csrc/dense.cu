@@ -70,7 +70,9 @@ __device__ __forceinline__ void load_tiles(double* As, double* Bs, const double*
 __global__ void __launch_bounds__(GEMM_THREADS, 1)
     k_gemm_f64(int M, int N, int K, double alpha, const double* __restrict__ A, long lda,
                const double* __restrict__ B, long ldb, double beta, double* C, long ldc,
-               unsigned long long* amax) {
+               unsigned long long* amax, int lower_only) {
+    // lower_only: tiles strictly above the diagonal of C are skipped (SYRK-style update)
+    if (lower_only && (int)(blockIdx.x * BN) > (int)(blockIdx.y * BM) + BM - 1) return;
     extern __shared__ __align__(16) double smem[];
     double* As = smem;
     double* Bs = smem + STAGES * A_STAGE;
@@ -153,139 +155,212 @@ void gemm_f64(int M, int N, int K, double alpha, const double* A, int lda, const
     }
     if (M <= 0 || N <= 0) return;
     dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-    k_gemm_f64<<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, amax);
+    k_gemm_f64<<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, amax, 0);
+    count_launch();
+}
+
+void gemm_f64_tri(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
+                  double beta, double* C, int ldc, cudaStream_t st) {
+    gemm_f64(0, 0, 0, 0, nullptr, 0, nullptr, 0, 0, nullptr, 0, nullptr, st);  // sets the smem attribute
+    if (M <= 0 || N <= 0) return;
+    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+    k_gemm_f64<<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                      nullptr, 1);
     count_launch();
 }
 
 // ------------------------------------------------------------------------
-// Blocked Gauss-Jordan inverse (SPD, no pivoting)
+// SPD inverse: blocked Cholesky A = L L^T, T = L^{-1}, A^{-1} = T^T T
 // ------------------------------------------------------------------------
-constexpr int GJ_NB = 64;
+constexpr int NB = 64;                       // panel width
+constexpr int SQ_SMEM = (int)(sizeof(double) * 2 * NB * (NB + 1));
 
-size_t gj_workspace_doubles(int n) {
-    // P (nb x nb), Cbuf (ld_of(n) x nb), Rbuf (nb x n, ld = nb)
-    return (size_t)GJ_NB * GJ_NB + (size_t)ld_of(n) * GJ_NB + (size_t)GJ_NB * (n + 8) + 64;
-}
+size_t chol_small_doubles(int n) { return (size_t)NB * NB + (size_t)NB * (n + 8) + 64; }
 
-// In-place Gauss-Jordan inverse of the kb x kb diagonal block (kb <= 64) in
-// shared memory; one CTA. Writes the inverse to P (kb x kb, ld GJ_NB).
-__global__ void __launch_bounds__(256) k_gj_diag(double* A, long lda, int k0, int kb, double* P,
-                                                 int* err) {
-    __shared__ double a[GJ_NB][GJ_NB + 1];  // a[row][col]
-    __shared__ double fcol[GJ_NB];
+// Unblocked Cholesky of the kb x kb diagonal block at (k0, k0) in shared
+// memory (lower triangle read), written back as L_kk; its inverse (lower)
+// goes to Linv (64 x 64, ld 64). One CTA.
+__global__ void __launch_bounds__(256) k_chol_diag(double* A, long lda, int k0, int kb, double* Linv,
+                                                   int* err) {
+    extern __shared__ double sm_[];
+    double(*a)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm_);
+    double(*x)[NB + 1] = a + NB;  // x[i][c]: column c of the inverse
     const int tid = threadIdx.x;
     for (int e = tid; e < kb * kb; e += blockDim.x) {
         int r = e % kb, c = e / kb;
-        a[r][c] = A[(k0 + r) + (long)(k0 + c) * lda];
+        a[r][c] = r >= c ? A[(k0 + r) + (long)(k0 + c) * lda] : 0.0;
     }
     __syncthreads();
     for (int p = 0; p < kb; ++p) {
-        double piv = a[p][p];
-        if (tid == 0 && !(piv > 0.0 && isfinite(piv))) atomicOr(err, ERRBIT_SINGULAR);
+        if (tid == 0) {
+            double d = a[p][p];
+            if (!(d > 0.0 && d <= 1.7976931348623157e308)) atomicOr(err, ERRBIT_SINGULAR);
+            a[p][p] = sqrt(d);
+        }
         __syncthreads();
-        // save column p (rows != p) and scale row p
-        for (int i = tid; i < kb; i += blockDim.x) fcol[i] = a[i][p];
+        double lp = a[p][p];
+        for (int i = p + 1 + tid; i < kb; i += blockDim.x) a[i][p] /= lp;
         __syncthreads();
-        double ip = 1.0 / piv;
-        for (int j = tid; j < kb; j += blockDim.x) a[p][j] = (j == p ? 1.0 : a[p][j]) * ip;
-        __syncthreads();
-        for (int e = tid; e < kb * kb; e += blockDim.x) {
-            int i = e % kb, j = e / kb;
-            if (i == p) continue;
-            double v = (j == p ? 0.0 : a[i][j]);
-            a[i][j] = v - fcol[i] * a[p][j];
+        const int m = kb - p - 1;  // trailing size
+        for (int e = tid; e < m * m; e += blockDim.x) {
+            int i = p + 1 + e % m, j = p + 1 + e / m;
+            if (j <= i) a[i][j] -= a[i][p] * a[j][p];
         }
         __syncthreads();
     }
     for (int e = tid; e < kb * kb; e += blockDim.x) {
         int r = e % kb, c = e / kb;
-        P[r + (long)c * GJ_NB] = a[r][c];
+        if (r >= c) A[(k0 + r) + (long)(k0 + c) * lda] = a[r][c];
+    }
+    // forward substitution, one thread per column of the inverse
+    if (tid < kb) {
+        const int c = tid;
+        for (int i = 0; i < c; ++i) x[i][c] = 0.0;
+        x[c][c] = 1.0 / a[c][c];
+        for (int i = c + 1; i < kb; ++i) {
+            double s = 0.0;
+            for (int j = c; j < i; ++j) s += a[i][j] * x[j][c];
+            x[i][c] = -s / a[i][i];
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < kb * kb; e += blockDim.x) {
+        int r = e % kb, c = e / kb;
+        Linv[r + (long)c * NB] = x[r][c];
     }
 }
 
-// Row panel: R(:, j) = P * A(k rows, j) for j outside the pivot block (0
-// inside), written back into A's pivot rows. Column panel: Cb(i, :) = A(i, k
-// cols) for i outside the pivot block (0 inside), A(i, k cols) = -Cb(i,:) P.
-// Pivot block: A_kk = P. blockIdx.y = 0 -> row panel, 1 -> column panel.
-__global__ void __launch_bounds__(256) k_gj_panels(double* A, long lda, int n, int k0, int kb,
-                                                   const double* __restrict__ P, double* Cb,
-                                                   long ldc, double* R) {
-    extern __shared__ double gj_smem[];
-    double(*sp)[GJ_NB + 1] = reinterpret_cast<double(*)[GJ_NB + 1]>(gj_smem);  // sp[r][c] = P(r, c)
-    double(*sx)[GJ_NB + 1] = sp + GJ_NB;                                        // chunk
+// Panel: L_ik = A_ik * Linv_kk^T for the 64-row chunk starting at i0 (rows
+// below the pivot block); written into A and transposed into R (R[q + i*NB] =
+// L(i, k0+q)) as the B operand of the trailing update.
+__global__ void __launch_bounds__(256) k_chol_panel(double* A, long lda, int n, int k0, int kb, int i0,
+                                                    const double* __restrict__ Linv, double* R) {
+    extern __shared__ double sm_[];
+    double(*sp)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm_);  // sp[q][r] = Linv(q, r)
+    double(*sx)[NB + 1] = sp + NB;                                   // sx[i][r] = A(row, k0 + r)
     const int tid = threadIdx.x;
+    const int r0 = i0 + blockIdx.x * NB;
+    const int rn = min(NB, n - r0);
+    if (rn <= 0) return;
     for (int e = tid; e < kb * kb; e += blockDim.x) {
-        int r = e % kb, c = e / kb;
-        sp[r][c] = P[r + (long)c * GJ_NB];
+        int q = e % kb, r = e / kb;
+        sp[q][r] = Linv[q + (long)r * NB];
     }
-    const int c0 = blockIdx.x * GJ_NB;  // chunk start (columns for the row panel, rows for the column panel)
-    const int cn = min(GJ_NB, n - c0);
-    if (cn <= 0) return;
-    if (blockIdx.y == 0) {
-        // sx[r][j] = A(k0 + r, c0 + j)
-        for (int e = tid; e < kb * cn; e += blockDim.x) {
-            int r = e % kb, j = e / kb;
-            sx[r][j] = A[(k0 + r) + (long)(c0 + j) * lda];
-        }
-        __syncthreads();
-        for (int e = tid; e < kb * cn; e += blockDim.x) {
-            int r = e % kb, j = e / kb;
-            int col = c0 + j;
-            double v;
-            if (col >= k0 && col < k0 + kb) {
-                v = 0.0;
-                A[(k0 + r) + (long)col * lda] = sp[r][col - k0];  // A_kk = P
-            } else {
-                double s = 0.0;
-                for (int q = 0; q < kb; ++q) s += sp[r][q] * sx[q][j];
-                v = s;
-                A[(k0 + r) + (long)col * lda] = s;
-            }
-            R[r + (long)col * GJ_NB] = v;
-        }
-    } else {
-        // sx[i][q] = A(c0 + i, k0 + q)
-        for (int e = tid; e < cn * kb; e += blockDim.x) {
-            int i = e % cn, q = e / cn;
-            sx[i][q] = A[(c0 + i) + (long)(k0 + q) * lda];
-        }
-        __syncthreads();
-        for (int e = tid; e < cn * kb; e += blockDim.x) {
-            int i = e % cn, q = e / cn;
-            int row = c0 + i;
-            if (row >= k0 && row < k0 + kb) {
-                Cb[row + (long)q * ldc] = 0.0;
-            } else {
-                double s = 0.0;
-                for (int r = 0; r < kb; ++r) s += sx[i][r] * sp[r][q];
-                Cb[row + (long)q * ldc] = sx[i][q];
-                A[row + (long)(k0 + q) * lda] = -s;
-            }
-        }
+    for (int e = tid; e < rn * kb; e += blockDim.x) {
+        int i = e % rn, r = e / rn;
+        sx[i][r] = A[(r0 + i) + (long)(k0 + r) * lda];
+    }
+    __syncthreads();
+    for (int e = tid; e < rn * kb; e += blockDim.x) {
+        int i = e % rn, q = e / rn;
+        double s = 0.0;
+        for (int r = 0; r <= q; ++r) s += sx[i][r] * sp[q][r];
+        A[(r0 + i) + (long)(k0 + q) * lda] = s;
+        R[q + (long)(r0 + i) * NB] = s;
     }
 }
 
-void gj_inverse(double* A, int n, int lda, double* ws, int* err, cudaStream_t st) {
-    double* P = ws;
-    double* Cb = P + GJ_NB * GJ_NB;
-    const int ldc = ld_of(n);
-    double* R = Cb + (size_t)ldc * GJ_NB;
-    cudaMemsetAsync(Cb, 0, sizeof(double) * ((size_t)ldc * GJ_NB + (size_t)GJ_NB * (n + 8)), st);
-    const int nchunks = (n + GJ_NB - 1) / GJ_NB;
-    const int panel_smem = (int)(sizeof(double) * 2 * GJ_NB * (GJ_NB + 1));
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_gj_panels, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_smem);
-        attr = true;
+// Inverse of every 64 x 64 diagonal block of the lower-triangular L (the
+// leaves of the recursive triangular inverse). One CTA per block.
+__global__ void __launch_bounds__(256) k_trtri_leaves(const double* __restrict__ L, long lda, int n,
+                                                      double* T, long ldt) {
+    extern __shared__ double sm_[];
+    double(*a)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm_);
+    double(*x)[NB + 1] = a + NB;
+    const int b0 = blockIdx.x * NB, bs = min(NB, n - b0);
+    const int tid = threadIdx.x;
+    for (int e = tid; e < bs * bs; e += blockDim.x) {
+        int r = e % bs, c = e / bs;
+        a[r][c] = r >= c ? L[(b0 + r) + (long)(b0 + c) * lda] : 0.0;
     }
-    for (int k0 = 0; k0 < n; k0 += GJ_NB) {
-        int kb = n - k0 < GJ_NB ? n - k0 : GJ_NB;
-        k_gj_diag<<<1, 256, 0, st>>>(A, lda, k0, kb, P, err);
-        k_gj_panels<<<dim3(nchunks, 2), 256, panel_smem, st>>>(A, lda, n, k0, kb, P, Cb, ldc, R);
-        count_launch(2);
-        // A -= Cb * R  (rank-kb update; pivot rows/cols receive zero updates)
-        gemm_f64(n, n, kb, -1.0, Cb, ldc, R, GJ_NB, 1.0, A, lda, nullptr, st);
+    __syncthreads();
+    if (tid < bs) {
+        const int c = tid;
+        for (int i = 0; i < c; ++i) x[i][c] = 0.0;
+        x[c][c] = 1.0 / a[c][c];
+        for (int i = c + 1; i < bs; ++i) {
+            double s = 0.0;
+            for (int j = c; j < i; ++j) s += a[i][j] * x[j][c];
+            x[i][c] = -s / a[i][i];
+        }
     }
+    __syncthreads();
+    for (int e = tid; e < bs * bs; e += blockDim.x) {
+        int r = e % bs, c = e / bs;
+        T[(b0 + r) + (long)(b0 + c) * ldt] = x[r][c];
+    }
+}
+
+// Tt = T^T (n x n), 32 x 32 tiles through shared memory.
+__global__ void k_transpose(const double* __restrict__ T, long ldt, int n, double* Tt, long ldo) {
+    __shared__ double t[32][33];
+    int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        int i = by + r, j = bx + threadIdx.x;
+        if (i < n && j < n) t[r][threadIdx.x] = T[i + (long)j * ldt];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        int j = bx + r, i = by + threadIdx.x;  // out(j, i) = T(i, j)
+        if (i < n && j < n) Tt[j + (long)i * ldo] = t[threadIdx.x][r];
+    }
+}
+
+namespace {
+void set_smem_attr() {
+    static bool done = false;
+    if (done) return;
+    cudaFuncSetAttribute(k_chol_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, SQ_SMEM);
+    cudaFuncSetAttribute(k_chol_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, SQ_SMEM);
+    cudaFuncSetAttribute(k_trtri_leaves, cudaFuncAttributeMaxDynamicSharedMemorySize, SQ_SMEM);
+    done = true;
+}
+
+// T[r0:r1, r0:r1] = inverse of L[r0:r1, r0:r1] given the inverted leaves:
+// T21 = -T22 * (L21 * T11), split at a multiple of 64.
+void trtri_merge(const double* L, int lda, double* T, int ldt, double* W, int ldw, int r0, int r1,
+                 cudaStream_t st) {
+    if (r1 - r0 <= NB) return;
+    int half = (r1 - r0) / 2;
+    int m = r0 + ((half + NB - 1) / NB) * NB;
+    if (m >= r1) m = r1 - NB;
+    trtri_merge(L, lda, T, ldt, W, ldw, r0, m, st);
+    trtri_merge(L, lda, T, ldt, W, ldw, m, r1, st);
+    const int m2 = r1 - m, m1 = m - r0;
+    gemm_f64(m2, m1, m1, 1.0, L + m + (long)r0 * lda, lda, T + r0 + (long)r0 * ldt, ldt, 0.0, W, ldw,
+             nullptr, st);
+    gemm_f64(m2, m1, m2, -1.0, T + m + (long)m * ldt, ldt, W, ldw, 0.0, T + m + (long)r0 * ldt, ldt,
+             nullptr, st);
+}
+}  // namespace
+
+void chol_inverse(double* A, int n, int lda, double* T, double* W, double* Tt, double* small, int* err,
+                  cudaStream_t st) {
+    set_smem_attr();
+    double* Linv = small;
+    double* R = small + NB * NB;
+    // 1. blocked right-looking Cholesky (lower triangle of A becomes L)
+    for (int k0 = 0; k0 < n; k0 += NB) {
+        const int kb = min(NB, n - k0), k1 = k0 + kb;
+        k_chol_diag<<<1, 256, SQ_SMEM, st>>>(A, lda, k0, kb, Linv, err);
+        count_launch();
+        if (k1 < n) {
+            const int rows = n - k1;
+            k_chol_panel<<<(rows + NB - 1) / NB, 256, SQ_SMEM, st>>>(A, lda, n, k0, kb, k1, Linv, R);
+            count_launch();
+            gemm_f64_tri(rows, rows, kb, -1.0, A + k1 + (long)k0 * lda, lda, R + (long)k1 * NB, NB, 1.0,
+                         A + k1 + (long)k1 * lda, lda, st);
+        }
+    }
+    // 2. T = L^{-1}: leaves, then recursive merges
+    k_trtri_leaves<<<(n + NB - 1) / NB, 256, SQ_SMEM, st>>>(A, lda, n, T, lda);
+    count_launch();
+    trtri_merge(A, lda, T, lda, W, lda, 0, n, st);
+    // 3. A^{-1} = T^T T
+    dim3 g((n + 31) / 32, (n + 31) / 32);
+    k_transpose<<<g, dim3(32, 8), 0, st>>>(T, lda, n, Tt, lda);
+    count_launch();
+    gemm_f64(n, n, n, 1.0, Tt, lda, T, lda, 0.0, A, lda, nullptr, st);
 }
 
 // ------------------------------------------------------------------------

@@ -48,6 +48,9 @@ struct SceneDev {
     double* iVs;          // 6*num_points upper triangle of the inverse of the scaled point block
     double* Ws;           // 27*num_obs scaled W_o = (J_c^T J_p)/(s s), 9x3 row-major
     double* Ys;           // 27*num_obs Y_o = W_o * iV_p, 9x3 row-major
+    int* deg;             // num_obs: point degree of each camera-grouped observation
+    int* tup_off;         // num_obs + 1: offsets of the Schur pair tuples
+    int4* tup;            // Schur pair tuples (o, o2, camera(o2), 0), grouped by camera
     int* err;             // device error bits
 };
 
@@ -57,7 +60,10 @@ void launch_build_index(SceneDev& s, cudaStream_t st);
 void launch_camera_blocks(const SceneDev& s, double* Z, int ldz, cudaStream_t st);
 void launch_point_blocks(const SceneDev& s, cudaStream_t st);
 void launch_obs_blocks(const SceneDev& s, cudaStream_t st);
-// Z(c,c') -= sum_p Y_o W_o'^T (upper camera-block triangle), then mirror.
+// Schur scatter: offsets (total = tup_off[num_obs]), tuples, then
+// Z(c,c') -= sum_p Y_o W_o'^T (upper camera-block triangle); mirror after.
+void launch_schur_offsets(const SceneDev& s, cudaStream_t st);
+void launch_schur_tuples(const SceneDev& s, cudaStream_t st);
 void launch_schur(const SceneDev& s, double* Z, int ldz, cudaStream_t st);
 void launch_mirror_upper(double* Z, int n, int ldz, cudaStream_t st);
 // Generic 9/12-entry-row repack for the J^T J export (camera-only rows allowed).
@@ -73,10 +79,16 @@ size_t scan_tmp_ints(int n);
 // epilogue folds max|C| into *amax (bit pattern of a non-negative double).
 void gemm_f64(int M, int N, int K, double alpha, const double* A, int lda, const double* B,
               int ldb, double beta, double* C, int ldc, unsigned long long* amax, cudaStream_t st);
-// In-place inverse of an SPD matrix by blocked Gauss-Jordan (no pivoting).
-// ws: workspace of gj_workspace_doubles(n) doubles. Sets ERRBIT_SINGULAR in err.
-size_t gj_workspace_doubles(int n);
-void gj_inverse(double* A, int n, int lda, double* ws, int* err, cudaStream_t st);
+// Same, skipping output tiles strictly above the diagonal (symmetric updates).
+void gemm_f64_tri(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
+                  double beta, double* C, int ldc, cudaStream_t st);
+// In-place inverse of an SPD matrix (n x n, lda): blocked Cholesky A = L L^T,
+// T = L^{-1} (recursive, GEMM-based), A^{-1} = T^T T. T, W, Tt: n x lda
+// scratch matrices whose padding rows are zero and whose T is zero on entry;
+// small: chol_small_doubles(n) doubles. Sets ERRBIT_SINGULAR in err.
+size_t chol_small_doubles(int n);
+void chol_inverse(double* A, int n, int lda, double* T, double* W, double* Tt, double* small, int* err,
+                  cudaStream_t st);
 // A <- A + lambda*I and symmetric Jacobi equilibration: A_s = E A E, E = diag(A_ii)^-1/2.
 void launch_shift_equilibrate(double* A, int n, int lda, double lambda, double* e, int* err,
                               cudaStream_t st);
