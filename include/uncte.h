@@ -103,8 +103,9 @@ int unc_compute_device(unc_context* ctx, const unc_options* opt, int num_rows, i
 /* Profiling of the dense Taylor-series products: when enabled, every
  * N x N x N product of the Taylor loop is bracketed by CUDA events on the
  * stream it runs on. unc_context_profile returns the number of products, their
- * summed device time (s) and their algorithmic flops (2 N^3 each) since the
- * last reset. */
+ * summed device time (s) and their algorithmic flops since the last reset.
+ * The powers of the symmetric inverse are symmetric, so a product computes
+ * its lower triangle only: N^2 (N + 1) flops (the reference spends 2 N^3). */
 int unc_context_set_profiling(unc_context* ctx, int enable);
 int unc_context_profile(unc_context* ctx, long long* launches, double* seconds, double* flops,
                         int reset);
@@ -127,6 +128,13 @@ int unc_dense_inverse_device(double* d_A, int n, int lda, void* stream);
 int unc_jtj_crs(int num_rows, int num_cols, const int* rows, const int* cols, const double* values,
                 int num_cams, int cam_params, long long* nnz, int* out_rows, int* out_cols,
                 double* out_vals);
+
+/* C = alpha * A * B + beta * C on the library's FP64 tensor-core GEMM (the
+ * dense products of the Taylor series, ScaledDenseMatrix.cpp:314-353). All
+ * matrices column-major in device memory; lda/ldb/ldc even; rows past M (A)
+ * and K (B) up to the next even row must be readable and finite. */
+int unc_gemm_f64_device(int M, int N, int K, double alpha, const double* d_A, int lda,
+                        const double* d_B, int ldb, double beta, double* d_C, int ldc, void* stream);
 
 /* Human-readable name of a status code, and the last error message of the
  * calling thread (empty when none). */

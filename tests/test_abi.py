@@ -14,7 +14,7 @@ from uncertaintyte_b200 import native
 def _declared(header):
     txt = open(os.path.join(ROOT, "include", header)).read()
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-    return sorted(set(re.findall(r"\b(unc_[a-z_]+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(unc_[a-z_0-9]+)\s*\(", txt)))
 
 
 def test_header_functions_are_exported():

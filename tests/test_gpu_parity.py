@@ -169,3 +169,22 @@ def test_dense_inverse_rejects_indefinite():
     with pytest.raises(native.UncError) as e:
         _dense_inverse_gpu(A)
     assert e.value.status == -6
+
+
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (7, 5, 3), (128, 128, 16), (130, 67, 33), (1800, 1800, 1800),
+                                   (257, 129, 64)])
+def test_gemm_f64_vs_torch(m, n, k):
+    """The FP64 product kernel against a plain torch FP64 matmul."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(m * 7 + n * 3 + k)
+    lda, ldb, ldc = (m + 7) & ~7, (k + 7) & ~7, (m + 7) & ~7
+    A = torch.zeros((k, lda), dtype=torch.float64, device="cuda")  # column-major storage
+    B = torch.zeros((n, ldb), dtype=torch.float64, device="cuda")
+    C = torch.randn((n, ldc), dtype=torch.float64, device="cuda", generator=g)
+    A[:, :m] = torch.randn((k, m), dtype=torch.float64, device="cuda", generator=g)
+    B[:, :k] = torch.randn((n, k), dtype=torch.float64, device="cuda", generator=g)
+    ref = 0.5 * (A[:, :m].T @ B[:, :k].T) - 2.0 * C[:, :m].T
+    native.gemm_f64_device(m, n, k, 0.5, A.data_ptr(), lda, B.data_ptr(), ldb, -2.0, C.data_ptr(), ldc)
+    torch.cuda.synchronize()
+    got = C[:, :m].T
+    assert torch.max(torch.abs(got - ref)).item() <= 1e-12 * max(1.0, k ** 0.5) * torch.max(torch.abs(ref)).item()

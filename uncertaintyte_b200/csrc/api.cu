@@ -25,7 +25,7 @@ struct unc_context {
     cudaStream_t stream = nullptr;
     void* ws = nullptr;
     size_t ws_bytes = 0;
-    void* tup = nullptr;  // Schur pair tuples (sized at run time)
+    void* tup = nullptr;  // Schur observation pairs (sized at run time)
     size_t tup_bytes = 0;
     cudaEvent_t ev[12] = {};
     // profiling of the Taylor-series products
@@ -96,15 +96,15 @@ size_t carve(char* base, const Plan& pl, bool host_io, long long nnz, int nrows,
     s.pt_ptr = c.take<int>((size_t)pl.P + 1);
     s.pt_obs = c.take<int>(pl.nobs);
     s.cursor = c.take<int>((size_t)pl.C + pl.P + 1);
-    s.scan_tmp = c.take<int>(scan_tmp_ints(std::max(pl.C, pl.P)));
+    s.scan_tmp = c.take<int>(scan_tmp_ints(std::max(std::max(pl.C, pl.P), pl.C * pl.C)));
     s.s_cam = c.take<double>((size_t)pl.C * 9);
     s.s_pt = c.take<double>((size_t)pl.P * 3);
     s.Vraw = c.take<double>((size_t)pl.P * 6);
     s.iVs = c.take<double>((size_t)pl.P * 6);
     s.Ws = c.take<double>((size_t)pl.nobs * 27);
     s.Ys = c.take<double>((size_t)pl.nobs * 27);
-    s.deg = c.take<int>(pl.nobs);
-    s.tup_off = c.take<int>((size_t)pl.nobs + 1);
+    s.blk_cnt = c.take<int>((size_t)pl.C * pl.C);
+    s.blk_ptr = c.take<int>((size_t)pl.C * pl.C + 1);
     s.err = c.take<int>(4);
     b.amax = c.take<unsigned long long>(4);
     const size_t nn = (size_t)pl.ld * pl.N;
@@ -192,23 +192,26 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     launch_point_blocks(s, sm);
     CK(cudaEventRecord(ev[3], sm));
     launch_obs_blocks(s, sm);
-    launch_schur_offsets(s, sm);
-    int ntup = 0;
-    CK(cudaMemcpyAsync(&ntup, s.tup_off + pl.nobs, sizeof(int), cudaMemcpyDeviceToHost, sm));
+    launch_schur_count(s, sm);
+    int npairs = 0;
+    CK(cudaMemcpyAsync(&npairs, s.blk_ptr + (size_t)pl.C * pl.C, sizeof(int), cudaMemcpyDeviceToHost, sm));
     CK(cudaEventRecord(ev[4], sm));
     CK(cudaStreamSynchronize(sm));
-    if (ntup < 0) return fail(UNC_ERR_TOO_LARGE, "more than 2^31 Schur pair terms");
-    if (ctx->tup_bytes < (size_t)ntup * sizeof(int4) + 16) {
+    if (npairs < 0) return fail(UNC_ERR_TOO_LARGE, "more than 2^31 co-visible observation pairs");
+    const size_t long_cap = (size_t)npairs / 1025 + 1;
+    const size_t need = (size_t)npairs * 8 + (long_cap + 1) * sizeof(int) + 64;
+    if (ctx->tup_bytes < need) {
         if (ctx->tup) cudaFree(ctx->tup);
         ctx->tup = nullptr;
         ctx->tup_bytes = 0;
-        size_t want = (size_t)ntup * sizeof(int4) + 16;
-        want += want / 4;  // headroom for the next scene
+        size_t want = need + need / 4;  // headroom for the next scene
         CK(cudaMalloc(&ctx->tup, want));
         ctx->tup_bytes = want;
     }
-    s.tup = reinterpret_cast<int4*>(ctx->tup);
-    launch_schur_tuples(s, sm);
+    s.pairs = reinterpret_cast<unsigned long long*>(ctx->tup);
+    s.long_list = reinterpret_cast<int*>(s.pairs + npairs + 1);
+    s.long_cap = (int)long_cap;
+    launch_camera_self(s, b.Z, ld, sm);
     launch_schur(s, b.Z, ld, sm);
     launch_mirror_upper(b.Z, N, ld, sm);
     CK(cudaEventRecord(ev[5], sm));
@@ -235,10 +238,13 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         CK(cudaEventRecord(ctx->pev[npev++], sm));
         return UNC_OK;
     };
+    // Every power X^(i+1) is symmetric: only the lower-triangle tiles of each
+    // product are computed (half the flops), then mirrored for the next product.
     CK(cudaMemsetAsync(b.amax, 0, 8, sm));
     if (int r = prof_mark()) return r;
-    gemm_f64(N, N, N, 1.0, X, ld, X, ld, 0.0, add, ld, b.amax, sm);
+    gemm_f64_ex(N, N, N, 1.0, X, ld, X, ld, 0.0, add, ld, b.amax, true, sm, false);
     if (int r = prof_mark()) return r;
+    launch_mirror_lower(add, N, ld, sm);
     double old_change = DBL_MAX;
     int iters = 0;
     unsigned long long amax_bits = 0;
@@ -257,8 +263,9 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         launch_axpy(b.iZ, add, k, N, ld, sm);
         CK(cudaMemsetAsync(b.amax, 0, 8, sm));
         if (int r = prof_mark()) return r;
-        gemm_f64(N, N, N, 1.0, add, ld, X, ld, 0.0, tmp, ld, b.amax, sm);
+        gemm_f64_ex(N, N, N, 1.0, add, ld, X, ld, 0.0, tmp, ld, b.amax, true, sm, false);
         if (int r = prof_mark()) return r;
+        launch_mirror_lower(tmp, N, ld, sm);
         std::swap(add, tmp);
     }
     CK(cudaEventRecord(ev[7], sm));
@@ -275,7 +282,7 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     for (size_t i = 0; i + 1 < npev; i += 2) {
         ctx->prof_seconds += ev_s(ctx->pev[i], ctx->pev[i + 1]);
         ctx->prof_launches += 1;
-        ctx->prof_flops += 2.0 * (double)N * N * N;
+        ctx->prof_flops += (double)N * N * (N + 1);  // symmetric product: lower half of 2 N^3
     }
     if (st) {
         st->lambda = lambda;
@@ -641,6 +648,17 @@ int unc_jtj_crs(int num_rows, int num_cols, const int* rows, const int* cols, co
         std::copy(ocol.begin(), ocol.end(), out_cols);
         std::copy(oval.begin(), oval.end(), out_vals);
     }
+    return UNC_OK;
+}
+
+int unc_gemm_f64_device(int M, int N, int K, double alpha, const double* d_A, int lda, const double* d_B,
+                        int ldb, double beta, double* d_C, int ldc, void* stream) {
+    g_last_error.clear();
+    if (M < 0 || N < 0 || K < 0 || !d_A || !d_B || !d_C || (lda & 1) || (ldb & 1) || lda < M || ldb < K ||
+        ldc < M || ((uintptr_t)d_A & 15) || ((uintptr_t)d_B & 15))
+        return fail(UNC_ERR_INVALID_ARG, "bad GEMM arguments");
+    gemm_f64(M, N, K, alpha, d_A, lda, d_B, ldb, beta, d_C, ldc, nullptr, (cudaStream_t)stream);
+    CK(cudaGetLastError());
     return UNC_OK;
 }
 

@@ -488,153 +488,236 @@ void launch_obs_blocks(const SceneDev& s, cudaStream_t st) {
     count_launch();
 }
 
-// Deterministic Schur scatter, in two kernels.
-//
-// k_pair_tuples: for every entry i of the camera-grouped observation list
-// (observation o of camera c, point p) write the tuples (o, o2, camera(o2))
-// for all observations o2 of p, at offsets from one exclusive scan of the
-// point degrees. The result lists, camera by camera, every (o, o2) pair that
-// contributes Y_o W_o2^T to the block row of c, in a fixed order.
-//
-// k_schur_rows: one CTA owns the block row of camera c (columns of cameras
-// [c0, c0 + kSchurChunk)) and accumulates it in shared memory:
-//   Z(c, c') -= sum over points p seen by c and c' of Y_o W_o'^T,  c' >= c.
-// Four thread groups split the target cameras (c' mod 4); inside a group
-// thread e < 81 owns element (row, col) = (e % 9, e / 9) of every 9x9 block,
-// so each output element receives its terms in one fixed order: bitwise
-// repeatable results. Z is written once (upper block triangle; inside the
-// diagonal block only row <= col) and mirrored afterwards.
-constexpr int kSchurChunk = 200;  // cameras per column chunk: 9 x 1800 doubles = 129.6 KB smem
-constexpr int kSchurSmem = 9 * 9 * kSchurChunk * (int)sizeof(double);
-constexpr int kSchurGroups = 4;
+// Self terms of the Schur complement: Z(c, c) -= sum over observations o of
+// camera c of Y_o W_o^T (= W_o iV_p W_o^T, symmetric). One warp per camera,
+// lanes stride over the camera's observations (ascending) and the 45 upper-
+// triangle sums are reduced across the warp in a fixed order. Only the upper
+// triangle of the diagonal block is updated (it is mirrored later).
+__global__ void __launch_bounds__(128) k_camera_self(int num_cams, const int* __restrict__ cam_ptr,
+                                                     const int* __restrict__ cam_obs,
+                                                     const double* __restrict__ Ws,
+                                                     const double* __restrict__ Ys, double* Z, long ldz) {
+    const int cam = blockIdx.x * 4 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (cam >= num_cams) return;
+    double acc[45];
+#pragma unroll
+    for (int t = 0; t < 45; ++t) acc[t] = 0.0;
+    for (int i = cam_ptr[cam] + lane; i < cam_ptr[cam + 1]; i += 32) {
+        const int o = cam_obs[i];
+        const double* y = Ys + 27L * o;
+        const double* w = Ws + 27L * o;
+        double yy[27], ww[27];
+#pragma unroll
+        for (int k = 0; k < 27; ++k) {
+            yy[k] = __ldg(y + k);
+            ww[k] = __ldg(w + k);
+        }
+#pragma unroll
+        for (int j = 0; j < 9; ++j)
+#pragma unroll
+            for (int k = j; k < 9; ++k)
+                acc[ut9(j, k)] += yy[3 * j] * ww[3 * k] + yy[3 * j + 1] * ww[3 * k + 1] + yy[3 * j + 2] * ww[3 * k + 2];
+    }
+#pragma unroll
+    for (int t = 0; t < 45; ++t) acc[t] = warp_sum(acc[t]);
+#pragma unroll
+    for (int j = 0; j < 9; ++j)
+#pragma unroll
+        for (int k = j; k < 9; ++k)
+            if (lane == ut9(j, k) || lane + 32 == ut9(j, k)) Z[(9L * cam + j) + (9L * cam + k) * ldz] -= acc[ut9(j, k)];
+}
 
-__global__ void k_point_degree(int n, const int* __restrict__ cam_obs, const int* __restrict__ obs_pt,
-                               const int* __restrict__ pt_ptr, const int* __restrict__ n_valid,
-                               int* __restrict__ deg) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    if (i >= *n_valid) {  // entries past the kept observations
-        deg[i] = 0;
+void launch_camera_self(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
+    if (s.num_cams == 0) return;
+    k_camera_self<<<(s.num_cams + 3) / 4, 128, 0, st>>>(s.num_cams, s.cam_ptr, s.cam_obs, s.Ws, s.Ys, Z, ldz);
+    count_launch();
+}
+
+// Deterministic Schur scatter: Z(c, c') -= sum over points p seen by both
+// cameras of Y_o W_o'^T, for c <= c' (upper block triangle).
+//
+//  1. k_pair_enum (count / scatter): every point lists its ordered
+//     observation pairs (o, o') with camera(o) <= camera(o'); pairs are
+//     counted per camera-pair block and scattered into a block-grouped list.
+//  2. the pairs of each block are sorted by (o, o') (warp rank sort, or a
+//     block bitonic sort for long lists), which fixes the summation order.
+//  3. k_schur_blocks: one warp per block reduces its pairs in registers (lane
+//     l owns elements l, l+32, l+64 of the 9x9 block) and writes the block of
+//     Z once. No floating-point atomics: results are bitwise repeatable.
+template <bool kScatter>
+__global__ void k_pair_enum(int num_points, int num_cams, const int* __restrict__ pt_ptr,
+                            const int* __restrict__ pt_obs, const int* __restrict__ obs_cam,
+                            int* cnt_or_cursor, unsigned long long* __restrict__ pairs) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= num_points) return;
+    const int b = pt_ptr[p], e = pt_ptr[p + 1];
+    for (int i = b; i < e; ++i) {
+        const int oa = pt_obs[i], ca = obs_cam[oa];
+        for (int k = b; k < e; ++k) {
+            const int ob = pt_obs[k], cb = obs_cam[ob];
+            if (ca > cb || k == i) continue;  // self pairs are reduced per camera (k_camera_self)
+            const long key = (long)ca * num_cams + cb;
+            if (kScatter) {
+                int pos = atomicAdd(cnt_or_cursor + key, 1);
+                pairs[pos] = ((unsigned long long)(unsigned)oa << 32) | (unsigned)ob;
+            } else {
+                atomicAdd(cnt_or_cursor + key, 1);
+            }
+        }
+    }
+}
+
+constexpr int kPairWarpCap = 1024;
+// long_list[0] counts the blocks with more than kPairWarpCap pairs; their ids
+// follow (capacity long_cap) and are sorted by k_sort_pairs_block.
+__global__ void k_sort_pairs_warp(long nseg, const int* __restrict__ ptr, unsigned long long* data,
+                                  int* long_list, int long_cap) {
+    __shared__ unsigned long long sh[4][kPairWarpCap];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long seg = (long)blockIdx.x * 4 + w;
+    if (seg >= nseg) return;
+    const int b = ptr[seg], n = ptr[seg + 1] - b;
+    if (n <= 1) return;
+    if (n > kPairWarpCap) {
+        if (lane == 0) {
+            int i = atomicAdd(long_list, 1);
+            if (i < long_cap) long_list[1 + i] = (int)seg;
+        }
         return;
     }
-    int p = obs_pt[cam_obs[i]];
-    deg[i] = pt_ptr[p + 1] - pt_ptr[p];
-}
-
-__global__ void k_pair_tuples(int n, const int* __restrict__ cam_obs, const int* __restrict__ obs_pt,
-                              const int* __restrict__ pt_ptr, const int* __restrict__ pt_obs,
-                              const int* __restrict__ obs_cam, const int* __restrict__ off,
-                              const int* __restrict__ n_valid, int4* __restrict__ tup) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || i >= *n_valid) return;
-    int o = cam_obs[i], p = obs_pt[o];
-    long long t = off[i];
-    for (int k = pt_ptr[p]; k < pt_ptr[p + 1]; ++k, ++t) {
-        int o2 = pt_obs[k];
-        tup[t] = make_int4(o, o2, obs_cam[o2], 0);
+    unsigned long long* s = sh[w];
+    for (int i = lane; i < n; i += 32) s[i] = data[b + i];
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) {
+        unsigned long long v = s[i];
+        int r = 0;
+        for (int j = 0; j < n; ++j) r += s[j] < v;
+        data[b + r] = v;
     }
 }
 
-__global__ void __launch_bounds__(96 * kSchurGroups) k_schur_rows(int num_cams,
-                                                                  const int* __restrict__ cam_ptr,
-                                                                  const int* __restrict__ off,
-                                                                  const int4* __restrict__ tup,
-                                                                  const double* __restrict__ Ws,
-                                                                  const double* __restrict__ Ys,
-                                                                  double* Z, long ldz) {
-    extern __shared__ double acc[];  // acc[row * (9 * kSchurChunk) + (c' - c0) * 9 + col]
-    const int c = blockIdx.x;
-    const int c0 = blockIdx.y * kSchurChunk;
-    const int cn = min(kSchurChunk, num_cams - c0);
-    if (c0 + cn <= c) return;  // chunk entirely left of the diagonal
-    const int W9 = 9 * kSchurChunk;
-    for (int i = threadIdx.x; i < 9 * W9; i += blockDim.x) acc[i] = 0.0;
-    __syncthreads();
-    const int g = threadIdx.x / 96, e = threadIdx.x % 96;
-    const int row = e % 9, col = e / 9;
-    const int lo = max(c, c0), hi = c0 + cn;
-    if (e < 81) {
-        const long long t0 = off[cam_ptr[c]], t1 = off[cam_ptr[c + 1]];  // tuples of camera c
-        long long t = t0;
-        for (; t + 4 <= t1; t += 4) {
-            int4 q[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) q[u] = __ldg(tup + t + u);
-            double v[4];
-            bool take[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                take[u] = q[u].z >= lo && q[u].z < hi && (q[u].z & (kSchurGroups - 1)) == g;
-                v[u] = 0.0;
-                if (take[u]) {
-                    const double* y = Ys + 27L * q[u].x + 3 * row;
-                    const double* w = Ws + 27L * q[u].y + 3 * col;
-                    v[u] = __ldg(y) * __ldg(w) + __ldg(y + 1) * __ldg(w + 1) + __ldg(y + 2) * __ldg(w + 2);
+constexpr int kPairBlockCap = 8192;
+__global__ void k_sort_pairs_block(const int* __restrict__ ptr, unsigned long long* data,
+                                   const int* __restrict__ long_list, int long_cap, int* err) {
+    extern __shared__ unsigned long long sb[];
+    const int nlong = min(long_list[0], long_cap);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && long_list[0] > long_cap) atomicOr(err, ERRBIT_SORT_CAP);
+    for (int t = blockIdx.x; t < nlong; t += gridDim.x) {
+        const int seg = long_list[1 + t];
+        const int b = ptr[seg], n = ptr[seg + 1] - b;
+        if (n > kPairBlockCap) {
+            if (threadIdx.x == 0) atomicOr(err, ERRBIT_SORT_CAP);
+            continue;
+        }
+        int m = 1;
+        while (m < n) m <<= 1;
+        for (int i = threadIdx.x; i < m; i += blockDim.x) sb[i] = i < n ? data[b + i] : ~0ull;
+        __syncthreads();
+        for (int k = 2; k <= m; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                    int l = i ^ j;
+                    if (l > i) {
+                        bool up = (i & k) == 0;
+                        unsigned long long x = sb[i], y = sb[l];
+                        if ((x > y) == up) {
+                            sb[i] = y;
+                            sb[l] = x;
+                        }
+                    }
                 }
+                __syncthreads();
             }
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (take[u]) acc[row * W9 + (q[u].z - c0) * 9 + col] += v[u];
-        }
-        for (; t < t1; ++t) {
-            int4 q = __ldg(tup + t);
-            if (q.z >= lo && q.z < hi && (q.z & (kSchurGroups - 1)) == g) {
-                const double* y = Ys + 27L * q.x + 3 * row;
-                const double* w = Ws + 27L * q.y + 3 * col;
-                acc[row * W9 + (q.z - c0) * 9 + col] +=
-                    __ldg(y) * __ldg(w) + __ldg(y + 1) * __ldg(w + 1) + __ldg(y + 2) * __ldg(w + 2);
-            }
-        }
+        for (int i = threadIdx.x; i < n; i += blockDim.x) data[b + i] = sb[i];
+        __syncthreads();
     }
+}
+
+// One CTA (8 warps) per camera-pair block. Warp w reduces pairs b+w, b+w+8,
+// ... (lane l owns elements l, l+32, l+64 of the 9x9 block); the 8 partial
+// blocks are then summed in warp order: a fixed summation order for every
+// element, so the result is bitwise repeatable.
+__global__ void __launch_bounds__(256) k_schur_blocks(int num_cams, const int* __restrict__ blk_ptr,
+                                                      const unsigned long long* __restrict__ pairs,
+                                                      const double* __restrict__ Ws,
+                                                      const double* __restrict__ Ys, double* Z, long ldz) {
+    __shared__ double part[8][81];
+    const long blk = blockIdx.x;
+    const int b = blk_ptr[blk], e = blk_ptr[blk + 1];
+    if (b == e) return;
+    const int ca = (int)(blk / num_cams), cb = (int)(blk - (long)ca * num_cams);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r0 = lane % 9, q0 = lane / 9;
+    const int r1 = (lane + 32) % 9, q1 = (lane + 32) / 9;
+    const int r2 = (lane + 64) % 9, q2 = (lane + 64) / 9;
+    const bool has2 = lane + 64 < 81;
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+    for (int i = b + w; i < e; i += 8) {
+        const unsigned long long pr = __ldg(pairs + i);
+        const double* y = Ys + 27L * (int)(pr >> 32);
+        const double* x = Ws + 27L * (int)(pr & 0xffffffffu);
+        acc0 += __ldg(y + 3 * r0) * __ldg(x + 3 * q0) + __ldg(y + 3 * r0 + 1) * __ldg(x + 3 * q0 + 1) +
+                __ldg(y + 3 * r0 + 2) * __ldg(x + 3 * q0 + 2);
+        acc1 += __ldg(y + 3 * r1) * __ldg(x + 3 * q1) + __ldg(y + 3 * r1 + 1) * __ldg(x + 3 * q1 + 1) +
+                __ldg(y + 3 * r1 + 2) * __ldg(x + 3 * q1 + 2);
+        if (has2)
+            acc2 += __ldg(y + 3 * r2) * __ldg(x + 3 * q2) + __ldg(y + 3 * r2 + 1) * __ldg(x + 3 * q2 + 1) +
+                    __ldg(y + 3 * r2 + 2) * __ldg(x + 3 * q2 + 2);
+    }
+    part[w][lane] = acc0;
+    part[w][lane + 32] = acc1;
+    if (has2) part[w][lane + 64] = acc2;
     __syncthreads();
-    // write: column-major Z, 9 consecutive rows per column
-    const int ncols = 9 * (hi - lo);
-    for (int idx = threadIdx.x; idx < 9 * ncols; idx += blockDim.x) {
-        const int r = idx % 9, q = idx / 9;
-        const int cc = lo + q / 9, cl = q % 9;
-        const double v = acc[r * W9 + (cc - c0) * 9 + cl];
-        double* z = Z + (9L * c + r) + (9L * cc + cl) * ldz;
-        if (cc == c) {
-            if (r <= cl) *z -= v;  // diagonal block holds U (scaled) already
+    if (threadIdx.x < 81) {
+        const int el = threadIdx.x, r = el % 9, q = el / 9;
+        double v = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v += part[k][el];
+        double* z = Z + (9L * ca + r) + (9L * cb + q) * ldz;
+        if (ca == cb) {
+            if (r <= q) *z -= v;  // diagonal block holds U (scaled) already
         } else {
             *z = -v;
         }
     }
 }
 
-// Degrees and offsets of the tuple list; returns nothing, the total is
-// tup_off[num_obs] (read back by the caller to size the tuple buffer).
-void launch_schur_offsets(const SceneDev& s, cudaStream_t st) {
-    const int n = s.num_obs;
-    if (n == 0) {
-        cudaMemsetAsync(s.tup_off, 0, sizeof(int), st);
-        return;
-    }
-    k_point_degree<<<(n + 255) / 256, 256, 0, st>>>(n, s.cam_obs, s.obs_pt, s.pt_ptr, s.cam_ptr + s.num_cams,
-                                                    s.deg);
-    count_launch();
-    exclusive_scan(s.deg, s.tup_off, n, s.scan_tmp, st);
-}
+size_t schur_blocks(int num_cams) { return (size_t)num_cams * num_cams; }
 
-void launch_schur_tuples(const SceneDev& s, cudaStream_t st) {
-    const int n = s.num_obs;
-    if (n == 0) return;
-    k_pair_tuples<<<(n + 255) / 256, 256, 0, st>>>(n, s.cam_obs, s.obs_pt, s.pt_ptr, s.pt_obs, s.obs_cam,
-                                                   s.tup_off, s.cam_ptr + s.num_cams, s.tup);
-    count_launch();
+void launch_schur_count(const SceneDev& s, cudaStream_t st) {
+    const long nblk = (long)s.num_cams * s.num_cams;
+    cudaMemsetAsync(s.blk_cnt, 0, sizeof(int) * (size_t)nblk, st);
+    if (s.num_points > 0) {
+        k_pair_enum<false><<<(s.num_points + 127) / 128, 128, 0, st>>>(s.num_points, s.num_cams, s.pt_ptr,
+                                                                       s.pt_obs, s.obs_cam, s.blk_cnt, nullptr);
+        count_launch();
+    }
+    exclusive_scan(s.blk_cnt, s.blk_ptr, (int)nblk, s.scan_tmp, st);
 }
 
 void launch_schur(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
-    if (s.num_cams == 0) return;
+    const long nblk = (long)s.num_cams * s.num_cams;
+    if (nblk == 0) return;
+    cudaMemcpyAsync(s.blk_cnt, s.blk_ptr, sizeof(int) * (size_t)nblk, cudaMemcpyDeviceToDevice, st);
+    if (s.num_points > 0) {
+        k_pair_enum<true><<<(s.num_points + 127) / 128, 128, 0, st>>>(s.num_points, s.num_cams, s.pt_ptr,
+                                                                      s.pt_obs, s.obs_cam, s.blk_cnt, s.pairs);
+        count_launch();
+    }
+    cudaMemsetAsync(s.long_list, 0, sizeof(int), st);
+    k_sort_pairs_warp<<<(unsigned)((nblk + 3) / 4), 128, 0, st>>>(nblk, s.blk_ptr, s.pairs, s.long_list,
+                                                                  s.long_cap);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_schur_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kSchurSmem);
+        cudaFuncSetAttribute(k_sort_pairs_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(kPairBlockCap * sizeof(unsigned long long)));
         attr = true;
     }
-    dim3 grid(s.num_cams, (s.num_cams + kSchurChunk - 1) / kSchurChunk);
-    k_schur_rows<<<grid, 96 * kSchurGroups, kSchurSmem, st>>>(s.num_cams, s.cam_ptr, s.tup_off, s.tup,
-                                                              s.Ws, s.Ys, Z, ldz);
-    count_launch();
+    k_sort_pairs_block<<<148, 1024, kPairBlockCap * sizeof(unsigned long long), st>>>(
+        s.blk_ptr, s.pairs, s.long_list, s.long_cap, s.err);
+    k_schur_blocks<<<(unsigned)nblk, 256, 0, st>>>(s.num_cams, s.blk_ptr, s.pairs, s.Ws, s.Ys, Z, ldz);
+    count_launch(3);
 }
 
 // Copy the strict upper triangle onto the lower one (32x32 tiles via smem).

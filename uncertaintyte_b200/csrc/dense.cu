@@ -20,7 +20,7 @@ constexpr int BM = 128, BN = 128, BK = 16, STAGES = 4;
 constexpr int LDA_S = BM + 8;   // As[k][m]: 136 doubles per k row (conflict-free fragment reads)
 constexpr int LDB_S = BK + 4;   // Bs[n][k]: 20 doubles per n row
 constexpr int A_STAGE = BK * LDA_S;
-constexpr int B_STAGE = BN * LDB_S;
+constexpr int B_STAGE = BN * LDB_S;  // >= BK * LDA_S (layout of a transposed B tile)
 constexpr int GEMM_THREADS = 256;
 constexpr size_t GEMM_SMEM = sizeof(double) * (size_t)STAGES * (A_STAGE + B_STAGE);
 
@@ -46,6 +46,7 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 // x BN cols of column-major B). Out-of-range chunks are zero-filled. Rows
 // past M (or K for B) inside the allocation are read as 16-byte pairs; the
 // buffers keep their padding rows at zero so those reads are inert.
+template <bool kTransB>
 __device__ __forceinline__ void load_tiles(double* As, double* Bs, const double* __restrict__ A,
                                            long lda, const double* __restrict__ B, long ldb, int M,
                                            int N, int K, int m0, int n0, int k0, int tid) {
@@ -57,16 +58,29 @@ __device__ __forceinline__ void load_tiles(double* As, double* Bs, const double*
         const double* src = p ? A + (m0 + m2) + (long)(k0 + k) * lda : A;
         cp_async16(As + k * LDA_S + m2, src, p);
     }
+    if (kTransB) {
+        // B(k, n) = B[n + k * ldb]: tile stored Bs[k][n] like A
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        int idx = tid + q * GEMM_THREADS;
-        int n = idx >> 3, k2 = (idx & 7) * 2;
-        bool p = (n0 + n < N) && (k0 + k2 < K);
-        const double* src = p ? B + (k0 + k2) + (long)(n0 + n) * ldb : B;
-        cp_async16(Bs + n * LDB_S + k2, src, p);
+        for (int q = 0; q < 4; ++q) {
+            int idx = tid + q * GEMM_THREADS;
+            int k = idx >> 6, n2 = (idx & 63) * 2;
+            bool p = (n0 + n2 < N) && (k0 + k < K);
+            const double* src = p ? B + (n0 + n2) + (long)(k0 + k) * ldb : B;
+            cp_async16(Bs + k * LDA_S + n2, src, p);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            int idx = tid + q * GEMM_THREADS;
+            int n = idx >> 3, k2 = (idx & 7) * 2;
+            bool p = (n0 + n < N) && (k0 + k2 < K);
+            const double* src = p ? B + (k0 + k2) + (long)(n0 + n) * ldb : B;
+            cp_async16(Bs + n * LDB_S + k2, src, p);
+        }
     }
 }
 
+template <bool kTransB>
 __global__ void __launch_bounds__(GEMM_THREADS, 1)
     k_gemm_f64(int M, int N, int K, double alpha, const double* __restrict__ A, long lda,
                const double* __restrict__ B, long ldb, double beta, double* C, long ldc,
@@ -90,7 +104,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
 
 #pragma unroll
     for (int s = 0; s < STAGES - 1; ++s) {
-        if (s < KT) load_tiles(As + s * A_STAGE, Bs + s * B_STAGE, A, lda, B, ldb, M, N, K, m0, n0, s * BK, tid);
+        if (s < KT) load_tiles<kTransB>(As + s * A_STAGE, Bs + s * B_STAGE, A, lda, B, ldb, M, N, K, m0, n0, s * BK, tid);
         cp_async_commit();
     }
     for (int kt = 0; kt < KT; ++kt) {
@@ -99,7 +113,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         int pf = kt + STAGES - 1;
         if (pf < KT) {
             int ps = pf % STAGES;
-            load_tiles(As + ps * A_STAGE, Bs + ps * B_STAGE, A, lda, B, ldb, M, N, K, m0, n0, pf * BK, tid);
+            load_tiles<kTransB>(As + ps * A_STAGE, Bs + ps * B_STAGE, A, lda, B, ldb, M, N, K, m0, n0, pf * BK, tid);
         }
         cp_async_commit();
         const double* as = As + (kt % STAGES) * A_STAGE;
@@ -110,7 +124,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
 #pragma unroll
             for (int i = 0; i < 4; ++i) af[i] = as[(kk + t) * LDA_S + wm + i * 8 + g];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) bf[j] = bs[(wn + j * 8 + g) * LDB_S + kk + t];
+            for (int j = 0; j < 8; ++j)
+                bf[j] = kTransB ? bs[(kk + t) * LDA_S + wn + j * 8 + g] : bs[(wn + j * 8 + g) * LDB_S + kk + t];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -146,26 +161,56 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     }
 }
 
-void gemm_f64(int M, int N, int K, double alpha, const double* A, int lda, const double* B,
-              int ldb, double beta, double* C, int ldc, unsigned long long* amax, cudaStream_t st) {
+void gemm_f64_ex(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
+                 double beta, double* C, int ldc, unsigned long long* amax, bool lower_only, cudaStream_t st,
+                 bool trans_b) {
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_gemm_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
+        cudaFuncSetAttribute(k_gemm_f64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
+        cudaFuncSetAttribute(k_gemm_f64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
         attr = true;
     }
     if (M <= 0 || N <= 0) return;
     dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-    k_gemm_f64<<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, amax, 0);
+    if (trans_b)
+        k_gemm_f64<true><<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                                amax, lower_only ? 1 : 0);
+    else
+        k_gemm_f64<false><<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                                 amax, lower_only ? 1 : 0);
     count_launch();
+}
+
+void gemm_f64(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
+              double beta, double* C, int ldc, unsigned long long* amax, cudaStream_t st) {
+    gemm_f64_ex(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, amax, false, st, false);
 }
 
 void gemm_f64_tri(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
                   double beta, double* C, int ldc, cudaStream_t st) {
-    gemm_f64(0, 0, 0, 0, nullptr, 0, nullptr, 0, 0, nullptr, 0, nullptr, st);  // sets the smem attribute
-    if (M <= 0 || N <= 0) return;
-    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-    k_gemm_f64<<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,
-                                                      nullptr, 1);
+    gemm_f64_ex(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, true, st, false);
+}
+
+// Copy the strict lower triangle onto the upper one (32 x 32 tiles).
+__global__ void k_mirror_lower(double* Z, int n, long ld) {
+    __shared__ double t[32][33];
+    const int bi = blockIdx.y, bj = blockIdx.x;  // tile row, tile col of the source (lower) tile
+    if (bj > bi) return;
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        int i = bi * 32 + r, j = bj * 32 + threadIdx.x;
+        t[r][threadIdx.x] = (i < n && j < n) ? Z[i + (long)j * ld] : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        int j = bj * 32 + r, i = bi * 32 + threadIdx.x;  // target (j, i) = source (i, j), i > j
+        if (i < n && j < n && i > j) Z[j + (long)i * ld] = t[threadIdx.x][r];
+    }
+}
+
+void launch_mirror_lower(double* Z, int n, int ld, cudaStream_t st) {
+    if (n == 0) return;
+    dim3 g((n + 31) / 32, (n + 31) / 32);
+    k_mirror_lower<<<g, dim3(32, 8), 0, st>>>(Z, n, ld);
     count_launch();
 }
 
@@ -173,121 +218,99 @@ void gemm_f64_tri(int M, int N, int K, double alpha, const double* A, int lda, c
 // SPD inverse: blocked Cholesky A = L L^T, T = L^{-1}, A^{-1} = T^T T
 // ------------------------------------------------------------------------
 constexpr int NB = 64;                       // panel width
-constexpr int SQ_SMEM = (int)(sizeof(double) * 2 * NB * (NB + 1));
 
-size_t chol_small_doubles(int n) { return (size_t)NB * NB + (size_t)NB * (n + 8) + 64; }
+size_t chol_small_doubles(int n) { (void)n; return (size_t)NB * NB + 64; }
 
-// Unblocked Cholesky of the kb x kb diagonal block at (k0, k0) in shared
-// memory (lower triangle read), written back as L_kk; its inverse (lower)
-// goes to Linv (64 x 64, ld 64). One CTA.
-__global__ void __launch_bounds__(256) k_chol_diag(double* A, long lda, int k0, int kb, double* Linv,
-                                                   int* err) {
-    extern __shared__ double sm_[];
-    double(*a)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm_);
-    double(*x)[NB + 1] = a + NB;  // x[i][c]: column c of the inverse
+// Cholesky of the kb x kb (kb <= 64) diagonal block at (k0, k0) and the
+// inverse of its factor in one CTA of 1024 threads. Thread t owns the
+// lower-triangle elements e = t and e = t + 1024 (row-major packing of the
+// 2080 elements of a 64 x 64 lower triangle) in registers, both of L and of
+// T = L^{-1}. Every elimination step publishes one column (and one row of T)
+// through shared memory and costs two barriers; the pivot scale rsqrt(d) is
+// applied on the fly, so no extra pass is needed.
+// Writes L_kk into A (lower), T_kk into the diagonal block of T, and T_kk^T
+// into LinvT (64 x 64, column-major: LinvT[k + 64 q] = T_kk(q, k)), the B
+// operand of the panel solve L_ik = A_ik T_kk^T.
+constexpr int kTri = NB * (NB + 1) / 2;  // 2080
+
+__device__ __forceinline__ void tri_rc(int e, int& i, int& j) {
+    // e = i (i + 1) / 2 + j, 0 <= j <= i
+    int r = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
+    while ((r + 1) * (r + 2) / 2 <= e) ++r;
+    while (r * (r + 1) / 2 > e) --r;
+    i = r;
+    j = e - r * (r + 1) / 2;
+}
+
+__global__ void __launch_bounds__(1024) k_chol_diag(double* A, long lda, int k0, int kb, double* T, long ldt,
+                                                    double* LinvT, int* err) {
+    __shared__ double colv[NB], rowt[NB], ilv[NB];
     const int tid = threadIdx.x;
-    for (int e = tid; e < kb * kb; e += blockDim.x) {
-        int r = e % kb, c = e / kb;
-        a[r][c] = r >= c ? A[(k0 + r) + (long)(k0 + c) * lda] : 0.0;
+    constexpr int E = (kTri + 1023) / 1024;  // 3 elements for the first threads, 2 for the rest
+    int ii[E], jj[E];
+    bool v[E];
+    double a[E], t[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+        const int e = tid + 1024 * k;
+        if (e < kTri) {
+            tri_rc(e, ii[k], jj[k]);
+        } else {
+            ii[k] = jj[k] = 0;
+        }
+        v[k] = e < kTri && ii[k] < kb;
+        a[k] = v[k] ? A[(k0 + ii[k]) + (long)(k0 + jj[k]) * lda] : 0.0;
     }
-    __syncthreads();
     for (int p = 0; p < kb; ++p) {
+#pragma unroll
+        for (int k = 0; k < E; ++k)
+            if (v[k] && jj[k] == p) colv[ii[k]] = a[k];
+        __syncthreads();
+        const double d = colv[p];
+        const double r = rsqrt(d);
         if (tid == 0) {
-            double d = a[p][p];
+            ilv[p] = r;
             if (!(d > 0.0 && d <= 1.7976931348623157e308)) atomicOr(err, ERRBIT_SINGULAR);
-            a[p][p] = sqrt(d);
         }
-        __syncthreads();
-        double lp = a[p][p];
-        for (int i = p + 1 + tid; i < kb; i += blockDim.x) a[i][p] /= lp;
-        __syncthreads();
-        const int m = kb - p - 1;  // trailing size
-        for (int e = tid; e < m * m; e += blockDim.x) {
-            int i = p + 1 + e % m, j = p + 1 + e / m;
-            if (j <= i) a[i][j] -= a[i][p] * a[j][p];
+#pragma unroll
+        for (int k = 0; k < E; ++k) {
+            if (!v[k]) continue;
+            if (jj[k] == p) a[k] = (ii[k] == p) ? d * r : a[k] * r;
+            else if (jj[k] > p) a[k] -= (colv[ii[k]] * r) * (colv[jj[k]] * r);
         }
         __syncthreads();
     }
-    for (int e = tid; e < kb * kb; e += blockDim.x) {
-        int r = e % kb, c = e / kb;
-        if (r >= c) A[(k0 + r) + (long)(k0 + c) * lda] = a[r][c];
-    }
-    // forward substitution, one thread per column of the inverse
-    if (tid < kb) {
-        const int c = tid;
-        for (int i = 0; i < c; ++i) x[i][c] = 0.0;
-        x[c][c] = 1.0 / a[c][c];
-        for (int i = c + 1; i < kb; ++i) {
-            double s = 0.0;
-            for (int j = c; j < i; ++j) s += a[i][j] * x[j][c];
-            x[i][c] = -s / a[i][i];
+    // T = L^{-1}: forward elimination on [L | I]
+#pragma unroll
+    for (int k = 0; k < E; ++k) t[k] = (v[k] && ii[k] == jj[k]) ? 1.0 : 0.0;
+    for (int p = 0; p < kb; ++p) {
+        const double r = ilv[p];
+#pragma unroll
+        for (int k = 0; k < E; ++k) {
+            if (!v[k]) continue;
+            if (ii[k] == p) {
+                t[k] *= r;
+                rowt[jj[k]] = t[k];
+            } else if (jj[k] == p && ii[k] > p) {
+                colv[ii[k]] = a[k];
+            }
         }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < E; ++k)
+            if (v[k] && ii[k] > p && jj[k] <= p) t[k] -= colv[ii[k]] * rowt[jj[k]];
+        __syncthreads();
     }
+    for (int e = tid; e < NB * NB; e += 1024) LinvT[e] = 0.0;
     __syncthreads();
-    for (int e = tid; e < kb * kb; e += blockDim.x) {
-        int r = e % kb, c = e / kb;
-        Linv[r + (long)c * NB] = x[r][c];
-    }
-}
-
-// Panel: L_ik = A_ik * Linv_kk^T for the 64-row chunk starting at i0 (rows
-// below the pivot block); written into A and transposed into R (R[q + i*NB] =
-// L(i, k0+q)) as the B operand of the trailing update.
-__global__ void __launch_bounds__(256) k_chol_panel(double* A, long lda, int n, int k0, int kb, int i0,
-                                                    const double* __restrict__ Linv, double* R) {
-    extern __shared__ double sm_[];
-    double(*sp)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm_);  // sp[q][r] = Linv(q, r)
-    double(*sx)[NB + 1] = sp + NB;                                   // sx[i][r] = A(row, k0 + r)
-    const int tid = threadIdx.x;
-    const int r0 = i0 + blockIdx.x * NB;
-    const int rn = min(NB, n - r0);
-    if (rn <= 0) return;
-    for (int e = tid; e < kb * kb; e += blockDim.x) {
-        int q = e % kb, r = e / kb;
-        sp[q][r] = Linv[q + (long)r * NB];
-    }
-    for (int e = tid; e < rn * kb; e += blockDim.x) {
-        int i = e % rn, r = e / rn;
-        sx[i][r] = A[(r0 + i) + (long)(k0 + r) * lda];
-    }
-    __syncthreads();
-    for (int e = tid; e < rn * kb; e += blockDim.x) {
-        int i = e % rn, q = e / rn;
-        double s = 0.0;
-        for (int r = 0; r <= q; ++r) s += sx[i][r] * sp[q][r];
-        A[(r0 + i) + (long)(k0 + q) * lda] = s;
-        R[q + (long)(r0 + i) * NB] = s;
-    }
-}
-
-// Inverse of every 64 x 64 diagonal block of the lower-triangular L (the
-// leaves of the recursive triangular inverse). One CTA per block.
-__global__ void __launch_bounds__(256) k_trtri_leaves(const double* __restrict__ L, long lda, int n,
-                                                      double* T, long ldt) {
-    extern __shared__ double sm_[];
-    double(*a)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm_);
-    double(*x)[NB + 1] = a + NB;
-    const int b0 = blockIdx.x * NB, bs = min(NB, n - b0);
-    const int tid = threadIdx.x;
-    for (int e = tid; e < bs * bs; e += blockDim.x) {
-        int r = e % bs, c = e / bs;
-        a[r][c] = r >= c ? L[(b0 + r) + (long)(b0 + c) * lda] : 0.0;
-    }
-    __syncthreads();
-    if (tid < bs) {
-        const int c = tid;
-        for (int i = 0; i < c; ++i) x[i][c] = 0.0;
-        x[c][c] = 1.0 / a[c][c];
-        for (int i = c + 1; i < bs; ++i) {
-            double s = 0.0;
-            for (int j = c; j < i; ++j) s += a[i][j] * x[j][c];
-            x[i][c] = -s / a[i][i];
-        }
-    }
-    __syncthreads();
-    for (int e = tid; e < bs * bs; e += blockDim.x) {
-        int r = e % bs, c = e / bs;
-        T[(b0 + r) + (long)(b0 + c) * ldt] = x[r][c];
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+        if (!v[k]) continue;
+        const int i = ii[k], j = jj[k];
+        A[(k0 + i) + (long)(k0 + j) * lda] = a[k];
+        T[(k0 + i) + (long)(k0 + j) * ldt] = t[k];
+        if (i != j) T[(k0 + j) + (long)(k0 + i) * ldt] = 0.0;
+        LinvT[j + (long)i * NB] = t[k];  // LinvT(k = j, q = i) = T(i, j)
     }
 }
 
@@ -307,14 +330,6 @@ __global__ void k_transpose(const double* __restrict__ T, long ldt, int n, doubl
 }
 
 namespace {
-void set_smem_attr() {
-    static bool done = false;
-    if (done) return;
-    cudaFuncSetAttribute(k_chol_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, SQ_SMEM);
-    cudaFuncSetAttribute(k_chol_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, SQ_SMEM);
-    cudaFuncSetAttribute(k_trtri_leaves, cudaFuncAttributeMaxDynamicSharedMemorySize, SQ_SMEM);
-    done = true;
-}
 
 // T[r0:r1, r0:r1] = inverse of L[r0:r1, r0:r1] given the inverted leaves:
 // T21 = -T22 * (L21 * T11), split at a multiple of 64.
@@ -336,31 +351,31 @@ void trtri_merge(const double* L, int lda, double* T, int ldt, double* W, int ld
 
 void chol_inverse(double* A, int n, int lda, double* T, double* W, double* Tt, double* small, int* err,
                   cudaStream_t st) {
-    set_smem_attr();
-    double* Linv = small;
-    double* R = small + NB * NB;
-    // 1. blocked right-looking Cholesky (lower triangle of A becomes L)
+    double* LinvT = small;
+    // 1. blocked right-looking Cholesky (lower triangle of A becomes L); the
+    //    diagonal blocks of T = L^{-1} are produced on the way
     for (int k0 = 0; k0 < n; k0 += NB) {
         const int kb = min(NB, n - k0), k1 = k0 + kb;
-        k_chol_diag<<<1, 256, SQ_SMEM, st>>>(A, lda, k0, kb, Linv, err);
+        k_chol_diag<<<1, 1024, 0, st>>>(A, lda, k0, kb, T, lda, LinvT, err);
         count_launch();
         if (k1 < n) {
             const int rows = n - k1;
-            k_chol_panel<<<(rows + NB - 1) / NB, 256, SQ_SMEM, st>>>(A, lda, n, k0, kb, k1, Linv, R);
-            count_launch();
-            gemm_f64_tri(rows, rows, kb, -1.0, A + k1 + (long)k0 * lda, lda, R + (long)k1 * NB, NB, 1.0,
-                         A + k1 + (long)k1 * lda, lda, st);
+            double* P = A + k1 + (long)k0 * lda;  // panel below the pivot block
+            // L_ik = A_ik T_kk^T, in place (each CTA owns its rows and all 64 columns)
+            gemm_f64_ex(rows, kb, kb, 1.0, P, lda, LinvT, NB, 0.0, P, lda, nullptr, false, st, false);
+            // A22 -= L_ik L_ik^T, lower tiles; B = panel^T read in place
+            gemm_f64_ex(rows, rows, kb, -1.0, P, lda, P, lda, 1.0, A + k1 + (long)k1 * lda, lda, nullptr, true,
+                        st, true);
         }
     }
-    // 2. T = L^{-1}: leaves, then recursive merges
-    k_trtri_leaves<<<(n + NB - 1) / NB, 256, SQ_SMEM, st>>>(A, lda, n, T, lda);
-    count_launch();
+    // 2. T = L^{-1}: recursive merges above the inverted diagonal blocks
     trtri_merge(A, lda, T, lda, W, lda, 0, n, st);
-    // 3. A^{-1} = T^T T
+    // 3. A^{-1} = T^T T (symmetric: lower-triangle tiles, then mirror)
     dim3 g((n + 31) / 32, (n + 31) / 32);
     k_transpose<<<g, dim3(32, 8), 0, st>>>(T, lda, n, Tt, lda);
     count_launch();
-    gemm_f64(n, n, n, 1.0, Tt, lda, T, lda, 0.0, A, lda, nullptr, st);
+    gemm_f64_ex(n, n, n, 1.0, Tt, lda, T, lda, 0.0, A, lda, nullptr, true, st, false);
+    launch_mirror_lower(A, n, lda, st);
 }
 
 // ------------------------------------------------------------------------

@@ -48,9 +48,11 @@ struct SceneDev {
     double* iVs;          // 6*num_points upper triangle of the inverse of the scaled point block
     double* Ws;           // 27*num_obs scaled W_o = (J_c^T J_p)/(s s), 9x3 row-major
     double* Ys;           // 27*num_obs Y_o = W_o * iV_p, 9x3 row-major
-    int* deg;             // num_obs: point degree of each camera-grouped observation
-    int* tup_off;         // num_obs + 1: offsets of the Schur pair tuples
-    int4* tup;            // Schur pair tuples (o, o2, camera(o2), 0), grouped by camera
+    int* blk_cnt;         // num_cams^2: pair counts, then scatter cursors, per camera-pair block
+    int* blk_ptr;         // num_cams^2 + 1: pair list offsets per block
+    unsigned long long* pairs;  // (o << 32 | o') per block, sorted inside a block
+    int* long_list;       // [count, ids...] of blocks with more than 1024 pairs
+    int long_cap;         // capacity of long_list ids
     int* err;             // device error bits
 };
 
@@ -60,10 +62,11 @@ void launch_build_index(SceneDev& s, cudaStream_t st);
 void launch_camera_blocks(const SceneDev& s, double* Z, int ldz, cudaStream_t st);
 void launch_point_blocks(const SceneDev& s, cudaStream_t st);
 void launch_obs_blocks(const SceneDev& s, cudaStream_t st);
-// Schur scatter: offsets (total = tup_off[num_obs]), tuples, then
-// Z(c,c') -= sum_p Y_o W_o'^T (upper camera-block triangle); mirror after.
-void launch_schur_offsets(const SceneDev& s, cudaStream_t st);
-void launch_schur_tuples(const SceneDev& s, cudaStream_t st);
+// Schur scatter: pair counts per camera-pair block (total = blk_ptr[C*C]),
+// then Z(c,c') -= sum_p Y_o W_o'^T (upper camera-block triangle); mirror after.
+void launch_schur_count(const SceneDev& s, cudaStream_t st);
+// Self terms Z(c,c) -= sum_o Y_o W_o^T (upper triangle of the diagonal blocks).
+void launch_camera_self(const SceneDev& s, double* Z, int ldz, cudaStream_t st);
 void launch_schur(const SceneDev& s, double* Z, int ldz, cudaStream_t st);
 void launch_mirror_upper(double* Z, int n, int ldz, cudaStream_t st);
 // Generic 9/12-entry-row repack for the J^T J export (camera-only rows allowed).
@@ -79,6 +82,13 @@ size_t scan_tmp_ints(int n);
 // epilogue folds max|C| into *amax (bit pattern of a non-negative double).
 void gemm_f64(int M, int N, int K, double alpha, const double* A, int lda, const double* B,
               int ldb, double beta, double* C, int ldc, unsigned long long* amax, cudaStream_t st);
+// General form: lower_only skips output tiles strictly above the diagonal
+// (symmetric results; mirror afterwards with launch_mirror_lower).
+// trans_b: B(k, n) is read from B[n + k * ldb] (the transpose of a column-major matrix).
+void gemm_f64_ex(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
+                 double beta, double* C, int ldc, unsigned long long* amax, bool lower_only, cudaStream_t st,
+                 bool trans_b = false);
+void launch_mirror_lower(double* Z, int n, int ld, cudaStream_t st);
 // Same, skipping output tiles strictly above the diagonal (symmetric updates).
 void gemm_f64_tri(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
                   double beta, double* C, int ldc, cudaStream_t st);

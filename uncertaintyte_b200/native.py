@@ -79,7 +79,7 @@ class UncStatistic(C.Structure):
 EXPORTS = ("unc_options_init", "unc_context_create", "unc_context_destroy", "unc_compute",
            "unc_context_set_profiling", "unc_context_profile",
            "unc_compute_device", "unc_workspace_bytes", "unc_dense_inverse_device", "unc_jtj_crs",
-           "unc_status_string", "unc_last_error", "unc_kernel_launches")
+           "unc_gemm_f64_device", "unc_status_string", "unc_last_error", "unc_kernel_launches")
 
 _lib = None
 
@@ -108,6 +108,8 @@ def lib():
     L.unc_dense_inverse_device.argtypes = [vp, C.c_int, C.c_int, vp]
     L.unc_jtj_crs.argtypes = [C.c_int, C.c_int, vp, vp, vp, C.c_int, C.c_int, P(C.c_longlong), vp,
                               vp, vp]
+    L.unc_gemm_f64_device.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, vp, C.c_int, vp, C.c_int,
+                                      C.c_double, vp, C.c_int, vp]
     L.unc_status_string.argtypes = [C.c_int]
     L.unc_status_string.restype = C.c_char_p
     L.unc_last_error.restype = C.c_char_p
@@ -228,6 +230,11 @@ def jtj_crs(num_rows: int, num_cols: int, rows, cols, vals, num_cams: int, cam_p
     _check(L.unc_jtj_crs(num_rows, num_cols, _ptr(rows), _ptr(cols), _ptr(vals), num_cams, cam_params,
                          C.byref(nnz), _ptr(orow), _ptr(ocol), _ptr(oval)))
     return orow, ocol, oval
+
+
+def gemm_f64_device(M, N, K, alpha, d_A, lda, d_B, ldb, beta, d_C, ldc, stream: int = 0) -> None:
+    """C = alpha A B + beta C (column-major device pointers) on the FP64 GEMM kernel."""
+    _check(lib().unc_gemm_f64_device(M, N, K, alpha, d_A, lda, d_B, ldb, beta, d_C, ldc, stream or None))
 
 
 def kernel_launches() -> int:
