@@ -10,7 +10,10 @@ camera and point covariances).
 
   value : solves/s with the Jacobian resident in HBM (unc_compute_device),
           L2 flushed (256 MB write) before every step, CUDA events on the
-          launching stream, max over ranks.
+          launching stream, max over ranks. Default precision "mixed": the
+          Taylor products run as int8-sliced tcgen05 GEMMs; the plain FP64
+          GPU path is timed on the same scene ("fp64_gpu") together with the
+          mixed-vs-FP64 maximum relative error per camera / point block.
   e2e   : solves/s through the public host API (unc_compute) from pinned
           host buffers, H2D of the Jacobian and D2H of all outputs inside.
   --impl reference : the CPU restatement of the reference algorithm (the
@@ -54,7 +57,7 @@ def _args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="medium")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "mixed", "mixed4", "mixed3"], default="mixed")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -110,9 +113,9 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def _traffic_from_profile(workload: str):
+def _traffic_from_profile(kernel: str, workload: str):
     """DRAM bytes per Taylor-product launch from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", f"gemm_f64_{workload}.md")
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
     if not os.path.exists(path):
         return None
     m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
@@ -171,7 +174,46 @@ def run_reference(a):
     return 0
 
 
+def _int8_peak_tops(torch, dev):
+    """cuBLASLt int8 GEMM (torch._int_mm) 8192^3, best of 5: the tensor-pipe
+    denominator for the int8-sliced products (MEASURED_PEAKS.json has bf16 only)."""
+    n = 8192
+    try:
+        a = torch.randint(-127, 127, (n, n), dtype=torch.int8, device=dev)
+        b = torch.randint(-127, 127, (n, n), dtype=torch.int8, device=dev)
+        torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = 0.0
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            e1.synchronize()
+            best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+        del a, b
+        torch.cuda.empty_cache()
+        return best
+    except Exception:
+        return None
+
+
+def _mixed_issued_ops(n: int, slices: int) -> float:
+    """int8 multiply-adds x 2 issued by one lower-triangle mixed product."""
+    nt = 128 if slices <= 4 else 96
+    kp = (n + 63) // 64 * 64
+    pairs = slices * (slices + 1) // 2
+    tiles = 0
+    for by in range((n + 127) // 128):
+        for bx in range((n + nt - 1) // nt):
+            if bx * nt <= by * 128 + 127:
+                tiles += 1
+    return 2.0 * pairs * tiles * 128 * nt * kp
+
+
 def run_ours(a):
+    import ctypes as C
+
     import torch
     import torch.distributed as dist
 
@@ -184,7 +226,9 @@ def run_ours(a):
         dist.init_process_group("nccl", device_id=dev, timeout=__import__("datetime").timedelta(seconds=300))
 
     jac = scenes.synthetic_jacobian(a.workload, seed=rank)
-    opts = native.make_options(jac, precision=a.precision)
+    prec = a.precision
+    opts = native.make_options(jac, precision=prec)
+    opts64 = native.make_options(jac, precision="fp64")
     d_rows = torch.from_numpy(jac.rows).to(dev)
     d_cols = torch.from_numpy(jac.cols).to(dev)
     d_vals = torch.from_numpy(jac.values).to(dev)
@@ -195,47 +239,70 @@ def run_ours(a):
     stream = torch.cuda.current_stream(dev)
     sptr = stream.cuda_stream
 
-    def step():
-        return native.compute_covariances_device(ctx, opts, jac.num_rows, jac.num_cols,
-                                                 d_rows.data_ptr(), d_cols.data_ptr(),
-                                                 d_vals.data_ptr(), d_cam.data_ptr(),
+    def step(o):
+        return native.compute_covariances_device(ctx, o, jac.num_rows, jac.num_cols, d_rows.data_ptr(),
+                                                 d_cols.data_ptr(), d_vals.data_ptr(), d_cam.data_ptr(),
                                                  d_pt.data_ptr(), sptr)
 
-    for _ in range(max(a.warmup, 0)):
-        flush.zero_()
-        step()
-    torch.cuda.synchronize()
+    def timed(o, steps, profile=False):
+        for _ in range(max(a.warmup, 0)):
+            flush.zero_()
+            step(o)
+        torch.cuda.synchronize()
+        if profile:
+            ctx.set_profiling(True)
+            ctx.profile(reset=True)
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = native.kernel_launches()
+        evs, st = [], None
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = step(o)
+            e1.record(stream)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        launches = native.kernel_launches() - l0
+        prof = ctx.profile(reset=True) if profile else None
+        ctx.set_profiling(False)
+        t = torch.tensor([sum(e0.elapsed_time(e1) for e0, e1 in evs) * 1e-3], dtype=torch.float64, device=dev)
+        if ws > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), st, launches, prof
 
-    ctx.set_profiling(True)
-    ctx.profile(reset=True)
+    # headline: the requested precision (mixed by default), clocks sampled during it
     clocks = ClockSampler(local)
     clocks.start()
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches0 = native.kernel_launches()
-    evs = []
-    stats = None
-    for _ in range(a.steps):
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        stats = step()
-        e1.record(stream)
-        evs.append((e0, e1))
-    torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
-    launches = native.kernel_launches() - launches0
+    t_main, stats, launches, prof = timed(opts, a.steps, profile=True)
     clk = clocks.stop()
-    ctx.set_profiling(False)
-    n_prod, prod_s, prod_flops = ctx.profile(reset=True)
-    t_local = sum(e0.elapsed_time(e1) for e0, e1 in evs) * 1e-3
-    t = torch.tensor([t_local], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    t_max = float(t.item())
-    value = ws * a.steps / t_max
+    cam_main, pt_main = d_cam.cpu().numpy().copy(), d_pt.cpu().numpy().copy()
+    value = ws * a.steps / t_main
+    # the plain FP64 GPU path on the same scene, and the mixed-vs-FP64 error
+    fp64 = None
+    if prec != "fp64":
+        t64, st64, _, _ = timed(opts64, max(3, a.steps // 2))
+        n64 = max(3, a.steps // 2)
+        c64, p64 = d_cam.cpu().numpy(), d_pt.cpu().numpy()
+
+        def blk(x, y, w):
+            import numpy as np
+            p = {45: 9, 6: 3}[w]
+            wt = np.sqrt(np.array([1.0 if i == j else 2.0 for i in range(p) for j in range(i, p)]))
+            x, y = x.reshape(-1, w) * wt, y.reshape(-1, w) * wt
+            den = np.linalg.norm(y, axis=1)
+            num = np.linalg.norm(x - y, axis=1)
+            return float(np.max(np.where(den > 0, num / np.where(den > 0, den, 1), num)))
+
+        fp64 = {"value": ws * n64 / t64, "unit": UNIT, "ms_per_step": 1e3 * t64 / n64,
+                "te_iterations": st64["te_iterations"],
+                "speedup_mixed_over_fp64": (t64 / n64) / (t_main / a.steps),
+                "mixed_vs_fp64_max_rel_err": {"camera_9x9": blk(cam_main, c64, 45),
+                                              "point_3x3": blk(pt_main, p64, 6), "bar": 1e-6}}
 
     # end to end through the public host API, pinned host buffers
     e2e_steps = a.e2e_steps or max(3, a.steps // 2)
@@ -244,7 +311,6 @@ def run_ours(a):
               torch.zeros(jac.num_cams * 45, dtype=torch.float64).pin_memory(),
               torch.zeros(jac.num_points * 6, dtype=torch.float64).pin_memory()]
     h_rows, h_cols, h_vals, h_cam, h_pt = (t.numpy() for t in pinned)
-    import ctypes as C
     L = native.lib()
 
     def e2e_step():
@@ -272,18 +338,32 @@ def run_ours(a):
     h2d = h_rows.nbytes + h_cols.nbytes + h_vals.nbytes
     d2h = h_cam.nbytes + h_pt.nbytes
 
-    # roofline of the dominant kernel (the N x N x N FP64 Taylor product)
+    # roofline of the dominant kernel (the Taylor-series product)
     roof = None
-    if rank == 0:
-        peak = _fp64_peak_tflops(torch, dev)
-        achieved = prod_flops / prod_s / 1e12 if prod_s > 0 else None
-        traffic = _traffic_from_profile(a.workload)
-        roof = {"bound": "tensor", "kernel": "k_gemm_f64 (Taylor-series product, DMMA m8n8k4)",
-                "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak if achieved else None, "traffic": traffic,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in "
-                               "MEASURED_PEAKS.json)",
-                "launches_timed": n_prod, "flops_per_launch": prod_flops / max(n_prod, 1)}
+    if rank == 0 and prof is not None and prof[1] > 0:
+        n_prod, prod_s, prod_flops = prof
+        N = 9 * jac.num_cams
+        if prec == "fp64":
+            peak = _fp64_peak_tflops(torch, dev)
+            achieved = prod_flops / prod_s / 1e12
+            roof = {"bound": "tensor", "kernel": "k_gemm_f64 (Taylor product, DMMA m8n8k4, lower tiles)",
+                    "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                    "traffic": _traffic_from_profile("f64", a.workload),
+                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in MEASURED_PEAKS.json)",
+                    "launches_timed": n_prod, "flops_per_launch": prod_flops / n_prod}
+        else:
+            slices = {"mixed": 5, "mixed4": 4, "mixed3": 3}[prec]
+            ops = _mixed_issued_ops(N, slices) * n_prod
+            achieved = ops / prod_s / 1e12
+            peak = _int8_peak_tops(torch, dev)
+            roof = {"bound": "tensor", "kernel": f"k_ozaki_gemm (tcgen05 kind::i8, TMA, {slices} slices, lower tiles)",
+                    "achieved": achieved, "peak": peak, "unit": "TOP/s int8",
+                    "frac": (achieved / peak) if peak else None,
+                    "traffic": _traffic_from_profile("ozaki", a.workload),
+                    "peak_source": "cuBLASLt int8 GEMM (torch._int_mm) 8192^3 measured in this run "
+                                   "(int8 is not in MEASURED_PEAKS.json)",
+                    "fp64_equivalent_tflops": prod_flops / prod_s / 1e12,
+                    "launches_timed": n_prod, "int8_ops_per_launch": ops / n_prod}
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -298,12 +378,14 @@ def run_ours(a):
                          f"OpenMP + OpenBLAS{', O(points x obs) point scan' if faithful else ''})"}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
-                "warmup": a.warmup, "ms_per_step": 1e3 * t_max / a.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "mixed",
+                "warmup": a.warmup, "ms_per_step": 1e3 * t_main / a.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if prec == "fp64" else "i8-sliced products, f64 elsewhere",
                 "data": "synthetic (seeded generator with the configuration's shapes; no public dataset)",
-                "config": {"workload": WORKLOADS[a.workload], "precision": a.precision,
+                "config": {"workload": WORKLOADS[a.workload], "precision": prec,
                            "l2": "flushed by a 256 MB write before every step",
                            "parallelism": f"replicas x{ws}", "te_iterations": stats["te_iterations"]},
+                "fp64_gpu": fp64,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h)},
                 "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk,

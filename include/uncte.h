@@ -42,8 +42,10 @@ extern "C" {
 #define UNC_TAYLOR_EXPANSION 2
 
 /* precision of the dense Taylor-series products */
-#define UNC_PRECISION_FP64 0  /* plain FP64 (DMMA) products: the parity path */
-#define UNC_PRECISION_MIXED 1 /* tensor-core split products + FP64 refinement */
+#define UNC_PRECISION_FP64 0    /* plain FP64 (DMMA) products: the parity path */
+#define UNC_PRECISION_MIXED 1   /* int8-sliced tensor-core products, 5 slices (~1e-10 per product) */
+#define UNC_PRECISION_MIXED4 2  /* same with 4 slices (~1e-8 per product, faster) */
+#define UNC_PRECISION_MIXED3 3  /* same with 3 slices (~1e-6 per product) */
 
 typedef struct unc_context unc_context;
 
@@ -57,7 +59,7 @@ typedef struct {
     int max_iter_te;    /* unused by the reference (-1); kept for layout parity */
     int pts2fix[3];     /* fixed point ids (TE); only the first two are sorted, as the reference does */
     int has_pts2fix;    /* 0 = no fixed points given */
-    int precision;      /* UNC_PRECISION_FP64 or UNC_PRECISION_MIXED */
+    int precision;      /* UNC_PRECISION_FP64 / _MIXED / _MIXED4 / _MIXED3 */
 } unc_options;
 
 /* Mirrors cov::Statistic (src/uncertaintyTE/uncertainty.h:73-82). Times are
@@ -135,6 +137,16 @@ int unc_jtj_crs(int num_rows, int num_cols, const int* rows, const int* cols, co
  * and K (B) up to the next even row must be readable and finite. */
 int unc_gemm_f64_device(int M, int N, int K, double alpha, const double* d_A, int lda,
                         const double* d_B, int ldb, double beta, double* d_C, int ldc, void* stream);
+
+/* C = P * X for symmetric n x n FP64 matrices P and X (column-major, leading
+ * dimension ld) on the tensor cores: both operands are split into `slices`
+ * (3..5) 7-bit integer slices with power-of-two row scales, the slice
+ * products run as tcgen05 int8 GEMMs with exact int32 accumulation, and the
+ * levels are combined in FP64 (relative error about 2^(-7 slices) of the row
+ * and column maxima). The mixed-precision Taylor products use this kernel.
+ * Scratch is allocated per call. */
+int unc_gemm_mixed_device(int n, const double* d_P, const double* d_X, int ld, double* d_C, int slices,
+                          void* stream);
 
 /* Human-readable name of a status code, and the last error message of the
  * calling thread (empty when none). */

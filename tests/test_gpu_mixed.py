@@ -1,0 +1,69 @@
+"""Mixed-precision Taylor products (int8-sliced tcgen05 GEMMs) against the
+FP64 GPU path and against torch FP64 products (needs a B200).
+
+Tolerance: the north-star bar for the mixed path is a maximum relative
+Frobenius error of 1e-6 per camera 9x9 block and per point 3x3 block against
+the FP64 result; MIXED_TOL below is that bar.
+"""
+import numpy as np
+import pytest
+
+from conftest import block_rel_err, golden_jacobian
+from uncertaintyte_b200 import native, scenes
+
+pytestmark = pytest.mark.gpu
+
+MIXED_TOL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = native.Context(0)
+    yield c
+    c.close()
+
+
+def _mixed_vs_fp64(jac, ctx, precision="mixed"):
+    c64, p64, s64 = native.compute_covariances(jac, ctx, precision="fp64")
+    cmp_, pmp, smp = native.compute_covariances(jac, ctx, precision=precision)
+    assert smp["te_iterations"] == s64["te_iterations"]
+    # the stop-rule values come from the products' max |entry|: same ~1e-8..1e-6 agreement
+    np.testing.assert_allclose(smp["cycle_change"], s64["cycle_change"], rtol=1e-5)
+    ec, ep = block_rel_err(cmp_, c64, 45), block_rel_err(pmp, p64, 6)
+    print(f"{precision}: cams {ec:.3e} points {ep:.3e}")
+    return ec, ep
+
+
+@pytest.mark.parametrize("name", ["small", "medium"])
+def test_mixed_vs_fp64_synthetic(ctx, name):
+    ec, ep = _mixed_vs_fp64(scenes.synthetic_jacobian(name, seed=0), ctx)
+    assert ec < MIXED_TOL and ep < MIXED_TOL
+
+
+def test_mixed_vs_fp64_daliborka(ctx):
+    ec, ep = _mixed_vs_fp64(golden_jacobian("daliborka"), ctx)
+    assert ec < MIXED_TOL and ep < MIXED_TOL
+
+
+def test_mixed4_is_faster_and_coarser(ctx):
+    """4 slices: ~1e-8 per camera block on the synthetic scenes (5 slices: ~1e-10)."""
+    jac = scenes.synthetic_jacobian("small", seed=1)
+    e5 = _mixed_vs_fp64(jac, ctx, "mixed")
+    e4 = _mixed_vs_fp64(jac, ctx, "mixed4")
+    assert e5[0] < 1e-8 and e5[0] <= e4[0] and e4[0] < MIXED_TOL
+
+
+@pytest.mark.parametrize("n,slices,tol", [(1, 4, 1e-6), (70, 4, 1e-5), (200, 4, 1e-5), (1800, 4, 1e-5),
+                                          (1800, 5, 1e-7), (257, 3, 1e-3), (130, 5, 1e-7)])
+def test_mixed_gemm_vs_torch(n, slices, tol):
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(n + slices)
+    A = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+    B = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+    P, X = A + A.T, B @ B.T / n
+    C = torch.zeros_like(P)
+    native.gemm_mixed_device(n, P.data_ptr(), X.data_ptr(), n, C.data_ptr(), slices)
+    torch.cuda.synchronize()
+    ref = (P @ X).T  # column-major C read row-major by torch
+    rel = ((C - ref).norm() / ref.norm()).item()
+    assert rel < tol, rel

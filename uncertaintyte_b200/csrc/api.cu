@@ -27,6 +27,8 @@ struct unc_context {
     size_t ws_bytes = 0;
     void* tup = nullptr;  // Schur observation pairs (sized at run time)
     size_t tup_bytes = 0;
+    void* mp = nullptr;   // int8 slice planes of the mixed-precision products
+    size_t mp_bytes = 0;
     cudaEvent_t ev[12] = {};
     // profiling of the Taylor-series products
     bool prof = false;
@@ -142,8 +144,8 @@ int check_options(const unc_options* o, int num_rows, int num_cols) {
     for (int i = 0; i < 3; ++i)
         if (o->pts2fix[i] < 0 || o->pts2fix[i] >= o->num_points)
             return fail(UNC_ERR_INVALID_ARG, "fixed point id out of range");
-    if (o->precision != UNC_PRECISION_FP64)
-        return fail(UNC_ERR_UNSUPPORTED, "mixed precision is not implemented in this build");
+    if (o->precision < UNC_PRECISION_FP64 || o->precision > UNC_PRECISION_MIXED3)
+        return fail(UNC_ERR_INVALID_ARG, "unknown precision");
     if (9LL * o->num_cams > 46000) return fail(UNC_ERR_TOO_LARGE, "9*num_cams above 46000");
     return UNC_OK;
 }
@@ -240,10 +242,46 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     };
     // Every power X^(i+1) is symmetric: only the lower-triangle tiles of each
     // product are computed (half the flops), then mirrored for the next product.
+    // FP64 mode: DMMA products. Mixed modes: int8-sliced tcgen05 products of
+    // the FP64 operands (X sliced once, each new power sliced per product).
+    const bool mixed = o->precision != UNC_PRECISION_FP64;
+    const int slices = o->precision == UNC_PRECISION_MIXED4 ? 4 : (o->precision == UNC_PRECISION_MIXED3 ? 3 : 5);
+    MixedOperand opP, opXa, opXb;
+    if (mixed) {
+        const size_t sb = (mixed_slice_bytes(N, slices) + 255) & ~size_t(255);
+        const size_t need = 2 * sb + 2 * sizeof(int) * ((size_t)N + 64) + 256;
+        if (ctx->mp_bytes < need) {
+            if (ctx->mp) cudaFree(ctx->mp);
+            ctx->mp = nullptr;
+            ctx->mp_bytes = 0;
+            CK(cudaMalloc(&ctx->mp, need));
+            ctx->mp_bytes = need;
+        }
+        char* w = (char*)ctx->mp;
+        int8_t* bufX = reinterpret_cast<int8_t*>(w);
+        int8_t* bufP = reinterpret_cast<int8_t*>(w + sb);
+        int* eX = reinterpret_cast<int*>(w + 2 * sb);
+        int* eP = eX + N + 64;
+        if (!mixed_plan(opXa, bufX, eX, N, slices, false) || !mixed_plan(opXb, bufX, eX, N, slices, true) ||
+            !mixed_plan(opP, bufP, eP, N, slices, false))
+            return fail(UNC_ERR_CUDA, "tensor-map encoding failed");
+        CK(cudaMemsetAsync(ctx->mp, 0, need, sm));  // slice padding must be zero
+        mixed_slice(X, ld, opXa, sm);
+    }
+    // the profiled region is the product kernel alone (slicing excluded)
+    auto product = [&](const double* P, double* out) -> int {
+        if (mixed) {
+            if (P != X) mixed_slice(P, ld, opP, sm);
+            if (int r = prof_mark()) return r;
+            mixed_gemm(P == X ? opXa : opP, opXb, out, ld, b.amax, true, s.err, sm);
+        } else {
+            if (int r = prof_mark()) return r;
+            gemm_f64_ex(N, N, N, 1.0, P, ld, X, ld, 0.0, out, ld, b.amax, true, sm, false);
+        }
+        return prof_mark();
+    };
     CK(cudaMemsetAsync(b.amax, 0, 8, sm));
-    if (int r = prof_mark()) return r;
-    gemm_f64_ex(N, N, N, 1.0, X, ld, X, ld, 0.0, add, ld, b.amax, true, sm, false);
-    if (int r = prof_mark()) return r;
+    if (int r = product(X, add)) return r;
     launch_mirror_lower(add, N, ld, sm);
     double old_change = DBL_MAX;
     int iters = 0;
@@ -262,9 +300,7 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         iters++;
         launch_axpy(b.iZ, add, k, N, ld, sm);
         CK(cudaMemsetAsync(b.amax, 0, 8, sm));
-        if (int r = prof_mark()) return r;
-        gemm_f64_ex(N, N, N, 1.0, add, ld, X, ld, 0.0, tmp, ld, b.amax, true, sm, false);
-        if (int r = prof_mark()) return r;
+        if (int r = product(add, tmp)) return r;
         launch_mirror_lower(tmp, N, ld, sm);
         std::swap(add, tmp);
     }
@@ -304,6 +340,7 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         return fail(UNC_ERR_LAYOUT, "Jacobian rows are not in the 2 x (9 camera + 3 point) observation layout");
     if (err & (ERRBIT_SINGULAR | ERRBIT_NONFINITE))
         return fail(UNC_ERR_SINGULAR, "non-positive pivot or non-finite value while inverting Z + lambda*I");
+    if (err & ERRBIT_TIMEOUT) return fail(UNC_ERR_CUDA, "tensor-core pipeline wait timed out");
     {
         double amax;
         memcpy(&amax, &amax_bits, 8);
@@ -384,6 +421,7 @@ int unc_context_destroy(unc_context* c) {
     for (cudaEvent_t e : c->pev) cudaEventDestroy(e);
     if (c->ws) cudaFree(c->ws);
     if (c->tup) cudaFree(c->tup);
+    if (c->mp) cudaFree(c->mp);
     for (int i = 0; i < 12; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -659,6 +697,41 @@ int unc_gemm_f64_device(int M, int N, int K, double alpha, const double* d_A, in
         return fail(UNC_ERR_INVALID_ARG, "bad GEMM arguments");
     gemm_f64(M, N, K, alpha, d_A, lda, d_B, ldb, beta, d_C, ldc, nullptr, (cudaStream_t)stream);
     CK(cudaGetLastError());
+    return UNC_OK;
+}
+
+int unc_gemm_mixed_device(int n, const double* d_P, const double* d_X, int ld, double* d_C, int slices,
+                          void* stream) {
+    g_last_error.clear();
+    if (n <= 0 || !d_P || !d_X || !d_C || ld < n || slices < 3 || slices > 5)
+        return fail(UNC_ERR_INVALID_ARG, "bad mixed GEMM arguments");
+    cudaStream_t sm = (cudaStream_t)stream;
+    const size_t sb = mixed_slice_bytes(n, slices);
+    char* ws = nullptr;
+    const size_t exp_off = 2 * ((sb + 255) & ~size_t(255));
+    CK(cudaMalloc(&ws, exp_off + 2 * sizeof(int) * ((size_t)n + 64) + 256));
+    int8_t* bufP = reinterpret_cast<int8_t*>(ws);
+    int8_t* bufX = reinterpret_cast<int8_t*>(ws + (exp_off / 2));
+    int* eP = reinterpret_cast<int*>(ws + exp_off);
+    int* eX = eP + n + 64;
+    int* err = eX + n + 64;
+    MixedOperand a, b;
+    if (!mixed_plan(a, bufP, eP, n, slices, false) || !mixed_plan(b, bufX, eX, n, slices, true)) {
+        cudaFree(ws);
+        return fail(UNC_ERR_CUDA, "tensor-map encoding failed");
+    }
+    int h_err = 0;
+    cudaError_t ce = cudaMemsetAsync(ws, 0, exp_off + 2 * sizeof(int) * ((size_t)n + 64) + 256, sm);
+    if (ce == cudaSuccess) {
+        mixed_slice(d_P, ld, a, sm);
+        mixed_slice(d_X, ld, b, sm);
+        mixed_gemm(a, b, d_C, ld, nullptr, false, err, sm);
+        ce = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, sm);
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(sm);
+    cudaFree(ws);
+    if (ce != cudaSuccess) return fail(UNC_ERR_CUDA, cudaGetErrorString(ce));
+    if (h_err & ERRBIT_TIMEOUT) return fail(UNC_ERR_CUDA, "tensor-core pipeline wait timed out");
     return UNC_OK;
 }
 

@@ -1,5 +1,6 @@
 // internal.h - shared declarations of the uncertaintyTE B200 kernels.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -13,6 +14,7 @@ enum : int {
     ERRBIT_SINGULAR = 2,    // non-positive or non-finite pivot
     ERRBIT_NONFINITE = 4,   // NaN / Inf produced
     ERRBIT_SORT_CAP = 8,    // a segment was too long to sort (order left nondeterministic)
+    ERRBIT_TIMEOUT = 16,    // a bounded device wait ran out (tensor-core pipeline)
 };
 
 constexpr int kCamParams = 9;
@@ -110,6 +112,25 @@ void launch_zero(double* p, size_t n, cudaStream_t st);
 // Camera output (a+b/2 quirk) and the unscaled 9x9 camera covariance blocks.
 void launch_camera_output(const double* iZ, int ldz, const double* s_cam, int num_cams,
                           double* cam_unc, double* sig, cudaStream_t st);
+
+// ---------------- mixed.cu ----------------
+// A symmetric FP64 operand sliced into `slices` int8 planes for the tcgen05
+// (kind::i8) products, with its TMA descriptor and per-row exponents.
+struct MixedOperand {
+    CUtensorMap map;
+    int8_t* buf;   // slices x rows x kp bytes, zero padding
+    int* exps;     // n row exponents
+    int n, slices, rows, kp;
+};
+int mixed_tile_n(int slices);
+size_t mixed_slice_bytes(int n, int slices);
+// Prepare the operand over buf/exps (as_b: box rows of the B operand). False
+// when the driver's tensor-map encoder is unavailable.
+bool mixed_plan(MixedOperand& op, int8_t* buf, int* exps, int n, int slices, bool as_b);
+void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st);
+// C = P * X from the slices of P (a) and X (b); lower_only: tiles on/below the diagonal.
+void mixed_gemm(const MixedOperand& a, const MixedOperand& b, double* C, int ldc, unsigned long long* amax,
+                bool lower_only, int* err, cudaStream_t st);
 
 // ---------------- points.cu ----------------
 void launch_point_cov(const SceneDev& s, const double* sig, double* pt_unc, cudaStream_t st);

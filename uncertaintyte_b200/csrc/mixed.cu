@@ -1,0 +1,424 @@
+// mixed.cu - mixed-precision Taylor-series products on the sm_100a tensor
+// cores (tcgen05, kind::i8), fed by TMA, accumulated in TMEM.
+//
+// A dense FP64 product C = P * X of symmetric operands is evaluated from
+// 7-bit integer slices of the operands (the Ozaki splitting):
+//
+//   row r of P:  P[r, :] = 2^e_r * (sum_{s=1..S} P_s[r, :] 2^(-7 s) + tail),  P_s int8
+//   row c of X:  X[c, :] = 2^f_c * (sum_{t=1..S} X_t[c, :] 2^(-7 t) + tail)
+//   C[r, c]     = 2^(e_r + f_c) * sum_{L=2..S+1} 2^(-7 L) * sum_{s+t=L} (P_s X_t^T)[r, c]
+//
+// The digits are rounded to nearest (|digit| <= 64, row scale chosen so that
+// |P[r, k]| 2^-e_r < 1/2): the tails are zero-mean, so their contributions
+// partly cancel over K instead of adding up with one sign as truncated digits
+// do. Each slice product is an int8 GEMM with exact int32 accumulation
+// ((L-1) K 64^2 < 2^31 for K < 10^5); products of the same level L share one
+// TMEM accumulator, and the FP64 epilogue combines the levels. The error is
+// about 2^(-7 S) relative to the row/column maxima: S = 5 gives ~1e-10 on the
+// Taylor products of the reference scenes, S = 4 ~1e-8. Both operands are
+// symmetric, so their columns are their rows and the column-major FP64
+// matrices are read as K-major operands.
+//
+// Kernel layout: 128 threads. Warp 0 lane 0 issues the TMA loads of the S
+// slices of both operands per 64-byte K block (3-stage mbarrier pipeline);
+// warp 1 lane 0 issues the tcgen05.mma (M = 128, N = 128, K = 32 bytes) and
+// commits each stage back to the producer; all four warps then read the
+// accumulators with tcgen05.ld and write FP64. Every mbarrier wait has an
+// iteration limit after which the kernel records ERRBIT_TIMEOUT and unwinds
+// (TMEM is always freed).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "internal.h"
+
+namespace unc {
+
+namespace mp {
+
+constexpr int BM = 128;         // tile rows (TMEM lanes)
+constexpr int BKB = 64;         // K bytes per pipeline stage (SWIZZLE_64B rows)
+constexpr int STAGES = 3;
+constexpr int THREADS = 128;
+constexpr long kSpinLimit = 1L << 26;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// bounded wait for the completion of phase `parity`; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+    const unsigned a = smem_u32(bar);
+    for (long it = 0; it < kSpinLimit; ++it) {
+        unsigned ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::
+            "r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// K-major shared-memory matrix descriptor, 64-byte swizzle: rows of 64 bytes,
+// 8-row groups 512 bytes apart (SBO), version 1 (sm_100).
+__device__ __forceinline__ uint64_t desc_sw64(const void* p) {
+    const uint64_t addr = smem_u32(p);
+    return ((addr >> 4) & 0x3FFFull) | (1ull << 16) | ((uint64_t)(512 >> 4) << 32) | (1ull << 46) |
+           (4ull << 61);
+}
+
+// instruction descriptor: kind::i8, signed A/B, S32 accumulate, K-major, M=128, N=n
+__host__ __device__ constexpr uint32_t idesc_i8(int n) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, bool acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc ? 1u : 0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+template <int NT, int S>
+struct Shape {
+    static constexpr int A_BOX = BM * BKB;                 // bytes of one A slice box
+    static constexpr int B_BOX = NT * BKB;                 // bytes of one B slice box
+    static constexpr int STAGE = S * (A_BOX + B_BOX);
+    static constexpr int LEVELS = S;                       // L = 2 .. S+1
+    static constexpr int TMEM_COLS = LEVELS * NT <= 256 ? (LEVELS * NT <= 128 ? 128 : 256) : 512;
+    static constexpr int SMEM = STAGES * STAGE + 1024 /*align*/ + 256 /*barriers*/;
+    static_assert(LEVELS * NT <= 512, "TMEM holds at most 512 accumulator columns");
+};
+
+}  // namespace mp
+
+using namespace mp;
+
+// Slice rows of a symmetric FP64 matrix (row j = column j, contiguous) into S
+// int8 planes out[s][j][k] (pitch kp bytes, plane stride rows_pad * kp) of
+// round-to-nearest digits in [-64, 64], and the row exponents e[j] with
+// max_k |A[j,k]| 2^-e < 1/2. One CTA per row.
+__global__ void __launch_bounds__(256) k_slice_rows(const double* __restrict__ A, long lda, int n, int S,
+                                                   int8_t* __restrict__ out, int rows_pad, int kp,
+                                                   int* __restrict__ exps) {
+    __shared__ double red[8];
+    const int j = blockIdx.x;
+    const double* col = A + (long)j * lda;
+    double m = 0.0;
+    for (int k = threadIdx.x; k < n; k += 256) m = fmax(m, fabs(col[k]));
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, d));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < 8 ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int d = 4; d > 0; d >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, d));
+        if (threadIdx.x == 0) red[0] = v;
+    }
+    __syncthreads();
+    int e = 0;
+    if (red[0] > 0.0 && red[0] <= 1.7976931348623157e308) frexp(red[0], &e);  // max * 2^-e in [0.5, 1)
+    e += 1;                                                                     // max * 2^-e in [0.25, 0.5)
+    if (threadIdx.x == 0) exps[j] = e;
+    const size_t plane = (size_t)rows_pad * kp;
+    int8_t* row = out + (size_t)j * kp;
+    for (int k0 = 4 * threadIdx.x; k0 < n; k0 += 4 * 256) {
+        double v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = (k0 + u < n) ? ldexp(col[k0 + u], -e) : 0.0;
+        for (int s = 0; s < S; ++s) {
+            char4 q;
+            signed char qs[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                v[u] *= 128.0;
+                const double t = rint(v[u]);  // |v| <= 64 before, |v - t| <= 1/2 after
+                v[u] -= t;
+                qs[u] = (signed char)(int)t;
+            }
+            q.x = qs[0];
+            q.y = qs[1];
+            q.z = qs[2];
+            q.w = qs[3];
+            if (k0 + 3 < n) {
+                *reinterpret_cast<char4*>(row + s * plane + k0) = q;
+            } else {
+                for (int u = 0; u < 4 && k0 + u < n; ++u) row[s * plane + k0 + u] = qs[u];
+            }
+        }
+    }
+}
+
+template <int NT, int S>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_ozaki_gemm(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int M, int N,
+                 int kp, int rowsA, int rowsB, const int* __restrict__ eA, const int* __restrict__ eB, double* C,
+                 long ldc, unsigned long long* amax, int lower_only, int* err) {
+    using Sh = Shape<NT, S>;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * NT;
+    if (lower_only && n0 > m0 + BM - 1) return;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * Sh::STAGE);
+    uint64_t* empty = full + STAGES;
+    uint64_t* done = empty + STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                     "r"(Sh::TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 32) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full + s, 1);
+            mbar_init(empty + s, 1);
+        }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const int KT = kp / BKB;
+
+    if (warp == 0) {
+      if (lane == 0) {
+        // TMA producer
+        bool ok = true;
+        int issued = 0;
+        for (int kt = 0; kt < KT && ok; ++kt) {
+            const int s = kt % STAGES;
+            const unsigned ph = (unsigned)(kt / STAGES) & 1u;
+            if (kt >= STAGES && !mbar_wait(empty + s, ph ^ 1u)) {
+                atomicOr(err, ERRBIT_TIMEOUT);
+                ok = false;
+                break;
+            }
+            uint8_t* st = base + s * Sh::STAGE;
+            mbar_expect_tx(full + s, Sh::STAGE);
+            for (int i = 0; i < S; ++i) tma_load_2d(st + i * Sh::A_BOX, &tA, kt * BKB, i * rowsA + m0, full + s);
+            for (int i = 0; i < S; ++i)
+                tma_load_2d(st + S * Sh::A_BOX + i * Sh::B_BOX, &tB, kt * BKB, i * rowsB + n0, full + s);
+            issued = kt + 1;
+        }
+        // no copy may be in flight when the CTA exits
+        for (int kt = issued - STAGES < 0 ? 0 : issued - STAGES; kt < issued; ++kt)
+            if (!mbar_wait(full + kt % STAGES, (unsigned)(kt / STAGES) & 1u)) atomicOr(err, ERRBIT_TIMEOUT);
+      }
+      __syncwarp();
+    } else if (warp == 1) {
+      if (lane == 0) {
+        // MMA issuer
+        const uint32_t idesc = idesc_i8(NT);
+        bool started[S];
+#pragma unroll
+        for (int l = 0; l < S; ++l) started[l] = false;
+        for (int kt = 0; kt < KT; ++kt) {
+            const int s = kt % STAGES;
+            if (!mbar_wait(full + s, (unsigned)(kt / STAGES) & 1u)) {
+                atomicOr(err, ERRBIT_TIMEOUT);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint8_t* st = base + s * Sh::STAGE;
+#pragma unroll
+            for (int kk = 0; kk < BKB / 32; ++kk) {
+#pragma unroll
+                for (int sa = 1; sa <= S; ++sa)
+#pragma unroll
+                    for (int sb = 1; sb <= S; ++sb) {
+                        if (sa + sb > S + 1) continue;
+                        const int l = sa + sb - 2;
+                        const uint64_t a = desc_sw64(st + (sa - 1) * Sh::A_BOX + kk * 32);
+                        const uint64_t b = desc_sw64(st + S * Sh::A_BOX + (sb - 1) * Sh::B_BOX + kk * 32);
+                        mma_i8(tmem + (uint32_t)(l * NT), a, b, idesc, started[l]);
+                        started[l] = true;
+                    }
+            }
+            mma_commit(empty + s);  // stage free once these MMAs completed
+        }
+        mma_commit(done);
+      }
+      __syncwarp();
+    }
+    // epilogue: every warp reads its 32 TMEM lanes (tile rows)
+    const bool ok = mbar_wait(done, 0);
+    if (!ok && lane == 0) atomicOr(err, ERRBIT_TIMEOUT);
+    __syncwarp();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const int row = m0 + warp * 32 + lane;
+    const int er = row < M ? eA[row] : 0;
+    double mx = 0.0;
+    if (ok) {
+        for (int c0 = 0; c0 < NT; c0 += 16) {
+            double v[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = 0.0;
+#pragma unroll
+            for (int l = S - 1; l >= 0; --l) {  // small levels first
+                int r[16];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(l * NT + c0), r);
+                const double w = ldexp(1.0, -7 * (l + 2));
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] += (double)r[j] * w;
+            }
+            if (row < M) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int col = n0 + c0 + j;
+                    if (col < N) {
+                        const double x = ldexp(v[j], er + eB[col]);
+                        C[row + (long)col * ldc] = x;
+                        const double ax = fabs(x);
+                        mx = fmax(mx, ax <= 1.7976931348623157e308 ? ax : __longlong_as_double(0x7ff0000000000000LL));
+                    }
+                }
+            }
+        }
+    }
+    if (amax) {
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, d));
+        if (lane == 0) atomicMax(amax, (unsigned long long)__double_as_longlong(mx));
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(Sh::TMEM_COLS));
+}
+
+// ------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 2-D map over `rows` rows of `kp` int8 (row pitch kp bytes), box = box_rows x 64 bytes, 64-byte swizzle
+bool make_map(CUtensorMap* map, const int8_t* base, int rows, int kp, int box_rows) {
+    auto enc = get_encode();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)kp};
+    cuuint32_t box[2] = {(cuuint32_t)BKB, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+template <int NT, int S>
+void set_attr_once() {
+    static bool done = false;
+    if (!done) {
+        cudaFuncSetAttribute(k_ozaki_gemm<NT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, Shape<NT, S>::SMEM);
+        done = true;
+    }
+}
+}  // namespace
+
+int mixed_tile_n(int slices) { return slices <= 4 ? 128 : 96; }  // slices * tile_n <= 512 TMEM columns
+
+static int mixed_rows(int n, int slices) {
+    const int nt = mixed_tile_n(slices);
+    const int ra = ((n + BM - 1) / BM) * BM, rb = ((n + nt - 1) / nt) * nt;
+    return ra > rb ? ra : rb;
+}
+
+size_t mixed_slice_bytes(int n, int slices) {
+    const int kp = ((n + BKB - 1) / BKB) * BKB;
+    return (size_t)slices * (size_t)mixed_rows(n, slices) * kp;
+}
+
+bool mixed_plan(MixedOperand& op, int8_t* buf, int* exps, int n, int slices, bool as_b) {
+    const int nt = mixed_tile_n(slices);
+    op.n = n;
+    op.slices = slices;
+    op.kp = ((n + BKB - 1) / BKB) * BKB;
+    op.rows = mixed_rows(n, slices);
+    op.buf = buf;
+    op.exps = exps;
+    return make_map(&op.map, buf, op.rows * slices, op.kp, as_b ? nt : BM);
+}
+
+void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st) {
+    k_slice_rows<<<op.n, 256, 0, st>>>(A, lda, op.n, op.slices, op.buf, op.rows, op.kp, op.exps);
+    count_launch();
+}
+
+void mixed_gemm(const MixedOperand& a, const MixedOperand& b, double* C, int ldc, unsigned long long* amax,
+                bool lower_only, int* err, cudaStream_t st) {
+    const int n = a.n;
+    if (a.slices == 4) {
+        set_attr_once<128, 4>();
+        dim3 grid((n + 127) / 128, (n + BM - 1) / BM);
+        k_ozaki_gemm<128, 4><<<grid, THREADS, Shape<128, 4>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
+                                                                         a.exps, b.exps, C, ldc, amax,
+                                                                         lower_only ? 1 : 0, err);
+    } else if (a.slices == 5) {
+        set_attr_once<96, 5>();
+        dim3 grid((n + 95) / 96, (n + BM - 1) / BM);
+        k_ozaki_gemm<96, 5><<<grid, THREADS, Shape<96, 5>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
+                                                                       a.exps, b.exps, C, ldc, amax,
+                                                                       lower_only ? 1 : 0, err);
+    } else {
+        set_attr_once<128, 3>();
+        dim3 grid((n + 127) / 128, (n + BM - 1) / BM);
+        k_ozaki_gemm<128, 3><<<grid, THREADS, Shape<128, 3>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
+                                                                         a.exps, b.exps, C, ldc, amax,
+                                                                         lower_only ? 1 : 0, err);
+    }
+    count_launch();
+}
+
+}  // namespace unc

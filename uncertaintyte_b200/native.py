@@ -21,7 +21,7 @@ UNC_OK = 0
 TAYLOR_EXPANSION = 2
 SVD_QR_ITERATION = 0
 SVD_DEVIDE_AND_CONQUER = 1
-PRECISION = {"fp64": 0, "mixed": 1}
+PRECISION = {"fp64": 0, "mixed": 1, "mixed4": 2, "mixed3": 3}
 
 
 class UncError(RuntimeError):
@@ -79,7 +79,8 @@ class UncStatistic(C.Structure):
 EXPORTS = ("unc_options_init", "unc_context_create", "unc_context_destroy", "unc_compute",
            "unc_context_set_profiling", "unc_context_profile",
            "unc_compute_device", "unc_workspace_bytes", "unc_dense_inverse_device", "unc_jtj_crs",
-           "unc_gemm_f64_device", "unc_status_string", "unc_last_error", "unc_kernel_launches")
+           "unc_gemm_f64_device", "unc_gemm_mixed_device", "unc_status_string", "unc_last_error",
+           "unc_kernel_launches")
 
 _lib = None
 
@@ -110,6 +111,7 @@ def lib():
                               vp, vp]
     L.unc_gemm_f64_device.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, vp, C.c_int, vp, C.c_int,
                                       C.c_double, vp, C.c_int, vp]
+    L.unc_gemm_mixed_device.argtypes = [C.c_int, vp, vp, C.c_int, vp, C.c_int, vp]
     L.unc_status_string.argtypes = [C.c_int]
     L.unc_status_string.restype = C.c_char_p
     L.unc_last_error.restype = C.c_char_p
@@ -235,6 +237,11 @@ def jtj_crs(num_rows: int, num_cols: int, rows, cols, vals, num_cams: int, cam_p
 def gemm_f64_device(M, N, K, alpha, d_A, lda, d_B, ldb, beta, d_C, ldc, stream: int = 0) -> None:
     """C = alpha A B + beta C (column-major device pointers) on the FP64 GEMM kernel."""
     _check(lib().unc_gemm_f64_device(M, N, K, alpha, d_A, lda, d_B, ldb, beta, d_C, ldc, stream or None))
+
+
+def gemm_mixed_device(n, d_P, d_X, ld, d_C, slices=4, stream: int = 0) -> None:
+    """C = P X for symmetric P, X on the int8-sliced tensor-core product."""
+    _check(lib().unc_gemm_mixed_device(n, d_P, d_X, ld, d_C, slices, stream or None))
 
 
 def kernel_launches() -> int:
