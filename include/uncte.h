@@ -121,6 +121,17 @@ long long unc_workspace_bytes(const unc_options* opt, int num_rows, int num_cols
  * Gauss-Jordan elimination on the GPU. Scratch is allocated per call. */
 int unc_dense_inverse_device(double* d_A, int n, int lda, void* stream);
 
+/* The same SPD inverse as unc_dense_inverse_device, for callers that cannot
+ * let a library allocate device memory (their device memory is reserved by
+ * their own pool allocator, or cudaMalloc/cudaFree would stall a latency-
+ * critical loop). No counterpart in the reference. It allocates nothing: its
+ * scratch is a fixed __device__ array of about 6.3 MB held by every device the
+ * library is loaded on, so n and lda are limited to 512 (UNC_ERR_TOO_LARGE
+ * beyond). All calls on a device share that array; calls that overlap on the
+ * GPU race. The first call on a device looks up the array's address; make it
+ * before any stream capture. Synchronous, like unc_dense_inverse_device. */
+int unc_dense_inverse_noalloc(double* d_A, int n, int lda, void* stream);
+
 /* SSM J^T J (trn() then operator*, ScaledSparseMatrix.cpp:384-388,517-539)
  * computed by the GPU block-assembly kernels and returned as host CRS in the
  * reference's pattern. Observations may have 12-entry rows (camera + point)
