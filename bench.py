@@ -53,7 +53,7 @@ UNIT = "solves/s"
 def _args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="medium")
@@ -81,19 +81,49 @@ class ClockSampler:
         self.device = device
         self.proc = None
 
-    def start(self):
+    def start(self, wait_s: float = 5.0):
+        """Start sampling; return once the first sample arrived (or after wait_s)."""
+        import threading
+        self.lines = []
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return
+        first = threading.Event()
+
+        def reader():
+            for line in self.proc.stdout:
+                self.lines.append((time.monotonic(), line))
+                first.set()
+
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+        first.wait(wait_s)
+
+    def mark(self, begin: bool):
+        """Bracket the timed region (host time just before / after it)."""
+        if begin:
+            self.t0 = time.monotonic()
+        else:
+            self.t1 = time.monotonic()
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
-        out, _ = self.proc.communicate(timeout=10)
+        try:
+            self.proc.wait(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=10)
+        t0, t1 = getattr(self, "t0", None), getattr(self, "t1", None)
+        inside = [ln for t, ln in self.lines if t0 is None or t0 <= t <= t1 + 0.06]
+        if not inside:  # region shorter than one sample: the first sample after it started
+            inside = [ln for t, ln in self.lines if t0 is None or t >= t0][:1]
+        out = "".join(inside)
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in out.strip().splitlines():
@@ -244,7 +274,7 @@ def run_ours(a):
                                                  d_cols.data_ptr(), d_vals.data_ptr(), d_cam.data_ptr(),
                                                  d_pt.data_ptr(), sptr)
 
-    def timed(o, steps, profile=False):
+    def timed(o, steps, profile=False, clocks=None):
         for _ in range(max(a.warmup, 0)):
             flush.zero_()
             step(o)
@@ -256,6 +286,8 @@ def run_ours(a):
             dist.barrier()
         torch.cuda.synchronize()
         l0 = native.kernel_launches()
+        if clocks is not None:
+            clocks.mark(True)
         evs, st = [], None
         for _ in range(steps):
             flush.zero_()
@@ -265,6 +297,8 @@ def run_ours(a):
             e1.record(stream)
             evs.append((e0, e1))
         torch.cuda.synchronize()
+        if clocks is not None:
+            clocks.mark(False)
         if ws > 1:
             dist.barrier()
         launches = native.kernel_launches() - l0
@@ -278,7 +312,7 @@ def run_ours(a):
     # headline: the requested precision (mixed by default), clocks sampled during it
     clocks = ClockSampler(local)
     clocks.start()
-    t_main, stats, launches, prof = timed(opts, a.steps, profile=True)
+    t_main, stats, launches, prof = timed(opts, a.steps, profile=True, clocks=clocks)
     clk = clocks.stop()
     cam_main, pt_main = d_cam.cpu().numpy().copy(), d_pt.cpu().numpy().copy()
     value = ws * a.steps / t_main

@@ -156,7 +156,7 @@ def test_dense_inverse_golden_spd():
 
 def test_dense_inverse_random_spd_sizes():
     rng = np.random.default_rng(0)
-    for n in (1, 7, 64, 65, 130, 700):
+    for n in (1, 7, 64, 65, 127, 130, 257, 700, 1801):
         Q = rng.standard_normal((n, n))
         A = Q @ Q.T + n * np.eye(n)
         Ai = _dense_inverse_gpu(A)

@@ -2,12 +2,15 @@
 // complement (sm_100a):
 //   * gemm_f64      : C = alpha*A*B + beta*C on DMMA (mma.sync m8n8k4 f64),
 //                     4-stage cp.async pipeline, optional fused max|C| for the
-//                     Taylor stop rule (ScaledDenseMatrix.cpp:207-216,314-353).
-//   * gj_inverse    : blocked Gauss-Jordan inverse of an SPD matrix; every
-//                     panel step is a rank-nb update on gemm_f64
+//                     Taylor stop rule (ScaledDenseMatrix.cpp:207-216,314-353),
+//                     lower-tile and triangular-operand (k range per tile) modes.
+//   * chol_inverse  : SPD inverse by recursive Cholesky that forms T = L^{-1}
+//                     on the way, then A^{-1} = T^T T; every step is a GEMM
 //                     (replaces dgetrf+dgetri in SDM::inv, ScaledDenseMatrix.cpp:232-279).
 //   * shift/equilibrate, un-equilibrate, axpy (iZupdate, compute.cpp:64-71),
 //     camera output with the reference's (a + b/2) quirk (compute.cpp:168-183).
+#include <algorithm>
+
 #include "internal.h"
 
 namespace unc {
@@ -84,9 +87,9 @@ template <bool kTransB>
 __global__ void __launch_bounds__(GEMM_THREADS, 1)
     k_gemm_f64(int M, int N, int K, double alpha, const double* __restrict__ A, long lda,
                const double* __restrict__ B, long ldb, double beta, double* C, long ldc,
-               unsigned long long* amax, int lower_only) {
-    // lower_only: tiles strictly above the diagonal of C are skipped (SYRK-style update)
-    if (lower_only && (int)(blockIdx.x * BN) > (int)(blockIdx.y * BM) + BM - 1) return;
+               unsigned long long* amax, int mode, double* part) {
+    // GEMM_LOWER: tiles strictly above the diagonal of C are skipped (SYRK-style update)
+    if ((mode & GEMM_LOWER) && (int)(blockIdx.x * BN) > (int)(blockIdx.y * BM) + BM - 1) return;
     extern __shared__ __align__(16) double smem[];
     double* As = smem;
     double* Bs = smem + STAGES * A_STAGE;
@@ -94,7 +97,21 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     const int wm = (warp & 3) * 32, wn = (warp >> 2) * 64;
     const int g = lane >> 2, t = lane & 3;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    const int KT = (K + BK - 1) / BK;
+    const bool wact = (m0 + wm < M) && (n0 + wn < N);
+    // triangular operands: the k range of this tile outside which a product term is zero
+    int kbeg = 0, kend = K;
+    if (mode & GEMM_KLO_M) kbeg = max(kbeg, m0);
+    if (mode & GEMM_KLO_N) kbeg = max(kbeg, n0);
+    if (mode & GEMM_KHI_M) kend = min(kend, m0 + BM);
+    if (mode & GEMM_KHI_N) kend = min(kend, n0 + BN);
+    int kt0 = kbeg / BK;
+    int KT = kend > kbeg ? (kend + BK - 1) / BK - kt0 : 0;  // k tiles of this output tile
+    if (gridDim.z > 1) {  // split-K: a contiguous share of the k tiles, partial sums to part
+        const int chunk = (KT + gridDim.z - 1) / gridDim.z;
+        const int b0 = min(KT, (int)blockIdx.z * chunk);
+        KT = min(KT, b0 + chunk) - b0;
+        kt0 += b0;
+    }
 
     double acc[4][8][2];
 #pragma unroll
@@ -104,7 +121,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
 
 #pragma unroll
     for (int s = 0; s < STAGES - 1; ++s) {
-        if (s < KT) load_tiles<kTransB>(As + s * A_STAGE, Bs + s * B_STAGE, A, lda, B, ldb, M, N, K, m0, n0, s * BK, tid);
+        if (s < KT)
+            load_tiles<kTransB>(As + s * A_STAGE, Bs + s * B_STAGE, A, lda, B, ldb, M, N, K, m0, n0,
+                                (kt0 + s) * BK, tid);
         cp_async_commit();
     }
     for (int kt = 0; kt < KT; ++kt) {
@@ -113,11 +132,13 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         int pf = kt + STAGES - 1;
         if (pf < KT) {
             int ps = pf % STAGES;
-            load_tiles<kTransB>(As + ps * A_STAGE, Bs + ps * B_STAGE, A, lda, B, ldb, M, N, K, m0, n0, pf * BK, tid);
+            load_tiles<kTransB>(As + ps * A_STAGE, Bs + ps * B_STAGE, A, lda, B, ldb, M, N, K, m0, n0,
+                                (kt0 + pf) * BK, tid);
         }
         cp_async_commit();
         const double* as = As + (kt % STAGES) * A_STAGE;
         const double* bs = Bs + (kt % STAGES) * B_STAGE;
+        if (!wact) continue;  // this warp's 32 x 64 sub-tile lies outside C
 #pragma unroll
         for (int kk = 0; kk < BK; kk += 4) {
             double af[4], bf[8];
@@ -133,6 +154,22 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         }
     }
     cp_async_wait<0>();
+
+    if (part) {  // raw partial tile of split blockIdx.z (M x N slab, leading dimension M)
+        double* P = part + (size_t)blockIdx.z * M * N;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            int row = m0 + wm + i * 8 + g;
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    int col = n0 + wn + j * 8 + t * 2 + h;
+                    if (row < M && col < N) P[row + (size_t)col * M] = acc[i][j][h];
+                }
+        }
+        return;
+    }
 
     double mx = 0.0;
 #pragma unroll
@@ -161,9 +198,36 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     }
 }
 
-void gemm_f64_ex(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
-                 double beta, double* C, int ldc, unsigned long long* amax, bool lower_only, cudaStream_t st,
-                 bool trans_b) {
+// C = alpha * sum_s part[s] + beta * C over the tiles the GEMM computed, the
+// splits summed in a fixed order (deterministic), max|C| folded into amax.
+__global__ void k_splitk_reduce(int M, int N, int splits, const double* __restrict__ part, double alpha,
+                                double beta, double* C, long ldc, unsigned long long* amax, int mode) {
+    const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    double mx = 0.0;
+    if (idx < (long)M * N) {
+        const int col = (int)(idx / M), row = (int)(idx - (long)col * M);
+        if (!((mode & GEMM_LOWER) && (col / BN) * BN > (row / BM) * BM + BM - 1)) {
+            double v = 0.0;
+            for (int s = 0; s < splits; ++s) v += part[(size_t)s * M * N + idx];
+            double* c = C + row + (long)col * ldc;
+            v *= alpha;
+            if (beta != 0.0) v += beta * *c;
+            *c = v;
+            const double av = fabs(v);
+            mx = av <= 1.7976931348623157e308 ? av : __longlong_as_double(0x7ff0000000000000LL);
+        }
+    }
+    if (amax) {
+        const int lane = threadIdx.x & 31;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, d));
+        if (lane == 0 && mx > 0.0) atomicMax(amax, (unsigned long long)__double_as_longlong(mx));
+    }
+}
+
+void gemm_f64_mode(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
+                   double beta, double* C, int ldc, unsigned long long* amax, int mode, cudaStream_t st,
+                   double* ws, size_t ws_doubles) {
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_gemm_f64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
@@ -172,13 +236,45 @@ void gemm_f64_ex(int M, int N, int K, double alpha, const double* A, int lda, co
     }
     if (M <= 0 || N <= 0) return;
     dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-    if (trans_b)
+    // split-K when the output has too few tiles to fill the SMs: each split
+    // keeps at least kMinSplitTiles k tiles, the partial slabs fit in ws
+    int tiles = 0;
+    if (mode & GEMM_LOWER) {
+        for (unsigned by = 0; by < grid.y; ++by)
+            for (unsigned bx = 0; bx < grid.x; ++bx) tiles += (int)(bx * BN) <= (int)(by * BM) + BM - 1;
+    } else {
+        tiles = (int)(grid.x * grid.y);
+    }
+    constexpr int kSMs = 148, kMinSplitTiles = 3, kMaxSplits = 16;
+    int splits = 1;
+    const int kt = (K + BK - 1) / BK;
+    if (ws && tiles > 0 && tiles < kSMs && kt >= 2 * kMinSplitTiles) {
+        splits = std::min(std::min(kSMs / tiles, kt / kMinSplitTiles), kMaxSplits);
+        const size_t slab = (size_t)M * N;
+        while (splits > 1 && (size_t)splits * slab > ws_doubles) --splits;
+    }
+    double* part = splits > 1 ? ws : nullptr;
+    grid.z = splits;
+    if (mode & GEMM_TRANS_B)
         k_gemm_f64<true><<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,
-                                                                amax, lower_only ? 1 : 0);
+                                                                amax, mode, part);
     else
         k_gemm_f64<false><<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,
-                                                                 amax, lower_only ? 1 : 0);
+                                                                 amax, mode, part);
     count_launch();
+    if (part) {
+        const long total = (long)M * N;
+        k_splitk_reduce<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(M, N, splits, part, alpha, beta, C, ldc,
+                                                                          amax, mode);
+        count_launch();
+    }
+}
+
+void gemm_f64_ex(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
+                 double beta, double* C, int ldc, unsigned long long* amax, bool lower_only, cudaStream_t st,
+                 bool trans_b) {
+    gemm_f64_mode(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, amax,
+                  (lower_only ? GEMM_LOWER : 0) | (trans_b ? GEMM_TRANS_B : 0), st);
 }
 
 void gemm_f64(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
@@ -215,102 +311,106 @@ void launch_mirror_lower(double* Z, int n, int ld, cudaStream_t st) {
 }
 
 // ------------------------------------------------------------------------
-// SPD inverse: blocked Cholesky A = L L^T, T = L^{-1}, A^{-1} = T^T T
+// SPD inverse: recursive Cholesky A = L L^T that forms T = L^{-1} on the
+// way, then A^{-1} = T^T T
 // ------------------------------------------------------------------------
-constexpr int NB = 64;                       // panel width
+constexpr int NB = 64;  // leaf size
 
 size_t chol_small_doubles(int n) { (void)n; return (size_t)NB * NB + 64; }
 
-// Cholesky of the kb x kb (kb <= 64) diagonal block at (k0, k0) and the
-// inverse of its factor in one CTA of 1024 threads. Thread t owns the
-// lower-triangle elements e = t and e = t + 1024 (row-major packing of the
-// 2080 elements of a 64 x 64 lower triangle) in registers, both of L and of
-// T = L^{-1}. Every elimination step publishes one column (and one row of T)
-// through shared memory and costs two barriers; the pivot scale rsqrt(d) is
-// applied on the fly, so no extra pass is needed.
-// Writes L_kk into A (lower), T_kk into the diagonal block of T, and T_kk^T
-// into LinvT (64 x 64, column-major: LinvT[k + 64 q] = T_kk(q, k)), the B
-// operand of the panel solve L_ik = A_ik T_kk^T.
-constexpr int kTri = NB * (NB + 1) / 2;  // 2080
+// Leaf: Cholesky of the kb x kb (kb <= 64) diagonal block of A at (k0, k0)
+// and T_kk = L_kk^{-1}, written as a full kb x kb block of T (zeros above the
+// diagonal). One CTA of 256 threads; the block and its inverse live in shared
+// memory and every loop stays rolled (a fully unrolled elimination is
+// instruction-fetch bound: each instruction would run once).
+//  * factor, step p: rank-1 update of the trailing square by a 16 x 16 thread
+//    grid (4 x 4 elements per thread, both factors cached in registers);
+//    column p-1 is scaled by 1/sqrt(d) in the same step (nobody reads it any
+//    more), so each step needs a single barrier.
+//  * inverse: forward elimination on [L | I], row p of T scaled one step
+//    later for the same reason.
+// Non-positive or non-finite pivots set ERRBIT_SINGULAR.
+constexpr int LEAF_THREADS = 256;
+constexpr int LEAF_LD = NB + 1;
+constexpr size_t LEAF_SMEM = sizeof(double) * (2 * NB * LEAF_LD + 2 * NB);
 
-__device__ __forceinline__ void tri_rc(int e, int& i, int& j) {
-    // e = i (i + 1) / 2 + j, 0 <= j <= i
-    int r = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
-    while ((r + 1) * (r + 2) / 2 <= e) ++r;
-    while (r * (r + 1) / 2 > e) --r;
-    i = r;
-    j = e - r * (r + 1) / 2;
-}
-
-__global__ void __launch_bounds__(1024) k_chol_diag(double* A, long lda, int k0, int kb, double* T, long ldt,
-                                                    double* LinvT, int* err) {
-    __shared__ double colv[NB], rowt[NB], ilv[NB];
-    const int tid = threadIdx.x;
-    constexpr int E = (kTri + 1023) / 1024;  // 3 elements for the first threads, 2 for the rest
-    int ii[E], jj[E];
-    bool v[E];
-    double a[E], t[E];
-#pragma unroll
-    for (int k = 0; k < E; ++k) {
-        const int e = tid + 1024 * k;
-        if (e < kTri) {
-            tri_rc(e, ii[k], jj[k]);
-        } else {
-            ii[k] = jj[k] = 0;
-        }
-        v[k] = e < kTri && ii[k] < kb;
-        a[k] = v[k] ? A[(k0 + ii[k]) + (long)(k0 + jj[k]) * lda] : 0.0;
+__global__ void __launch_bounds__(LEAF_THREADS) k_chol_leaf(const double* __restrict__ A, long lda, int k0,
+                                                            int kb, double* T, long ldt, int* err) {
+    extern __shared__ __align__(16) double lsm[];
+    double* S = lsm;                     // S[i * LEAF_LD + j]: the block, then L (lower)
+    double* Ts = lsm + NB * LEAF_LD;     // T = L^{-1}
+    double* rs = Ts + NB * LEAF_LD;      // 1 / sqrt(pivot)
+    double* ri = rs + NB;                // 1 / L(p, p)
+    const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+    for (int e = tid; e < NB * NB; e += LEAF_THREADS) {
+        const int i = e & (NB - 1), j = e >> 6;  // column-major walk: coalesced reads of A
+        S[i * LEAF_LD + j] = (i < kb && j < kb && j <= i) ? A[(k0 + i) + (long)(k0 + j) * lda] : 0.0;
+        Ts[i * LEAF_LD + j] = (i == j && i < kb) ? 1.0 : 0.0;
     }
+    __syncthreads();
     for (int p = 0; p < kb; ++p) {
-#pragma unroll
-        for (int k = 0; k < E; ++k)
-            if (v[k] && jj[k] == p) colv[ii[k]] = a[k];
-        __syncthreads();
-        const double d = colv[p];
+        const double d = S[p * LEAF_LD + p];
         const double r = rsqrt(d);
         if (tid == 0) {
-            ilv[p] = r;
+            rs[p] = r;
             if (!(d > 0.0 && d <= 1.7976931348623157e308)) atomicOr(err, ERRBIT_SINGULAR);
         }
-#pragma unroll
-        for (int k = 0; k < E; ++k) {
-            if (!v[k]) continue;
-            if (jj[k] == p) a[k] = (ii[k] == p) ? d * r : a[k] * r;
-            else if (jj[k] > p) a[k] -= (colv[ii[k]] * r) * (colv[jj[k]] * r);
+        if (p > 0 && tid < kb - p + 1) {  // delayed scaling of column p - 1 (rows >= p - 1)
+            const int i = p - 1 + tid;
+            S[i * LEAF_LD + p - 1] *= rs[p - 1];
         }
-        __syncthreads();
-    }
-    // T = L^{-1}: forward elimination on [L | I]
+        double ci[4], cj[4];
 #pragma unroll
-    for (int k = 0; k < E; ++k) t[k] = (v[k] && ii[k] == jj[k]) ? 1.0 : 0.0;
-    for (int p = 0; p < kb; ++p) {
-        const double r = ilv[p];
+        for (int u = 0; u < 4; ++u) {
+            const int i = p + 1 + ty + 16 * u, j = p + 1 + tx + 16 * u;
+            ci[u] = i < kb ? S[i * LEAF_LD + p] * r : 0.0;
+            cj[u] = j < kb ? S[j * LEAF_LD + p] * r : 0.0;
+        }
 #pragma unroll
-        for (int k = 0; k < E; ++k) {
-            if (!v[k]) continue;
-            if (ii[k] == p) {
-                t[k] *= r;
-                rowt[jj[k]] = t[k];
-            } else if (jj[k] == p && ii[k] > p) {
-                colv[ii[k]] = a[k];
+        for (int u = 0; u < 4; ++u) {
+            const int i = p + 1 + ty + 16 * u;
+            if (i >= kb) break;
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                const int j = p + 1 + tx + 16 * w;
+                if (j > i) break;
+                S[i * LEAF_LD + j] -= ci[u] * cj[w];
             }
         }
         __syncthreads();
+    }
+    if (tid == 0 && kb > 0) S[(kb - 1) * LEAF_LD + kb - 1] *= rs[kb - 1];
+    __syncthreads();
+    if (tid < kb) ri[tid] = 1.0 / S[tid * LEAF_LD + tid];
+    __syncthreads();
+    for (int p = 0; p < kb; ++p) {
+        const double ip = ri[p];
+        if (p > 0 && tid < p) Ts[(p - 1) * LEAF_LD + tid] *= ri[p - 1];  // delayed scaling of row p - 1
+        double tp[4];
 #pragma unroll
-        for (int k = 0; k < E; ++k)
-            if (v[k] && ii[k] > p && jj[k] <= p) t[k] -= colv[ii[k]] * rowt[jj[k]];
+        for (int w = 0; w < 4; ++w) {
+            const int j = tx + 16 * w;
+            tp[w] = j <= p ? Ts[p * LEAF_LD + j] * ip : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = p + 1 + ty + 16 * u;
+            if (i >= kb) break;
+            const double lip = S[i * LEAF_LD + p];
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                const int j = tx + 16 * w;
+                if (j > p) break;
+                Ts[i * LEAF_LD + j] -= lip * tp[w];
+            }
+        }
         __syncthreads();
     }
-    for (int e = tid; e < NB * NB; e += 1024) LinvT[e] = 0.0;
+    if (kb > 0 && tid < kb) Ts[(kb - 1) * LEAF_LD + tid] *= ri[kb - 1];
     __syncthreads();
-#pragma unroll
-    for (int k = 0; k < E; ++k) {
-        if (!v[k]) continue;
-        const int i = ii[k], j = jj[k];
-        A[(k0 + i) + (long)(k0 + j) * lda] = a[k];
-        T[(k0 + i) + (long)(k0 + j) * ldt] = t[k];
-        if (i != j) T[(k0 + j) + (long)(k0 + i) * ldt] = 0.0;
-        LinvT[j + (long)i * NB] = t[k];  // LinvT(k = j, q = i) = T(i, j)
+    for (int e = tid; e < kb * kb; e += LEAF_THREADS) {
+        const int j = e / kb, i = e - j * kb;  // column-major walk: coalesced writes of T
+        T[(k0 + i) + (long)(k0 + j) * ldt] = Ts[i * LEAF_LD + j];
     }
 }
 
@@ -331,50 +431,55 @@ __global__ void k_transpose(const double* __restrict__ T, long ldt, int n, doubl
 
 namespace {
 
-// T[r0:r1, r0:r1] = inverse of L[r0:r1, r0:r1] given the inverted leaves:
-// T21 = -T22 * (L21 * T11), split at a multiple of 64.
-void trtri_merge(const double* L, int lda, double* T, int ldt, double* W, int ldw, int r0, int r1,
-                 cudaStream_t st) {
-    if (r1 - r0 <= NB) return;
-    int half = (r1 - r0) / 2;
-    int m = r0 + ((half + NB - 1) / NB) * NB;
+// Factor A[r0:r1, r0:r1] (already updated by the earlier panels) and write
+// T[r0:r1, r0:r1] = L^{-1}. With the split [r0, m) [m, r1):
+//   L21 = A21 T11^T                 (into W; T11^T upper triangular)
+//   A22 -= L21 L21^T                (lower tiles)
+//   X   = L21 T11                   (into the A21 slot; T11 lower triangular)
+//   recurse on A22 -> T22
+//   T21 = -T22 X                    (T22 lower triangular)
+// Every product is a GEMM whose k loop skips the zero triangle of its
+// triangular operand, so the whole recursion costs n^3 / 3 + n^3 / 3 flops.
+void chol_rec(double* A, int lda, double* T, double* W, double* ws, size_t wsd, int r0, int r1, int* err,
+              cudaStream_t st) {
+    const int n = r1 - r0;
+    if (n <= NB) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_chol_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEAF_SMEM);
+            attr = true;
+        }
+        k_chol_leaf<<<1, LEAF_THREADS, LEAF_SMEM, st>>>(A, lda, r0, n, T, lda, err);
+        count_launch();
+        return;
+    }
+    int m = r0 + ((n / 2 + NB - 1) / NB) * NB;
     if (m >= r1) m = r1 - NB;
-    trtri_merge(L, lda, T, ldt, W, ldw, r0, m, st);
-    trtri_merge(L, lda, T, ldt, W, ldw, m, r1, st);
-    const int m2 = r1 - m, m1 = m - r0;
-    gemm_f64(m2, m1, m1, 1.0, L + m + (long)r0 * lda, lda, T + r0 + (long)r0 * ldt, ldt, 0.0, W, ldw,
-             nullptr, st);
-    gemm_f64(m2, m1, m2, -1.0, T + m + (long)m * ldt, ldt, W, ldw, 0.0, T + m + (long)r0 * ldt, ldt,
-             nullptr, st);
+    const int h1 = m - r0, h2 = r1 - m;
+    chol_rec(A, lda, T, W, ws, wsd, r0, m, err, st);
+    double* A21 = A + m + (long)r0 * lda;
+    const double* T11 = T + r0 + (long)r0 * lda;
+    gemm_f64_mode(h2, h1, h1, 1.0, A21, lda, T11, lda, 0.0, W, lda, nullptr, GEMM_TRANS_B | GEMM_KHI_N, st, ws,
+                  wsd);
+    gemm_f64_mode(h2, h2, h1, -1.0, W, lda, W, lda, 1.0, A + m + (long)m * lda, lda, nullptr,
+                  GEMM_TRANS_B | GEMM_LOWER, st, ws, wsd);
+    gemm_f64_mode(h2, h1, h1, 1.0, W, lda, T11, lda, 0.0, A21, lda, nullptr, GEMM_KLO_N, st, ws, wsd);
+    chol_rec(A, lda, T, W, ws, wsd, m, r1, err, st);
+    gemm_f64_mode(h2, h1, h2, -1.0, T + m + (long)m * lda, lda, A21, lda, 0.0, T + m + (long)r0 * lda, lda,
+                  nullptr, GEMM_KHI_M, st, ws, wsd);
 }
 }  // namespace
 
 void chol_inverse(double* A, int n, int lda, double* T, double* W, double* Tt, double* small, int* err,
                   cudaStream_t st) {
-    double* LinvT = small;
-    // 1. blocked right-looking Cholesky (lower triangle of A becomes L); the
-    //    diagonal blocks of T = L^{-1} are produced on the way
-    for (int k0 = 0; k0 < n; k0 += NB) {
-        const int kb = min(NB, n - k0), k1 = k0 + kb;
-        k_chol_diag<<<1, 1024, 0, st>>>(A, lda, k0, kb, T, lda, LinvT, err);
-        count_launch();
-        if (k1 < n) {
-            const int rows = n - k1;
-            double* P = A + k1 + (long)k0 * lda;  // panel below the pivot block
-            // L_ik = A_ik T_kk^T, in place (each CTA owns its rows and all 64 columns)
-            gemm_f64_ex(rows, kb, kb, 1.0, P, lda, LinvT, NB, 0.0, P, lda, nullptr, false, st, false);
-            // A22 -= L_ik L_ik^T, lower tiles; B = panel^T read in place
-            gemm_f64_ex(rows, rows, kb, -1.0, P, lda, P, lda, 1.0, A + k1 + (long)k1 * lda, lda, nullptr, true,
-                        st, true);
-        }
-    }
-    // 2. T = L^{-1}: recursive merges above the inverted diagonal blocks
-    trtri_merge(A, lda, T, lda, W, lda, 0, n, st);
-    // 3. A^{-1} = T^T T (symmetric: lower-triangle tiles, then mirror)
+    (void)small;
+    // Tt is free until the final product: split-K partial sums of the recursion
+    chol_rec(A, lda, T, W, Tt, (size_t)n * lda, 0, n, err, st);
+    // A^{-1} = T^T T: lower tiles, k >= the tile's first row (T lower triangular), then mirror
     dim3 g((n + 31) / 32, (n + 31) / 32);
     k_transpose<<<g, dim3(32, 8), 0, st>>>(T, lda, n, Tt, lda);
     count_launch();
-    gemm_f64_ex(n, n, n, 1.0, Tt, lda, T, lda, 0.0, A, lda, nullptr, true, st, false);
+    gemm_f64_mode(n, n, n, 1.0, Tt, lda, T, lda, 0.0, A, lda, nullptr, GEMM_LOWER | GEMM_KLO_M, st);
     launch_mirror_lower(A, n, lda, st);
 }
 

@@ -90,14 +90,32 @@ void gemm_f64(int M, int N, int K, double alpha, const double* A, int lda, const
 void gemm_f64_ex(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
                  double beta, double* C, int ldc, unsigned long long* amax, bool lower_only, cudaStream_t st,
                  bool trans_b = false);
+// Mode bits of gemm_f64_mode. The k-range bits restrict the k loop of the
+// output tile at (m0, n0) when an operand is triangular (terms outside the
+// range are zero): KLO_M k >= m0, KLO_N k >= n0, KHI_M k < m0 + 128,
+// KHI_N k < n0 + 128 (tile size 128 x 128).
+enum : int {
+    GEMM_LOWER = 1,
+    GEMM_TRANS_B = 2,
+    GEMM_KLO_M = 4,
+    GEMM_KLO_N = 8,
+    GEMM_KHI_M = 16,
+    GEMM_KHI_N = 32,
+};
+// ws (ws_doubles): optional scratch that enables split-K for outputs with
+// fewer tiles than SMs (partials summed in a fixed order by a second kernel).
+void gemm_f64_mode(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
+                   double beta, double* C, int ldc, unsigned long long* amax, int mode, cudaStream_t st,
+                   double* ws = nullptr, size_t ws_doubles = 0);
 void launch_mirror_lower(double* Z, int n, int ld, cudaStream_t st);
 // Same, skipping output tiles strictly above the diagonal (symmetric updates).
 void gemm_f64_tri(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
                   double beta, double* C, int ldc, cudaStream_t st);
-// In-place inverse of an SPD matrix (n x n, lda): blocked Cholesky A = L L^T,
-// T = L^{-1} (recursive, GEMM-based), A^{-1} = T^T T. T, W, Tt: n x lda
-// scratch matrices whose padding rows are zero and whose T is zero on entry;
-// small: chol_small_doubles(n) doubles. Sets ERRBIT_SINGULAR in err.
+// In-place inverse of an SPD matrix (n x n, lda): recursive Cholesky that
+// forms T = L^{-1} directly (64 x 64 leaves, GEMM merges), then A^{-1} = T^T T.
+// T, W, Tt: n x lda scratch matrices, all finite, T zero on entry; small:
+// chol_small_doubles(n) doubles (unused by the recursive form, kept for the
+// workspace layout). Sets ERRBIT_SINGULAR in err.
 size_t chol_small_doubles(int n);
 void chol_inverse(double* A, int n, int lda, double* T, double* W, double* Tt, double* small, int* err,
                   cudaStream_t st);
