@@ -228,17 +228,24 @@ def _int8_peak_tops(torch, dev):
         return None
 
 
+def _lower_tiles(n: int, nt: int) -> int:
+    return sum(min((by * 128 + 127) // nt + 1, (n + nt - 1) // nt) for by in range((n + 127) // 128))
+
+
+def _mixed_tile_n(n: int, slices: int) -> int:
+    """Output tile width of the int8-sliced product (the library's wave-cost rule)."""
+    if slices <= 4:
+        return 128
+    w96, w64 = -(-_lower_tiles(n, 96) // 148), -(-_lower_tiles(n, 64) // 148)
+    return 64 if w64 * 80 < w96 * 112 else 96
+
+
 def _mixed_issued_ops(n: int, slices: int) -> float:
     """int8 multiply-adds x 2 issued by one lower-triangle mixed product."""
-    nt = 128 if slices <= 4 else 96
+    nt = _mixed_tile_n(n, slices)
     kp = (n + 63) // 64 * 64
     pairs = slices * (slices + 1) // 2
-    tiles = 0
-    for by in range((n + 127) // 128):
-        for bx in range((n + nt - 1) // nt):
-            if bx * nt <= by * 128 + 127:
-                tiles += 1
-    return 2.0 * pairs * tiles * 128 * nt * kp
+    return 2.0 * pairs * _lower_tiles(n, nt) * 128 * nt * kp
 
 
 def run_ours(a):
@@ -390,7 +397,8 @@ def run_ours(a):
             ops = _mixed_issued_ops(N, slices) * n_prod
             achieved = ops / prod_s / 1e12
             peak = _int8_peak_tops(torch, dev)
-            roof = {"bound": "tensor", "kernel": f"k_ozaki_gemm (tcgen05 kind::i8, TMA, {slices} slices, lower tiles)",
+            roof = {"bound": "tensor", "kernel": f"k_ozaki_gemm (tcgen05 kind::i8, TMA, {slices} slices, "
+                                                 f"128x{_mixed_tile_n(N, slices)} lower tiles)",
                     "achieved": achieved, "peak": peak, "unit": "TOP/s int8",
                     "frac": (achieved / peak) if peak else None,
                     "traffic": _traffic_from_profile("ozaki", a.workload),

@@ -19,13 +19,28 @@ namespace unc {
 // GEMM
 // ------------------------------------------------------------------------
 namespace {
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 4;
-constexpr int LDA_S = BM + 8;   // As[k][m]: 136 doubles per k row (conflict-free fragment reads)
-constexpr int LDB_S = BK + 4;   // Bs[n][k]: 20 doubles per n row
-constexpr int A_STAGE = BK * LDA_S;
-constexpr int B_STAGE = BN * LDB_S;  // >= BK * LDA_S (layout of a transposed B tile)
-constexpr int GEMM_THREADS = 256;
-constexpr size_t GEMM_SMEM = sizeof(double) * (size_t)STAGES * (A_STAGE + B_STAGE);
+constexpr int BK = 16, STAGES = 4, GEMM_THREADS = 256;
+constexpr int LDB_S = BK + 4;  // Bs[n][k]: 20 doubles per n row (conflict-free fragment reads)
+
+// Output tile BM x BN computed by 8 warps of WM x WN (FM x FN fragments of
+// the 8 x 8 DMMA result). Shared-memory rows are padded by 8 doubles so the
+// fragment reads of a warp hit distinct banks.
+template <int BM_, int BN_, int WM_, int WN_>
+struct GemmCfg {
+    static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_;
+    static constexpr int WARPS_M = BM / WM;
+    static_assert((BM / WM) * (BN / WN) == GEMM_THREADS / 32, "8 warps per CTA");
+    static constexpr int FM = WM / 8, FN = WN / 8;
+    static constexpr int LDA_S = BM + 8;   // As[k][m]
+    static constexpr int LDBT_S = BN + 8;  // Bs[k][n] (transposed B)
+    static constexpr int A_STAGE = BK * LDA_S;
+    static constexpr int B_STAGE = (BN * LDB_S > BK * LDBT_S) ? BN * LDB_S : BK * LDBT_S;
+    static constexpr size_t SMEM = sizeof(double) * (size_t)STAGES * (A_STAGE + B_STAGE);
+    static constexpr int A_CHUNKS = BM * BK / 2 / GEMM_THREADS;  // 16-byte copies per thread
+    static constexpr int B_CHUNKS = BN * BK / 2 / GEMM_THREADS;
+};
+using CfgBig = GemmCfg<128, 128, 32, 64>;   // 1 CTA per SM (151 KB shared)
+using CfgSmall = GemmCfg<64, 64, 16, 32>;   // small outputs: 4x the CTAs (78 KB shared)
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
     unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -48,32 +63,34 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 // Tile loader: A tile (BM rows x BK cols of column-major A), B tile (BK rows
 // x BN cols of column-major B). Out-of-range chunks are zero-filled. Rows
 // past M (or K for B) inside the allocation are read as 16-byte pairs; the
-// buffers keep their padding rows at zero so those reads are inert.
-template <bool kTransB>
+// values there only meet zero-filled partners or land in unstored rows, so
+// they must merely be finite.
+template <class Cfg, bool kTransB>
 __device__ __forceinline__ void load_tiles(double* As, double* Bs, const double* __restrict__ A,
                                            long lda, const double* __restrict__ B, long ldb, int M,
                                            int N, int K, int m0, int n0, int k0, int tid) {
+    constexpr int AH = Cfg::BM / 2, BH = Cfg::BN / 2;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        int idx = tid + q * GEMM_THREADS;  // 0..1023
-        int k = idx >> 6, m2 = (idx & 63) * 2;
+    for (int q = 0; q < Cfg::A_CHUNKS; ++q) {
+        int idx = tid + q * GEMM_THREADS;
+        int k = idx / AH, m2 = (idx % AH) * 2;
         bool p = (m0 + m2 < M) && (k0 + k < K);
         const double* src = p ? A + (m0 + m2) + (long)(k0 + k) * lda : A;
-        cp_async16(As + k * LDA_S + m2, src, p);
+        cp_async16(As + k * Cfg::LDA_S + m2, src, p);
     }
     if (kTransB) {
         // B(k, n) = B[n + k * ldb]: tile stored Bs[k][n] like A
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < Cfg::B_CHUNKS; ++q) {
             int idx = tid + q * GEMM_THREADS;
-            int k = idx >> 6, n2 = (idx & 63) * 2;
+            int k = idx / BH, n2 = (idx % BH) * 2;
             bool p = (n0 + n2 < N) && (k0 + k < K);
             const double* src = p ? B + (n0 + n2) + (long)(k0 + k) * ldb : B;
-            cp_async16(Bs + k * LDA_S + n2, src, p);
+            cp_async16(Bs + k * Cfg::LDBT_S + n2, src, p);
         }
     } else {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < Cfg::B_CHUNKS; ++q) {
             int idx = tid + q * GEMM_THREADS;
             int n = idx >> 3, k2 = (idx & 7) * 2;
             bool p = (n0 + n < N) && (k0 + k2 < K);
@@ -83,18 +100,19 @@ __device__ __forceinline__ void load_tiles(double* As, double* Bs, const double*
     }
 }
 
-template <bool kTransB>
-__global__ void __launch_bounds__(GEMM_THREADS, 1)
+template <class Cfg, bool kTransB>
+__global__ void __launch_bounds__(GEMM_THREADS, (Cfg::BM == 128 ? 1 : 2))
     k_gemm_f64(int M, int N, int K, double alpha, const double* __restrict__ A, long lda,
                const double* __restrict__ B, long ldb, double beta, double* C, long ldc,
                unsigned long long* amax, int mode, double* part) {
+    constexpr int BM = Cfg::BM, BN = Cfg::BN, FM = Cfg::FM, FN = Cfg::FN;
     // GEMM_LOWER: tiles strictly above the diagonal of C are skipped (SYRK-style update)
     if ((mode & GEMM_LOWER) && (int)(blockIdx.x * BN) > (int)(blockIdx.y * BM) + BM - 1) return;
     extern __shared__ __align__(16) double smem[];
     double* As = smem;
-    double* Bs = smem + STAGES * A_STAGE;
+    double* Bs = smem + STAGES * Cfg::A_STAGE;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = (warp & 3) * 32, wn = (warp >> 2) * 64;
+    const int wm = (warp % Cfg::WARPS_M) * Cfg::WM, wn = (warp / Cfg::WARPS_M) * Cfg::WN;
     const int g = lane >> 2, t = lane & 3;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const bool wact = (m0 + wm < M) && (n0 + wn < N);
@@ -113,17 +131,17 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         kt0 += b0;
     }
 
-    double acc[4][8][2];
+    double acc[FM][FN][2];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < FM; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int j = 0; j < FN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
 #pragma unroll
     for (int s = 0; s < STAGES - 1; ++s) {
         if (s < KT)
-            load_tiles<kTransB>(As + s * A_STAGE, Bs + s * B_STAGE, A, lda, B, ldb, M, N, K, m0, n0,
-                                (kt0 + s) * BK, tid);
+            load_tiles<Cfg, kTransB>(As + s * Cfg::A_STAGE, Bs + s * Cfg::B_STAGE, A, lda, B, ldb, M, N, K, m0,
+                                     n0, (kt0 + s) * BK, tid);
         cp_async_commit();
     }
     for (int kt = 0; kt < KT; ++kt) {
@@ -132,25 +150,25 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         int pf = kt + STAGES - 1;
         if (pf < KT) {
             int ps = pf % STAGES;
-            load_tiles<kTransB>(As + ps * A_STAGE, Bs + ps * B_STAGE, A, lda, B, ldb, M, N, K, m0, n0,
-                                (kt0 + pf) * BK, tid);
+            load_tiles<Cfg, kTransB>(As + ps * Cfg::A_STAGE, Bs + ps * Cfg::B_STAGE, A, lda, B, ldb, M, N, K,
+                                     m0, n0, (kt0 + pf) * BK, tid);
         }
         cp_async_commit();
-        const double* as = As + (kt % STAGES) * A_STAGE;
-        const double* bs = Bs + (kt % STAGES) * B_STAGE;
-        if (!wact) continue;  // this warp's 32 x 64 sub-tile lies outside C
+        const double* as = As + (kt % STAGES) * Cfg::A_STAGE;
+        const double* bs = Bs + (kt % STAGES) * Cfg::B_STAGE;
+        if (!wact) continue;  // this warp's sub-tile lies outside C
 #pragma unroll
         for (int kk = 0; kk < BK; kk += 4) {
-            double af[4], bf[8];
+            double af[FM], bf[FN];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) af[i] = as[(kk + t) * LDA_S + wm + i * 8 + g];
+            for (int i = 0; i < FM; ++i) af[i] = as[(kk + t) * Cfg::LDA_S + wm + i * 8 + g];
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
-                bf[j] = kTransB ? bs[(kk + t) * LDA_S + wn + j * 8 + g] : bs[(wn + j * 8 + g) * LDB_S + kk + t];
+            for (int j = 0; j < FN; ++j)
+                bf[j] = kTransB ? bs[(kk + t) * Cfg::LDBT_S + wn + j * 8 + g] : bs[(wn + j * 8 + g) * LDB_S + kk + t];
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < FM; ++i)
 #pragma unroll
-                for (int j = 0; j < 8; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+                for (int j = 0; j < FN; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
         }
     }
     cp_async_wait<0>();
@@ -158,10 +176,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     if (part) {  // raw partial tile of split blockIdx.z (M x N slab, leading dimension M)
         double* P = part + (size_t)blockIdx.z * M * N;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < FM; ++i) {
             int row = m0 + wm + i * 8 + g;
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
+            for (int j = 0; j < FN; ++j)
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     int col = n0 + wn + j * 8 + t * 2 + h;
@@ -173,10 +191,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
 
     double mx = 0.0;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < FM; ++i) {
         int row = m0 + wm + i * 8 + g;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
+        for (int j = 0; j < FN; ++j) {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 int col = n0 + wn + j * 8 + t * 2 + h;
@@ -198,15 +216,17 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     }
 }
 
-// C = alpha * sum_s part[s] + beta * C over the tiles the GEMM computed, the
-// splits summed in a fixed order (deterministic), max|C| folded into amax.
+// C = alpha * sum_s part[s] + beta * C over the tiles the GEMM computed
+// (tile size bm x bn), the splits summed in a fixed order (deterministic),
+// max|C| folded into amax.
 __global__ void k_splitk_reduce(int M, int N, int splits, const double* __restrict__ part, double alpha,
-                                double beta, double* C, long ldc, unsigned long long* amax, int mode) {
+                                double beta, double* C, long ldc, unsigned long long* amax, int mode, int bm,
+                                int bn) {
     const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
     double mx = 0.0;
     if (idx < (long)M * N) {
         const int col = (int)(idx / M), row = (int)(idx - (long)col * M);
-        if (!((mode & GEMM_LOWER) && (col / BN) * BN > (row / BM) * BM + BM - 1)) {
+        if (!((mode & GEMM_LOWER) && (col / bn) * bn > (row / bm) * bm + bm - 1)) {
             double v = 0.0;
             for (int s = 0; s < splits; ++s) v += part[(size_t)s * M * N + idx];
             double* c = C + row + (long)col * ldc;
@@ -225,49 +245,67 @@ __global__ void k_splitk_reduce(int M, int N, int splits, const double* __restri
     }
 }
 
-void gemm_f64_mode(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
-                   double beta, double* C, int ldc, unsigned long long* amax, int mode, cudaStream_t st,
-                   double* ws, size_t ws_doubles) {
+namespace {
+template <class Cfg>
+int active_tiles(dim3 grid, int mode) {
+    if (!(mode & GEMM_LOWER)) return (int)(grid.x * grid.y);
+    int tiles = 0;
+    for (unsigned by = 0; by < grid.y; ++by)
+        for (unsigned bx = 0; bx < grid.x; ++bx) tiles += (int)(bx * Cfg::BN) <= (int)(by * Cfg::BM) + Cfg::BM - 1;
+    return tiles;
+}
+
+template <class Cfg>
+void launch_gemm(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb, double beta,
+                 double* C, int ldc, unsigned long long* amax, int mode, cudaStream_t st, double* ws,
+                 size_t ws_doubles) {
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_gemm_f64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
-        cudaFuncSetAttribute(k_gemm_f64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
+        cudaFuncSetAttribute(k_gemm_f64<Cfg, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+        cudaFuncSetAttribute(k_gemm_f64<Cfg, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
         attr = true;
     }
-    if (M <= 0 || N <= 0) return;
-    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+    dim3 grid((N + Cfg::BN - 1) / Cfg::BN, (M + Cfg::BM - 1) / Cfg::BM);
     // split-K when the output has too few tiles to fill the SMs: each split
     // keeps at least kMinSplitTiles k tiles, the partial slabs fit in ws
-    int tiles = 0;
-    if (mode & GEMM_LOWER) {
-        for (unsigned by = 0; by < grid.y; ++by)
-            for (unsigned bx = 0; bx < grid.x; ++bx) tiles += (int)(bx * BN) <= (int)(by * BM) + BM - 1;
-    } else {
-        tiles = (int)(grid.x * grid.y);
-    }
+    const int tiles = active_tiles<Cfg>(grid, mode);
     constexpr int kSMs = 148, kMinSplitTiles = 3, kMaxSplits = 16;
+    const int slots = kSMs * (Cfg::BM == 128 ? 1 : 2);
     int splits = 1;
     const int kt = (K + BK - 1) / BK;
-    if (ws && tiles > 0 && tiles < kSMs && kt >= 2 * kMinSplitTiles) {
-        splits = std::min(std::min(kSMs / tiles, kt / kMinSplitTiles), kMaxSplits);
+    if (ws && tiles > 0 && tiles < slots && kt >= 2 * kMinSplitTiles) {
+        splits = std::min(std::min(slots / tiles, kt / kMinSplitTiles), kMaxSplits);
         const size_t slab = (size_t)M * N;
         while (splits > 1 && (size_t)splits * slab > ws_doubles) --splits;
     }
     double* part = splits > 1 ? ws : nullptr;
     grid.z = splits;
     if (mode & GEMM_TRANS_B)
-        k_gemm_f64<true><<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,
-                                                                amax, mode, part);
+        k_gemm_f64<Cfg, true><<<grid, GEMM_THREADS, Cfg::SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
+                                                                     ldc, amax, mode, part);
     else
-        k_gemm_f64<false><<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,
-                                                                 amax, mode, part);
+        k_gemm_f64<Cfg, false><<<grid, GEMM_THREADS, Cfg::SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
+                                                                      ldc, amax, mode, part);
     count_launch();
     if (part) {
         const long total = (long)M * N;
         k_splitk_reduce<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(M, N, splits, part, alpha, beta, C, ldc,
-                                                                          amax, mode);
+                                                                          amax, mode, Cfg::BM, Cfg::BN);
         count_launch();
     }
+}
+}  // namespace
+
+void gemm_f64_mode(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
+                   double beta, double* C, int ldc, unsigned long long* amax, int mode, cudaStream_t st,
+                   double* ws, size_t ws_doubles) {
+    if (M <= 0 || N <= 0) return;
+    // 64 x 64 tiles when 128 x 128 tiles would leave most SMs idle
+    const dim3 g128((N + 127) / 128, (M + 127) / 128);
+    if (active_tiles<CfgBig>(g128, mode) * 4 <= 148)
+        launch_gemm<CfgSmall>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, amax, mode, st, ws, ws_doubles);
+    else
+        launch_gemm<CfgBig>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, amax, mode, st, ws, ws_doubles);
 }
 
 void gemm_f64_ex(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
@@ -320,17 +358,18 @@ size_t chol_small_doubles(int n) { (void)n; return (size_t)NB * NB + 64; }
 
 // Leaf: Cholesky of the kb x kb (kb <= 64) diagonal block of A at (k0, k0)
 // and T_kk = L_kk^{-1}, written as a full kb x kb block of T (zeros above the
-// diagonal). One CTA of 256 threads; the block and its inverse live in shared
+// diagonal). One CTA of 512 threads; the block and its inverse live in shared
 // memory and every loop stays rolled (a fully unrolled elimination is
 // instruction-fetch bound: each instruction would run once).
-//  * factor, step p: rank-1 update of the trailing square by a 16 x 16 thread
-//    grid (4 x 4 elements per thread, both factors cached in registers);
+//  * factor, step p: rank-1 update of the trailing square by a 32 x 16 thread
+//    grid (2 x 4 elements per thread, both factors cached in registers);
 //    column p-1 is scaled by 1/sqrt(d) in the same step (nobody reads it any
 //    more), so each step needs a single barrier.
 //  * inverse: forward elimination on [L | I], row p of T scaled one step
 //    later for the same reason.
 // Non-positive or non-finite pivots set ERRBIT_SINGULAR.
-constexpr int LEAF_THREADS = 256;
+constexpr int LEAF_THREADS = 512;
+constexpr int LEAF_RY = NB / (LEAF_THREADS / 16);  // rows per thread in the 16-column thread grid
 constexpr int LEAF_LD = NB + 1;
 constexpr size_t LEAF_SMEM = sizeof(double) * (2 * NB * LEAF_LD + 2 * NB);
 
@@ -359,24 +398,34 @@ __global__ void __launch_bounds__(LEAF_THREADS) k_chol_leaf(const double* __rest
             const int i = p - 1 + tid;
             S[i * LEAF_LD + p - 1] *= rs[p - 1];
         }
-        double ci[4], cj[4];
+        // rank-1 update of the whole trailing square (the upper half is never
+        // read as L): 16 loads, 16 FMAs, 16 stores per thread, all independent
+        double ci[LEAF_RY], cj[4], v[LEAF_RY][4];
+        constexpr int SY = LEAF_THREADS / 16;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int i = p + 1 + ty + 16 * u, j = p + 1 + tx + 16 * u;
+        for (int u = 0; u < LEAF_RY; ++u) {
+            const int i = p + 1 + ty + SY * u;
             ci[u] = i < kb ? S[i * LEAF_LD + p] * r : 0.0;
-            cj[u] = j < kb ? S[j * LEAF_LD + p] * r : 0.0;
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int i = p + 1 + ty + 16 * u;
-            if (i >= kb) break;
+        for (int w = 0; w < 4; ++w) {
+            const int j = p + 1 + tx + 16 * w;
+            cj[w] = j < kb ? S[j * LEAF_LD + p] * r : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < LEAF_RY; ++u)
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
-                const int j = p + 1 + tx + 16 * w;
-                if (j > i) break;
-                S[i * LEAF_LD + j] -= ci[u] * cj[w];
+                const int i = p + 1 + ty + SY * u, j = p + 1 + tx + 16 * w;
+                v[u][w] = (i < kb && j < kb) ? S[i * LEAF_LD + j] : 0.0;
             }
-        }
+#pragma unroll
+        for (int u = 0; u < LEAF_RY; ++u)
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                const int i = p + 1 + ty + SY * u, j = p + 1 + tx + 16 * w;
+                if (i < kb && j < kb) S[i * LEAF_LD + j] = v[u][w] - ci[u] * cj[w];
+            }
         __syncthreads();
     }
     if (tid == 0 && kb > 0) S[(kb - 1) * LEAF_LD + kb - 1] *= rs[kb - 1];
@@ -386,24 +435,32 @@ __global__ void __launch_bounds__(LEAF_THREADS) k_chol_leaf(const double* __rest
     for (int p = 0; p < kb; ++p) {
         const double ip = ri[p];
         if (p > 0 && tid < p) Ts[(p - 1) * LEAF_LD + tid] *= ri[p - 1];  // delayed scaling of row p - 1
-        double tp[4];
+        double tp[4], li[LEAF_RY], v[LEAF_RY][4];
+        constexpr int SY = LEAF_THREADS / 16;
 #pragma unroll
         for (int w = 0; w < 4; ++w) {
             const int j = tx + 16 * w;
             tp[w] = j <= p ? Ts[p * LEAF_LD + j] * ip : 0.0;
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int i = p + 1 + ty + 16 * u;
-            if (i >= kb) break;
-            const double lip = S[i * LEAF_LD + p];
+        for (int u = 0; u < LEAF_RY; ++u) {
+            const int i = p + 1 + ty + SY * u;
+            li[u] = i < kb ? S[i * LEAF_LD + p] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < LEAF_RY; ++u)
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
-                const int j = tx + 16 * w;
-                if (j > p) break;
-                Ts[i * LEAF_LD + j] -= lip * tp[w];
+                const int i = p + 1 + ty + SY * u, j = tx + 16 * w;
+                v[u][w] = (i < kb && j <= p) ? Ts[i * LEAF_LD + j] : 0.0;
             }
-        }
+#pragma unroll
+        for (int u = 0; u < LEAF_RY; ++u)
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                const int i = p + 1 + ty + SY * u, j = tx + 16 * w;
+                if (i < kb && j <= p) Ts[i * LEAF_LD + j] = v[u][w] - li[u] * tp[w];
+            }
         __syncthreads();
     }
     if (kb > 0 && tid < kb) Ts[(kb - 1) * LEAF_LD + tid] *= ri[kb - 1];

@@ -140,7 +140,7 @@ struct MixedOperand {
     int* exps;     // n row exponents
     int n, slices, rows, kp;
 };
-int mixed_tile_n(int slices);
+int mixed_tile_n(int slices, int n);
 size_t mixed_slice_bytes(int n, int slices);
 // Prepare the operand over buf/exps (as_b: box rows of the B operand). False
 // when the driver's tensor-map encoder is unavailable.

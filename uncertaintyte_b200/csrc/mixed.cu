@@ -367,10 +367,32 @@ void set_attr_once() {
 }
 }  // namespace
 
-int mixed_tile_n(int slices) { return slices <= 4 ? 128 : 96; }  // slices * tile_n <= 512 TMEM columns
+// Output tile width: slices * tile_n <= 512 TMEM columns, so 128 for up to 4
+// slices and 96 for 5. For 5 slices a 64-wide tile is taken when it needs
+// fewer tile-waves on the 148 SMs: the lower-triangle tile count of an n x n
+// product is what fills the machine at moderate n (n = 1800: 164 tiles of
+// 128 x 96 take two waves, the second 16 tiles deep; 239 tiles of 128 x 64
+// also take two, each 2/3 as long). Cost model: waves x (tile_n + 16), the
+// 16 standing for the per-tile prologue and epilogue.
+static int lower_tiles(int n, int nt) {
+    int tiles = 0;
+    const int by_n = (n + BM - 1) / BM, bx_n = (n + nt - 1) / nt;
+    for (int by = 0; by < by_n; ++by) {
+        const int last = (by * BM + BM - 1) / nt;  // last tile column on or below the diagonal
+        tiles += (last + 1 < bx_n ? last + 1 : bx_n);
+    }
+    return tiles;
+}
+
+int mixed_tile_n(int slices, int n) {
+    if (slices <= 4) return 128;
+    constexpr int kSMs = 148;
+    const long w96 = (lower_tiles(n, 96) + kSMs - 1) / kSMs, w64 = (lower_tiles(n, 64) + kSMs - 1) / kSMs;
+    return w64 * (64 + 16) < w96 * (96 + 16) ? 64 : 96;
+}
 
 static int mixed_rows(int n, int slices) {
-    const int nt = mixed_tile_n(slices);
+    const int nt = mixed_tile_n(slices, n);
     const int ra = ((n + BM - 1) / BM) * BM, rb = ((n + nt - 1) / nt) * nt;
     return ra > rb ? ra : rb;
 }
@@ -381,7 +403,7 @@ size_t mixed_slice_bytes(int n, int slices) {
 }
 
 bool mixed_plan(MixedOperand& op, int8_t* buf, int* exps, int n, int slices, bool as_b) {
-    const int nt = mixed_tile_n(slices);
+    const int nt = mixed_tile_n(slices, n);
     op.n = n;
     op.slices = slices;
     op.kp = ((n + BKB - 1) / BKB) * BKB;
@@ -405,6 +427,12 @@ void mixed_gemm(const MixedOperand& a, const MixedOperand& b, double* C, int ldc
         k_ozaki_gemm<128, 4><<<grid, THREADS, Shape<128, 4>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
                                                                          a.exps, b.exps, C, ldc, amax,
                                                                          lower_only ? 1 : 0, err);
+    } else if (a.slices == 5 && mixed_tile_n(5, n) == 64) {
+        set_attr_once<64, 5>();
+        dim3 grid((n + 63) / 64, (n + BM - 1) / BM);
+        k_ozaki_gemm<64, 5><<<grid, THREADS, Shape<64, 5>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
+                                                                       a.exps, b.exps, C, ldc, amax,
+                                                                       lower_only ? 1 : 0, err);
     } else if (a.slices == 5) {
         set_attr_once<96, 5>();
         dim3 grid((n + 95) / 96, (n + BM - 1) / BM);
