@@ -117,9 +117,21 @@ long long unc_workspace_bytes(const unc_options* opt, int num_rows, int num_cols
 
 /* SDM::inv (src/uncertaintyTE/ScaledDenseMatrix.cpp:232-279) for a
  * symmetric positive-definite n x n matrix in device memory (column-major,
- * leading dimension lda >= n, lda even): inverted in place by blocked
- * Gauss-Jordan elimination on the GPU. Scratch is allocated per call. */
+ * leading dimension lda >= n, lda even): inverted in place on the GPU
+ * (equilibration, recursive Cholesky forming L^-1, then L^-T L^-1). Scratch
+ * is allocated per call. */
 int unc_dense_inverse_device(double* d_A, int n, int lda, void* stream);
+
+/* The pseudo-inverse step of svdInverse (src/uncertaintyTE/compute.cpp:200-245)
+ * for a symmetric positive semi-definite n x n matrix in device memory
+ * (column-major, ld >= n, ld even), in place: the remove_n smallest singular
+ * values are dropped (remove_n in 0..31), or with remove_n == -1 every
+ * singular value <= epsilon (at most 20 of them). Only the dropped
+ * eigenvectors are computed (subspace iteration on the shifted inverse), the
+ * rest follows from one Cholesky inverse of the matrix with those directions
+ * lifted and a two-sided projection. UNC_ERR_SINGULAR when a kept eigenvalue is
+ * not positive. Scratch (4 n x ld matrices) is allocated per call. */
+int unc_pinv_psd_device(double* d_M, int n, int ld, int remove_n, double epsilon, void* stream);
 
 /* The same SPD inverse as unc_dense_inverse_device, for callers that cannot
  * let a library allocate device memory (their device memory is reserved by

@@ -58,6 +58,23 @@ def test_option_validation_is_host_side():
     assert e.value.status == -7  # UNC_ERR_UNSUPPORTED
 
 
+def test_svd_option_validation_is_host_side():
+    """The SVD algorithms densify (9C + 3P)^2 J^T J: sizes above 46000 and more
+    than 31 removed singular values are refused before any CUDA call."""
+    from conftest import golden_jacobian
+    jac = golden_jacobian("cube")
+    jac.num_points += 20000
+    jac.num_cols = 9 * jac.num_cams + 3 * jac.num_points
+    with pytest.raises(native.UncError) as e:
+        native.compute_covariances(jac, algorithm=0)
+    assert e.value.status == -8  # UNC_ERR_TOO_LARGE
+    jac = golden_jacobian("cube")
+    jac.svd_remove_n = 40
+    with pytest.raises(native.UncError) as e:
+        native.compute_covariances(jac, algorithm=1)
+    assert e.value.status == -7  # UNC_ERR_UNSUPPORTED
+
+
 def test_workspace_estimate_scales_with_cameras():
     from conftest import golden_jacobian
     jac = golden_jacobian("daliborka")

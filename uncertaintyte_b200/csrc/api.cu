@@ -53,19 +53,6 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
-// Bump allocator over one device allocation; every piece 256-byte aligned.
-struct Carver {
-    char* base;
-    size_t off = 0;
-    template <class T>
-    T* take(size_t n) {
-        off = (off + 255) & ~size_t(255);
-        T* p = reinterpret_cast<T*>(base ? base + off : nullptr);
-        off += n * sizeof(T);
-        return p;
-    }
-};
-
 struct Plan {
     int C, P, nobs, N, ld;
 };
@@ -138,8 +125,15 @@ int check_options(const unc_options* o, int num_rows, int num_cols) {
         return fail(UNC_ERR_UNSUPPORTED, "only 9 camera parameters are supported");
     if ((long long)num_cols != 9LL * o->num_cams + 3LL * o->num_points)
         return fail(UNC_ERR_INVALID_ARG, "num_cols != 9*num_cams + 3*num_points");
-    if (o->algorithm != UNC_TAYLOR_EXPANSION)
-        return fail(UNC_ERR_UNSUPPORTED, "SVD algorithms are not implemented in this build");
+    if (o->algorithm == UNC_SVD_QR_ITERATION || o->algorithm == UNC_SVD_DEVIDE_AND_CONQUER) {
+        // dense (9C + 3P)^2 J^T J plus four scratch matrices of that size
+        const long long n = 9LL * o->num_cams + 3LL * o->num_points;
+        if (n > 46000) return fail(UNC_ERR_TOO_LARGE, "SVD algorithms: 9*num_cams + 3*num_points above 46000");
+        if (o->svd_remove_n < -1 || o->svd_remove_n > 31)
+            return fail(UNC_ERR_UNSUPPORTED, "svd_remove_n must be -1 (epsilon rule) or 0..31");
+        return UNC_OK;
+    }
+    if (o->algorithm != UNC_TAYLOR_EXPANSION) return fail(UNC_ERR_INVALID_ARG, "unknown algorithm");
     if (!o->has_pts2fix) return fail(UNC_ERR_NO_FIXED_POINTS, "TAYLOR_EXPANSION needs three fixed points");
     for (int i = 0; i < 3; ++i)
         if (o->pts2fix[i] < 0 || o->pts2fix[i] >= o->num_points)
@@ -148,6 +142,10 @@ int check_options(const unc_options* o, int num_rows, int num_cols) {
         return fail(UNC_ERR_INVALID_ARG, "unknown precision");
     if (9LL * o->num_cams > 46000) return fail(UNC_ERR_TOO_LARGE, "9*num_cams above 46000");
     return UNC_OK;
+}
+
+bool is_svd(const unc_options* o) {
+    return o->algorithm == UNC_SVD_QR_ITERATION || o->algorithm == UNC_SVD_DEVIDE_AND_CONQUER;
 }
 
 // factorial() of compute.cpp:57-62: 32-bit signed, wraps from 13! on.
@@ -449,6 +447,18 @@ int unc_compute_device(unc_context* ctx, const unc_options* o, int num_rows, int
     if (((uintptr_t)d_cols & 15) || ((uintptr_t)d_values & 15))
         return fail(UNC_ERR_INVALID_ARG, "cols/values must be 16-byte aligned");
     CK(cudaSetDevice(ctx->device));
+    cudaStream_t sm = stream ? (cudaStream_t)stream : ctx->stream;
+    if (is_svd(o)) {
+        const size_t bytes = svd_workspace_bytes(o->num_cams, o->num_points, num_rows / 2, false, 0, num_rows);
+        rc = ensure_ws(ctx, bytes);
+        if (rc) return rc;
+        if (st) {
+            memset(st, 0, sizeof(*st));
+            st->device_bytes = (long long)bytes;
+        }
+        return svd_pipeline((char*)ctx->ws, o, num_rows, 24LL * (num_rows / 2), d_rows, d_cols, d_values,
+                            d_cam_unc, d_pt_unc, false, st, ctx->ev, sm);
+    }
     Plan pl = make_plan(o, num_rows);
     Buffers b;
     size_t bytes = carve(nullptr, pl, false, 0, num_rows, b);
@@ -459,7 +469,6 @@ int unc_compute_device(unc_context* ctx, const unc_options* o, int num_rows, int
         memset(st, 0, sizeof(*st));
         st->device_bytes = (long long)bytes;
     }
-    cudaStream_t sm = stream ? (cudaStream_t)stream : ctx->stream;
     // the arrays are trusted to hold the reference layout's 24 entries per observation
     return run_pipeline(ctx, o, num_rows, 24LL * pl.nobs, d_rows, d_cols, d_values, d_cam_unc, d_pt_unc,
                         b, pl, st, sm);
@@ -485,6 +494,17 @@ int unc_compute(unc_context* ctx, const unc_options* o, int num_rows, int num_co
     const long long nnz = rows[num_rows];
     if (nnz < 0 || rows[0] != 0) return fail(UNC_ERR_INVALID_ARG, "rowptr must start at 0 and end at nnz >= 0");
     CK(cudaSetDevice(ctx->device));
+    if (is_svd(o)) {
+        const size_t bytes = svd_workspace_bytes(o->num_cams, o->num_points, num_rows / 2, true, nnz, num_rows);
+        rc = ensure_ws(ctx, bytes);
+        if (rc) return rc;
+        if (st) {
+            memset(st, 0, sizeof(*st));
+            st->device_bytes = (long long)bytes;
+        }
+        return svd_pipeline((char*)ctx->ws, o, num_rows, nnz, rows, cols, values, cam_unc, pt_unc, true, st,
+                            ctx->ev, ctx->stream);
+    }
     Plan pl = make_plan(o, num_rows);
     Buffers b;
     size_t bytes = carve(nullptr, pl, true, nnz, num_rows, b);

@@ -610,9 +610,10 @@ __global__ void k_camera_output(const double* __restrict__ iZ, long ldz,
     if (c >= num_cams || e >= 81) return;
     int j = e / 9, k = e - j * 9;
     long r = 9L * c + j, q = 9L * c + k;
-    double dj = 1.0 / s_cam[r], dk = 1.0 / s_cam[q];
+    // s_cam == nullptr: no column scaling (the SVD path, removeScaleJ4Z with d = NULL)
+    double dj = s_cam ? 1.0 / s_cam[r] : 1.0, dk = s_cam ? 1.0 / s_cam[q] : 1.0;
     double a = iZ[r + q * ldz], b = iZ[q + r * ldz];
-    sig[81L * c + e] = a * dj * dk;
+    if (sig) sig[81L * c + e] = a * dj * dk;
     if (k >= j) {
         int t = j * 9 - (j * (j - 1)) / 2 + (k - j);
         cam_unc[45L * c + t] = (a + b / 2) * dj * dk;

@@ -6,6 +6,8 @@
 
 #include <string>
 
+#include "../../include/uncte.h"
+
 namespace unc {
 
 // Device-side error bits (accumulated with atomicOr into a device int).
@@ -24,6 +26,20 @@ constexpr int kObsVals = 24;  // one observation = 2 rows x (9 camera + 3 point)
 inline int ld_of(int n) { return (n + 7) & ~7; }
 
 extern thread_local std::string g_last_error;
+
+// Bump allocator over one device allocation; every piece 256-byte aligned.
+// With base == nullptr it only measures the total size.
+struct Carver {
+    char* base;
+    size_t off = 0;
+    template <class T>
+    T* take(size_t n) {
+        off = (off + 255) & ~size_t(255);
+        T* p = reinterpret_cast<T*>(base ? base + off : nullptr);
+        off += n * sizeof(T);
+        return p;
+    }
+};
 extern long long g_launches;
 inline void count_launch(int n = 1) { __atomic_add_fetch(&g_launches, n, __ATOMIC_RELAXED); }
 
@@ -149,6 +165,32 @@ void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st);
 // C = P * X from the slices of P (a) and X (b); lower_only: tiles on/below the diagonal.
 void mixed_gemm(const MixedOperand& a, const MixedOperand& b, double* C, int ldc, unsigned long long* amax,
                 bool lower_only, int* err, cudaStream_t st);
+
+// ---------------- svd.cu ----------------
+// Scratch of the PSD pseudo-inverse (n x ld matrices and p x n blocks).
+struct PinvBuffers {
+    double *G, *T, *W, *Tt;        // shifted inverse, Cholesky-inverse scratch
+    double *X, *Y, *MX, *MX2;      // n x 32 subspace blocks
+    double *H, *Wr, *S;            // 32 x 32
+    double *theta, *res, *e;
+    int* err;
+    unsigned long long* dmax;
+};
+struct PinvInfo {
+    int iterations, removed;
+    double shift, residual, lambda_removed_max, lambda_kept_min;
+};
+size_t pinv_carve(char* base, int n, int ld, PinvBuffers& b);
+// In place: M (n x ld, symmetric PSD) <- its pseudo-inverse without the
+// remove_n smallest |eigenvalues| (remove_n >= 0) or without those with
+// |eigenvalue| <= eps (remove_n == -1). Synchronises the stream.
+int pinv_psd(double* M, int n, int ld, int remove_n, double eps, const PinvBuffers& b, cudaStream_t sm,
+             PinvInfo* info);
+// SVD_QR_ITERATION / SVD_DEVIDE_AND_CONQUER of computeCovariances; ev: 6 events.
+size_t svd_workspace_bytes(int C, int P, int nobs, bool host_io, long long nnz, int nrows);
+int svd_pipeline(char* ws, const unc_options* o, int num_rows, long long nnz, const int* rows, const int* cols,
+                 const double* vals, double* cam_unc, double* pt_unc, bool host_io, unc_statistic* st,
+                 cudaEvent_t* ev, cudaStream_t sm);
 
 // ---------------- points.cu ----------------
 void launch_point_cov(const SceneDev& s, const double* sig, double* pt_unc, cudaStream_t st);

@@ -79,7 +79,7 @@ class UncStatistic(C.Structure):
 EXPORTS = ("unc_options_init", "unc_context_create", "unc_context_destroy", "unc_compute",
            "unc_context_set_profiling", "unc_context_profile",
            "unc_compute_device", "unc_workspace_bytes", "unc_dense_inverse_device",
-           "unc_dense_inverse_noalloc", "unc_jtj_crs",
+           "unc_dense_inverse_noalloc", "unc_pinv_psd_device", "unc_jtj_crs",
            "unc_gemm_f64_device", "unc_gemm_mixed_device", "unc_status_string", "unc_last_error",
            "unc_kernel_launches")
 
@@ -109,6 +109,7 @@ def lib():
     L.unc_workspace_bytes.restype = C.c_longlong
     L.unc_dense_inverse_device.argtypes = [vp, C.c_int, C.c_int, vp]
     L.unc_dense_inverse_noalloc.argtypes = [vp, C.c_int, C.c_int, vp]
+    L.unc_pinv_psd_device.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, vp]
     L.unc_jtj_crs.argtypes = [C.c_int, C.c_int, vp, vp, vp, C.c_int, C.c_int, P(C.c_longlong), vp,
                               vp, vp]
     L.unc_gemm_f64_device.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, vp, C.c_int, vp, C.c_int,
@@ -222,6 +223,13 @@ def dense_inverse_device(d_ptr: int, n: int, lda: int, stream: int = 0) -> None:
 def dense_inverse_noalloc(d_ptr: int, n: int, lda: int, stream: int = 0) -> None:
     """In-place SPD inverse with no device allocation (static scratch, n and lda <= 512)."""
     _check(lib().unc_dense_inverse_noalloc(d_ptr, n, lda, stream or None))
+
+
+def pinv_psd_device(d_ptr: int, n: int, ld: int, remove_n: int = 7, epsilon: float = 1e-10,
+                    stream: int = 0) -> None:
+    """In-place pseudo-inverse of a PSD matrix without its remove_n smallest
+    singular values (remove_n = -1: without those <= epsilon)."""
+    _check(lib().unc_pinv_psd_device(d_ptr, n, ld, remove_n, epsilon, stream or None))
 
 
 def jtj_crs(num_rows: int, num_cols: int, rows, cols, vals, num_cams: int, cam_params: int = 9):
