@@ -35,6 +35,7 @@ extern "C" {
 #define UNC_ERR_SINGULAR (-6)      /* non-positive pivot or non-finite value in the dense inverse */
 #define UNC_ERR_UNSUPPORTED (-7)   /* option combination not implemented (message: unc_last_error) */
 #define UNC_ERR_TOO_LARGE (-8)     /* size above a documented limit */
+#define UNC_ERR_TIMEOUT (-9)       /* unc_server_wait: the request is still running */
 
 /* algorithm selector, same values as include/uncertainty.h:11-13 */
 #define UNC_SVD_QR_ITERATION 0
@@ -114,6 +115,43 @@ int unc_context_profile(unc_context* ctx, long long* launches, double* seconds, 
 
 /* Device bytes unc_compute_device would use for this problem (admission). */
 long long unc_workspace_bytes(const unc_options* opt, int num_rows, int num_cols);
+
+/* Device bytes one unc_compute call needs for this Jacobian (host arrays):
+ * the workspace with the input copies, the Schur pair list (counted from the
+ * point columns of the rows) and the int8 slices of the mixed modes. -1 for
+ * invalid options. No counterpart in the reference (admission control). */
+long long unc_request_bytes(const unc_options* opt, int num_rows, int num_cols, const int* rows,
+                            const int* cols);
+
+/* Device buffers a context keeps between calls: their size, and a release
+ * (the next call allocates again). No counterpart in the reference. */
+long long unc_context_device_bytes(const unc_context* ctx);
+int unc_context_release(unc_context* ctx);
+
+/* ---- Request server: many reconstructions on one GPU (no counterpart in the
+ * reference, which computes one reconstruction per call and is not
+ * re-entrant, src/uncertaintyTE/compute.cpp:461-468).
+ * max_inflight worker threads, each with its own context (stream and reused
+ * workspace), run requests concurrently; a request starts when a worker is
+ * free and its unc_request_bytes fit in max_device_bytes (<= 0: 90 % of the
+ * free device memory at creation) next to the running ones. The host arrays of
+ * a request (Jacobian in, covariances out) must stay valid until
+ * unc_server_wait has returned its result. Results do not depend on what else
+ * runs. Thread-safe. */
+typedef struct unc_server unc_server;
+int unc_server_create(int device, long long max_device_bytes, int max_inflight, unc_server** out);
+/* Queue one computeCovariances; *id identifies it. UNC_ERR_OUT_OF_MEMORY when
+ * the request alone exceeds the budget; option errors as unc_compute. */
+int unc_server_submit(unc_server* srv, const unc_options* opt, int num_rows, int num_cols, const int* rows,
+                      const int* cols, const double* values, double* cam_unc, double* pt_unc, long long* id);
+/* Wait up to timeout_s seconds (< 0: no limit) for request id; UNC_OK when it
+ * finished (its own status in *status, statistics, submit-to-finish latency and
+ * queueing time in seconds), UNC_ERR_TIMEOUT when it still runs. A finished
+ * request is collected once. */
+int unc_server_wait(unc_server* srv, long long id, double timeout_s, int* status, unc_statistic* st,
+                    double* latency_s, double* queue_s);
+/* Finish every queued and running request, then stop the workers. */
+int unc_server_destroy(unc_server* srv);
 
 /* SDM::inv (src/uncertaintyTE/ScaledDenseMatrix.cpp:232-279) for a
  * symmetric positive-definite n x n matrix in device memory (column-major,

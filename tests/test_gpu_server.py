@@ -1,0 +1,83 @@
+"""Request server: continuous batching of many reconstructions on one GPU.
+
+Each result must be the same alone and in a mix: the server runs several
+requests concurrently on separate streams, and every request's arithmetic uses
+fixed reduction orders and no atomics, so the comparison is bitwise.
+"""
+import numpy as np
+import pytest
+
+from uncertaintyte_b200 import native, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _jobs():
+    """Mixed sizes (8 .. 90 cameras), both precisions, one SVD request."""
+    out = []
+    for i, C in enumerate([8, 40, 12, 90, 25, 60, 9, 33, 70, 16]):
+        jac = scenes.scene_jacobian(scenes.make_sized_scene(C, 60, 4, seed=100 + i))
+        out.append((jac, "fp64" if i % 3 == 0 else "mixed", None))
+    svd = scenes.scene_jacobian(scenes.make_sized_scene(10, 30, 3, seed=7))
+    out.append((svd, "fp64", 0))
+    return out
+
+
+def _alone(jobs):
+    ctx = native.Context()
+    res = [native.compute_covariances(j, ctx, algorithm=a, precision=p)[:2] for j, p, a in jobs]
+    ctx.close()
+    return res
+
+
+def test_results_identical_alone_and_in_the_mix():
+    jobs = _jobs()
+    ref = _alone(jobs)
+    srv = native.Server(max_inflight=4)
+    ids = [srv.submit(j, precision=p, algorithm=a) for j, p, a in jobs]
+    got = [srv.wait(i)[:2] for i in ids]
+    srv.close()
+    for (c0, p0), (c1, p1) in zip(ref, got):
+        np.testing.assert_array_equal(c0, c1)
+        np.testing.assert_array_equal(p0, p1)
+
+
+def test_tight_budget_serialises_but_completes():
+    jobs = _jobs()[:6]
+    need = max(native.request_bytes(j, precision=p, algorithm=a) for j, p, a in jobs)
+    ref = _alone(jobs)
+    srv = native.Server(max_device_bytes=int(need * 1.2), max_inflight=4)
+    ids = [srv.submit(j, precision=p, algorithm=a) for j, p, a in jobs]
+    out = [srv.wait(i) for i in ids]
+    srv.close()
+    for (c0, p0), (c1, p1, st, lat, que) in zip(ref, out):
+        np.testing.assert_array_equal(c0, c1)
+        np.testing.assert_array_equal(p0, p1)
+        assert lat >= que >= 0.0
+
+
+def test_request_above_budget_is_refused():
+    jac = scenes.scene_jacobian(scenes.make_sized_scene(40, 60, 4, seed=3))
+    srv = native.Server(max_device_bytes=1 << 20, max_inflight=2)
+    with pytest.raises(native.UncError) as e:
+        srv.submit(jac)
+    assert e.value.status == -5  # UNC_ERR_OUT_OF_MEMORY
+    srv.close()
+
+
+def test_wait_timeout_and_single_collection():
+    jac = scenes.scene_jacobian(scenes.make_sized_scene(120, 150, 4, seed=11))
+    srv = native.Server(max_inflight=1)
+    rid = srv.submit(jac)
+    try:
+        srv.wait(rid, timeout=0.0)
+        finished_early = True
+    except native.UncError as e:
+        assert e.status == -9  # UNC_ERR_TIMEOUT: still running
+        finished_early = False
+    if not finished_early:
+        cam, pt, st, lat, que = srv.wait(rid)
+        assert np.isfinite(cam).all() and st["te_iterations"] > 0
+    with pytest.raises(native.UncError):
+        srv.wait(rid)  # already collected
+    srv.close()

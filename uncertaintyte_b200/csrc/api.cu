@@ -107,14 +107,22 @@ size_t carve(char* base, const Plan& pl, bool host_io, long long nnz, int nrows,
     return c.off + 256;
 }
 
-int ensure_ws(unc_context* ctx, size_t bytes) {
-    if (ctx->ws_bytes >= bytes) return UNC_OK;
-    if (ctx->ws) cudaFree(ctx->ws);
-    ctx->ws = nullptr;
-    ctx->ws_bytes = 0;
-    CK(cudaMalloc(&ctx->ws, bytes));
-    ctx->ws_bytes = bytes;
+// Grow-only context buffer, allocated in stream order on the call's stream:
+// several contexts (one per host thread) can run concurrently on one GPU, and
+// a cudaFree would synchronise the whole device under all of them. Every call
+// ends with a stream synchronisation, so the old buffer is idle when freed.
+int grow_buffer(void** p, size_t* have, size_t need, size_t want, cudaStream_t sm) {
+    if (*have >= need) return UNC_OK;
+    if (*p) CK(cudaFreeAsync(*p, sm));
+    *p = nullptr;
+    *have = 0;
+    CK(cudaMallocAsync(p, want, sm));
+    *have = want;
     return UNC_OK;
+}
+
+int ensure_ws(unc_context* ctx, size_t bytes, cudaStream_t sm) {
+    return grow_buffer(&ctx->ws, &ctx->ws_bytes, bytes, bytes, sm);
 }
 
 int check_options(const unc_options* o, int num_rows, int num_cols) {
@@ -200,14 +208,8 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     if (npairs < 0) return fail(UNC_ERR_TOO_LARGE, "more than 2^31 co-visible observation pairs");
     const size_t long_cap = (size_t)npairs / 1025 + 1;
     const size_t need = (size_t)npairs * 8 + (long_cap + 1) * sizeof(int) + 64;
-    if (ctx->tup_bytes < need) {
-        if (ctx->tup) cudaFree(ctx->tup);
-        ctx->tup = nullptr;
-        ctx->tup_bytes = 0;
-        size_t want = need + need / 4;  // headroom for the next scene
-        CK(cudaMalloc(&ctx->tup, want));
-        ctx->tup_bytes = want;
-    }
+    // headroom for the next scene
+    if (int r = grow_buffer(&ctx->tup, &ctx->tup_bytes, need, need + need / 4, sm)) return r;
     s.pairs = reinterpret_cast<unsigned long long*>(ctx->tup);
     s.long_list = reinterpret_cast<int*>(s.pairs + npairs + 1);
     s.long_cap = (int)long_cap;
@@ -248,13 +250,7 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     if (mixed) {
         const size_t sb = (mixed_slice_bytes(N, slices) + 255) & ~size_t(255);
         const size_t need = 2 * sb + 2 * sizeof(int) * ((size_t)N + 64) + 256;
-        if (ctx->mp_bytes < need) {
-            if (ctx->mp) cudaFree(ctx->mp);
-            ctx->mp = nullptr;
-            ctx->mp_bytes = 0;
-            CK(cudaMalloc(&ctx->mp, need));
-            ctx->mp_bytes = need;
-        }
+        if (int r = grow_buffer(&ctx->mp, &ctx->mp_bytes, need, need, sm)) return r;
         char* w = (char*)ctx->mp;
         int8_t* bufX = reinterpret_cast<int8_t*>(w);
         int8_t* bufP = reinterpret_cast<int8_t*>(w + sb);
@@ -417,14 +413,63 @@ int unc_context_destroy(unc_context* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (cudaEvent_t e : c->pev) cudaEventDestroy(e);
-    if (c->ws) cudaFree(c->ws);
-    if (c->tup) cudaFree(c->tup);
-    if (c->mp) cudaFree(c->mp);
+    unc_context_release(c);
     for (int i = 0; i < 12; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return UNC_OK;
+}
+
+int unc_context_release(unc_context* c) {
+    if (!c) return fail(UNC_ERR_INVALID_ARG, "ctx is NULL");
+    cudaSetDevice(c->device);
+    void** bufs[3] = {&c->ws, &c->tup, &c->mp};
+    size_t* sizes[3] = {&c->ws_bytes, &c->tup_bytes, &c->mp_bytes};
+    for (int i = 0; i < 3; ++i) {
+        if (*bufs[i]) cudaFreeAsync(*bufs[i], c->stream);
+        *bufs[i] = nullptr;
+        *sizes[i] = 0;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return UNC_OK;
+}
+
+long long unc_context_device_bytes(const unc_context* c) {
+    if (!c) return -1;
+    return (long long)(c->ws_bytes + c->tup_bytes + c->mp_bytes);
+}
+
+long long unc_request_bytes(const unc_options* o, int num_rows, int num_cols, const int* rows, const int* cols) {
+    if (!o || num_rows < 0 || !rows || !cols) return -1;
+    if (check_options(o, num_rows, num_cols) != UNC_OK) return -1;
+    const long long nnz = rows[num_rows];
+    const int nobs = num_rows / 2;
+    if (is_svd(o)) return (long long)svd_workspace_bytes(o->num_cams, o->num_points, nobs, true, nnz, num_rows);
+    Plan pl = make_plan(o, num_rows);
+    Buffers b;
+    long long bytes = (long long)carve(nullptr, pl, true, nnz, num_rows, b);
+    // Schur pair list: observation pairs that share a point (counted per point
+    // from the first point column of each observation row), with headroom
+    std::vector<int> per_pt(pl.P > 0 ? pl.P : 1, 0);
+    const int cam_cols = 9 * pl.C;
+    for (int ob = 0; ob < nobs; ++ob) {
+        const int r0 = rows[2 * ob], r1 = rows[2 * ob + 1];
+        for (int k = r0; k < r1; ++k)
+            if (cols[k] >= cam_cols) {
+                const int p = (cols[k] - cam_cols) / 3;
+                if (p >= 0 && p < pl.P) ++per_pt[p];
+                break;
+            }
+    }
+    long long pairs = 0;
+    for (int c : per_pt) pairs += (long long)c * (c - 1) / 2;
+    bytes += (pairs * 8 + pairs / 1025 * 4 + 64) * 5 / 4;
+    if (o->precision != UNC_PRECISION_FP64) {
+        const int slices = o->precision == UNC_PRECISION_MIXED4 ? 4 : (o->precision == UNC_PRECISION_MIXED3 ? 3 : 5);
+        bytes += 2 * (long long)((mixed_slice_bytes(pl.N, slices) + 255) & ~size_t(255)) + 8LL * (pl.N + 64) + 256;
+    }
+    return bytes;
 }
 
 long long unc_workspace_bytes(const unc_options* o, int num_rows, int num_cols) {
@@ -450,7 +495,7 @@ int unc_compute_device(unc_context* ctx, const unc_options* o, int num_rows, int
     cudaStream_t sm = stream ? (cudaStream_t)stream : ctx->stream;
     if (is_svd(o)) {
         const size_t bytes = svd_workspace_bytes(o->num_cams, o->num_points, num_rows / 2, false, 0, num_rows);
-        rc = ensure_ws(ctx, bytes);
+        rc = ensure_ws(ctx, bytes, sm);
         if (rc) return rc;
         if (st) {
             memset(st, 0, sizeof(*st));
@@ -462,7 +507,7 @@ int unc_compute_device(unc_context* ctx, const unc_options* o, int num_rows, int
     Plan pl = make_plan(o, num_rows);
     Buffers b;
     size_t bytes = carve(nullptr, pl, false, 0, num_rows, b);
-    rc = ensure_ws(ctx, bytes);
+    rc = ensure_ws(ctx, bytes, sm);
     if (rc) return rc;
     carve((char*)ctx->ws, pl, false, 0, num_rows, b);
     if (st) {
@@ -494,28 +539,28 @@ int unc_compute(unc_context* ctx, const unc_options* o, int num_rows, int num_co
     const long long nnz = rows[num_rows];
     if (nnz < 0 || rows[0] != 0) return fail(UNC_ERR_INVALID_ARG, "rowptr must start at 0 and end at nnz >= 0");
     CK(cudaSetDevice(ctx->device));
+    cudaStream_t sm = ctx->stream;
     if (is_svd(o)) {
         const size_t bytes = svd_workspace_bytes(o->num_cams, o->num_points, num_rows / 2, true, nnz, num_rows);
-        rc = ensure_ws(ctx, bytes);
+        rc = ensure_ws(ctx, bytes, sm);
         if (rc) return rc;
         if (st) {
             memset(st, 0, sizeof(*st));
             st->device_bytes = (long long)bytes;
         }
         return svd_pipeline((char*)ctx->ws, o, num_rows, nnz, rows, cols, values, cam_unc, pt_unc, true, st,
-                            ctx->ev, ctx->stream);
+                            ctx->ev, sm);
     }
     Plan pl = make_plan(o, num_rows);
     Buffers b;
     size_t bytes = carve(nullptr, pl, true, nnz, num_rows, b);
-    rc = ensure_ws(ctx, bytes);
+    rc = ensure_ws(ctx, bytes, sm);
     if (rc) return rc;
     carve((char*)ctx->ws, pl, true, nnz, num_rows, b);
     if (st) {
         memset(st, 0, sizeof(*st));
         st->device_bytes = (long long)bytes;
     }
-    cudaStream_t sm = ctx->stream;
     CK(cudaMemcpyAsync(b.rows, rows, sizeof(int) * ((size_t)num_rows + 1), cudaMemcpyHostToDevice, sm));
     CK(cudaMemcpyAsync(b.cols, cols, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, sm));
     CK(cudaMemcpyAsync(b.vals, values, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice, sm));
@@ -766,6 +811,7 @@ const char* unc_status_string(int s) {
         case UNC_ERR_SINGULAR: return "UNC_ERR_SINGULAR";
         case UNC_ERR_UNSUPPORTED: return "UNC_ERR_UNSUPPORTED";
         case UNC_ERR_TOO_LARGE: return "UNC_ERR_TOO_LARGE";
+        case UNC_ERR_TIMEOUT: return "UNC_ERR_TIMEOUT";
         default: return "UNC_ERR_UNKNOWN";
     }
 }

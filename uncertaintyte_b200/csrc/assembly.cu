@@ -708,12 +708,11 @@ void launch_schur(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
     cudaMemsetAsync(s.long_list, 0, sizeof(int), st);
     k_sort_pairs_warp<<<(unsigned)((nblk + 3) / 4), 128, 0, st>>>(nblk, s.blk_ptr, s.pairs, s.long_list,
                                                                   s.long_cap);
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
         cudaFuncSetAttribute(k_sort_pairs_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(kPairBlockCap * sizeof(unsigned long long)));
-        attr = true;
-    }
+    });
     k_sort_pairs_block<<<148, 1024, kPairBlockCap * sizeof(unsigned long long), st>>>(
         s.blk_ptr, s.pairs, s.long_list, s.long_cap, s.err);
     k_schur_blocks<<<(unsigned)nblk, 256, 0, st>>>(s.num_cams, s.blk_ptr, s.pairs, s.Ws, s.Ys, Z, ldz);

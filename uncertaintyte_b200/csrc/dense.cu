@@ -259,12 +259,11 @@ template <class Cfg>
 void launch_gemm(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb, double beta,
                  double* C, int ldc, unsigned long long* amax, int mode, cudaStream_t st, double* ws,
                  size_t ws_doubles) {
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
         cudaFuncSetAttribute(k_gemm_f64<Cfg, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
         cudaFuncSetAttribute(k_gemm_f64<Cfg, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
-        attr = true;
-    }
+    });
     dim3 grid((N + Cfg::BN - 1) / Cfg::BN, (M + Cfg::BM - 1) / Cfg::BM);
     // split-K when the output has too few tiles to fill the SMs: each split
     // keeps at least kMinSplitTiles k tiles, the partial slabs fit in ws
@@ -501,11 +500,10 @@ void chol_rec(double* A, int lda, double* T, double* W, double* ws, size_t wsd, 
               cudaStream_t st) {
     const int n = r1 - r0;
     if (n <= NB) {
-        static bool attr = false;
-        if (!attr) {
+        static std::atomic<unsigned long long> attr{0};
+        once_per_device(attr, [] {
             cudaFuncSetAttribute(k_chol_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEAF_SMEM);
-            attr = true;
-        }
+        });
         k_chol_leaf<<<1, LEAF_THREADS, LEAF_SMEM, st>>>(A, lda, r0, n, T, lda, err);
         count_launch();
         return;

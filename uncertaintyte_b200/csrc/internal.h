@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+#include <mutex>
 #include <string>
 
 #include "../../include/uncte.h"
@@ -26,6 +28,22 @@ constexpr int kObsVals = 24;  // one observation = 2 rows x (9 camera + 3 point)
 inline int ld_of(int n) { return (n + 7) & ~7; }
 
 extern thread_local std::string g_last_error;
+
+// Runs f() once per device (ordinal < 64) for one call site, from any thread:
+// per-function CUDA attributes are per device, and several host threads
+// (one per context) may launch the same kernels concurrently.
+template <class F>
+void once_per_device(std::atomic<unsigned long long>& done, F&& f) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ULL << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.load(std::memory_order_relaxed) & bit) return;
+    f();
+    done.fetch_or(bit, std::memory_order_release);
+}
 
 // Bump allocator over one device allocation; every piece 256-byte aligned.
 // With base == nullptr it only measures the total size.

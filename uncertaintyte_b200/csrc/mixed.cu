@@ -332,14 +332,15 @@ __global__ void __launch_bounds__(THREADS, 1)
 // ------------------------------------------------------------------------
 namespace {
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
+    // a driver entry point: the same for every device; resolved once, thread-safe
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         cudaDriverEntryPointQueryResult q;
         void* p = nullptr;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
+            return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    }();
     return fn;
 }
 
@@ -359,11 +360,10 @@ bool make_map(CUtensorMap* map, const int8_t* base, int rows, int kp, int box_ro
 
 template <int NT, int S>
 void set_attr_once() {
-    static bool done = false;
-    if (!done) {
+    static std::atomic<unsigned long long> done{0};
+    once_per_device(done, [] {
         cudaFuncSetAttribute(k_ozaki_gemm<NT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, Shape<NT, S>::SMEM);
-        done = true;
-    }
+    });
 }
 }  // namespace
 

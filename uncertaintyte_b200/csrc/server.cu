@@ -1,0 +1,257 @@
+// server.cu - a request loop for many reconstructions on one GPU (host code).
+//
+// The reference computes one reconstruction per call and is not re-entrant
+// (global MAGMA init/finalize and a fixed OpenMP thread count per call,
+// compute.cpp:461-468, 539). This server has no counterpart there: callers
+// submit reconstructions of any size as they arrive and wait for them later.
+//
+// * Continuous batching: `max_inflight` worker threads, each with its own
+//   context (CUDA stream + device workspace kept between requests). A request
+//   that arrives while others run starts as soon as a worker is free and its
+//   device memory fits; the kernels of all running requests overlap on the GPU
+//   (different streams), the host-side waits of one request block only its
+//   worker.
+// * Admission by device-memory footprint (unc_request_bytes: the dense Schur
+//   complement and its inverse buffers, the block storage, the pair list, the
+//   int8 slices): the sum over running requests and idle workspaces stays
+//   within `max_device_bytes`. Idle workspaces are released when that makes a
+//   request fit. Later requests may start ahead of a waiting one (backfill) at
+//   most kMaxBypass times, so large requests are not starved.
+// * Each result depends only on its own inputs (no atomics in the arithmetic,
+//   fixed reduction orders): alone or in a mix, a request gives the same bytes.
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/uncte.h"
+#include "internal.h"
+
+namespace {
+
+constexpr int kMaxBypass = 16;
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    long long id = 0;
+    unc_options opt{};
+    int num_rows = 0, num_cols = 0;
+    const int* rows = nullptr;
+    const int* cols = nullptr;
+    const double* vals = nullptr;
+    double* cam = nullptr;
+    double* pt = nullptr;
+    long long bytes = 0;
+    int bypassed = 0;
+    bool done = false;
+    int status = UNC_OK;
+    std::string error;
+    unc_statistic st{};
+    Clock::time_point t_submit, t_start, t_end;
+};
+
+struct Worker {
+    unc_context* ctx = nullptr;
+    long long committed = 0;  // device bytes held or promised (workspace, or the running request's footprint)
+    bool busy = false;
+    std::thread th;
+};
+
+}  // namespace
+
+struct unc_server {
+    int device = 0;
+    long long budget = 0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<std::shared_ptr<Request>> pending;
+    std::unordered_map<long long, std::shared_ptr<Request>> all;
+    std::vector<std::unique_ptr<Worker>> workers;
+    long long next_id = 1;
+    bool stopping = false;
+    int running = 0;
+    long long completed = 0;
+};
+
+namespace {
+
+long long committed_except(const unc_server* s, const Worker* w) {
+    long long t = 0;
+    for (auto& v : s->workers)
+        if (v.get() != w) t += v->committed;
+    return t;
+}
+
+// Under the lock: the request worker `w` may start now, or nullptr.
+std::shared_ptr<Request> pick(unc_server* s, Worker* w) {
+    for (size_t i = 0; i < s->pending.size(); ++i) {
+        auto& r = s->pending[i];
+        const long long mine = std::max(w->committed, r->bytes);
+        bool fits = committed_except(s, w) + mine <= s->budget;
+        if (!fits) {
+            // release idle workspaces (not this worker's) and look again
+            for (auto& v : s->workers)
+                if (v.get() != w && !v->busy && v->committed > 0 && v->ctx) {
+                    unc_context_release(v->ctx);
+                    v->committed = 0;
+                }
+            fits = committed_except(s, w) + mine <= s->budget;
+        }
+        if (fits) {
+            auto req = r;
+            for (size_t j = 0; j < i; ++j) s->pending[j]->bypassed++;
+            s->pending.erase(s->pending.begin() + (long)i);
+            w->committed = mine;
+            return req;
+        }
+        if (r->bypassed >= kMaxBypass) break;  // the head waits for memory; nobody overtakes it any more
+    }
+    return nullptr;
+}
+
+void worker_loop(unc_server* s, Worker* w) {
+    cudaSetDevice(s->device);
+    if (unc_context_create(s->device, &w->ctx) != UNC_OK) w->ctx = nullptr;
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        std::shared_ptr<Request> r;
+        s->cv_work.wait(lk, [&] { return (r = pick(s, w)) != nullptr || (s->stopping && s->pending.empty()); });
+        if (!r) break;
+        w->busy = true;
+        s->running++;
+        lk.unlock();
+        r->t_start = Clock::now();
+        int rc = w->ctx ? unc_compute(w->ctx, &r->opt, r->num_rows, r->num_cols, r->rows, r->cols, r->vals, r->cam,
+                                      r->pt, &r->st)
+                        : UNC_ERR_CUDA;
+        std::string err = rc != UNC_OK ? unc_last_error() : std::string();
+        r->t_end = Clock::now();
+        lk.lock();
+        r->status = rc;
+        r->error = err;
+        r->done = true;
+        w->busy = false;
+        w->committed = w->ctx ? unc_context_device_bytes(w->ctx) : 0;  // what the workspace now holds
+        s->running--;
+        s->completed++;
+        s->cv_done.notify_all();
+        s->cv_work.notify_all();  // memory may have come free for a waiting request
+    }
+    lk.unlock();
+    if (w->ctx) unc_context_destroy(w->ctx);
+    w->ctx = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int unc_server_create(int device, long long max_device_bytes, int max_inflight, unc_server** out) {
+    if (!out || max_inflight <= 0 || max_inflight > 64) {
+        unc::g_last_error = "unc_server_create: out must be non-NULL and max_inflight in 1..64";
+        return UNC_ERR_INVALID_ARG;
+    }
+    *out = nullptr;
+    cudaError_t e = cudaSetDevice(device);
+    size_t free_b = 0, total_b = 0;
+    if (e == cudaSuccess) e = cudaMemGetInfo(&free_b, &total_b);
+    if (e != cudaSuccess) {
+        unc::g_last_error = std::string("unc_server_create: ") + cudaGetErrorString(e);
+        return UNC_ERR_CUDA;
+    }
+    auto* s = new unc_server();
+    s->device = device;
+    s->budget = max_device_bytes > 0 ? max_device_bytes : (long long)(free_b / 10 * 9);
+    for (int i = 0; i < max_inflight; ++i) s->workers.emplace_back(new Worker());
+    for (auto& w : s->workers) w->th = std::thread(worker_loop, s, w.get());
+    *out = s;
+    return UNC_OK;
+}
+
+int unc_server_submit(unc_server* s, const unc_options* opt, int num_rows, int num_cols, const int* rows,
+                      const int* cols, const double* values, double* cam_unc, double* pt_unc, long long* id) {
+    if (!s || !opt || !rows || !cols || !values || !cam_unc || !pt_unc || !id) {
+        unc::g_last_error = "unc_server_submit: null argument";
+        return UNC_ERR_INVALID_ARG;
+    }
+    const long long bytes = unc_request_bytes(opt, num_rows, num_cols, rows, cols);
+    if (bytes < 0) return unc_compute(nullptr, opt, num_rows, num_cols, rows, cols, values, cam_unc, pt_unc,
+                                      nullptr);  // reports the option error without running anything
+    auto r = std::make_shared<Request>();
+    r->opt = *opt;
+    r->num_rows = num_rows;
+    r->num_cols = num_cols;
+    r->rows = rows;
+    r->cols = cols;
+    r->vals = values;
+    r->cam = cam_unc;
+    r->pt = pt_unc;
+    r->bytes = bytes;
+    r->t_submit = Clock::now();
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stopping) {
+        unc::g_last_error = "unc_server_submit: server is shutting down";
+        return UNC_ERR_INVALID_ARG;
+    }
+    if (bytes > s->budget) {
+        unc::g_last_error = "unc_server_submit: request needs " + std::to_string(bytes) +
+                            " device bytes, above the server's budget of " + std::to_string(s->budget);
+        return UNC_ERR_OUT_OF_MEMORY;
+    }
+    r->id = s->next_id++;
+    s->all[r->id] = r;
+    s->pending.push_back(r);
+    *id = r->id;
+    s->cv_work.notify_all();
+    return UNC_OK;
+}
+
+int unc_server_wait(unc_server* s, long long id, double timeout_s, int* status, unc_statistic* st,
+                    double* latency_s, double* queue_s) {
+    if (!s) {
+        unc::g_last_error = "unc_server_wait: server is NULL";
+        return UNC_ERR_INVALID_ARG;
+    }
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) {
+        unc::g_last_error = "unc_server_wait: unknown request id (or already collected)";
+        return UNC_ERR_INVALID_ARG;
+    }
+    std::shared_ptr<Request> r = it->second;
+    auto ready = [&] { return r->done; };
+    if (timeout_s < 0) {
+        s->cv_done.wait(lk, ready);
+    } else if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), ready)) {
+        unc::g_last_error = "unc_server_wait: request still running";
+        return UNC_ERR_TIMEOUT;
+    }
+    s->all.erase(it);
+    if (status) *status = r->status;
+    if (st) *st = r->st;
+    if (latency_s) *latency_s = std::chrono::duration<double>(r->t_end - r->t_submit).count();
+    if (queue_s) *queue_s = std::chrono::duration<double>(r->t_start - r->t_submit).count();
+    if (r->status != UNC_OK) unc::g_last_error = r->error;
+    return UNC_OK;
+}
+
+int unc_server_destroy(unc_server* s) {
+    if (!s) return UNC_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stopping = true;
+        s->cv_work.notify_all();
+    }
+    for (auto& w : s->workers)
+        if (w->th.joinable()) w->th.join();
+    delete s;
+    return UNC_OK;
+}
+
+}  // extern "C"

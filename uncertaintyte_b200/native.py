@@ -81,7 +81,8 @@ EXPORTS = ("unc_options_init", "unc_context_create", "unc_context_destroy", "unc
            "unc_compute_device", "unc_workspace_bytes", "unc_dense_inverse_device",
            "unc_dense_inverse_noalloc", "unc_pinv_psd_device", "unc_jtj_crs",
            "unc_gemm_f64_device", "unc_gemm_mixed_device", "unc_status_string", "unc_last_error",
-           "unc_kernel_launches")
+           "unc_kernel_launches", "unc_request_bytes", "unc_context_device_bytes", "unc_context_release",
+           "unc_server_create", "unc_server_submit", "unc_server_wait", "unc_server_destroy")
 
 _lib = None
 
@@ -110,6 +111,16 @@ def lib():
     L.unc_dense_inverse_device.argtypes = [vp, C.c_int, C.c_int, vp]
     L.unc_dense_inverse_noalloc.argtypes = [vp, C.c_int, C.c_int, vp]
     L.unc_pinv_psd_device.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, vp]
+    L.unc_request_bytes.argtypes = [P(UncOptions), C.c_int, C.c_int, vp, vp]
+    L.unc_request_bytes.restype = C.c_longlong
+    L.unc_context_device_bytes.argtypes = [vp]
+    L.unc_context_device_bytes.restype = C.c_longlong
+    L.unc_context_release.argtypes = [vp]
+    L.unc_server_create.argtypes = [C.c_int, C.c_longlong, C.c_int, P(vp)]
+    L.unc_server_submit.argtypes = [vp, P(UncOptions), C.c_int, C.c_int, vp, vp, vp, vp, vp, P(C.c_longlong)]
+    L.unc_server_wait.argtypes = [vp, C.c_longlong, C.c_double, P(C.c_int), P(UncStatistic), P(C.c_double),
+                                  P(C.c_double)]
+    L.unc_server_destroy.argtypes = [vp]
     L.unc_jtj_crs.argtypes = [C.c_int, C.c_int, vp, vp, vp, C.c_int, C.c_int, P(C.c_longlong), vp,
                               vp, vp]
     L.unc_gemm_f64_device.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, vp, C.c_int, vp, C.c_int,
@@ -209,6 +220,61 @@ def compute_covariances_device(ctx: Context, opts: UncOptions, num_rows: int, nu
     _check(lib().unc_compute_device(ctx.handle, C.byref(opts), num_rows, num_cols, d_rows, d_cols,
                                     d_vals, d_cam, d_pt, C.byref(st), stream or None))
     return st.as_dict()
+
+
+class Server:
+    """Request server on one GPU (continuous batching, admission by device bytes).
+
+    submit() queues a reconstruction and returns its id; wait() returns
+    (cam, pt, stats, latency_s, queue_s) once it has finished. The arrays of a
+    request are kept alive here until its result is collected."""
+
+    def __init__(self, device: int = 0, max_device_bytes: int = 0, max_inflight: int = 4):
+        self._h = C.c_void_p()
+        _check(lib().unc_server_create(device, max_device_bytes, max_inflight, C.byref(self._h)))
+        self._live = {}
+
+    def submit(self, jac: Jacobian, precision: str = "mixed", algorithm: Optional[int] = None) -> int:
+        o = make_options(jac, algorithm, precision)
+        rows = np.ascontiguousarray(jac.rows, dtype=np.int32)
+        cols = np.ascontiguousarray(jac.cols, dtype=np.int32)
+        vals = np.ascontiguousarray(jac.values, dtype=np.float64)
+        cam = np.zeros(jac.num_cams * 45)
+        pt = np.zeros(jac.num_points * 6)
+        rid = C.c_longlong()
+        _check(lib().unc_server_submit(self._h, C.byref(o), jac.num_rows, jac.num_cols, _ptr(rows), _ptr(cols),
+                                       _ptr(vals), _ptr(cam), _ptr(pt), C.byref(rid)))
+        self._live[rid.value] = (o, rows, cols, vals, cam, pt)
+        return rid.value
+
+    def wait(self, rid: int, timeout: float = -1.0):
+        status = C.c_int()
+        st = UncStatistic()
+        lat, que = C.c_double(), C.c_double()
+        _check(lib().unc_server_wait(self._h, rid, timeout, C.byref(status), C.byref(st), C.byref(lat),
+                                     C.byref(que)))
+        _, _, _, _, cam, pt = self._live.pop(rid)
+        _check(status.value)
+        return cam, pt, st.as_dict(), lat.value, que.value
+
+    def close(self):
+        if self._h:
+            lib().unc_server_destroy(self._h)
+            self._h = C.c_void_p()
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def request_bytes(jac: Jacobian, precision: str = "mixed", algorithm: Optional[int] = None) -> int:
+    o = make_options(jac, algorithm, precision)
+    rows = np.ascontiguousarray(jac.rows, dtype=np.int32)
+    cols = np.ascontiguousarray(jac.cols, dtype=np.int32)
+    return int(lib().unc_request_bytes(C.byref(o), jac.num_rows, jac.num_cols, _ptr(rows), _ptr(cols)))
 
 
 def workspace_bytes(jac: Jacobian) -> int:

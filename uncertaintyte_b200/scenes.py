@@ -242,6 +242,43 @@ def make_scene(name: str, seed: int = 0) -> Scene:
     return Scene(cams, pts, obs_cam[o].astype(np.int32), obs_pt[o].astype(np.int32))
 
 
+def make_sized_scene(num_cams: int, points_per_cam: int, lam: float, seed: int = 0, window: int = 48) -> Scene:
+    """A scene of any size for the batched and serving workloads: num_cams
+    cameras on a sphere cap (r = 20, 15-60 degrees from the pole) looking at
+    the origin, f ~ U(800, 1200), k1, k2 ~ N(0, 1e-2); points_per_cam * num_cams
+    points uniform in a 4 x 4 x 2 box; each point seen by 2 + Poisson(lam)
+    distinct cameras drawn from the `window` cameras nearest to it in azimuth."""
+    rng = np.random.default_rng(seed)
+    C, P = int(num_cams), int(points_per_cam) * int(num_cams)
+    th = np.arccos(rng.uniform(np.cos(np.radians(60)), np.cos(np.radians(15)), C))
+    ph = rng.uniform(0, 2 * np.pi, C)
+    centers = 20 * np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], 1)
+    f = rng.uniform(800, 1200, C)
+    pts = rng.uniform([-2, -2, -1], [2, 2, 1], (P, 3))
+    aa = _look_at_aa(centers, np.zeros(3))
+    k12 = rng.normal(0, 1e-2, (C, 2))
+    cams = np.concatenate([aa, centers, f[:, None], k12], axis=1)
+    w = min(window, C)
+    counts = np.minimum(2 + rng.poisson(lam, P), w)
+    order = np.argsort(ph)
+    pt_az = np.mod(np.arctan2(pts[:, 1], pts[:, 0]), 2 * np.pi)
+    idx = np.searchsorted(ph[order], pt_az)
+    start = np.clip(idx - w // 2, 0, C - w)
+    sel, mask = _choose(rng, P, counts, w, start)
+    sel = order[sel]
+    obs_pt = np.repeat(np.arange(P), counts)
+    obs_cam = sel[mask]
+    key = obs_pt.astype(np.int64) * (C + 1) + obs_cam
+    o = np.argsort(key, kind="stable")
+    return Scene(cams, pts, obs_cam[o].astype(np.int32), obs_pt[o].astype(np.int32))
+
+
+def sample_camera_counts(n: int, median: float, sigma: float, lo: int, hi: int, seed: int) -> np.ndarray:
+    """Camera counts lognormal(median, sigma) clipped to [lo, hi] (batched / serving workloads)."""
+    rng = np.random.default_rng(seed)
+    return np.clip(np.round(median * np.exp(sigma * rng.standard_normal(n))), lo, hi).astype(int)
+
+
 def scene_jacobian(scene: Scene, with_fixed: bool = True) -> Jacobian:
     """CRS Jacobian (reference layout) of a synthetic scene."""
     C, P = len(scene.cams), len(scene.points)
