@@ -45,6 +45,10 @@ WORKLOADS = {
     "small": "small scene: 10 cams (ring r=10), 500 pts, 2+Poisson(4) obs/pt, N=90, TAYLOR_EXPANSION",
     "large": "large scene: 2000 cams (3-loop trajectory), 500k pts, 2+Poisson(5) obs/pt, N=18000, "
              "TAYLOR_EXPANSION",
+    "batch": "256 uneven scenes: cams lognormal(median 60, sigma 1) clipped [8,400], pts = 150 x cams, "
+             "2+Poisson(4) obs/pt, TAYLOR_EXPANSION",
+    "serve": "request stream: Poisson arrivals, scenes from a seeded pool of 32 with cams lognormal(median 150, "
+             "sigma 1.2) clipped [8,3000], pts = 200 x cams, 2+Poisson(5) obs/pt, TAYLOR_EXPANSION",
 }
 METRIC = "covariance solve throughput (1 / solve time)"
 UNIT = "solves/s"
@@ -60,6 +64,11 @@ def _args():
     ap.add_argument("--precision", choices=["fp64", "mixed", "mixed4", "mixed3"], default="mixed")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scenes", type=int, default=256, help="batch: number of scenes")
+    ap.add_argument("--requests", type=int, default=200, help="serve: requests per precision")
+    ap.add_argument("--rate", type=float, default=10.0, help="serve: Poisson arrival rate (requests/s)")
+    ap.add_argument("--pool", type=int, default=32, help="serve: distinct scenes the requests draw from")
+    ap.add_argument("--inflight", type=int, default=8, help="batch/serve: concurrent requests on the GPU")
     return ap.parse_args()
 
 
@@ -179,8 +188,10 @@ def run_reference(a):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from uncertaintyte_b200 import scenes
-    jac = scenes.synthetic_jacobian(a.workload, seed=0)
     cores = os.cpu_count() or 1
+    if a.workload in ("batch", "serve"):
+        return _reference_many(a, oracle, cores)
+    jac = scenes.synthetic_jacobian(a.workload, seed=0)
     faithful = a.workload != "large"
     for _ in range(a.warmup):
         oracle.compute(jac, threads=cores, faithful_point_scan=faithful)
@@ -200,6 +211,39 @@ def run_reference(a):
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _reference_many(a, oracle, cores, budget_s: float = 20.0):
+    """CPU oracle over the batched / serving scenes, one after another, for
+    about budget_s seconds (a bounded sample of the workload)."""
+    kind = a.workload
+    counts, jacs = _scene_set(kind, a.scenes if kind == "batch" else a.pool, seed=0 if kind == "batch" else 1)
+    if kind == "serve":  # the requests' scenes in stream order
+        picks = np.random.default_rng(2).integers(0, len(jacs), a.requests)
+        jacs = [jacs[k] for k in picks]
+    oracle.compute(jacs[0], threads=cores)
+    ts, t_all = [], time.perf_counter()
+    for j in jacs:
+        t0 = time.perf_counter()
+        oracle.compute(j, threads=cores, faithful_point_scan=True)
+        ts.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_all > budget_s:
+            break
+    n = len(ts)
+    if kind == "batch":
+        value, unit, metric, hib = n / sum(ts), "scenes/s", "batched covariance solves (256 uneven scenes)", True
+    else:
+        value, unit, metric, hib = 1e3 * _pct(ts, 50), "ms (p50 latency)", \
+            "served latency p50/p99 and throughput (mixed precision)", False
+    sample = f"the first {n} of the workload's scenes, one after another, faithful point scan"
+    line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": a.gpus, "steps": n,
+            "warmup": 1, "ms_per_step": 1e3 * sum(ts) / n, "higher_is_better": hib, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, no public dataset)",
+            "config": {"workload": WORKLOADS[kind], "threads": cores}, "per_scene_ms": _dist_ms(ts),
+            "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -442,10 +486,171 @@ def run_ours(a):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# batched (256 uneven scenes) and serving (Poisson request stream) workloads
+# ---------------------------------------------------------------------------
+def _gen_scene(args):
+    C, ppc, lam, seed = args
+    from uncertaintyte_b200 import scenes
+    return scenes.scene_jacobian(scenes.make_sized_scene(C, ppc, lam, seed))
+
+
+def _scene_set(kind: str, n: int, seed: int):
+    """Scenes of the batched / serving workloads, generated in spawned processes."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+
+    from uncertaintyte_b200 import scenes
+    if kind == "batch":
+        counts, ppc, lam = scenes.sample_camera_counts(n, 60, 1.0, 8, 400, seed), 150, 4
+    else:
+        counts, ppc, lam = scenes.sample_camera_counts(n, 150, 1.2, 8, 3000, seed), 200, 5
+    jobs = [(int(C), ppc, lam, seed * 100003 + i) for i, C in enumerate(counts)]
+    with ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1), mp_context=mp.get_context("spawn")) as ex:
+        jacs = list(ex.map(_gen_scene, jobs))
+    return counts, jacs
+
+
+def _pct(x, q):
+    return float(np.percentile(np.asarray(x), q)) if len(x) else None
+
+
+def _dist_ms(x):
+    return {"p50": 1e3 * _pct(x, 50), "p90": 1e3 * _pct(x, 90), "p99": 1e3 * _pct(x, 99),
+            "max": 1e3 * float(np.max(x)), "mean": 1e3 * float(np.mean(x))}
+
+
+def run_batch(a):
+    ws, rank, local = _dist()
+    counts, jacs = _scene_set("batch", a.scenes, seed=rank)
+    from uncertaintyte_b200 import native
+    prec = a.precision
+    ctx = native.Context(local)
+    for j in jacs[:4]:
+        native.compute_covariances(j, ctx, precision=prec)
+    # per-scene sequential loop through the public host API
+    seq_t, seq_res = [], []
+    l0 = native.kernel_launches()
+    t0 = time.perf_counter()
+    for j in jacs:
+        ts = time.perf_counter()
+        c, p, _ = native.compute_covariances(j, ctx, precision=prec)
+        seq_t.append(time.perf_counter() - ts)
+        seq_res.append((c, p))
+    t_seq = time.perf_counter() - t0
+    ctx.close()
+    # the same scenes submitted at once to the request server
+    srv = native.Server(local, 0, a.inflight)
+    for rid in [srv.submit(j, precision=prec) for j in jacs[:a.inflight]]:
+        srv.wait(rid)
+    clocks = ClockSampler(local)
+    clocks.start()
+    clocks.mark(True)
+    l1 = native.kernel_launches()
+    t0 = time.perf_counter()
+    ids = [srv.submit(j, precision=prec) for j in jacs]
+    out = [srv.wait(i) for i in ids]
+    t_b = time.perf_counter() - t0
+    launches = native.kernel_launches() - l1
+    clocks.mark(False)
+    clk = clocks.stop()
+    srv.close()
+    identical = all(np.array_equal(c0, o[0]) and np.array_equal(p0, o[1]) for (c0, p0), o in zip(seq_res, out))
+    n = len(jacs)
+    h2d = sum(j.rows.nbytes + j.cols.nbytes + j.values.nbytes for j in jacs)
+    d2h = sum(8 * (45 * j.num_cams + 6 * j.num_points) for j in jacs)
+    line = {"metric": "batched covariance solves (256 uneven scenes)", "value": n / t_b, "unit": "scenes/s",
+            "n_gpus": ws, "steps": 1, "warmup": 1, "ms_per_step": 1e3 * t_b, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == "fp64" else "i8-sliced products, f64 elsewhere",
+            "data": "synthetic (seeded generator with the configuration's shapes; no public dataset)",
+            "config": {"workload": WORKLOADS["batch"], "precision": prec, "inflight": a.inflight,
+                       "cams_total": int(np.sum(counts)), "cams_median": float(np.median(counts)),
+                       "timing": "host wall clock, host arrays in and out (end to end)"},
+            "sequential_loop": {"seconds": t_seq, "scenes_per_s": n / t_seq, "per_scene_ms": _dist_ms(seq_t),
+                                "gpu_launches": int(l1 - l0)},
+            "batched": {"seconds": t_b, "speedup_vs_sequential": t_seq / t_b,
+                        "completion_latency_ms": _dist_ms([o[3] for o in out]),
+                        "identical_to_sequential": bool(identical)},
+            "e2e": {"value": n / t_b, "unit": "scenes/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches), "clocks": clk}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serve(a):
+    ws, rank, local = _dist()
+    counts, jacs = _scene_set("serve", a.pool, seed=1 + rank)
+    from uncertaintyte_b200 import native
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    rng = np.random.default_rng(2 + rank)
+    picks = rng.integers(0, len(jacs), a.requests)
+    gaps = rng.exponential(1.0 / a.rate, a.requests)
+    res, first = {}, {}
+    clk = None
+    for prec in ("mixed", "fp64"):
+        srv = native.Server(local, 0, a.inflight)
+        warm = [srv.submit(j, precision=prec) for j in jacs]  # every pool scene once, untimed
+        first[prec] = [srv.wait(i)[:2] for i in warm]
+        clocks = ClockSampler(local) if prec == "mixed" else None
+        if clocks:
+            clocks.start()
+            clocks.mark(True)
+        ids = []
+        t0 = time.perf_counter()
+        due = t0
+        for k in range(a.requests):
+            due += gaps[k]
+            wait = due - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            ids.append(srv.submit(jacs[picks[k]], precision=prec))
+        out = [srv.wait(i) for i in ids]
+        t1 = time.perf_counter()
+        if clocks:
+            clocks.mark(False)
+            clk = clocks.stop()
+        srv.close()
+        lat, que = [o[3] for o in out], [o[4] for o in out]
+        res[prec] = {"latency_ms": _dist_ms(lat), "queue_ms": _dist_ms(que),
+                     "throughput_req_s": a.requests / (t1 - t0), "seconds": t1 - t0}
+    from conftest import block_rel_err
+    ec = max(block_rel_err(m[0], f[0], 45) for m, f in zip(first["mixed"], first["fp64"]))
+    ep = max(block_rel_err(m[1], f[1], 6) for m, f in zip(first["mixed"], first["fp64"]))
+    m = res["mixed"]
+    line = {"metric": "served latency p50/p99 and throughput (mixed precision)", "value": m["latency_ms"]["p50"],
+            "unit": "ms (p50 latency)", "p99_ms": m["latency_ms"]["p99"],
+            "throughput_req_s": m["throughput_req_s"], "n_gpus": ws, "steps": a.requests, "warmup": a.pool,
+            "ms_per_step": 1e3 * m["seconds"] / a.requests, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "i8-sliced products, f64 elsewhere",
+            "data": "synthetic (seeded pool of scenes with the configuration's shapes; no public dataset)",
+            "config": {"workload": WORKLOADS["serve"], "requests": a.requests, "rate_req_s": a.rate,
+                       "inflight": a.inflight, "pool_cams": sorted(int(c) for c in counts),
+                       "timing": "submit to result, host wall clock, host arrays in and out"},
+            "mixed": m, "fp64": res["fp64"],
+            "p99_speedup_mixed_over_fp64": res["fp64"]["latency_ms"]["p99"] / m["latency_ms"]["p99"],
+            "mixed_vs_fp64_max_rel_err": {"camera_9x9": ec, "point_3x3": ep, "bar": 1e-6},
+            "e2e": {"value": m["latency_ms"]["p50"], "unit": "ms (p50 latency)",
+                    "h2d_bytes_per_step": int(np.mean([jacs[k].values.nbytes + jacs[k].cols.nbytes
+                                                        + jacs[k].rows.nbytes for k in picks])),
+                    "d2h_bytes_per_step": int(np.mean([8 * (45 * jacs[k].num_cams + 6 * jacs[k].num_points)
+                                                       for k in picks]))},
+            "clocks": clk}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = _args()
     if a.impl == "reference":
         return run_reference(a)
+    if a.workload == "batch":
+        return run_batch(a)
+    if a.workload == "serve":
+        return run_serve(a)
     return run_ours(a)
 
 

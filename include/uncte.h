@@ -127,6 +127,10 @@ long long unc_request_bytes(const unc_options* opt, int num_rows, int num_cols, 
  * (the next call allocates again). No counterpart in the reference. */
 long long unc_context_device_bytes(const unc_context* ctx);
 int unc_context_release(unc_context* ctx);
+/* Run the context's work on the device's highest-priority stream (high != 0)
+ * or a default-priority one: latency-sensitive small requests next to large
+ * ones. No counterpart in the reference. */
+int unc_context_set_priority(unc_context* ctx, int high);
 
 /* ---- Request server: many reconstructions on one GPU (no counterpart in the
  * reference, which computes one reconstruction per call and is not

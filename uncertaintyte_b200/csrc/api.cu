@@ -30,6 +30,7 @@ struct unc_context {
     void* mp = nullptr;   // int8 slice planes of the mixed-precision products
     size_t mp_bytes = 0;
     cudaEvent_t ev[12] = {};
+    int priority = 0;  // of `stream` (0: the default priority)
     // profiling of the Taylor-series products
     bool prof = false;
     std::vector<cudaEvent_t> pev;
@@ -432,6 +433,24 @@ int unc_context_release(unc_context* c) {
         *sizes[i] = 0;
     }
     CK(cudaStreamSynchronize(c->stream));
+    return UNC_OK;
+}
+
+int unc_context_set_priority(unc_context* c, int high) {
+    if (!c) return fail(UNC_ERR_INVALID_ARG, "ctx is NULL");
+    int least = 0, greatest = 0;
+    CK(cudaSetDevice(c->device));
+    CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    const int want = high ? greatest : least;
+    if (want == c->priority) return UNC_OK;
+    cudaStream_t s = nullptr;
+    CK(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, want));
+    if (c->stream) {
+        cudaStreamSynchronize(c->stream);
+        cudaStreamDestroy(c->stream);
+    }
+    c->stream = s;
+    c->priority = want;
     return UNC_OK;
 }
 

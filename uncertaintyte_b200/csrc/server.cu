@@ -17,6 +17,10 @@
 //   within `max_device_bytes`. Idle workspaces are released when that makes a
 //   request fit. Later requests may start ahead of a waiting one (backfill) at
 //   most kMaxBypass times, so large requests are not starved.
+// * Small requests (footprint <= kSmallBytes) run on high-priority streams,
+//   so the block scheduler serves their kernels ahead of a large request's
+//   GEMM tiles, and a quarter of the workers take small requests only, so a
+//   burst of large requests cannot hold every slot.
 // * Each result depends only on its own inputs (no atomics in the arithmetic,
 //   fixed reduction orders): alone or in a mix, a request gives the same bytes.
 #include <chrono>
@@ -35,6 +39,7 @@
 namespace {
 
 constexpr int kMaxBypass = 16;
+constexpr long long kSmallBytes = 1LL << 30;
 
 using Clock = std::chrono::steady_clock;
 
@@ -48,6 +53,7 @@ struct Request {
     double* cam = nullptr;
     double* pt = nullptr;
     long long bytes = 0;
+    bool small = false;
     int bypassed = 0;
     bool done = false;
     int status = UNC_OK;
@@ -60,6 +66,7 @@ struct Worker {
     unc_context* ctx = nullptr;
     long long committed = 0;  // device bytes held or promised (workspace, or the running request's footprint)
     bool busy = false;
+    bool small_only = false;  // reserved for small requests
     std::thread th;
 };
 
@@ -92,6 +99,7 @@ long long committed_except(const unc_server* s, const Worker* w) {
 std::shared_ptr<Request> pick(unc_server* s, Worker* w) {
     for (size_t i = 0; i < s->pending.size(); ++i) {
         auto& r = s->pending[i];
+        if (w->small_only && !r->small) continue;  // not this worker's kind; no bypass counted
         const long long mine = std::max(w->committed, r->bytes);
         bool fits = committed_except(s, w) + mine <= s->budget;
         if (!fits) {
@@ -105,7 +113,8 @@ std::shared_ptr<Request> pick(unc_server* s, Worker* w) {
         }
         if (fits) {
             auto req = r;
-            for (size_t j = 0; j < i; ++j) s->pending[j]->bypassed++;
+            for (size_t j = 0; j < i; ++j)
+                if (!w->small_only || s->pending[j]->small) s->pending[j]->bypassed++;
             s->pending.erase(s->pending.begin() + (long)i);
             w->committed = mine;
             return req;
@@ -127,6 +136,7 @@ void worker_loop(unc_server* s, Worker* w) {
         s->running++;
         lk.unlock();
         r->t_start = Clock::now();
+        if (w->ctx) unc_context_set_priority(w->ctx, r->small ? 1 : 0);
         int rc = w->ctx ? unc_compute(w->ctx, &r->opt, r->num_rows, r->num_cols, r->rows, r->cols, r->vals, r->cam,
                                       r->pt, &r->st)
                         : UNC_ERR_CUDA;
@@ -169,6 +179,7 @@ int unc_server_create(int device, long long max_device_bytes, int max_inflight, 
     s->device = device;
     s->budget = max_device_bytes > 0 ? max_device_bytes : (long long)(free_b / 10 * 9);
     for (int i = 0; i < max_inflight; ++i) s->workers.emplace_back(new Worker());
+    for (int i = 0; i < max_inflight / 4; ++i) s->workers[i]->small_only = true;
     for (auto& w : s->workers) w->th = std::thread(worker_loop, s, w.get());
     *out = s;
     return UNC_OK;
@@ -193,6 +204,7 @@ int unc_server_submit(unc_server* s, const unc_options* opt, int num_rows, int n
     r->cam = cam_unc;
     r->pt = pt_unc;
     r->bytes = bytes;
+    r->small = bytes <= kSmallBytes;
     r->t_submit = Clock::now();
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stopping) {

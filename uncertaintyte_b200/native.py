@@ -82,6 +82,7 @@ EXPORTS = ("unc_options_init", "unc_context_create", "unc_context_destroy", "unc
            "unc_dense_inverse_noalloc", "unc_pinv_psd_device", "unc_jtj_crs",
            "unc_gemm_f64_device", "unc_gemm_mixed_device", "unc_status_string", "unc_last_error",
            "unc_kernel_launches", "unc_request_bytes", "unc_context_device_bytes", "unc_context_release",
+           "unc_context_set_priority",
            "unc_server_create", "unc_server_submit", "unc_server_wait", "unc_server_destroy")
 
 _lib = None
@@ -116,6 +117,7 @@ def lib():
     L.unc_context_device_bytes.argtypes = [vp]
     L.unc_context_device_bytes.restype = C.c_longlong
     L.unc_context_release.argtypes = [vp]
+    L.unc_context_set_priority.argtypes = [vp, C.c_int]
     L.unc_server_create.argtypes = [C.c_int, C.c_longlong, C.c_int, P(vp)]
     L.unc_server_submit.argtypes = [vp, P(UncOptions), C.c_int, C.c_int, vp, vp, vp, vp, vp, P(C.c_longlong)]
     L.unc_server_wait.argtypes = [vp, C.c_longlong, C.c_double, P(C.c_int), P(UncStatistic), P(C.c_double),
