@@ -357,113 +357,170 @@ size_t chol_small_doubles(int n) { (void)n; return (size_t)NB * NB + 64; }
 
 // Leaf: Cholesky of the kb x kb (kb <= 64) diagonal block of A at (k0, k0)
 // and T_kk = L_kk^{-1}, written as a full kb x kb block of T (zeros above the
-// diagonal). One CTA of 512 threads; the block and its inverse live in shared
-// memory and every loop stays rolled (a fully unrolled elimination is
-// instruction-fetch bound: each instruction would run once).
-//  * factor, step p: rank-1 update of the trailing square by a 32 x 16 thread
-//    grid (2 x 4 elements per thread, both factors cached in registers);
-//    column p-1 is scaled by 1/sqrt(d) in the same step (nobody reads it any
-//    more), so each step needs a single barrier.
-//  * inverse: forward elimination on [L | I], row p of T scaled one step
-//    later for the same reason.
+// diagonal). One CTA of 512 threads, the block (S) and its inverse (Ts) in
+// shared memory, blocked in 16-column panels so that few steps are
+// block-wide (a column-at-a-time elimination is 128 dependent barrier steps
+// and latency-bound):
+//  * per panel: one warp factors the 16 x 16 diagonal block in registers
+//    (lane = row, columns broadcast by shuffle) and writes its inverse
+//    D = L_qq^{-1} into the diagonal block of Ts; all threads solve the rows below, L_iq = A_iq D^T;
+//    then one rank-16 update of the trailing square;
+//  * inverse: block forward substitution by block rows,
+//    T_ij = -D_i sum_{k=j}^{i-1} L_ik T_kj (j < i), T_ii = D_i.
 // Non-positive or non-finite pivots set ERRBIT_SINGULAR.
 constexpr int LEAF_THREADS = 512;
-constexpr int LEAF_RY = NB / (LEAF_THREADS / 16);  // rows per thread in the 16-column thread grid
 constexpr int LEAF_LD = NB + 1;
-constexpr size_t LEAF_SMEM = sizeof(double) * (2 * NB * LEAF_LD + 2 * NB);
+constexpr int LEAF_PW = 16;  // panel width
+constexpr size_t LEAF_SMEM = sizeof(double) * (2 * NB * LEAF_LD);
 
 __global__ void __launch_bounds__(LEAF_THREADS) k_chol_leaf(const double* __restrict__ A, long lda, int k0,
                                                             int kb, double* T, long ldt, int* err) {
     extern __shared__ __align__(16) double lsm[];
-    double* S = lsm;                     // S[i * LEAF_LD + j]: the block, then L (lower)
-    double* Ts = lsm + NB * LEAF_LD;     // T = L^{-1}
-    double* rs = Ts + NB * LEAF_LD;      // 1 / sqrt(pivot)
-    double* ri = rs + NB;                // 1 / L(p, p)
-    const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+    double* S = lsm;                  // S[i * LEAF_LD + j]: the block, then L (lower)
+    double* Ts = lsm + NB * LEAF_LD;  // T = L^{-1}
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     for (int e = tid; e < NB * NB; e += LEAF_THREADS) {
         const int i = e & (NB - 1), j = e >> 6;  // column-major walk: coalesced reads of A
         S[i * LEAF_LD + j] = (i < kb && j < kb && j <= i) ? A[(k0 + i) + (long)(k0 + j) * lda] : 0.0;
-        Ts[i * LEAF_LD + j] = (i == j && i < kb) ? 1.0 : 0.0;
+        Ts[i * LEAF_LD + j] = 0.0;
     }
     __syncthreads();
-    for (int p = 0; p < kb; ++p) {
-        const double d = S[p * LEAF_LD + p];
-        const double r = rsqrt(d);
-        if (tid == 0) {
-            rs[p] = r;
-            if (!(d > 0.0 && d <= 1.7976931348623157e308)) atomicOr(err, ERRBIT_SINGULAR);
-        }
-        if (p > 0 && tid < kb - p + 1) {  // delayed scaling of column p - 1 (rows >= p - 1)
-            const int i = p - 1 + tid;
-            S[i * LEAF_LD + p - 1] *= rs[p - 1];
-        }
-        // rank-1 update of the whole trailing square (the upper half is never
-        // read as L): 16 loads, 16 FMAs, 16 stores per thread, all independent
-        double ci[LEAF_RY], cj[4], v[LEAF_RY][4];
-        constexpr int SY = LEAF_THREADS / 16;
+    const int npan = (kb + LEAF_PW - 1) / LEAF_PW;
+    for (int q = 0; q < npan; ++q) {
+        const int c0 = q * LEAF_PW, b = min(LEAF_PW, kb - c0);
+        // (A) warp 0: Cholesky of the diagonal block, then D = its inverse, in
+        // registers (lane l holds row l; column p is broadcast by shuffle)
+        if (warp == 0) {
+            const int l = lane;
+            double a[LEAF_PW], t[LEAF_PW], rinv[LEAF_PW];
 #pragma unroll
-        for (int u = 0; u < LEAF_RY; ++u) {
-            const int i = p + 1 + ty + SY * u;
-            ci[u] = i < kb ? S[i * LEAF_LD + p] * r : 0.0;
-        }
+            for (int j = 0; j < LEAF_PW; ++j)
+                a[j] = (l < b && j <= l && j < b) ? S[(c0 + l) * LEAF_LD + c0 + j] : 0.0;
 #pragma unroll
-        for (int w = 0; w < 4; ++w) {
-            const int j = p + 1 + tx + 16 * w;
-            cj[w] = j < kb ? S[j * LEAF_LD + p] * r : 0.0;
-        }
+            for (int p = 0; p < LEAF_PW; ++p) {
+                if (p < b) {
+                    const double d = __shfl_sync(0xffffffffu, a[p], p);
+                    const double r = rsqrt(d);
+                    rinv[p] = r;  // 1 / L(p, p)
+                    if (l == 0 && !(d > 0.0 && d <= 1.7976931348623157e308)) atomicOr(err, ERRBIT_SINGULAR);
+                    if (l == p) a[p] = d * r;
+                    if (l > p) a[p] *= r;
+                    const double lp = a[p];
 #pragma unroll
-        for (int u = 0; u < LEAF_RY; ++u)
-#pragma unroll
-            for (int w = 0; w < 4; ++w) {
-                const int i = p + 1 + ty + SY * u, j = p + 1 + tx + 16 * w;
-                v[u][w] = (i < kb && j < kb) ? S[i * LEAF_LD + j] : 0.0;
+                    for (int j = p + 1; j < LEAF_PW; ++j) {
+                        const double ljp = __shfl_sync(0xffffffffu, lp, j);  // L(j, p) from lane j
+                        if (l >= j && l < b) a[j] -= lp * ljp;
+                    }
+                }
             }
+            // lane l: column l of D, D(r, l) = (delta_rl - sum_{l<=k<r} L(r, k) D(k, l)) / L(r, r)
 #pragma unroll
-        for (int u = 0; u < LEAF_RY; ++u)
+            for (int r = 0; r < LEAF_PW; ++r) {
+                double s0 = (r == l) ? 1.0 : 0.0, s1 = 0.0;
 #pragma unroll
-            for (int w = 0; w < 4; ++w) {
-                const int i = p + 1 + ty + SY * u, j = p + 1 + tx + 16 * w;
-                if (i < kb && j < kb) S[i * LEAF_LD + j] = v[u][w] - ci[u] * cj[w];
+                for (int k = 0; k < r; ++k) {
+                    const double v = __shfl_sync(0xffffffffu, a[k], r) * t[k];
+                    if (k & 1) s1 -= v; else s0 -= v;
+                }
+                t[r] = (r >= l && r < b) ? (s0 + s1) * rinv[r] : 0.0;
             }
+            if (l < b) {
+#pragma unroll
+                for (int j = 0; j < LEAF_PW; ++j) {
+                    if (j <= l) S[(c0 + l) * LEAF_LD + c0 + j] = a[j];
+                    if (j < b) Ts[(c0 + j) * LEAF_LD + c0 + l] = t[j];
+                }
+            }
+        }
+        __syncthreads();
+        // (B) rows below the diagonal block: L(i, c0 + j) = sum_{k <= j} A(i, c0 + k) D(j, k)
+        const int r0 = c0 + b, m = kb - r0;
+        double v[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int e = tid + u * LEAF_THREADS;
+            v[u] = 0.0;
+            if (e < m * b) {
+                const int i = r0 + e / b, j = e - (e / b) * b;
+                double s0 = 0.0, s1 = 0.0;
+                int k = 0;
+                for (; k + 1 <= j; k += 2) {
+                    s0 += S[i * LEAF_LD + c0 + k] * Ts[(c0 + j) * LEAF_LD + c0 + k];
+                    s1 += S[i * LEAF_LD + c0 + k + 1] * Ts[(c0 + j) * LEAF_LD + c0 + k + 1];
+                }
+                if (k <= j) s0 += S[i * LEAF_LD + c0 + k] * Ts[(c0 + j) * LEAF_LD + c0 + k];
+                v[u] = s0 + s1;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int e = tid + u * LEAF_THREADS;
+            if (e < m * b) {
+                const int i = r0 + e / b, j = e - (e / b) * b;
+                S[i * LEAF_LD + c0 + j] = v[u];
+            }
+        }
+        __syncthreads();
+        // (C) trailing update S[i][j] -= sum_k L(i, c0 + k) L(j, c0 + k), i, j >= r0
+        for (int e = tid; e < m * m; e += LEAF_THREADS) {
+            const int i = r0 + e / m, j = r0 + e - (e / m) * m;
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < LEAF_PW; ++k)
+                if (k < b) acc[k & 3] += S[i * LEAF_LD + c0 + k] * S[j * LEAF_LD + c0 + k];
+            S[i * LEAF_LD + j] -= (acc[0] + acc[1]) + (acc[2] + acc[3]);
+        }
         __syncthreads();
     }
-    if (tid == 0 && kb > 0) S[(kb - 1) * LEAF_LD + kb - 1] *= rs[kb - 1];
-    __syncthreads();
-    if (tid < kb) ri[tid] = 1.0 / S[tid * LEAF_LD + tid];
-    __syncthreads();
-    for (int p = 0; p < kb; ++p) {
-        const double ip = ri[p];
-        if (p > 0 && tid < p) Ts[(p - 1) * LEAF_LD + tid] *= ri[p - 1];  // delayed scaling of row p - 1
-        double tp[4], li[LEAF_RY], v[LEAF_RY][4];
-        constexpr int SY = LEAF_THREADS / 16;
+    // block forward substitution for the off-diagonal blocks of T
+    for (int bi = 1; bi < npan; ++bi) {
+        const int ri = bi * LEAF_PW, bsz = min(LEAF_PW, kb - ri);
+        const int cnt = bi * LEAF_PW * bsz;  // (j, r, c): block column j < bi, row r < bsz, column c < 16
+        // U_j = sum_{k=j}^{bi-1} L_{bi,k} T_{k,j}, kept in T_{bi,j}
+        for (int e = tid; e < cnt; e += LEAF_THREADS) {
+            const int j = e / (LEAF_PW * bsz), rc = e - j * (LEAF_PW * bsz);
+            const int r = rc / LEAF_PW, c = rc - r * LEAF_PW;
+            const int col = j * LEAF_PW + c;
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            int k = col;
+            for (; k + 3 < ri; k += 4) {
 #pragma unroll
-        for (int w = 0; w < 4; ++w) {
-            const int j = tx + 16 * w;
-            tp[w] = j <= p ? Ts[p * LEAF_LD + j] * ip : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < LEAF_RY; ++u) {
-            const int i = p + 1 + ty + SY * u;
-            li[u] = i < kb ? S[i * LEAF_LD + p] : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < LEAF_RY; ++u)
-#pragma unroll
-            for (int w = 0; w < 4; ++w) {
-                const int i = p + 1 + ty + SY * u, j = tx + 16 * w;
-                v[u][w] = (i < kb && j <= p) ? Ts[i * LEAF_LD + j] : 0.0;
+                for (int u = 0; u < 4; ++u) acc[u] += S[(ri + r) * LEAF_LD + k + u] * Ts[(k + u) * LEAF_LD + col];
             }
+            for (; k < ri; ++k) acc[0] += S[(ri + r) * LEAF_LD + k] * Ts[k * LEAF_LD + col];
+            Ts[(ri + r) * LEAF_LD + col] = (acc[0] + acc[1]) + (acc[2] + acc[3]);
+        }
+        __syncthreads();
+        // T_{bi,j} = -D_bi U_j
+        double w[3];
 #pragma unroll
-        for (int u = 0; u < LEAF_RY; ++u)
+        for (int u = 0; u < 3; ++u) {
+            const int e = tid + u * LEAF_THREADS;
+            w[u] = 0.0;
+            if (e < cnt) {
+                const int j = e / (LEAF_PW * bsz), rc = e - j * (LEAF_PW * bsz);
+                const int r = rc / LEAF_PW, c = rc - r * LEAF_PW;
+                const int col = j * LEAF_PW + c;
+                double acc[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-            for (int w = 0; w < 4; ++w) {
-                const int i = p + 1 + ty + SY * u, j = tx + 16 * w;
-                if (i < kb && j <= p) Ts[i * LEAF_LD + j] = v[u][w] - li[u] * tp[w];
+                for (int mm = 0; mm < LEAF_PW; ++mm)
+                    if (mm <= r) acc[mm & 3] += Ts[(ri + r) * LEAF_LD + ri + mm] * Ts[(ri + mm) * LEAF_LD + col];
+                w[u] = -((acc[0] + acc[1]) + (acc[2] + acc[3]));
             }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+            const int e = tid + u * LEAF_THREADS;
+            if (e < cnt) {
+                const int j = e / (LEAF_PW * bsz), rc = e - j * (LEAF_PW * bsz);
+                const int r = rc / LEAF_PW, c = rc - r * LEAF_PW;
+                Ts[(ri + r) * LEAF_LD + j * LEAF_PW + c] = w[u];
+            }
+        }
         __syncthreads();
     }
-    if (kb > 0 && tid < kb) Ts[(kb - 1) * LEAF_LD + tid] *= ri[kb - 1];
-    __syncthreads();
     for (int e = tid; e < kb * kb; e += LEAF_THREADS) {
         const int j = e / kb, i = e - j * kb;  // column-major walk: coalesced writes of T
         T[(k0 + i) + (long)(k0 + j) * ldt] = Ts[i * LEAF_LD + j];
