@@ -79,6 +79,22 @@ def _dist():
     return ws, rank, local
 
 
+def max_over_ranks(seconds: float, device) -> float:
+    """The slowest rank's time (every rank calls this at the same point)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(seconds)
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world_size: int, steps_per_rank: int, max_seconds: float) -> float:
+    """Whole-job solves/s of independent replicas: all ranks' steps over the slowest rank's time."""
+    return world_size * steps_per_rank / max_seconds
+
+
 class ClockSampler:
     """nvidia-smi clocks/throttle reasons sampled during the timed region."""
 
@@ -355,10 +371,8 @@ def run_ours(a):
         launches = native.kernel_launches() - l0
         prof = ctx.profile(reset=True) if profile else None
         ctx.set_profiling(False)
-        t = torch.tensor([sum(e0.elapsed_time(e1) for e0, e1 in evs) * 1e-3], dtype=torch.float64, device=dev)
-        if ws > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item()), st, launches, prof
+        t = max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in evs) * 1e-3, dev)
+        return t, st, launches, prof
 
     # headline: the requested precision (mixed by default), clocks sampled during it
     clocks = ClockSampler(local)
@@ -366,7 +380,7 @@ def run_ours(a):
     t_main, stats, launches, prof = timed(opts, a.steps, profile=True, clocks=clocks)
     clk = clocks.stop()
     cam_main, pt_main = d_cam.cpu().numpy().copy(), d_pt.cpu().numpy().copy()
-    value = ws * a.steps / t_main
+    value = replica_throughput(ws, a.steps, t_main)
     # the plain FP64 GPU path on the same scene, and the mixed-vs-FP64 error
     fp64 = None
     if prec != "fp64":
@@ -416,10 +430,7 @@ def run_ours(a):
         t0 = time.perf_counter()
         e2e_step()
         te += time.perf_counter() - t0
-    te_t = torch.tensor([te], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(te_t, op=dist.ReduceOp.MAX)
-    e2e_value = ws * e2e_steps / float(te_t.item())
+    e2e_value = replica_throughput(ws, e2e_steps, max_over_ranks(te, dev))
     h2d = h_rows.nbytes + h_cols.nbytes + h_vals.nbytes
     d2h = h_cam.nbytes + h_pt.nbytes
 
