@@ -65,6 +65,7 @@ struct Buffers {
     SceneDev s;
     double *Z, *iZ, *add, *tmp, *e, *gjws, *sig;
     unsigned long long* amax;
+    TeState* te;
 };
 
 // Lay out the workspace; with base == nullptr only the size is computed.
@@ -97,6 +98,7 @@ size_t carve(char* base, const Plan& pl, bool host_io, long long nnz, int nrows,
     s.blk_ptr = c.take<int>((size_t)pl.C * pl.C + 1);
     s.err = c.take<int>(4);
     b.amax = c.take<unsigned long long>(4);
+    b.te = c.take<TeState>(1);
     const size_t nn = (size_t)pl.ld * pl.N;
     b.Z = c.take<double>(nn);
     b.iZ = c.take<double>(nn);
@@ -264,39 +266,35 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         mixed_slice(X, ld, opXa, sm);
     }
     // the profiled region is the product kernel alone (slicing excluded)
-    auto product = [&](const double* P, double* out) -> int {
+    auto product = [&](const double* P, double* out, const int* skip) -> int {
         if (mixed) {
-            if (P != X) mixed_slice(P, ld, opP, sm);
+            if (P != X) mixed_slice(P, ld, opP, sm, skip);
             if (int r = prof_mark()) return r;
-            mixed_gemm(P == X ? opXa : opP, opXb, out, ld, b.amax, true, s.err, sm);
+            mixed_gemm(P == X ? opXa : opP, opXb, out, ld, b.amax, true, s.err, sm, skip);
         } else {
             if (int r = prof_mark()) return r;
-            gemm_f64_ex(N, N, N, 1.0, P, ld, X, ld, 0.0, out, ld, b.amax, true, sm, false);
+            gemm_f64_mode(N, N, N, 1.0, P, ld, X, ld, 0.0, out, ld, b.amax, GEMM_LOWER, sm, nullptr, 0, skip);
         }
         return prof_mark();
     };
+    // The stop rule runs on the device (k_te_decide): the host launches all 19
+    // iterations without waiting; once the rule fires, the remaining kernels
+    // return at once. k = lambda^i / factorial(i-1) is evaluated here exactly
+    // as before (32-bit factorial wrap included).
+    TeState te0{};
+    te0.old_change = DBL_MAX;
+    CK(cudaMemcpyAsync(b.te, &te0, sizeof(TeState), cudaMemcpyHostToDevice, sm));
+    const int* skip = &b.te->done;
     CK(cudaMemsetAsync(b.amax, 0, 8, sm));
-    if (int r = product(X, add)) return r;
+    if (int r = product(X, add, nullptr)) return r;
     launch_mirror_lower(add, N, ld, sm);
-    double old_change = DBL_MAX;
-    int iters = 0;
-    unsigned long long amax_bits = 0;
     for (int i = 1; i < 20; ++i) {
-        CK(cudaMemcpyAsync(&amax_bits, b.amax, 8, cudaMemcpyDeviceToHost, sm));
-        CK(cudaStreamSynchronize(sm));
-        double amax;
-        memcpy(&amax, &amax_bits, 8);
-        amax = std::max(amax, DBL_MIN);  // absMax starts at DBL_MIN (ScaledDenseMatrix.cpp:208)
-        double k = pow(lambda, i) / factorial_i32(i - 1);
-        double change = fabs(k * amax);
-        if (change < 1e-5 || change > old_change) break;
-        old_change = change;
-        if (st) st->cycle_change[iters] = change;
-        iters++;
-        launch_axpy(b.iZ, add, k, N, ld, sm);
+        const double k = pow(lambda, i) / factorial_i32(i - 1);
+        launch_te_decide(b.te, b.amax, k, sm);
+        launch_axpy_te(b.iZ, add, b.te, N, ld, sm);
         CK(cudaMemsetAsync(b.amax, 0, 8, sm));
-        if (int r = product(add, tmp)) return r;
-        launch_mirror_lower(tmp, N, ld, sm);
+        if (int r = product(add, tmp, skip)) return r;
+        launch_mirror_lower(tmp, N, ld, sm, skip);
         std::swap(add, tmp);
     }
     CK(cudaEventRecord(ev[7], sm));
@@ -307,9 +305,14 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     CK(cudaEventRecord(ev[8], sm));
 
     int err = 0;
+    TeState te{};
     CK(cudaMemcpyAsync(&err, s.err, sizeof(int), cudaMemcpyDeviceToHost, sm));
+    CK(cudaMemcpyAsync(&te, b.te, sizeof(TeState), cudaMemcpyDeviceToHost, sm));
     CK(cudaStreamSynchronize(sm));
     CK(cudaGetLastError());
+    const int iters = te.iters;
+    // products actually computed: the first one and one per performed iteration
+    npev = std::min(npev, (size_t)2 * (iters + 1));
     for (size_t i = 0; i + 1 < npev; i += 2) {
         ctx->prof_seconds += ev_s(ctx->pev[i], ctx->pev[i + 1]);
         ctx->prof_launches += 1;
@@ -319,6 +322,7 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         st->lambda = lambda;
         for (int i = 0; i < 3; ++i) st->fixed_pts[i] = fx[i];
         st->te_iterations = iters;
+        for (int i = 0; i < iters && i < 20; ++i) st->cycle_change[i] = te.change[i];
         st->time_create_j = ev_s(ev[0], ev[1]);
         st->time_fix_j = ev_s(ev[1], ev[2]);
         st->time_norm_j = ev_s(ev[2], ev[3]);
@@ -336,11 +340,7 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     if (err & (ERRBIT_SINGULAR | ERRBIT_NONFINITE))
         return fail(UNC_ERR_SINGULAR, "non-positive pivot or non-finite value while inverting Z + lambda*I");
     if (err & ERRBIT_TIMEOUT) return fail(UNC_ERR_CUDA, "tensor-core pipeline wait timed out");
-    {
-        double amax;
-        memcpy(&amax, &amax_bits, 8);
-        if (!(amax <= DBL_MAX)) return fail(UNC_ERR_SINGULAR, "non-finite Taylor-series power");
-    }
+    if (te.bad) return fail(UNC_ERR_SINGULAR, "non-finite Taylor-series power");
     return UNC_OK;
 }
 

@@ -104,8 +104,9 @@ template <class Cfg, bool kTransB>
 __global__ void __launch_bounds__(GEMM_THREADS, (Cfg::BM == 128 ? 1 : 2))
     k_gemm_f64(int M, int N, int K, double alpha, const double* __restrict__ A, long lda,
                const double* __restrict__ B, long ldb, double beta, double* C, long ldc,
-               unsigned long long* amax, int mode, double* part) {
+               unsigned long long* amax, int mode, double* part, const int* skip) {
     constexpr int BM = Cfg::BM, BN = Cfg::BN, FM = Cfg::FM, FN = Cfg::FN;
+    if (skip && *skip) return;
     // GEMM_LOWER: tiles strictly above the diagonal of C are skipped (SYRK-style update)
     if ((mode & GEMM_LOWER) && (int)(blockIdx.x * BN) > (int)(blockIdx.y * BM) + BM - 1) return;
     extern __shared__ __align__(16) double smem[];
@@ -221,7 +222,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, (Cfg::BM == 128 ? 1 : 2))
 // max|C| folded into amax.
 __global__ void k_splitk_reduce(int M, int N, int splits, const double* __restrict__ part, double alpha,
                                 double beta, double* C, long ldc, unsigned long long* amax, int mode, int bm,
-                                int bn) {
+                                int bn, const int* skip) {
+    if (skip && *skip) return;
     const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
     double mx = 0.0;
     if (idx < (long)M * N) {
@@ -258,7 +260,7 @@ int active_tiles(dim3 grid, int mode) {
 template <class Cfg>
 void launch_gemm(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb, double beta,
                  double* C, int ldc, unsigned long long* amax, int mode, cudaStream_t st, double* ws,
-                 size_t ws_doubles) {
+                 size_t ws_doubles, const int* skip) {
     static std::atomic<unsigned long long> attr{0};
     once_per_device(attr, [] {
         cudaFuncSetAttribute(k_gemm_f64<Cfg, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
@@ -281,15 +283,15 @@ void launch_gemm(int M, int N, int K, double alpha, const double* A, int lda, co
     grid.z = splits;
     if (mode & GEMM_TRANS_B)
         k_gemm_f64<Cfg, true><<<grid, GEMM_THREADS, Cfg::SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
-                                                                     ldc, amax, mode, part);
+                                                                     ldc, amax, mode, part, skip);
     else
         k_gemm_f64<Cfg, false><<<grid, GEMM_THREADS, Cfg::SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
-                                                                      ldc, amax, mode, part);
+                                                                      ldc, amax, mode, part, skip);
     count_launch();
     if (part) {
         const long total = (long)M * N;
         k_splitk_reduce<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(M, N, splits, part, alpha, beta, C, ldc,
-                                                                          amax, mode, Cfg::BM, Cfg::BN);
+                                                                          amax, mode, Cfg::BM, Cfg::BN, skip);
         count_launch();
     }
 }
@@ -297,14 +299,14 @@ void launch_gemm(int M, int N, int K, double alpha, const double* A, int lda, co
 
 void gemm_f64_mode(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
                    double beta, double* C, int ldc, unsigned long long* amax, int mode, cudaStream_t st,
-                   double* ws, size_t ws_doubles) {
+                   double* ws, size_t ws_doubles, const int* skip) {
     if (M <= 0 || N <= 0) return;
     // 64 x 64 tiles when 128 x 128 tiles would leave most SMs idle
     const dim3 g128((N + 127) / 128, (M + 127) / 128);
     if (active_tiles<CfgBig>(g128, mode) * 4 <= 148)
-        launch_gemm<CfgSmall>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, amax, mode, st, ws, ws_doubles);
+        launch_gemm<CfgSmall>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, amax, mode, st, ws, ws_doubles, skip);
     else
-        launch_gemm<CfgBig>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, amax, mode, st, ws, ws_doubles);
+        launch_gemm<CfgBig>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, amax, mode, st, ws, ws_doubles, skip);
 }
 
 void gemm_f64_ex(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
@@ -325,7 +327,8 @@ void gemm_f64_tri(int M, int N, int K, double alpha, const double* A, int lda, c
 }
 
 // Copy the strict lower triangle onto the upper one (32 x 32 tiles).
-__global__ void k_mirror_lower(double* Z, int n, long ld) {
+__global__ void k_mirror_lower(double* Z, int n, long ld, const int* skip) {
+    if (skip && *skip) return;
     __shared__ double t[32][33];
     const int bi = blockIdx.y, bj = blockIdx.x;  // tile row, tile col of the source (lower) tile
     if (bj > bi) return;
@@ -340,10 +343,10 @@ __global__ void k_mirror_lower(double* Z, int n, long ld) {
     }
 }
 
-void launch_mirror_lower(double* Z, int n, int ld, cudaStream_t st) {
+void launch_mirror_lower(double* Z, int n, int ld, cudaStream_t st, const int* skip) {
     if (n == 0) return;
     dim3 g((n + 31) / 32, (n + 31) / 32);
-    k_mirror_lower<<<g, dim3(32, 8), 0, st>>>(Z, n, ld);
+    k_mirror_lower<<<g, dim3(32, 8), 0, st>>>(Z, n, ld, skip);
     count_launch();
 }
 
@@ -648,6 +651,44 @@ __global__ void k_axpy(double* Y, const double* __restrict__ X, double k, int n,
 void launch_axpy(double* Y, const double* X, double k, int n, int ld, cudaStream_t st) {
     long total = (long)n * n;
     k_axpy<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(Y, X, k, n, ld);
+    count_launch();
+}
+
+__global__ void k_te_decide(TeState* s, const unsigned long long* amax_bits, double k) {
+    if (threadIdx.x != 0 || blockIdx.x != 0 || s->done) return;
+    double amax = __longlong_as_double((long long)*amax_bits);
+    amax = fmax(amax, 2.2250738585072014e-308);  // absMax starts at DBL_MIN (ScaledDenseMatrix.cpp:208)
+    if (!(amax <= 1.7976931348623157e308)) s->bad = 1;
+    const double change = fabs(k * amax);
+    if (change < 1e-5 || change > s->old_change) {  // compute.cpp:150-152
+        s->done = 1;
+        return;
+    }
+    s->old_change = change;
+    if (s->iters < 20) s->change[s->iters] = change;
+    s->iters += 1;
+    s->coef = k;
+}
+
+void launch_te_decide(TeState* s, const unsigned long long* amax, double k, cudaStream_t st) {
+    k_te_decide<<<1, 32, 0, st>>>(s, amax, k);
+    count_launch();
+}
+
+__global__ void k_axpy_te(double* Y, const double* __restrict__ X, const TeState* s, int n, long ld) {
+    if (s->done) return;
+    const double k = s->coef;
+    long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long total = (long)n * n;
+    if (idx >= total) return;
+    int c = (int)(idx / n), r = (int)(idx - (long)c * n);
+    long o = r + c * ld;
+    Y[o] = Y[o] + k * X[o];
+}
+
+void launch_axpy_te(double* Y, const double* X, const TeState* s, int n, int ld, cudaStream_t st) {
+    long total = (long)n * n;
+    k_axpy_te<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(Y, X, s, n, ld);
     count_launch();
 }
 

@@ -138,10 +138,12 @@ enum : int {
 };
 // ws (ws_doubles): optional scratch that enables split-K for outputs with
 // fewer tiles than SMs (partials summed in a fixed order by a second kernel).
+// skip: optional device flag; when it is non-zero the kernels return at once
+// (the Taylor loop launches all its iterations and stops on the device).
 void gemm_f64_mode(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
                    double beta, double* C, int ldc, unsigned long long* amax, int mode, cudaStream_t st,
-                   double* ws = nullptr, size_t ws_doubles = 0);
-void launch_mirror_lower(double* Z, int n, int ld, cudaStream_t st);
+                   double* ws = nullptr, size_t ws_doubles = 0, const int* skip = nullptr);
+void launch_mirror_lower(double* Z, int n, int ld, cudaStream_t st, const int* skip = nullptr);
 // Same, skipping output tiles strictly above the diagonal (symmetric updates).
 void gemm_f64_tri(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb,
                   double beta, double* C, int ldc, cudaStream_t st);
@@ -160,6 +162,22 @@ void launch_shift_equilibrate(double* A, int n, int lda, double lambda, double* 
 void launch_unequilibrate(double* X, int n, int lda, const double* e, double* Y, cudaStream_t st);
 // Y <- Y + k*X  (N x N, column-major)
 void launch_axpy(double* Y, const double* X, double k, int n, int ld, cudaStream_t st);
+
+// Device-side control of the Taylor loop (compute.cpp:141-160): the stop rule
+// runs on the device so that the host never waits inside the loop.
+struct TeState {
+    int done;               // the loop has stopped: later iteration kernels return at once
+    int bad;                // a power was not finite
+    int iters;              // iterations performed
+    double old_change;      // previous |k * max|add||
+    double coef;            // k of the current iteration (read by the axpy)
+    double change[20];      // cycle_change record
+};
+// One thread: change = |k * max(amax, DBL_MIN)|; stop when change < 1e-5 or
+// change > old_change, else record it and publish k for the axpy.
+void launch_te_decide(TeState* s, const unsigned long long* amax, double k, cudaStream_t st);
+// Y <- Y + s->coef * X unless s->done.
+void launch_axpy_te(double* Y, const double* X, const TeState* s, int n, int ld, cudaStream_t st);
 void launch_zero(double* p, size_t n, cudaStream_t st);
 // Camera output (a+b/2 quirk) and the unscaled 9x9 camera covariance blocks.
 void launch_camera_output(const double* iZ, int ldz, const double* s_cam, int num_cams,
@@ -179,10 +197,10 @@ size_t mixed_slice_bytes(int n, int slices);
 // Prepare the operand over buf/exps (as_b: box rows of the B operand). False
 // when the driver's tensor-map encoder is unavailable.
 bool mixed_plan(MixedOperand& op, int8_t* buf, int* exps, int n, int slices, bool as_b);
-void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st);
+void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st, const int* skip = nullptr);
 // C = P * X from the slices of P (a) and X (b); lower_only: tiles on/below the diagonal.
 void mixed_gemm(const MixedOperand& a, const MixedOperand& b, double* C, int ldc, unsigned long long* amax,
-                bool lower_only, int* err, cudaStream_t st);
+                bool lower_only, int* err, cudaStream_t st, const int* skip = nullptr);
 
 // ---------------- svd.cu ----------------
 // Scratch of the PSD pseudo-inverse (n x ld matrices and p x n blocks).

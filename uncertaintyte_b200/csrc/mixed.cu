@@ -136,7 +136,8 @@ using namespace mp;
 // max_k |A[j,k]| 2^-e < 1/2. One CTA per row.
 __global__ void __launch_bounds__(256) k_slice_rows(const double* __restrict__ A, long lda, int n, int S,
                                                    int8_t* __restrict__ out, int rows_pad, int kp,
-                                                   int* __restrict__ exps) {
+                                                   int* __restrict__ exps, const int* skip) {
+    if (skip && *skip) return;
     __shared__ double red[8];
     const int j = blockIdx.x;
     const double* col = A + (long)j * lda;
@@ -190,8 +191,9 @@ template <int NT, int S>
 __global__ void __launch_bounds__(THREADS, 1)
     k_ozaki_gemm(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int M, int N,
                  int kp, int rowsA, int rowsB, const int* __restrict__ eA, const int* __restrict__ eB, double* C,
-                 long ldc, unsigned long long* amax, int lower_only, int* err) {
+                 long ldc, unsigned long long* amax, int lower_only, int* err, const int* skip) {
     using Sh = Shape<NT, S>;
+    if (skip && *skip) return;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * NT;
     if (lower_only && n0 > m0 + BM - 1) return;
     extern __shared__ uint8_t smem_raw[];
@@ -413,38 +415,38 @@ bool mixed_plan(MixedOperand& op, int8_t* buf, int* exps, int n, int slices, boo
     return make_map(&op.map, buf, op.rows * slices, op.kp, as_b ? nt : BM);
 }
 
-void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st) {
-    k_slice_rows<<<op.n, 256, 0, st>>>(A, lda, op.n, op.slices, op.buf, op.rows, op.kp, op.exps);
+void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st, const int* skip) {
+    k_slice_rows<<<op.n, 256, 0, st>>>(A, lda, op.n, op.slices, op.buf, op.rows, op.kp, op.exps, skip);
     count_launch();
 }
 
 void mixed_gemm(const MixedOperand& a, const MixedOperand& b, double* C, int ldc, unsigned long long* amax,
-                bool lower_only, int* err, cudaStream_t st) {
+                bool lower_only, int* err, cudaStream_t st, const int* skip) {
     const int n = a.n;
     if (a.slices == 4) {
         set_attr_once<128, 4>();
         dim3 grid((n + 127) / 128, (n + BM - 1) / BM);
         k_ozaki_gemm<128, 4><<<grid, THREADS, Shape<128, 4>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
                                                                          a.exps, b.exps, C, ldc, amax,
-                                                                         lower_only ? 1 : 0, err);
+                                                                         lower_only ? 1 : 0, err, skip);
     } else if (a.slices == 5 && mixed_tile_n(5, n) == 64) {
         set_attr_once<64, 5>();
         dim3 grid((n + 63) / 64, (n + BM - 1) / BM);
         k_ozaki_gemm<64, 5><<<grid, THREADS, Shape<64, 5>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
                                                                        a.exps, b.exps, C, ldc, amax,
-                                                                       lower_only ? 1 : 0, err);
+                                                                       lower_only ? 1 : 0, err, skip);
     } else if (a.slices == 5) {
         set_attr_once<96, 5>();
         dim3 grid((n + 95) / 96, (n + BM - 1) / BM);
         k_ozaki_gemm<96, 5><<<grid, THREADS, Shape<96, 5>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
                                                                        a.exps, b.exps, C, ldc, amax,
-                                                                       lower_only ? 1 : 0, err);
+                                                                       lower_only ? 1 : 0, err, skip);
     } else {
         set_attr_once<128, 3>();
         dim3 grid((n + 127) / 128, (n + BM - 1) / BM);
         k_ozaki_gemm<128, 3><<<grid, THREADS, Shape<128, 3>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
                                                                          a.exps, b.exps, C, ldc, amax,
-                                                                         lower_only ? 1 : 0, err);
+                                                                         lower_only ? 1 : 0, err, skip);
     }
     count_launch();
 }
