@@ -116,6 +116,24 @@ int unc_context_profile(unc_context* ctx, long long* launches, double* seconds, 
 /* Device bytes unc_compute_device would use for this problem (admission). */
 long long unc_workspace_bytes(const unc_options* opt, int num_rows, int num_cols);
 
+/* The Jacobian of the reprojection residuals built on the GPU from the scene,
+ * replacing Ceres Evaluate (src/uncertaintyTE/JacobianComposer.cpp:123-166,
+ * src/matlab/matlabInterface.cpp:182-200) for the SnavelyReprojectionError
+ * camera (snavely_reprojection_error.h:309-350, unit parameter weights):
+ * cams 9 per camera [angle-axis, centre, f, k1, k2], points 3 per point,
+ * observation camera / point ids. Writes the reference CRS layout (rows
+ * 2 num_obs + 1, cols / values 24 per observation: 9 camera then 3 point
+ * columns per row), all device pointers; synchronous. */
+int unc_jacobian_device(int num_cams, int num_points, int num_obs, const double* d_cams, const double* d_points,
+                        const int* d_obs_cam, const int* d_obs_pt, int* d_rows, int* d_cols, double* d_values,
+                        void* stream);
+/* computeCovariances from the scene on host arrays (opt->num_obs
+ * observations): only cameras, points and observation ids cross PCIe, the
+ * Jacobian is built on the device (unc_jacobian_device), then the same
+ * pipeline as unc_compute. */
+int unc_compute_scene(unc_context* ctx, const unc_options* opt, const double* cams, const double* points,
+                      const int* obs_cam, const int* obs_pt, double* cam_unc, double* pt_unc, unc_statistic* st);
+
 /* Device bytes one unc_compute call needs for this Jacobian (host arrays):
  * the workspace with the input copies, the Schur pair list (counted from the
  * point columns of the rows) and the int8 slices of the mixed modes. -1 for

@@ -29,6 +29,8 @@ struct unc_context {
     size_t tup_bytes = 0;
     void* mp = nullptr;   // int8 slice planes of the mixed-precision products
     size_t mp_bytes = 0;
+    void* jac = nullptr;  // unc_compute_scene: scene inputs, the generated CRS Jacobian, outputs
+    size_t jac_bytes = 0;
     cudaEvent_t ev[12] = {};
     int priority = 0;  // of `stream` (0: the default priority)
     // profiling of the Taylor-series products
@@ -425,9 +427,9 @@ int unc_context_destroy(unc_context* c) {
 int unc_context_release(unc_context* c) {
     if (!c) return fail(UNC_ERR_INVALID_ARG, "ctx is NULL");
     cudaSetDevice(c->device);
-    void** bufs[3] = {&c->ws, &c->tup, &c->mp};
-    size_t* sizes[3] = {&c->ws_bytes, &c->tup_bytes, &c->mp_bytes};
-    for (int i = 0; i < 3; ++i) {
+    void** bufs[4] = {&c->ws, &c->tup, &c->mp, &c->jac};
+    size_t* sizes[4] = {&c->ws_bytes, &c->tup_bytes, &c->mp_bytes, &c->jac_bytes};
+    for (int i = 0; i < 4; ++i) {
         if (*bufs[i]) cudaFreeAsync(*bufs[i], c->stream);
         *bufs[i] = nullptr;
         *sizes[i] = 0;
@@ -456,7 +458,7 @@ int unc_context_set_priority(unc_context* c, int high) {
 
 long long unc_context_device_bytes(const unc_context* c) {
     if (!c) return -1;
-    return (long long)(c->ws_bytes + c->tup_bytes + c->mp_bytes);
+    return (long long)(c->ws_bytes + c->tup_bytes + c->mp_bytes + c->jac_bytes);
 }
 
 long long unc_request_bytes(const unc_options* o, int num_rows, int num_cols, const int* rows, const int* cols) {
@@ -593,6 +595,81 @@ int unc_compute(unc_context* ctx, const unc_options* o, int num_rows, int num_co
     for (int p = (int)head; p < pl.P; ++p) {
         if (p == b.s.fix[0] || p == b.s.fix[1] || p == b.s.fix[2]) continue;
         CK(cudaMemcpyAsync(pt_unc + 6L * p, b.pt_out + 6L * p, sizeof(double) * 6, cudaMemcpyDeviceToHost, sm));
+    }
+    CK(cudaStreamSynchronize(sm));
+    return UNC_OK;
+}
+
+int unc_compute_scene(unc_context* ctx, const unc_options* o, const double* cams, const double* points,
+                      const int* obs_cam, const int* obs_pt, double* cam_unc, double* pt_unc, unc_statistic* st) {
+    g_last_error.clear();
+    if (!o) return fail(UNC_ERR_INVALID_ARG, "options is NULL");
+    const int C = o->num_cams, P = o->num_points, nobs = o->num_obs;
+    const int num_rows = 2 * nobs, num_cols = 9 * C + 3 * P;
+    int rc = check_options(o, num_rows, num_cols);
+    if (rc) return rc;
+    if (!cams || (P && !points) || (nobs && (!obs_cam || !obs_pt)) || !cam_unc || !pt_unc)
+        return fail(UNC_ERR_INVALID_ARG, "null pointer");
+    unc_context* own = nullptr;
+    if (!ctx) {
+        rc = unc_context_create(0, &own);
+        if (rc) return rc;
+        ctx = own;
+    }
+    struct Guard {
+        unc_context* c;
+        ~Guard() { unc_context_destroy(c); }
+    } guard{own};
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t sm = ctx->stream;
+    Carver c{nullptr};
+    auto lay = [&](Carver& k, double*& dc, double*& dp, int*& oc, int*& op, int*& rows, int*& cols, double*& vals,
+                   double*& co, double*& po, int*& err) {
+        dc = k.take<double>(9 * (size_t)C);
+        dp = k.take<double>(3 * (size_t)P);
+        oc = k.take<int>(nobs);
+        op = k.take<int>(nobs);
+        rows = k.take<int>(2 * (size_t)nobs + 1);
+        cols = k.take<int>(24 * (size_t)nobs);
+        vals = k.take<double>(24 * (size_t)nobs);
+        co = k.take<double>(45 * (size_t)C);
+        po = k.take<double>(6 * (size_t)P);
+        err = k.take<int>(4);
+    };
+    double *dc, *dp, *dv, *co, *po;
+    int *oc, *op, *drows, *dcols, *derr;
+    lay(c, dc, dp, oc, op, drows, dcols, dv, co, po, derr);
+    const size_t bytes = c.off + 256;
+    if (int r = grow_buffer(&ctx->jac, &ctx->jac_bytes, bytes, bytes, sm)) return r;
+    Carver k{(char*)ctx->jac};
+    lay(k, dc, dp, oc, op, drows, dcols, dv, co, po, derr);
+    CK(cudaMemcpyAsync(dc, cams, sizeof(double) * 9 * (size_t)C, cudaMemcpyHostToDevice, sm));
+    if (P) CK(cudaMemcpyAsync(dp, points, sizeof(double) * 3 * (size_t)P, cudaMemcpyHostToDevice, sm));
+    if (nobs) {
+        CK(cudaMemcpyAsync(oc, obs_cam, sizeof(int) * (size_t)nobs, cudaMemcpyHostToDevice, sm));
+        CK(cudaMemcpyAsync(op, obs_pt, sizeof(int) * (size_t)nobs, cudaMemcpyHostToDevice, sm));
+    }
+    CK(cudaMemsetAsync(derr, 0, sizeof(int), sm));
+    if (launch_scene_jacobian(C, P, nobs, dc, dp, oc, op, drows, dcols, dv, derr, sm) != UNC_OK)
+        return fail(UNC_ERR_CUDA, "scene Jacobian launch failed");
+    int h_err = 0;
+    CK(cudaMemcpyAsync(&h_err, derr, sizeof(int), cudaMemcpyDeviceToHost, sm));
+    CK(cudaStreamSynchronize(sm));
+    if (h_err & ERRBIT_LAYOUT) return fail(UNC_ERR_INVALID_ARG, "camera or point id out of range");
+    rc = unc_compute_device(ctx, o, num_rows, num_cols, drows, dcols, dv, co, po, st, sm);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(cam_unc, co, sizeof(double) * 45 * (size_t)C, cudaMemcpyDeviceToHost, sm));
+    if (is_svd(o)) {
+        if (P) CK(cudaMemcpyAsync(pt_unc, po, sizeof(double) * 6 * (size_t)P, cudaMemcpyDeviceToHost, sm));
+    } else {  // the fixed points' slots are left as the caller had them (compute.cpp:511,526)
+        int fx[3] = {o->pts2fix[0], o->pts2fix[1], o->pts2fix[2]};
+        std::sort(fx, fx + 2);
+        size_t head = P > 3 ? (size_t)(P - 3) : 0;
+        if (head) CK(cudaMemcpyAsync(pt_unc, po, sizeof(double) * 6 * head, cudaMemcpyDeviceToHost, sm));
+        for (int q = (int)head; q < P; ++q) {
+            if (q == fx[0] || q == fx[1] || q == fx[2]) continue;
+            CK(cudaMemcpyAsync(pt_unc + 6L * q, po + 6L * q, sizeof(double) * 6, cudaMemcpyDeviceToHost, sm));
+        }
     }
     CK(cudaStreamSynchronize(sm));
     return UNC_OK;

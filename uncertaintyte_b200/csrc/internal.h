@@ -228,6 +228,13 @@ int svd_pipeline(char* ws, const unc_options* o, int num_rows, long long nnz, co
                  const double* vals, double* cam_unc, double* pt_unc, bool host_io, unc_statistic* st,
                  cudaEvent_t* ev, cudaStream_t sm);
 
+// ---------------- jacobian.cu ----------------
+// Analytic reprojection Jacobian of a scene in the reference CRS layout
+// (rows: 2 * num_obs + 1, cols / vals: 24 per observation).
+int launch_scene_jacobian(int num_cams, int num_points, int num_obs, const double* cams, const double* pts,
+                          const int* obs_cam, const int* obs_pt, int* rows, int* cols, double* vals, int* err,
+                          cudaStream_t st);
+
 // ---------------- points.cu ----------------
 void launch_point_cov(const SceneDev& s, const double* sig, double* pt_unc, cudaStream_t st);
 

@@ -82,7 +82,7 @@ EXPORTS = ("unc_options_init", "unc_context_create", "unc_context_destroy", "unc
            "unc_dense_inverse_noalloc", "unc_pinv_psd_device", "unc_jtj_crs",
            "unc_gemm_f64_device", "unc_gemm_mixed_device", "unc_status_string", "unc_last_error",
            "unc_kernel_launches", "unc_request_bytes", "unc_context_device_bytes", "unc_context_release",
-           "unc_context_set_priority",
+           "unc_context_set_priority", "unc_jacobian_device", "unc_compute_scene",
            "unc_server_create", "unc_server_submit", "unc_server_wait", "unc_server_destroy")
 
 _lib = None
@@ -118,6 +118,8 @@ def lib():
     L.unc_context_device_bytes.restype = C.c_longlong
     L.unc_context_release.argtypes = [vp]
     L.unc_context_set_priority.argtypes = [vp, C.c_int]
+    L.unc_jacobian_device.argtypes = [C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.unc_compute_scene.argtypes = [vp, P(UncOptions), vp, vp, vp, vp, vp, vp, P(UncStatistic)]
     L.unc_server_create.argtypes = [C.c_int, C.c_longlong, C.c_int, P(vp)]
     L.unc_server_submit.argtypes = [vp, P(UncOptions), C.c_int, C.c_int, vp, vp, vp, vp, vp, P(C.c_longlong)]
     L.unc_server_wait.argtypes = [vp, C.c_longlong, C.c_double, P(C.c_int), P(UncStatistic), P(C.c_double),
@@ -222,6 +224,30 @@ def compute_covariances_device(ctx: Context, opts: UncOptions, num_rows: int, nu
     _check(lib().unc_compute_device(ctx.handle, C.byref(opts), num_rows, num_cols, d_rows, d_cols,
                                     d_vals, d_cam, d_pt, C.byref(st), stream or None))
     return st.as_dict()
+
+
+def compute_covariances_scene(scene, pts2fix, ctx: Optional[Context] = None, precision: str = "fp64",
+                              algorithm: int = TAYLOR_EXPANSION, svd_remove_n: int = 7):
+    """computeCovariances from a scene (cams C x 9, points P x 3, obs_cam, obs_pt):
+    the Jacobian is built on the GPU. Returns (cam (C*45,), pt (P*6,), stats)."""
+    cams = np.ascontiguousarray(scene.cams, dtype=np.float64)
+    pts = np.ascontiguousarray(scene.points, dtype=np.float64)
+    oc = np.ascontiguousarray(scene.obs_cam, dtype=np.int32)
+    op = np.ascontiguousarray(scene.obs_pt, dtype=np.int32)
+    o = UncOptions()
+    lib().unc_options_init(C.byref(o), len(cams), 9, len(pts), len(oc))
+    o.algorithm = algorithm
+    o.svd_remove_n = svd_remove_n
+    if pts2fix is not None:
+        o.pts2fix[:] = [int(x) for x in pts2fix]
+        o.has_pts2fix = 1
+    o.precision = PRECISION[precision]
+    cam = np.zeros(len(cams) * 45)
+    pt = np.zeros(len(pts) * 6)
+    st = UncStatistic()
+    _check(lib().unc_compute_scene(ctx.handle if ctx else None, C.byref(o), _ptr(cams), _ptr(pts), _ptr(oc),
+                                   _ptr(op), _ptr(cam), _ptr(pt), C.byref(st)))
+    return cam, pt, st.as_dict()
 
 
 class Server:
