@@ -4,6 +4,7 @@
 // Replaces computeCovariances (compute.cpp:458-540). Host code; every
 // arithmetic step runs in the kernels of assembly.cu / dense.cu / points.cu.
 #include <algorithm>
+#include <array>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -16,9 +17,18 @@
 namespace unc {
 thread_local std::string g_last_error;
 long long g_launches = 0;
+thread_local long long g_thread_launches = 0;
 }  // namespace unc
 
 using namespace unc;
+
+using GraphKey = std::array<unsigned long long, 8>;
+struct StageGraph {
+    GraphKey key{};
+    cudaGraphExec_t exec = nullptr;
+    size_t npev = 0;          // profiling events recorded by the stage
+    long long launches = 0;   // kernels the stage launches (added to the counter on every replay)
+};
 
 struct unc_context {
     int device = 0;
@@ -33,6 +43,10 @@ struct unc_context {
     size_t jac_bytes = 0;
     cudaEvent_t ev[12] = {};
     int priority = 0;  // of `stream` (0: the default priority)
+    // dense-stage graphs: a stage seen twice with the same key is captured and
+    // replayed (kStageGraphs most recent kept)
+    std::vector<StageGraph> graphs;
+    std::vector<GraphKey> seen;
     // profiling of the Taylor-series products
     bool prof = false;
     std::vector<cudaEvent_t> pev;
@@ -161,6 +175,65 @@ bool is_svd(const unc_options* o) {
     return o->algorithm == UNC_SVD_QR_ITERATION || o->algorithm == UNC_SVD_DEVIDE_AND_CONQUER;
 }
 
+constexpr size_t kStageGraphs = 8, kSeenKeys = 16;
+
+void drop_graphs(unc_context* ctx) {
+    for (auto& g : ctx->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    ctx->graphs.clear();
+    ctx->seen.clear();
+}
+
+// Run a fixed launch sequence (the dense stage) on sm. A key seen before is
+// captured into a CUDA graph and replayed from then on: several hundred small
+// launches cost one graph launch. Keys name the sizes, the options that change
+// kernel arguments and every buffer address, so a replay is the same work.
+// If capture or instantiation fails, the stage runs directly.
+template <class F>
+int run_stage(unc_context* ctx, const GraphKey& key, cudaStream_t sm, F&& stage, size_t& npev) {
+    for (auto& g : ctx->graphs)
+        if (g.key == key) {
+            npev = g.npev;
+            CK(cudaGraphLaunch(g.exec, sm));
+            count_launch((int)g.launches);
+            return UNC_OK;
+        }
+    const bool again = std::find(ctx->seen.begin(), ctx->seen.end(), key) != ctx->seen.end();
+    if (!again) {
+        if (ctx->seen.size() >= kSeenKeys) ctx->seen.erase(ctx->seen.begin());
+        ctx->seen.push_back(key);
+        return stage();
+    }
+    const long long l0 = g_thread_launches;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool ok = cudaStreamBeginCapture(sm, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    int rc = UNC_OK;
+    if (ok) {
+        rc = stage();
+        ok = cudaStreamEndCapture(sm, &graph) == cudaSuccess && rc == UNC_OK && graph;
+    }
+    if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    const long long launches = g_thread_launches - l0;  // this thread's launches were captured, not run
+    __atomic_sub_fetch(&g_launches, launches, __ATOMIC_RELAXED);
+    g_thread_launches -= launches;
+    if (!ok) {
+        cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        npev = 0;
+        return stage();
+    }
+    if (ctx->graphs.size() >= kStageGraphs) {
+        cudaGraphExecDestroy(ctx->graphs.front().exec);
+        ctx->graphs.erase(ctx->graphs.begin());
+    }
+    ctx->graphs.push_back(StageGraph{key, exec, npev, launches});
+    CK(cudaGraphLaunch(exec, sm));
+    count_launch((int)launches);
+    return UNC_OK;
+}
+
 // factorial() of compute.cpp:57-62: 32-bit signed, wraps from 13! on.
 int32_t factorial_i32(int n) {
     uint32_t f = 1;
@@ -170,7 +243,10 @@ int32_t factorial_i32(int n) {
 
 float ev_s(cudaEvent_t a, cudaEvent_t b) {
     float ms = 0;
-    cudaEventElapsedTime(&ms, a, b);
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        cudaGetLastError();  // leave no error behind for the next call's checks
+        return 0.0f;
+    }
     return ms * 1e-3f;
 }
 
@@ -225,15 +301,29 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
 
     double lambda = o->lambda;
     if (lambda == -1) lambda = pow(10, -1.2653 * log10((double)N) - 2.9415);  // compute.cpp:124-125
-    launch_shift_equilibrate(b.Z, N, ld, lambda, b.e, s.err, sm);
-    chol_inverse(b.Z, N, ld, b.iZ, b.add, b.tmp, b.gjws, s.err, sm);
-    launch_unequilibrate(b.Z, N, ld, b.e, b.iZ, sm);  // X in Z, iZ = X
-    CK(cudaEventRecord(ev[6], sm));
 
-    // Taylor expansion (compute.cpp:141-160): iZ = X + sum lambda^i/(i-1)! X^(i+1)
+    // Every power X^(i+1) is symmetric: only the lower-triangle tiles of each
+    // product are computed (half the flops), then mirrored for the next product.
+    // FP64 mode: DMMA products. Mixed modes: int8-sliced tcgen05 products of
+    // the FP64 operands (X sliced once, each new power sliced per product).
+    const bool mixed = o->precision != UNC_PRECISION_FP64;
+    const int slices = o->precision == UNC_PRECISION_MIXED4 ? 4 : (o->precision == UNC_PRECISION_MIXED3 ? 3 : 5);
+    MixedOperand opP, opXa, opXb;
+    size_t mp_need = 0;
+    if (mixed) {  // host-side preparation: buffers and tensor maps
+        const size_t sb = (mixed_slice_bytes(N, slices) + 255) & ~size_t(255);
+        mp_need = 2 * sb + 2 * sizeof(int) * ((size_t)N + 64) + 256;
+        if (int r = grow_buffer(&ctx->mp, &ctx->mp_bytes, mp_need, mp_need, sm)) return r;
+        char* w = (char*)ctx->mp;
+        int8_t* bufX = reinterpret_cast<int8_t*>(w);
+        int8_t* bufP = reinterpret_cast<int8_t*>(w + sb);
+        int* eX = reinterpret_cast<int*>(w + 2 * sb);
+        int* eP = eX + N + 64;
+        if (!mixed_plan(opXa, bufX, eX, N, slices, false) || !mixed_plan(opXb, bufX, eX, N, slices, true) ||
+            !mixed_plan(opP, bufP, eP, N, slices, false))
+            return fail(UNC_ERR_CUDA, "tensor-map encoding failed");
+    }
     const double* X = b.Z;
-    double* add = b.add;
-    double* tmp = b.tmp;
     size_t npev = 0;
     auto prof_mark = [&]() -> int {
         if (!ctx->prof) return UNC_OK;
@@ -245,28 +335,6 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         CK(cudaEventRecord(ctx->pev[npev++], sm));
         return UNC_OK;
     };
-    // Every power X^(i+1) is symmetric: only the lower-triangle tiles of each
-    // product are computed (half the flops), then mirrored for the next product.
-    // FP64 mode: DMMA products. Mixed modes: int8-sliced tcgen05 products of
-    // the FP64 operands (X sliced once, each new power sliced per product).
-    const bool mixed = o->precision != UNC_PRECISION_FP64;
-    const int slices = o->precision == UNC_PRECISION_MIXED4 ? 4 : (o->precision == UNC_PRECISION_MIXED3 ? 3 : 5);
-    MixedOperand opP, opXa, opXb;
-    if (mixed) {
-        const size_t sb = (mixed_slice_bytes(N, slices) + 255) & ~size_t(255);
-        const size_t need = 2 * sb + 2 * sizeof(int) * ((size_t)N + 64) + 256;
-        if (int r = grow_buffer(&ctx->mp, &ctx->mp_bytes, need, need, sm)) return r;
-        char* w = (char*)ctx->mp;
-        int8_t* bufX = reinterpret_cast<int8_t*>(w);
-        int8_t* bufP = reinterpret_cast<int8_t*>(w + sb);
-        int* eX = reinterpret_cast<int*>(w + 2 * sb);
-        int* eP = eX + N + 64;
-        if (!mixed_plan(opXa, bufX, eX, N, slices, false) || !mixed_plan(opXb, bufX, eX, N, slices, true) ||
-            !mixed_plan(opP, bufP, eP, N, slices, false))
-            return fail(UNC_ERR_CUDA, "tensor-map encoding failed");
-        CK(cudaMemsetAsync(ctx->mp, 0, need, sm));  // slice padding must be zero
-        mixed_slice(X, ld, opXa, sm);
-    }
     // the profiled region is the product kernel alone (slicing excluded)
     auto product = [&](const double* P, double* out, const int* skip) -> int {
         if (mixed) {
@@ -279,27 +347,64 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         }
         return prof_mark();
     };
-    // The stop rule runs on the device (k_te_decide): the host launches all 19
-    // iterations without waiting; once the rule fires, the remaining kernels
-    // return at once. k = lambda^i / factorial(i-1) is evaluated here exactly
-    // as before (32-bit factorial wrap included).
-    TeState te0{};
-    te0.old_change = DBL_MAX;
-    CK(cudaMemcpyAsync(b.te, &te0, sizeof(TeState), cudaMemcpyHostToDevice, sm));
-    const int* skip = &b.te->done;
-    CK(cudaMemsetAsync(b.amax, 0, 8, sm));
-    if (int r = product(X, add, nullptr)) return r;
-    launch_mirror_lower(add, N, ld, sm);
-    for (int i = 1; i < 20; ++i) {
-        const double k = pow(lambda, i) / factorial_i32(i - 1);
-        launch_te_decide(b.te, b.amax, k, sm);
-        launch_axpy_te(b.iZ, add, b.te, N, ld, sm);
+    // The dense stage, a fixed launch sequence for given sizes and buffers:
+    // equilibration, the SPD inverse (SDM::inv, ScaledDenseMatrix.cpp:232-279)
+    // and the Taylor expansion (compute.cpp:141-160),
+    //   iZ = X + sum lambda^i/(i-1)! X^(i+1).
+    // The stop rule runs on the device (k_te_decide): all 19 iterations are
+    // launched and, once the rule fires, the remaining kernels return at once;
+    // k = lambda^i / factorial(i-1) is evaluated here (32-bit factorial wrap).
+    auto inverse_stage = [&]() -> int {
+        launch_shift_equilibrate(b.Z, N, ld, lambda, b.e, s.err, sm);
+        chol_inverse(b.Z, N, ld, b.iZ, b.add, b.tmp, b.gjws, s.err, sm);
+        launch_unequilibrate(b.Z, N, ld, b.e, b.iZ, sm);  // X in Z, iZ = X
+        return UNC_OK;
+    };
+    auto taylor_stage = [&]() -> int {
+        double* add = b.add;
+        double* tmp = b.tmp;
+        if (mixed) {
+            CK(cudaMemsetAsync(ctx->mp, 0, mp_need, sm));  // slice padding must be zero
+            mixed_slice(X, ld, opXa, sm);
+        }
+        launch_te_init(b.te, sm);
+        const int* skip = &b.te->done;
         CK(cudaMemsetAsync(b.amax, 0, 8, sm));
-        if (int r = product(add, tmp, skip)) return r;
-        launch_mirror_lower(tmp, N, ld, sm, skip);
-        std::swap(add, tmp);
+        if (int r = product(X, add, nullptr)) return r;
+        launch_mirror_lower(add, N, ld, sm);
+        for (int i = 1; i < 20; ++i) {
+            const double k = pow(lambda, i) / factorial_i32(i - 1);
+            launch_te_decide(b.te, b.amax, k, sm);
+            launch_axpy_te(b.iZ, add, b.te, N, ld, sm);
+            CK(cudaMemsetAsync(b.amax, 0, 8, sm));
+            if (int r = product(add, tmp, skip)) return r;
+            launch_mirror_lower(tmp, N, ld, sm, skip);
+            std::swap(add, tmp);
+        }
+        return UNC_OK;
+    };
+    while (ctx->prof && ctx->pev.size() < 2 * 20 + 2) {  // events exist before any capture
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        ctx->pev.push_back(e);
     }
-    CK(cudaEventRecord(ev[7], sm));
+    {
+        unsigned long long lam_bits;
+        memcpy(&lam_bits, &lambda, 8);
+        // events are recorded between the graphs (elapsed times of events
+        // recorded inside a graph are not available); per-product profiling
+        // runs the stages directly
+        GraphKey key = {1ULL, (unsigned long long)N, (unsigned long long)ld, lam_bits,
+                        (unsigned long long)(uintptr_t)b.Z, (unsigned long long)(uintptr_t)b.gjws,
+                        (unsigned long long)(uintptr_t)s.err, 0ULL};
+        size_t none = 0;
+        if (int r = ctx->prof ? inverse_stage() : run_stage(ctx, key, sm, inverse_stage, none)) return r;
+        CK(cudaEventRecord(ev[6], sm));
+        key[0] = 2ULL;
+        key[7] = ((unsigned long long)o->precision << 56) ^ (unsigned long long)(uintptr_t)ctx->mp;
+        if (int r = ctx->prof ? taylor_stage() : run_stage(ctx, key, sm, taylor_stage, npev)) return r;
+        CK(cudaEventRecord(ev[7], sm));
+    }
 
     launch_camera_output(b.iZ, ld, s.s_cam, pl.C, cam_out, b.sig, sm);
     if (pl.P > 3) CK(cudaMemsetAsync(pt_out, 0, sizeof(double) * 6 * ((size_t)pl.P - 3), sm));
@@ -381,7 +486,12 @@ int unc_context_create(int device, unc_context** out) {
     unc_context* c = new unc_context();
     c->device = device;
     cudaError_t e = cudaSetDevice(device);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {  // kernel attributes now, never inside a stream capture
+        prepare_assembly_kernels();
+        prepare_dense_kernels();
+        prepare_mixed_kernels();
+        e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    }
     for (int i = 0; i < 12 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
     if (e != cudaSuccess) {
         g_last_error = std::string("context creation: ") + cudaGetErrorString(e);
@@ -415,8 +525,8 @@ int unc_context_destroy(unc_context* c) {
     if (!c) return UNC_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (cudaEvent_t e : c->pev) cudaEventDestroy(e);
     unc_context_release(c);
+    for (cudaEvent_t e : c->pev) cudaEventDestroy(e);
     for (int i = 0; i < 12; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -427,6 +537,7 @@ int unc_context_destroy(unc_context* c) {
 int unc_context_release(unc_context* c) {
     if (!c) return fail(UNC_ERR_INVALID_ARG, "ctx is NULL");
     cudaSetDevice(c->device);
+    drop_graphs(c);  // they name the buffers freed below
     void** bufs[4] = {&c->ws, &c->tup, &c->mp, &c->jac};
     size_t* sizes[4] = {&c->ws_bytes, &c->tup_bytes, &c->mp_bytes, &c->jac_bytes};
     for (int i = 0; i < 4; ++i) {

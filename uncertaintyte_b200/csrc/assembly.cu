@@ -696,6 +696,14 @@ void launch_schur_count(const SceneDev& s, cudaStream_t st) {
     exclusive_scan(s.blk_cnt, s.blk_ptr, (int)nblk, s.scan_tmp, st);
 }
 
+void prepare_assembly_kernels() {
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
+        return cudaFuncSetAttribute(k_sort_pairs_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kPairBlockCap * sizeof(unsigned long long))) == cudaSuccess;
+    });
+}
+
 void launch_schur(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
     const long nblk = (long)s.num_cams * s.num_cams;
     if (nblk == 0) return;
@@ -708,11 +716,7 @@ void launch_schur(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
     cudaMemsetAsync(s.long_list, 0, sizeof(int), st);
     k_sort_pairs_warp<<<(unsigned)((nblk + 3) / 4), 128, 0, st>>>(nblk, s.blk_ptr, s.pairs, s.long_list,
                                                                   s.long_cap);
-    static std::atomic<unsigned long long> attr{0};
-    once_per_device(attr, [] {
-        cudaFuncSetAttribute(k_sort_pairs_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(kPairBlockCap * sizeof(unsigned long long)));
-    });
+    prepare_assembly_kernels();
     k_sort_pairs_block<<<148, 1024, kPairBlockCap * sizeof(unsigned long long), st>>>(
         s.blk_ptr, s.pairs, s.long_list, s.long_cap, s.err);
     k_schur_blocks<<<(unsigned)nblk, 256, 0, st>>>(s.num_cams, s.blk_ptr, s.pairs, s.Ws, s.Ys, Z, ldz);

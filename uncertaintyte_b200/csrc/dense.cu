@@ -258,14 +258,21 @@ int active_tiles(dim3 grid, int mode) {
 }
 
 template <class Cfg>
+void gemm_attr() {
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
+        return cudaFuncSetAttribute(k_gemm_f64<Cfg, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)Cfg::SMEM) == cudaSuccess &&
+               cudaFuncSetAttribute(k_gemm_f64<Cfg, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)Cfg::SMEM) == cudaSuccess;
+    });
+}
+
+template <class Cfg>
 void launch_gemm(int M, int N, int K, double alpha, const double* A, int lda, const double* B, int ldb, double beta,
                  double* C, int ldc, unsigned long long* amax, int mode, cudaStream_t st, double* ws,
                  size_t ws_doubles, const int* skip) {
-    static std::atomic<unsigned long long> attr{0};
-    once_per_device(attr, [] {
-        cudaFuncSetAttribute(k_gemm_f64<Cfg, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
-        cudaFuncSetAttribute(k_gemm_f64<Cfg, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
-    });
+    gemm_attr<Cfg>();
     dim3 grid((N + Cfg::BN - 1) / Cfg::BN, (M + Cfg::BM - 1) / Cfg::BM);
     // split-K when the output has too few tiles to fill the SMs: each split
     // keeps at least kMinSplitTiles k tiles, the partial slabs fit in ws
@@ -545,6 +552,16 @@ __global__ void k_transpose(const double* __restrict__ T, long ldt, int n, doubl
     }
 }
 
+void prepare_dense_kernels() {
+    gemm_attr<CfgBig>();
+    gemm_attr<CfgSmall>();
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
+        return cudaFuncSetAttribute(k_chol_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEAF_SMEM) ==
+               cudaSuccess;
+    });
+}
+
 namespace {
 
 // Factor A[r0:r1, r0:r1] (already updated by the earlier panels) and write
@@ -560,10 +577,7 @@ void chol_rec(double* A, int lda, double* T, double* W, double* ws, size_t wsd, 
               cudaStream_t st) {
     const int n = r1 - r0;
     if (n <= NB) {
-        static std::atomic<unsigned long long> attr{0};
-        once_per_device(attr, [] {
-            cudaFuncSetAttribute(k_chol_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEAF_SMEM);
-        });
+        prepare_dense_kernels();
         k_chol_leaf<<<1, LEAF_THREADS, LEAF_SMEM, st>>>(A, lda, r0, n, T, lda, err);
         count_launch();
         return;
@@ -668,6 +682,21 @@ __global__ void k_te_decide(TeState* s, const unsigned long long* amax_bits, dou
     if (s->iters < 20) s->change[s->iters] = change;
     s->iters += 1;
     s->coef = k;
+}
+
+__global__ void k_te_init(TeState* s) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    s->done = 0;
+    s->bad = 0;
+    s->iters = 0;
+    s->old_change = 1.7976931348623157e308;  // DBL_MAX (compute.cpp:140)
+    s->coef = 0.0;
+    for (int i = 0; i < 20; ++i) s->change[i] = 0.0;
+}
+
+void launch_te_init(TeState* s, cudaStream_t st) {
+    k_te_init<<<1, 32, 0, st>>>(s);
+    count_launch();
 }
 
 void launch_te_decide(TeState* s, const unsigned long long* amax, double k, cudaStream_t st) {

@@ -29,9 +29,11 @@ inline int ld_of(int n) { return (n + 7) & ~7; }
 
 extern thread_local std::string g_last_error;
 
-// Runs f() once per device (ordinal < 64) for one call site, from any thread:
-// per-function CUDA attributes are per device, and several host threads
-// (one per context) may launch the same kernels concurrently.
+// Runs f() (returning true on success) until it succeeds once per device
+// (ordinal < 64) for one call site, from any thread: per-function CUDA
+// attributes are per device, and several host threads (one per context) may
+// launch the same kernels concurrently. prepare_kernels() runs every such site
+// when a context is created, outside any stream capture.
 template <class F>
 void once_per_device(std::atomic<unsigned long long>& done, F&& f) {
     int dev = 0;
@@ -41,9 +43,12 @@ void once_per_device(std::atomic<unsigned long long>& done, F&& f) {
     static std::mutex mu;
     std::lock_guard<std::mutex> lock(mu);
     if (done.load(std::memory_order_relaxed) & bit) return;
-    f();
-    done.fetch_or(bit, std::memory_order_release);
+    if (f()) done.fetch_or(bit, std::memory_order_release);
 }
+// Per-device set-up of the kernels' shared-memory attributes (current device).
+void prepare_assembly_kernels();
+void prepare_dense_kernels();
+void prepare_mixed_kernels();
 
 // Bump allocator over one device allocation; every piece 256-byte aligned.
 // With base == nullptr it only measures the total size.
@@ -59,7 +64,11 @@ struct Carver {
     }
 };
 extern long long g_launches;
-inline void count_launch(int n = 1) { __atomic_add_fetch(&g_launches, n, __ATOMIC_RELAXED); }
+extern thread_local long long g_thread_launches;
+inline void count_launch(int n = 1) {
+    __atomic_add_fetch(&g_launches, n, __ATOMIC_RELAXED);
+    g_thread_launches += n;
+}
 
 // ---------------- assembly.cu ----------------
 struct SceneDev {
@@ -176,6 +185,8 @@ struct TeState {
 // One thread: change = |k * max(amax, DBL_MIN)|; stop when change < 1e-5 or
 // change > old_change, else record it and publish k for the axpy.
 void launch_te_decide(TeState* s, const unsigned long long* amax, double k, cudaStream_t st);
+// Reset the state (not done, no iteration, old change = DBL_MAX).
+void launch_te_init(TeState* s, cudaStream_t st);
 // Y <- Y + s->coef * X unless s->done.
 void launch_axpy_te(double* Y, const double* X, const TeState* s, int n, int ld, cudaStream_t st);
 void launch_zero(double* p, size_t n, cudaStream_t st);

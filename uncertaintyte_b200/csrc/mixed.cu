@@ -364,10 +364,18 @@ template <int NT, int S>
 void set_attr_once() {
     static std::atomic<unsigned long long> done{0};
     once_per_device(done, [] {
-        cudaFuncSetAttribute(k_ozaki_gemm<NT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, Shape<NT, S>::SMEM);
+        return cudaFuncSetAttribute(k_ozaki_gemm<NT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    Shape<NT, S>::SMEM) == cudaSuccess;
     });
 }
 }  // namespace
+
+void prepare_mixed_kernels() {
+    set_attr_once<128, 4>();
+    set_attr_once<64, 5>();
+    set_attr_once<96, 5>();
+    set_attr_once<128, 3>();
+}
 
 // Output tile width: slices * tile_n <= 512 TMEM columns, so 128 for up to 4
 // slices and 96 for 5. For 5 slices a 64-wide tile is taken when it needs
