@@ -134,6 +134,19 @@ int unc_jacobian_device(int num_cams, int num_points, int num_obs, const double*
 int unc_compute_scene(unc_context* ctx, const unc_options* opt, const double* cams, const double* points,
                       const int* obs_cam, const int* obs_pt, double* cam_unc, double* pt_unc, unc_statistic* st);
 
+/* Eigen-decompositions of many small covariance blocks (the Uncertainty
+ * accessors, src/uncertaintyTE/uncertainty.cpp:74-183), one warp per block:
+ * packed upper triangles of block_params x block_params blocks (45 values for
+ * 9 camera parameters, 6 for points), sub-block [sub_offset, sub_offset +
+ * sub_dim) of each (the camera centre: 3, 3). Eigenvalues descending
+ * (sub_dim per block); eigenvectors (optional, NULL to skip) as columns in the
+ * same order, sub_dim x sub_dim per block, column-major. _device: device
+ * pointers; the other form takes host arrays. block_params <= 9. */
+int unc_block_eigen_device(const double* d_packed, int num_blocks, int block_params, int sub_offset, int sub_dim,
+                           double* d_values, double* d_vectors, void* stream);
+int unc_block_eigen(const double* packed, int num_blocks, int block_params, int sub_offset, int sub_dim,
+                    double* values, double* vectors);
+
 /* Device bytes one unc_compute call needs for this Jacobian (host arrays):
  * the workspace with the input copies, the Schur pair list (counted from the
  * point columns of the rows) and the int8 slices of the mixed modes. -1 for

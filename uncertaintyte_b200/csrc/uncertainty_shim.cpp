@@ -26,59 +26,6 @@ unc_context* thread_context() {
     return h.ctx;
 }
 
-// symmetric eigen-decomposition (cyclic Jacobi), n <= 16, row-major in/out
-void sym_eig(int n, std::vector<double> a, std::vector<double>& w, std::vector<double>& v) {
-    v.assign((size_t)n * n, 0.0);
-    for (int i = 0; i < n; ++i) v[(size_t)i * n + i] = 1.0;
-    for (int sweep = 0; sweep < 100; ++sweep) {
-        double off = 0, dia = 0;
-        for (int i = 0; i < n; ++i)
-            for (int j = 0; j < n; ++j)
-                (i == j ? dia : off) += std::fabs(a[(size_t)i * n + j]);
-        if (off <= 1e-300 || off < dia * 1e-17) break;
-        for (int p = 0; p < n - 1; ++p)
-            for (int q = p + 1; q < n; ++q) {
-                double apq = a[(size_t)p * n + q];
-                if (apq == 0) continue;
-                double theta = (a[(size_t)q * n + q] - a[(size_t)p * n + p]) / (2 * apq);
-                double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1));
-                double c = 1 / std::sqrt(t * t + 1), s = t * c;
-                for (int k = 0; k < n; ++k) {
-                    double akp = a[(size_t)k * n + p], akq = a[(size_t)k * n + q];
-                    a[(size_t)k * n + p] = c * akp - s * akq;
-                    a[(size_t)k * n + q] = s * akp + c * akq;
-                }
-                for (int k = 0; k < n; ++k) {
-                    double apk = a[(size_t)p * n + k], aqk = a[(size_t)q * n + k];
-                    a[(size_t)p * n + k] = c * apk - s * aqk;
-                    a[(size_t)q * n + k] = s * apk + c * aqk;
-                }
-                for (int k = 0; k < n; ++k) {
-                    double vkp = v[(size_t)k * n + p], vkq = v[(size_t)k * n + q];
-                    v[(size_t)k * n + p] = c * vkp - s * vkq;
-                    v[(size_t)k * n + q] = s * vkp + c * vkq;
-                }
-            }
-    }
-    w.resize(n);
-    for (int i = 0; i < n; ++i) w[i] = a[(size_t)i * n + i];
-}
-
-// eigenvalues sorted descending with their eigenvectors (columns)
-void sorted_eig(int n, const std::vector<double>& m, std::vector<double>& w, std::vector<double>& vec) {
-    std::vector<double> wv, vv;
-    sym_eig(n, m, wv, vv);
-    std::vector<int> idx(n);
-    for (int i = 0; i < n; ++i) idx[i] = i;
-    std::sort(idx.begin(), idx.end(), [&](int a, int b) { return wv[a] > wv[b]; });
-    w.resize(n);
-    vec.resize((size_t)n * n);
-    for (int c = 0; c < n; ++c) {
-        w[c] = wv[idx[c]];
-        for (int r = 0; r < n; ++r) vec[(size_t)r * n + c] = vv[(size_t)r * n + idx[c]];
-    }
-}
-
 double dist3(const double* a, const double* b) {
     double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
     return std::sqrt(dx * dx + dy * dy + dz * dz);
@@ -122,26 +69,19 @@ const std::vector<double> Uncertainty::getCamerasUncMatrices() const {
     return out;
 }
 
+// eigen-decompositions of all blocks in one GPU call (uncertainty.cpp:74-115)
 const std::vector<double> Uncertainty::getCamerasUncEigenValues() const {
-    std::vector<double> out;
-    for (std::size_t i = 0; i < _numCams; i++) {
-        std::vector<double> w, v;
-        sorted_eig((int)_camParams, getCameraUncMatrix((int)i), w, v);
-        out.insert(out.end(), w.begin(), w.end());
-    }
+    std::vector<double> out(_numCams * _camParams);
+    int rc = unc_block_eigen(_camerasUnc.data(), (int)_numCams, (int)_camParams, 0, (int)_camParams, out.data(),
+                             nullptr);
+    if (rc != UNC_OK) throw Error(rc, std::string("getCamerasUncEigenValues: ") + unc_last_error());
     return out;
 }
 
 const std::vector<double> Uncertainty::getCamerasCentersUncEigVec() const {
-    std::vector<double> out;
-    for (std::size_t i = 0; i < _numCams; i++) {
-        std::vector<double> m = getCameraUncMatrix((int)i), b(9), w, v;
-        for (int r = 0; r < 3; ++r)
-            for (int c = 0; c < 3; ++c) b[r * 3 + c] = m[(3 + r) * _camParams + (3 + c)];
-        sorted_eig(3, b, w, v);
-        for (int c = 0; c < 3; ++c)
-            for (int r = 0; r < 3; ++r) out.push_back(v[r * 3 + c]);
-    }
+    std::vector<double> vals(_numCams * 3), out(_numCams * 9);
+    int rc = unc_block_eigen(_camerasUnc.data(), (int)_numCams, (int)_camParams, 3, 3, vals.data(), out.data());
+    if (rc != UNC_OK) throw Error(rc, std::string("getCamerasCentersUncEigVec: ") + unc_last_error());
     return out;
 }
 
@@ -162,24 +102,18 @@ const std::vector<double> Uncertainty::getPointsUncMatrices() const {
     return out;
 }
 
+// eigen-decompositions of all point blocks in one GPU call (uncertainty.cpp:146-183)
 const std::vector<double> Uncertainty::getPointsUncEigenValues() const {
-    std::vector<double> out;
-    for (std::size_t i = 0; i < _numPoints; i++) {
-        std::vector<double> w, v;
-        sorted_eig(3, getPointUncMatrix((int)i), w, v);
-        out.insert(out.end(), w.begin(), w.end());
-    }
+    std::vector<double> out(_numPoints * 3);
+    int rc = unc_block_eigen(_pointsUnc.data(), (int)_numPoints, 3, 0, 3, out.data(), nullptr);
+    if (rc != UNC_OK) throw Error(rc, std::string("getPointsUncEigenValues: ") + unc_last_error());
     return out;
 }
 
 const std::vector<double> Uncertainty::getPointsUncEigVectors() const {
-    std::vector<double> out;
-    for (std::size_t i = 0; i < _numPoints; i++) {
-        std::vector<double> w, v;
-        sorted_eig(3, getPointUncMatrix((int)i), w, v);
-        for (int c = 0; c < 3; ++c)
-            for (int r = 0; r < 3; ++r) out.push_back(v[r * 3 + c]);
-    }
+    std::vector<double> vals(_numPoints * 3), out(_numPoints * 9);
+    int rc = unc_block_eigen(_pointsUnc.data(), (int)_numPoints, 3, 0, 3, vals.data(), out.data());
+    if (rc != UNC_OK) throw Error(rc, std::string("getPointsUncEigVectors: ") + unc_last_error());
     return out;
 }
 

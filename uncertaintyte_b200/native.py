@@ -83,6 +83,7 @@ EXPORTS = ("unc_options_init", "unc_context_create", "unc_context_destroy", "unc
            "unc_gemm_f64_device", "unc_gemm_mixed_device", "unc_status_string", "unc_last_error",
            "unc_kernel_launches", "unc_request_bytes", "unc_context_device_bytes", "unc_context_release",
            "unc_context_set_priority", "unc_jacobian_device", "unc_compute_scene",
+           "unc_block_eigen_device", "unc_block_eigen",
            "unc_server_create", "unc_server_submit", "unc_server_wait", "unc_server_destroy")
 
 _lib = None
@@ -118,6 +119,8 @@ def lib():
     L.unc_context_device_bytes.restype = C.c_longlong
     L.unc_context_release.argtypes = [vp]
     L.unc_context_set_priority.argtypes = [vp, C.c_int]
+    L.unc_block_eigen_device.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp]
+    L.unc_block_eigen.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp]
     L.unc_jacobian_device.argtypes = [C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp]
     L.unc_compute_scene.argtypes = [vp, P(UncOptions), vp, vp, vp, vp, vp, vp, P(UncStatistic)]
     L.unc_server_create.argtypes = [C.c_int, C.c_longlong, C.c_int, P(vp)]
@@ -248,6 +251,20 @@ def compute_covariances_scene(scene, pts2fix, ctx: Optional[Context] = None, pre
     _check(lib().unc_compute_scene(ctx.handle if ctx else None, C.byref(o), _ptr(cams), _ptr(pts), _ptr(oc),
                                    _ptr(op), _ptr(cam), _ptr(pt), C.byref(st)))
     return cam, pt, st.as_dict()
+
+
+def block_eigen(packed, block_params: int, sub_offset: int = 0, sub_dim: Optional[int] = None,
+                vectors: bool = True):
+    """Eigenvalues (descending) and eigenvectors of packed upper-triangle blocks on the GPU."""
+    packed = np.ascontiguousarray(packed, dtype=np.float64)
+    per = block_params * (block_params + 1) // 2
+    nb = packed.size // per
+    dim = block_params if sub_dim is None else sub_dim
+    vals = np.zeros(nb * dim)
+    vecs = np.zeros(nb * dim * dim) if vectors else None
+    _check(lib().unc_block_eigen(_ptr(packed), nb, block_params, sub_offset, dim, _ptr(vals),
+                                 _ptr(vecs) if vectors else None))
+    return vals.reshape(nb, dim), (vecs.reshape(nb, dim, dim) if vectors else None)
 
 
 class Server:
