@@ -147,6 +147,25 @@ int unc_block_eigen_device(const double* d_packed, int num_blocks, int block_par
 int unc_block_eigen(const double* packed, int num_blocks, int block_params, int sub_offset, int sub_dim,
                     double* values, double* vectors);
 
+/* ---- .jacob input (src/uncertaintyTE/JacobianIO.cpp:32-63) ----
+ * Header of a text .jacob file or of its binary form (this library's: a
+ * 64-byte header starting "UNCJACB1", then the three arrays as stored in
+ * memory). The text body is parsed by all host threads. Errors:
+ * UNC_ERR_INVALID_ARG with unc_last_error(). */
+typedef struct {
+    double lambda;
+    int num_cams, cam_params, num_points, num_obs;
+    int pts2fix[3];     /* -1 -1 -1: none */
+    int num_rows, num_cols;
+    long long nnz;
+    int binary;         /* 1: the binary form */
+} unc_jacob_header;
+int unc_jacob_read_header(const char* path, unc_jacob_header* header);
+/* rows: num_rows + 1, cols / values: nnz (caller-allocated). */
+int unc_jacob_read(const char* path, const unc_jacob_header* header, int* rows, int* cols, double* values);
+int unc_jacob_write_binary(const char* path, const unc_jacob_header* header, const int* rows, const int* cols,
+                           const double* values);
+
 /* Device bytes one unc_compute call needs for this Jacobian (host arrays):
  * the workspace with the input copies, the Schur pair list (counted from the
  * point columns of the rows) and the int8 slices of the mixed modes. -1 for

@@ -16,71 +16,57 @@
 #include <vector>
 
 #include "uncertainty.h"
+#include "uncte.h"
 
 namespace {
 
-bool read_file(const std::string& path, std::string& out) {
-    std::ifstream f(path, std::ios::binary);
-    if (!f.good()) return false;
-    std::ostringstream ss;
-    ss << f.rdbuf();
-    out = ss.str();
-    return true;
-}
-
 // JacobianIO::loadJacobian (JacobianIO.cpp:32-63) with a fast tokenizer;
 // '#' starts a comment (the documented template carries some).
+// JacobianIO::loadJacobian (JacobianIO.cpp:32-63) through the library's
+// parser: text (all host threads) or this library's binary form.
 bool load_jacob(const std::string& path, cov::Options& opt, ceres::CRSMatrix& J) {
-    std::string text;
-    if (!read_file(path, text)) {
-        std::cerr << "\nThe input file doesn't exist.\n";
+    unc_jacob_header h;
+    if (unc_jacob_read_header(path.c_str(), &h) != UNC_OK) {
+        std::cerr << "\n" << unc_last_error() << "\n";
         return false;
     }
-    for (size_t i = 0; i < text.size(); ++i)
-        if (text[i] == '#')
-            while (i < text.size() && text[i] != '\n') text[i++] = ' ';
-    const char* p = text.c_str();
-    char* end = nullptr;
-    auto num = [&](double& v) {
-        v = strtod(p, &end);
-        if (end == p) return false;
-        p = end;
-        return true;
-    };
-    double h[11];
-    for (double& v : h)
-        if (!num(v)) return false;
     opt._algorithm = cov::eAlgorithmSvdTaylorExpansion;
     opt._epsilon = 1e-10;
     opt._svdRemoveN = 7;
     opt._maxIterTE = -1;
-    opt._lambda = h[0];
-    opt._numCams = (int)h[1];
-    opt._camParams = (int)h[2];
-    opt._numPoints = (int)h[3];
-    opt._numObs = (int)h[4];
-    if (h[5] >= 0 && h[6] >= 0 && h[7] >= 0) opt.setPts2Fix((int)h[5], (int)h[6], (int)h[7]);
-    J.num_rows = (int)h[8];
-    J.num_cols = (int)h[9];
-    long nnz = (long)h[10];
-    J.rows.resize((size_t)J.num_rows + 1);
-    J.cols.resize(nnz);
-    J.values.resize(nnz);
-    for (auto& r : J.rows) {
-        long v = strtol(p, &end, 10);
-        if (end == p) return false;
-        p = end;
-        r = (int)v;
+    opt._lambda = h.lambda;
+    opt._numCams = h.num_cams;
+    opt._camParams = h.cam_params;
+    opt._numPoints = h.num_points;
+    opt._numObs = h.num_obs;
+    if (h.pts2fix[0] >= 0 && h.pts2fix[1] >= 0 && h.pts2fix[2] >= 0)
+        opt.setPts2Fix(h.pts2fix[0], h.pts2fix[1], h.pts2fix[2]);
+    J.num_rows = h.num_rows;
+    J.num_cols = h.num_cols;
+    J.rows.resize((size_t)h.num_rows + 1);
+    J.cols.resize((size_t)h.nnz);
+    J.values.resize((size_t)h.nnz);
+    if (unc_jacob_read(path.c_str(), &h, J.rows.data(), J.cols.data(), J.values.data()) != UNC_OK) {
+        std::cerr << "\n" << unc_last_error() << "\n";
+        return false;
     }
-    for (auto& c : J.cols) {
-        long v = strtol(p, &end, 10);
-        if (end == p) return false;
-        p = end;
-        c = (int)v;
-    }
-    for (auto& v : J.values)
-        if (!num(v)) return false;
     return true;
+}
+
+// -write_binary=<path>: the same Jacobian in this library's binary form
+bool save_binary(const std::string& path, const cov::Options& opt, const ceres::CRSMatrix& J) {
+    unc_jacob_header h{};
+    h.lambda = opt._lambda;
+    h.num_cams = opt._numCams;
+    h.cam_params = opt._camParams;
+    h.num_points = opt._numPoints;
+    h.num_obs = opt._numObs;
+    for (int i = 0; i < 3; ++i) h.pts2fix[i] = opt._pts2fix ? opt._pts2fix[i] : -1;
+    h.num_rows = J.num_rows;
+    h.num_cols = J.num_cols;
+    h.nnz = (long long)J.values.size();
+    h.binary = 1;
+    return unc_jacob_write_binary(path.c_str(), &h, J.rows.data(), J.cols.data(), J.values.data()) == UNC_OK;
 }
 
 // saveResults (IO.cpp:15-60); times are true seconds.
@@ -156,6 +142,15 @@ int main(int argc, char** argv) {
     if (!load_jacob(in, opt, J)) {
         std::cerr << "cannot read " << in << "\n";
         return 1;
+    }
+    const std::string bin = flag(argc, argv, "write_binary", "");
+    if (!bin.empty()) {
+        if (!save_binary(bin, opt, J)) {
+            std::cerr << "cannot write " << bin << ": " << unc_last_error() << "\n";
+            return 1;
+        }
+        std::cout << "wrote " << bin << "\n";
+        return 0;
     }
     if (has_flag(argc, argv, "force_alg")) opt._algorithm = cov::EAlgorithm_stringToEnum(alg);
     opt._precision = prec == "MIXED" ? cov::ePrecisionMixed : cov::ePrecisionFP64;

@@ -60,7 +60,16 @@ def _tokens(path: str) -> np.ndarray:
 
 
 def load_jacob(path: str) -> Jacobian:
-    """Read a `.jacob` file (JacobianIO::loadJacobian, JacobianIO.cpp:32-63)."""
+    """Read a `.jacob` file (JacobianIO::loadJacobian, JacobianIO.cpp:32-63), text
+    or binary, with the library's parallel parser."""
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"The input file doesn't exist: {path}")
+    from . import native
+    return native.read_jacob(path)
+
+
+def load_jacob_numpy(path: str) -> Jacobian:
+    """The same with numpy alone (one Python token per number: small files)."""
     if not os.path.exists(path):
         raise FileNotFoundError(f"The input file doesn't exist: {path}")
     t = _tokens(path)

@@ -83,7 +83,8 @@ EXPORTS = ("unc_options_init", "unc_context_create", "unc_context_destroy", "unc
            "unc_gemm_f64_device", "unc_gemm_mixed_device", "unc_status_string", "unc_last_error",
            "unc_kernel_launches", "unc_request_bytes", "unc_context_device_bytes", "unc_context_release",
            "unc_context_set_priority", "unc_jacobian_device", "unc_compute_scene",
-           "unc_block_eigen_device", "unc_block_eigen",
+           "unc_block_eigen_device", "unc_block_eigen", "unc_jacob_read_header", "unc_jacob_read",
+           "unc_jacob_write_binary",
            "unc_server_create", "unc_server_submit", "unc_server_wait", "unc_server_destroy")
 
 _lib = None
@@ -119,6 +120,9 @@ def lib():
     L.unc_context_device_bytes.restype = C.c_longlong
     L.unc_context_release.argtypes = [vp]
     L.unc_context_set_priority.argtypes = [vp, C.c_int]
+    L.unc_jacob_read_header.argtypes = [C.c_char_p, P(UncJacobHeader)]
+    L.unc_jacob_read.argtypes = [C.c_char_p, P(UncJacobHeader), vp, vp, vp]
+    L.unc_jacob_write_binary.argtypes = [C.c_char_p, P(UncJacobHeader), vp, vp, vp]
     L.unc_block_eigen_device.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp]
     L.unc_block_eigen.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp]
     L.unc_jacobian_device.argtypes = [C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp]
@@ -164,6 +168,40 @@ def make_options(jac: Jacobian, algorithm: Optional[int] = None, precision: str 
         o.has_pts2fix = 1
     o.precision = PRECISION[precision]
     return o
+
+
+class UncJacobHeader(C.Structure):
+    _fields_ = [("lam", C.c_double), ("num_cams", C.c_int), ("cam_params", C.c_int), ("num_points", C.c_int),
+                ("num_obs", C.c_int), ("pts2fix", C.c_int * 3), ("num_rows", C.c_int), ("num_cols", C.c_int),
+                ("nnz", C.c_longlong), ("binary", C.c_int)]
+
+
+def read_jacob(path: str) -> Jacobian:
+    """A `.jacob` file (text, parsed by all host threads, or the binary form) as a Jacobian."""
+    h = UncJacobHeader()
+    bp = os.fsencode(path)
+    _check(lib().unc_jacob_read_header(bp, C.byref(h)))
+    rows = np.empty(h.num_rows + 1, dtype=np.int32)
+    cols = np.empty(h.nnz, dtype=np.int32)
+    vals = np.empty(h.nnz, dtype=np.float64)
+    _check(lib().unc_jacob_read(bp, C.byref(h), _ptr(rows), _ptr(cols), _ptr(vals)))
+    fix = np.array(list(h.pts2fix), dtype=np.int32)
+    return Jacobian(h.num_cams, h.cam_params, h.num_points, h.num_obs, h.num_rows, h.num_cols, rows, cols, vals,
+                    float(h.lam), fix if (fix >= 0).all() else None, algorithm=2, epsilon=1e-10, svd_remove_n=7)
+
+
+def write_jacob_binary(path: str, jac: Jacobian) -> None:
+    """The binary form of a `.jacob` file (64-byte header, then the three arrays)."""
+    h = UncJacobHeader()
+    h.lam = jac.lam
+    h.num_cams, h.cam_params, h.num_points, h.num_obs = jac.num_cams, jac.cam_params, jac.num_points, jac.num_obs
+    fix = jac.pts2fix if jac.pts2fix is not None else [-1, -1, -1]
+    h.pts2fix[:] = [int(x) for x in fix]
+    h.num_rows, h.num_cols, h.nnz, h.binary = jac.num_rows, jac.num_cols, int(jac.rows[-1]), 1
+    rows = np.ascontiguousarray(jac.rows, dtype=np.int32)
+    cols = np.ascontiguousarray(jac.cols, dtype=np.int32)
+    vals = np.ascontiguousarray(jac.values, dtype=np.float64)
+    _check(lib().unc_jacob_write_binary(os.fsencode(path), C.byref(h), _ptr(rows), _ptr(cols), _ptr(vals)))
 
 
 class Context:
