@@ -407,6 +407,17 @@ def run_ours(a):
                 "mixed_vs_fp64_max_rel_err": {"camera_9x9": blk(cam_main, c64, 45),
                                               "point_3x3": blk(pt_main, p64, 6), "bar": 1e-6}}
 
+    # the SVD algorithm on the same scene (pseudo-inverse of the camera Schur
+    # complement: the full-J^T J SVD needs (9C + 3P)^2 doubles)
+    svd_gpu = None
+    if 9 * jac.num_cams <= 46000 and a.workload != "large":
+        opts_svd = native.make_options(jac, algorithm=native.SVD_SCHUR)
+        n_svd = 3
+        t_svd, st_svd, _, _ = timed(opts_svd, n_svd)
+        svd_gpu = {"value": ws * n_svd / t_svd, "unit": UNIT, "ms_per_step": 1e3 * t_svd / n_svd,
+                   "algorithm": "SVD_SCHUR (pseudo-inverse of Z without its 7 smallest eigenvalues)",
+                   "subspace_iterations": st_svd["te_iterations"]}
+
     # end to end through the public host API, pinned host buffers
     e2e_steps = a.e2e_steps or max(3, a.steps // 2)
     pinned = [torch.from_numpy(jac.rows).pin_memory(), torch.from_numpy(jac.cols).pin_memory(),
@@ -518,6 +529,7 @@ def run_ours(a):
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h)},
                 "e2e_scene": e2e_scene,
+                "svd_schur_gpu": svd_gpu,
                 "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
                 "stage_seconds": {k: stats[k] for k in ("time_create_j", "time_fix_j", "time_norm_j",
                                                         "time_multiply_jj", "time_compose_z",

@@ -52,7 +52,9 @@ namespace cov {
 enum EAlgorithm {
     eAlgorithmSvdQrIteration = 0,
     eAlgorithmSvdDeviceAndconquer = 1,
-    eAlgorithmSvdTaylorExpansion = 2
+    eAlgorithmSvdTaylorExpansion = 2,
+    /* extension: SVD pseudo-inverse of the camera Schur complement (UNC_SVD_SCHUR) */
+    eAlgorithmSvdSchur = 3
 };
 
 /* precision of the dense Taylor-series products (new; appended field) */
@@ -63,6 +65,7 @@ inline std::string EAlgorithm_enumToString(EAlgorithm alg) {
         case eAlgorithmSvdQrIteration: return "SVD_QR_ITERATION";
         case eAlgorithmSvdDeviceAndconquer: return "SVD_DEVIDE_AND_CONQUER";
         case eAlgorithmSvdTaylorExpansion: return "TAYLOR_EXPANSION";
+        case eAlgorithmSvdSchur: return "SVD_SCHUR";
         default: return "not defined";
     }
 }
@@ -71,6 +74,7 @@ inline EAlgorithm EAlgorithm_stringToEnum(const std::string& algorithm) {
     if (algorithm == "SVD_QR_ITERATION") return eAlgorithmSvdQrIteration;
     if (algorithm == "SVD_DEVIDE_AND_CONQUER") return eAlgorithmSvdDeviceAndconquer;
     if (algorithm == "TAYLOR_EXPANSION") return eAlgorithmSvdTaylorExpansion;
+    if (algorithm == "SVD_SCHUR") return eAlgorithmSvdSchur;
     throw std::runtime_error(std::string("Unrecognized algorithm: ") + algorithm);
 }
 

@@ -41,6 +41,12 @@ extern "C" {
 #define UNC_SVD_QR_ITERATION 0
 #define UNC_SVD_DEVIDE_AND_CONQUER 1
 #define UNC_TAYLOR_EXPANSION 2
+/* This library's extension (no counterpart in the reference): the SVD
+ * pseudo-inverse of the camera Schur complement Z of the full J^T J (no fixed
+ * points) instead of the full J^T J, for scenes whose (9C + 3P)^2 matrix does
+ * not fit; point covariances then come from the point stage of the Taylor
+ * path. The gauge is the minimum-norm one in camera coordinates. */
+#define UNC_SVD_SCHUR 3
 
 /* precision of the dense Taylor-series products */
 #define UNC_PRECISION_FP64 0    /* plain FP64 (DMMA) products: the parity path */

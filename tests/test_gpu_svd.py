@@ -117,3 +117,76 @@ def test_svd_path_daliborka_runs_and_repeats():
     assert np.isfinite(c1).all() and np.isfinite(p1).all()
     np.testing.assert_array_equal(c1, c2)
     np.testing.assert_array_equal(p1, p2)
+
+
+def _schur_reference(jac, k=7, sample_points=None):
+    """numpy restatement of the SVD on the camera Schur complement (this
+    library's extension): Z = U - W V^-1 W^T of the unscaled, unfixed J^T J, its
+    pseudo-inverse without the k smallest eigenvalues (eigh and SVD routes),
+    camera outputs (a + b/2) and point covariances D^-1 + D^-1 (sum_o W_o^T
+    Sigma_c W_o) D^-1 with the camera blocks of the pseudo-inverse."""
+    import scipy.sparse as sp
+    C, Pn = jac.num_cams, jac.num_points
+    n = 9 * C
+    J = sp.csr_matrix((jac.values, jac.cols, jac.rows), shape=(jac.num_rows, jac.num_cols))
+    M = (J.T @ J).tocsr()
+    U = M[:n, :n].toarray()
+    W = M[:n, n:].tocsc()
+    Vb = np.array([M[n + 3 * p:n + 3 * p + 3, n + 3 * p:n + 3 * p + 3].toarray() for p in range(Pn)])
+    iV = np.linalg.inv(Vb)
+    iVs = sp.block_diag(list(iV), format="csr")
+    Z = U - (W @ iVs @ W.T).toarray()
+    Z = 0.5 * (Z + Z.T)
+    w, Q = np.linalg.eigh(Z)
+    keep = np.ones(n, bool)
+    keep[np.argsort(np.abs(w))[:k]] = False
+    P_e = (Q[:, keep] / w[keep]) @ Q[:, keep].T
+    Us, s, Vt = np.linalg.svd(Z)
+    P_s = (Us[:, :n - k] / s[:n - k]) @ Vt[:n - k]
+
+    def outputs(P):
+        cam = []
+        for c in range(C):
+            B = P[9 * c:9 * c + 9, 9 * c:9 * c + 9]
+            cam += [B[j, i] + B[i, j] / 2 for j in range(9) for i in range(j, 9)]
+        pts = range(Pn) if sample_points is None else sample_points
+        pt = np.zeros((Pn, 6))
+        Wd = W.tocsc()
+        for p in pts:
+            Wp = Wd[:, 3 * p:3 * p + 3].toarray()  # 9C x 3
+            S = np.zeros((3, 3))
+            for c in np.nonzero(np.abs(Wp).sum(axis=1).reshape(C, 9).sum(axis=1))[0]:
+                Wc = Wp[9 * c:9 * c + 9]
+                S += Wc.T @ P[9 * c:9 * c + 9, 9 * c:9 * c + 9] @ Wc
+            cov = iV[p] + iV[p] @ S @ iV[p]
+            pt[p] = [cov[0, 0], cov[0, 1], cov[0, 2], cov[1, 1], cov[1, 2], cov[2, 2]]
+        return np.array(cam), pt.reshape(-1)
+    return outputs(P_e), outputs(P_s)
+
+
+def test_svd_schur_small_scene_vs_numpy():
+    jac = scenes.synthetic_jacobian("small", seed=0)
+    (ce, pe), (cs, ps) = _schur_reference(jac)
+    cam, pt, st = native.compute_covariances(jac, algorithm=native.SVD_SCHUR)
+    floor_c, floor_p = block_rel_err(ce, cs, 45), block_rel_err(pe, ps, 6)
+    ec, ep = block_rel_err(cam, ce, 45), block_rel_err(pt, pe, 6)
+    print(f"svd on Z: cams {ec:.2e} (eigh vs svd {floor_c:.2e}) points {ep:.2e} (floor {floor_p:.2e})")
+    assert ec <= max(4 * floor_c, 1e-9)
+    assert ep <= max(4 * floor_p, 1e-9)
+    assert st["te_iterations"] > 0
+
+
+def test_svd_schur_medium_scene_cameras():
+    """The medium scene (N = 1800), where the full-J^T J SVD would need 184 GB."""
+    jac = scenes.synthetic_jacobian("medium", seed=0)
+    (ce, pe), (cs, ps) = _schur_reference(jac, sample_points=range(0, jac.num_points, 997))
+    cam, pt, st = native.compute_covariances(jac, algorithm=native.SVD_SCHUR)
+    floor_c = block_rel_err(ce, cs, 45)
+    ec = block_rel_err(cam, ce, 45)
+    sel = np.zeros(jac.num_points, bool)
+    sel[list(range(0, jac.num_points, 997))] = True
+    ep = block_rel_err(pt.reshape(-1, 6)[sel], pe.reshape(-1, 6)[sel], 6)
+    floor_p = block_rel_err(pe.reshape(-1, 6)[sel], ps.reshape(-1, 6)[sel], 6)
+    print(f"svd on Z (medium): cams {ec:.2e} (floor {floor_c:.2e}) sampled points {ep:.2e} (floor {floor_p:.2e})")
+    assert ec <= max(4 * floor_c, 1e-9)
+    assert ep <= max(4 * floor_p, 1e-9)

@@ -72,6 +72,7 @@ int fail(int code, const std::string& msg) {
 
 struct Plan {
     int C, P, nobs, N, ld;
+    bool svd_schur;  // UNC_SVD_SCHUR: pseudo-inverse of the camera Schur complement
 };
 
 struct Buffers {
@@ -82,6 +83,7 @@ struct Buffers {
     double *Z, *iZ, *add, *tmp, *e, *gjws, *sig;
     unsigned long long* amax;
     TeState* te;
+    PinvBuffers pb;  // UNC_SVD_SCHUR only
 };
 
 // Lay out the workspace; with base == nullptr only the size is computed.
@@ -123,6 +125,10 @@ size_t carve(char* base, const Plan& pl, bool host_io, long long nnz, int nrows,
     b.e = c.take<double>(pl.N);
     b.gjws = c.take<double>(chol_small_doubles(pl.N));
     b.sig = c.take<double>((size_t)pl.C * 81);
+    if (pl.svd_schur) {
+        const size_t used = (c.off + 255) & ~size_t(255);
+        return used + pinv_carve(base ? base + used : nullptr, pl.N, pl.ld, b.pb);
+    }
     return c.off + 256;
 }
 
@@ -156,6 +162,12 @@ int check_options(const unc_options* o, int num_rows, int num_cols) {
         // dense (9C + 3P)^2 J^T J plus four scratch matrices of that size
         const long long n = 9LL * o->num_cams + 3LL * o->num_points;
         if (n > 46000) return fail(UNC_ERR_TOO_LARGE, "SVD algorithms: 9*num_cams + 3*num_points above 46000");
+        if (o->svd_remove_n < -1 || o->svd_remove_n > 31)
+            return fail(UNC_ERR_UNSUPPORTED, "svd_remove_n must be -1 (epsilon rule) or 0..31");
+        return UNC_OK;
+    }
+    if (o->algorithm == UNC_SVD_SCHUR) {
+        if (9LL * o->num_cams > 46000) return fail(UNC_ERR_TOO_LARGE, "9*num_cams above 46000");
         if (o->svd_remove_n < -1 || o->svd_remove_n > 31)
             return fail(UNC_ERR_UNSUPPORTED, "svd_remove_n must be -1 (epsilon rule) or 0..31");
         return UNC_OK;
@@ -264,7 +276,8 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     s.J = vals;
     int fx[3] = {o->pts2fix[0], o->pts2fix[1], o->pts2fix[2]};
     std::sort(fx, fx + 2);  // the reference sorts only the first two ids (compute.cpp:285)
-    s.has_fix = 1;
+    s.has_fix = pl.svd_schur ? 0 : 1;  // the SVD on Z keeps every point
+    if (pl.svd_schur) fx[0] = fx[1] = fx[2] = -1;
     for (int i = 0; i < 3; ++i) s.fix[i] = fx[i];
     const int N = pl.N, ld = pl.ld;
     cudaEvent_t* ev = ctx->ev;
@@ -298,6 +311,45 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     launch_schur(s, b.Z, ld, sm);
     launch_mirror_upper(b.Z, N, ld, sm);
     CK(cudaEventRecord(ev[5], sm));
+
+    PinvInfo pinfo{};
+    if (pl.svd_schur) {
+        // pseudo-inverse of the unscaled Z = S Z_s S (s: camera column norms)
+        // without its svd_remove_n smallest eigenvalues, then iZ_s = S P S so
+        // that the camera output's d_j d_k iZ_s(j, k) is P(j, k)
+        launch_unequilibrate(b.Z, N, ld, s.s_cam, nullptr, sm);
+        const double eps = o->epsilon < 0 ? 1e-10 : o->epsilon;
+        if (int r = pinv_psd(b.Z, N, ld, o->svd_remove_n, eps, b.pb, sm, &pinfo)) return r;
+        CK(cudaEventRecord(ev[6], sm));
+        launch_unequilibrate(b.Z, N, ld, s.s_cam, b.iZ, sm);
+        CK(cudaEventRecord(ev[7], sm));
+        launch_camera_output(b.iZ, ld, s.s_cam, pl.C, cam_out, b.sig, sm);
+        if (pl.P > 0) CK(cudaMemsetAsync(pt_out, 0, sizeof(double) * 6 * (size_t)pl.P, sm));
+        launch_point_cov(s, b.sig, pt_out, sm);
+        CK(cudaEventRecord(ev[8], sm));
+        int err = 0;
+        CK(cudaMemcpyAsync(&err, s.err, sizeof(int), cudaMemcpyDeviceToHost, sm));
+        CK(cudaStreamSynchronize(sm));
+        CK(cudaGetLastError());
+        if (st) {
+            st->lambda = 0;
+            for (int i = 0; i < 3; ++i) st->fixed_pts[i] = -1;
+            st->te_iterations = pinfo.iterations;  // subspace iterations
+            st->time_create_j = ev_s(ev[0], ev[1]);
+            st->time_fix_j = ev_s(ev[1], ev[2]);
+            st->time_norm_j = ev_s(ev[2], ev[3]);
+            st->time_multiply_jj = ev_s(ev[3], ev[4]);
+            st->time_compose_z = ev_s(ev[4], ev[5]);
+            st->time_inv_z = ev_s(ev[5], ev[6]);
+            st->time_pts_unc = ev_s(ev[7], ev[8]);
+            st->time_all = ev_s(ev[0], ev[8]);
+        }
+        if (err & ERRBIT_LAYOUT)
+            return fail(UNC_ERR_LAYOUT, "Jacobian rows are not in the 2 x (9 camera + 3 point) observation layout");
+        if (err & (ERRBIT_SINGULAR | ERRBIT_NONFINITE))
+            return fail(UNC_ERR_SINGULAR, "singular point block or non-finite value");
+        return UNC_OK;
+    }
 
     double lambda = o->lambda;
     if (lambda == -1) lambda = pow(10, -1.2653 * log10((double)N) - 2.9415);  // compute.cpp:124-125
@@ -458,6 +510,7 @@ Plan make_plan(const unc_options* o, int num_rows) {
     pl.nobs = num_rows / 2;
     pl.N = 9 * pl.C;
     pl.ld = ld_of(pl.N);
+    pl.svd_schur = o->algorithm == UNC_SVD_SCHUR;
     return pl;
 }
 
@@ -701,7 +754,8 @@ int unc_compute(unc_context* ctx, const unc_options* o, int num_rows, int num_co
     CK(cudaMemcpyAsync(cam_unc, b.cam_out, sizeof(double) * 45 * (size_t)pl.C, cudaMemcpyDeviceToHost, sm));
     // Points: slots [0, 6(P-3)) are written (zeroed or computed); of the last
     // three points only the non-fixed ones are written (compute.cpp:511,526).
-    size_t head = pl.P > 3 ? (size_t)(pl.P - 3) : 0;
+    // The SVD on Z fixes no point: every slot is written.
+    size_t head = pl.svd_schur ? (size_t)pl.P : (pl.P > 3 ? (size_t)(pl.P - 3) : 0);
     if (head) CK(cudaMemcpyAsync(pt_unc, b.pt_out, sizeof(double) * 6 * head, cudaMemcpyDeviceToHost, sm));
     for (int p = (int)head; p < pl.P; ++p) {
         if (p == b.s.fix[0] || p == b.s.fix[1] || p == b.s.fix[2]) continue;
@@ -770,7 +824,7 @@ int unc_compute_scene(unc_context* ctx, const unc_options* o, const double* cams
     rc = unc_compute_device(ctx, o, num_rows, num_cols, drows, dcols, dv, co, po, st, sm);
     if (rc) return rc;
     CK(cudaMemcpyAsync(cam_unc, co, sizeof(double) * 45 * (size_t)C, cudaMemcpyDeviceToHost, sm));
-    if (is_svd(o)) {
+    if (is_svd(o) || o->algorithm == UNC_SVD_SCHUR) {  // no fixed point
         if (P) CK(cudaMemcpyAsync(pt_unc, po, sizeof(double) * 6 * (size_t)P, cudaMemcpyDeviceToHost, sm));
     } else {  // the fixed points' slots are left as the caller had them (compute.cpp:511,526)
         int fx[3] = {o->pts2fix[0], o->pts2fix[1], o->pts2fix[2]};

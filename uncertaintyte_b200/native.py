@@ -20,6 +20,7 @@ LIB_PATH = os.path.join(_HERE, "libuncte.so")
 UNC_OK = 0
 TAYLOR_EXPANSION = 2
 SVD_QR_ITERATION = 0
+SVD_SCHUR = 3  # extension: SVD pseudo-inverse of the camera Schur complement
 SVD_DEVIDE_AND_CONQUER = 1
 PRECISION = {"fp64": 0, "mixed": 1, "mixed4": 2, "mixed3": 3}
 
