@@ -388,14 +388,18 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         return UNC_OK;
     };
     // the profiled region is the product kernel alone (slicing excluded)
+    // Each product writes its lower triangle and, transposed, the upper one
+    // (the powers are symmetric). In mixed mode the Taylor update iZ += k P of
+    // the power being sliced rides along in the slicing kernel.
     auto product = [&](const double* P, double* out, const int* skip) -> int {
         if (mixed) {
-            if (P != X) mixed_slice(P, ld, opP, sm, skip);
+            if (P != X) mixed_slice(P, ld, opP, sm, skip, b.iZ, b.te);
             if (int r = prof_mark()) return r;
-            mixed_gemm(P == X ? opXa : opP, opXb, out, ld, b.amax, true, s.err, sm, skip);
+            mixed_gemm(P == X ? opXa : opP, opXb, out, ld, b.amax, true, s.err, sm, skip, true);
         } else {
             if (int r = prof_mark()) return r;
-            gemm_f64_mode(N, N, N, 1.0, P, ld, X, ld, 0.0, out, ld, b.amax, GEMM_LOWER, sm, nullptr, 0, skip);
+            gemm_f64_mode(N, N, N, 1.0, P, ld, X, ld, 0.0, out, ld, b.amax, GEMM_LOWER | GEMM_MIRROR, sm, nullptr,
+                          0, skip);
         }
         return prof_mark();
     };
@@ -423,14 +427,12 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         const int* skip = &b.te->done;
         CK(cudaMemsetAsync(b.amax, 0, 8, sm));
         if (int r = product(X, add, nullptr)) return r;
-        launch_mirror_lower(add, N, ld, sm);
         for (int i = 1; i < 20; ++i) {
             const double k = pow(lambda, i) / factorial_i32(i - 1);
             launch_te_decide(b.te, b.amax, k, sm);
-            launch_axpy_te(b.iZ, add, b.te, N, ld, sm);
+            if (!mixed) launch_axpy_te(b.iZ, add, b.te, N, ld, sm);
             CK(cudaMemsetAsync(b.amax, 0, 8, sm));
             if (int r = product(add, tmp, skip)) return r;
-            launch_mirror_lower(tmp, N, ld, sm, skip);
             std::swap(add, tmp);
         }
         return UNC_OK;

@@ -199,11 +199,12 @@ __global__ void __launch_bounds__(GEMM_THREADS, (Cfg::BM == 128 ? 1 : 2))
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 int col = n0 + wn + j * 8 + t * 2 + h;
-                if (row < M && col < N) {
+                if (row < M && col < N && (!(mode & GEMM_MIRROR) || row >= col)) {
                     double* c = C + row + (long)col * ldc;
                     double v = alpha * acc[i][j][h];
                     if (beta != 0.0) v += beta * *c;
                     *c = v;
+                    if ((mode & GEMM_MIRROR) && row > col) C[col + (long)row * ldc] = v;
                     double av = fabs(v);
                     mx = fmax(mx, av <= 1.7976931348623157e308 ? av : __longlong_as_double(0x7ff0000000000000LL));
                 }
@@ -228,13 +229,15 @@ __global__ void k_splitk_reduce(int M, int N, int splits, const double* __restri
     double mx = 0.0;
     if (idx < (long)M * N) {
         const int col = (int)(idx / M), row = (int)(idx - (long)col * M);
-        if (!((mode & GEMM_LOWER) && (col / bn) * bn > (row / bm) * bm + bm - 1)) {
+        if (!((mode & GEMM_LOWER) && (col / bn) * bn > (row / bm) * bm + bm - 1) &&
+            !((mode & GEMM_MIRROR) && row < col)) {
             double v = 0.0;
             for (int s = 0; s < splits; ++s) v += part[(size_t)s * M * N + idx];
             double* c = C + row + (long)col * ldc;
             v *= alpha;
             if (beta != 0.0) v += beta * *c;
             *c = v;
+            if ((mode & GEMM_MIRROR) && row > col) C[col + (long)row * ldc] = v;
             const double av = fabs(v);
             mx = av <= 1.7976931348623157e308 ? av : __longlong_as_double(0x7ff0000000000000LL);
         }

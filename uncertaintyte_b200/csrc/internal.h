@@ -144,6 +144,7 @@ enum : int {
     GEMM_KLO_N = 8,
     GEMM_KHI_M = 16,
     GEMM_KHI_N = 32,
+    GEMM_MIRROR = 64,  // symmetric C: write the lower triangle at (i, j) and (j, i), nothing above it directly
 };
 // ws (ws_doubles): optional scratch that enables split-K for outputs with
 // fewer tiles than SMs (partials summed in a fixed order by a second kernel).
@@ -208,10 +209,15 @@ size_t mixed_slice_bytes(int n, int slices);
 // Prepare the operand over buf/exps (as_b: box rows of the B operand). False
 // when the driver's tensor-map encoder is unavailable.
 bool mixed_plan(MixedOperand& op, int8_t* buf, int* exps, int n, int slices, bool as_b);
-void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st, const int* skip = nullptr);
-// C = P * X from the slices of P (a) and X (b); lower_only: tiles on/below the diagonal.
+struct TeState;
+// Y, te (optional): Y += te->coef * A while A is sliced, unless te->done.
+void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st, const int* skip = nullptr,
+                 double* Y = nullptr, const TeState* te = nullptr);
+// C = P * X from the slices of P (a) and X (b); lower_only: tiles on/below the
+// diagonal; mirror: the result's lower triangle is also written transposed
+// into the upper one (a symmetric product needs no separate mirror pass).
 void mixed_gemm(const MixedOperand& a, const MixedOperand& b, double* C, int ldc, unsigned long long* amax,
-                bool lower_only, int* err, cudaStream_t st, const int* skip = nullptr);
+                bool lower_only, int* err, cudaStream_t st, const int* skip = nullptr, bool mirror = false);
 
 // ---------------- svd.cu ----------------
 // Scratch of the PSD pseudo-inverse (n x ld matrices and p x n blocks).

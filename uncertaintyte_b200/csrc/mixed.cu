@@ -134,9 +134,17 @@ using namespace mp;
 // int8 planes out[s][j][k] (pitch kp bytes, plane stride rows_pad * kp) of
 // round-to-nearest digits in [-64, 64], and the row exponents e[j] with
 // max_k |A[j,k]| 2^-e < 1/2. One CTA per row.
+// 2^e exactly (bit pattern for normal exponents): v * pow2(e) == ldexp(v, e)
+__device__ __forceinline__ double pow2(int e) {
+    return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52) : ldexp(1.0, e);
+}
+
+// Y (optional): Y += te->coef * A on the way (the Taylor update iZ += k add of
+// the power being sliced, compute.cpp:64-71), unless te->done.
 __global__ void __launch_bounds__(256) k_slice_rows(const double* __restrict__ A, long lda, int n, int S,
                                                    int8_t* __restrict__ out, int rows_pad, int kp,
-                                                   int* __restrict__ exps, const int* skip) {
+                                                   int* __restrict__ exps, const int* skip, double* Y,
+                                                   const TeState* te) {
     if (skip && *skip) return;
     __shared__ double red[8];
     const int j = blockIdx.x;
@@ -158,12 +166,18 @@ __global__ void __launch_bounds__(256) k_slice_rows(const double* __restrict__ A
     if (red[0] > 0.0 && red[0] <= 1.7976931348623157e308) frexp(red[0], &e);  // max * 2^-e in [0.5, 1)
     e += 1;                                                                     // max * 2^-e in [0.25, 0.5)
     if (threadIdx.x == 0) exps[j] = e;
+    if (Y) {
+        const double c = te->coef;
+        double* y = Y + (long)j * lda;
+        for (int k = threadIdx.x; k < n; k += 256) y[k] += c * col[k];
+    }
+    const double sc = pow2(-e);
     const size_t plane = (size_t)rows_pad * kp;
     int8_t* row = out + (size_t)j * kp;
     for (int k0 = 4 * threadIdx.x; k0 < n; k0 += 4 * 256) {
         double v[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) v[u] = (k0 + u < n) ? ldexp(col[k0 + u], -e) : 0.0;
+        for (int u = 0; u < 4; ++u) v[u] = (k0 + u < n) ? col[k0 + u] * sc : 0.0;
         for (int s = 0; s < S; ++s) {
             char4 q;
             signed char qs[4];
@@ -191,7 +205,7 @@ template <int NT, int S>
 __global__ void __launch_bounds__(THREADS, 1)
     k_ozaki_gemm(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int M, int N,
                  int kp, int rowsA, int rowsB, const int* __restrict__ eA, const int* __restrict__ eB, double* C,
-                 long ldc, unsigned long long* amax, int lower_only, int* err, const int* skip) {
+                 long ldc, unsigned long long* amax, int lower_only, int* err, const int* skip, int mirror) {
     using Sh = Shape<NT, S>;
     if (skip && *skip) return;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * NT;
@@ -285,7 +299,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       __syncwarp();
     }
     // epilogue: every warp reads its 32 TMEM lanes (tile rows)
-    const bool ok = mbar_wait(done, 0);
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(done, 0));  // warp-uniform
     if (!ok && lane == 0) atomicOr(err, ERRBIT_TIMEOUT);
     __syncwarp();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
@@ -310,10 +324,16 @@ __global__ void __launch_bounds__(THREADS, 1)
                 for (int j = 0; j < 16; ++j) {
                     const int col = n0 + c0 + j;
                     if (col < N) {
-                        const double x = ldexp(v[j], er + eB[col]);
-                        C[row + (long)col * ldc] = x;
-                        const double ax = fabs(x);
-                        mx = fmax(mx, ax <= 1.7976931348623157e308 ? ax : __longlong_as_double(0x7ff0000000000000LL));
+                        const double x = v[j] * pow2(er + eB[col]);
+                        // mirror: the lower triangle is written at (row, col) and at
+                        // (col, row); nothing above the diagonal is written directly
+                        if (!mirror || row >= col) {
+                            C[row + (long)col * ldc] = x;
+                            const double ax = fabs(x);
+                            mx = fmax(mx, ax <= 1.7976931348623157e308 ? ax
+                                                                       : __longlong_as_double(0x7ff0000000000000LL));
+                        }
+                        if (mirror && row > col) C[col + (long)row * ldc] = x;
                     }
                 }
             }
@@ -423,38 +443,39 @@ bool mixed_plan(MixedOperand& op, int8_t* buf, int* exps, int n, int slices, boo
     return make_map(&op.map, buf, op.rows * slices, op.kp, as_b ? nt : BM);
 }
 
-void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st, const int* skip) {
-    k_slice_rows<<<op.n, 256, 0, st>>>(A, lda, op.n, op.slices, op.buf, op.rows, op.kp, op.exps, skip);
+void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st, const int* skip, double* Y,
+                 const TeState* te) {
+    k_slice_rows<<<op.n, 256, 0, st>>>(A, lda, op.n, op.slices, op.buf, op.rows, op.kp, op.exps, skip, Y, te);
     count_launch();
 }
 
 void mixed_gemm(const MixedOperand& a, const MixedOperand& b, double* C, int ldc, unsigned long long* amax,
-                bool lower_only, int* err, cudaStream_t st, const int* skip) {
+                bool lower_only, int* err, cudaStream_t st, const int* skip, bool mirror) {
     const int n = a.n;
     if (a.slices == 4) {
         set_attr_once<128, 4>();
         dim3 grid((n + 127) / 128, (n + BM - 1) / BM);
         k_ozaki_gemm<128, 4><<<grid, THREADS, Shape<128, 4>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
                                                                          a.exps, b.exps, C, ldc, amax,
-                                                                         lower_only ? 1 : 0, err, skip);
+                                                                         lower_only ? 1 : 0, err, skip, mirror ? 1 : 0);
     } else if (a.slices == 5 && mixed_tile_n(5, n) == 64) {
         set_attr_once<64, 5>();
         dim3 grid((n + 63) / 64, (n + BM - 1) / BM);
         k_ozaki_gemm<64, 5><<<grid, THREADS, Shape<64, 5>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
                                                                        a.exps, b.exps, C, ldc, amax,
-                                                                       lower_only ? 1 : 0, err, skip);
+                                                                       lower_only ? 1 : 0, err, skip, mirror ? 1 : 0);
     } else if (a.slices == 5) {
         set_attr_once<96, 5>();
         dim3 grid((n + 95) / 96, (n + BM - 1) / BM);
         k_ozaki_gemm<96, 5><<<grid, THREADS, Shape<96, 5>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
                                                                        a.exps, b.exps, C, ldc, amax,
-                                                                       lower_only ? 1 : 0, err, skip);
+                                                                       lower_only ? 1 : 0, err, skip, mirror ? 1 : 0);
     } else {
         set_attr_once<128, 3>();
         dim3 grid((n + 127) / 128, (n + BM - 1) / BM);
         k_ozaki_gemm<128, 3><<<grid, THREADS, Shape<128, 3>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
                                                                          a.exps, b.exps, C, ldc, amax,
-                                                                         lower_only ? 1 : 0, err, skip);
+                                                                         lower_only ? 1 : 0, err, skip, mirror ? 1 : 0);
     }
     count_launch();
 }
