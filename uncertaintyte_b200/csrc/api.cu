@@ -112,6 +112,7 @@ size_t carve(char* base, const Plan& pl, bool host_io, long long nnz, int nrows,
     s.iVs = c.take<double>((size_t)pl.P * 6);
     s.Ws = c.take<double>((size_t)pl.nobs * 27);
     s.Ys = c.take<double>((size_t)pl.nobs * 27);
+    s.cam_part = c.take<double>(45 * camera_tile_slots(pl.C, pl.nobs));
     s.blk_cnt = c.take<int>((size_t)pl.C * pl.C);
     s.blk_ptr = c.take<int>((size_t)pl.C * pl.C + 1);
     s.err = c.take<int>(4);
@@ -301,12 +302,14 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     CK(cudaStreamSynchronize(sm));
     if (npairs < 0) return fail(UNC_ERR_TOO_LARGE, "more than 2^31 co-visible observation pairs");
     const size_t long_cap = (size_t)npairs / 1025 + 1;
-    const size_t need = (size_t)npairs * 8 + (long_cap + 1) * sizeof(int) + 64;
+    const size_t nz_ints = schur_list_ints(pl.C, npairs);
+    const size_t need = (size_t)npairs * 8 + (long_cap + 1 + nz_ints) * sizeof(int) + 64;
     // headroom for the next scene
     if (int r = grow_buffer(&ctx->tup, &ctx->tup_bytes, need, need + need / 4, sm)) return r;
     s.pairs = reinterpret_cast<unsigned long long*>(ctx->tup);
     s.long_list = reinterpret_cast<int*>(s.pairs + npairs + 1);
     s.long_cap = (int)long_cap;
+    s.nz_list = s.long_list + long_cap + 1;
     launch_camera_self(s, b.Z, ld, sm);
     launch_schur(s, b.Z, ld, sm);
     launch_mirror_upper(b.Z, N, ld, sm);

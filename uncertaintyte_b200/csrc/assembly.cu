@@ -336,59 +336,141 @@ __device__ __forceinline__ void load_pt_rows(const double* __restrict__ J, int o
     p1[0] = c.y; p1[1] = d.x; p1[2] = d.y;
 }
 
-// One warp per camera: segmented warp reduction of sum_o Jc_o^T Jc_o (45
-// upper-triangle values), column norms s = sqrt(diag), scaled block U/(s s)
-// written into the diagonal block of Z (both triangles).
-template <bool kScaled>
-__global__ void __launch_bounds__(128) k_camera_blocks(int num_cams, const double* __restrict__ J,
-                                                       const int* __restrict__ cam_ptr,
-                                                       const int* __restrict__ cam_obs,
-                                                       double* __restrict__ s_cam, double* Z, int ldz) {
-    int cam = blockIdx.x * 4 + (threadIdx.x >> 5);
-    int lane = threadIdx.x & 31;
-    if (cam >= num_cams) return;
-    double acc[45];
-#pragma unroll
-    for (int t = 0; t < 45; ++t) acc[t] = 0.0;
-    int b = cam_ptr[cam], e = cam_ptr[cam + 1];
-    for (int i = b + lane; i < e; i += 32) {
-        double r0[9], r1[9];
-        load_cam_rows(J, cam_obs[i], r0, r1);
-#pragma unroll
-        for (int j = 0; j < 9; ++j)
-#pragma unroll
-            for (int k = j; k < 9; ++k) acc[ut9(j, k)] += r0[j] * r0[k] + r1[j] * r1[k];
-    }
-#pragma unroll
-    for (int t = 0; t < 45; ++t) acc[t] = warp_sum(acc[t]);
-    double s[9];
-#pragma unroll
-    for (int j = 0; j < 9; ++j) s[j] = sqrt(acc[ut9(j, j)]);
-    if (lane < 9 && s_cam) s_cam[9 * cam + lane] = s[lane];
-    // 45 upper-triangle values over 32 lanes: lane l writes t = l and t = l + 32
-#pragma unroll
-    for (int j = 0; j < 9; ++j)
-#pragma unroll
-        for (int k = j; k < 9; ++k) {
-            if (lane == ut9(j, k) || lane + 32 == ut9(j, k)) {
-                double v = acc[ut9(j, k)];
-                if (kScaled) {
-                    // J <- J * diag(1/s) skipping s == 0 (ScaledSparseMatrix.cpp:352-356)
-                    if (s[j] != 0) v *= 1.0 / s[j];
-                    if (s[k] != 0) v *= 1.0 / s[k];
-                }
-                long r = 9L * cam + j, c = 9L * cam + k;
-                Z[r + c * ldz] = v;
-                Z[c + r * ldz] = v;
-            }
-        }
+// ------------------------------------------------------------------------
+// per-camera observation tiles
+// ------------------------------------------------------------------------
+// The observations of camera c, cam_obs[cam_ptr[c], cam_ptr[c+1]), are cut
+// into tiles of kObsTile. Camera c owns the tile slots [base(c), base(c+1))
+// with base(c) = c + cam_ptr[c] / kObsTile: never fewer than its tiles, since
+// ceil((B - A) / T) <= floor(B / T) - floor(A / T) + 1. Slots past a camera's
+// last tile are empty. The slot count base(C) is bounded on the host by
+// C + num_obs / kObsTile, so the grids need no read-back; a CTA finds its
+// camera by binary search over cam_ptr. Per-tile partial sums are combined per
+// camera in slot order: a fixed summation order, bitwise repeatable.
+constexpr int kObsTile = 256;
+constexpr int kTileGroups = 5;  // 45 upper-triangle elements x 5 groups = 225 of the 256 threads
+
+size_t camera_tile_slots(int num_cams, int num_obs) { return (size_t)num_cams + num_obs / kObsTile + 1; }
+
+__device__ __forceinline__ int tile_base(const int* __restrict__ cam_ptr, int c) {
+    return c + cam_ptr[c] / kObsTile;
 }
+
+struct ObsTile {
+    int cam, begin, end;
+};
+
+__device__ __forceinline__ bool find_tile(const int* __restrict__ cam_ptr, int num_cams, int k, ObsTile& t) {
+    if (k >= tile_base(cam_ptr, num_cams)) return false;
+    int lo = 0, hi = num_cams;  // tile_base(lo) <= k < tile_base(hi)
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (tile_base(cam_ptr, mid) <= k)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    t.cam = lo;
+    t.end = cam_ptr[lo + 1];
+    t.begin = min(cam_ptr[lo] + (k - tile_base(cam_ptr, lo)) * kObsTile, t.end);
+    t.end = min(t.begin + kObsTile, t.end);
+    return true;
+}
+
+// (j, k), j <= k, of upper-triangle element el (inverse of ut9)
+__device__ __forceinline__ void ut9_inv(int el, int& j, int& k) {
+    j = 0;
+    while (j < 8 && ut9(j + 1, j + 1) <= el) ++j;
+    k = j + (el - ut9(j, j));
+}
+
+// U = sum_o Jc_o^T Jc_o per tile: the tile's 18 camera values per observation
+// are staged in shared memory (odd row stride: conflict-free), then thread
+// (el, g) sums element el over the tile's observations g, g + 5, ...
+constexpr int kGramStride = 19;
+__global__ void __launch_bounds__(kObsTile) k_camera_gram_tiles(int num_cams, const double* __restrict__ J,
+                                                                const int* __restrict__ cam_ptr,
+                                                                const int* __restrict__ cam_obs,
+                                                                double* __restrict__ part) {
+    __shared__ double sj[kObsTile * kGramStride];
+    __shared__ double red[kTileGroups][45];
+    ObsTile tile;
+    if (!find_tile(cam_ptr, num_cams, blockIdx.x, tile)) return;
+    const int n = tile.end - tile.begin, t = threadIdx.x;
+    if (t < n) {
+        double r0[9], r1[9];
+        load_cam_rows(J, cam_obs[tile.begin + t], r0, r1);
+        double* row = sj + t * kGramStride;
+#pragma unroll
+        for (int j = 0; j < 9; ++j) {
+            row[j] = r0[j];
+            row[9 + j] = r1[j];
+        }
+    }
+    __syncthreads();
+    if (t < 45 * kTileGroups) {
+        const int el = t % 45, g = t / 45;
+        int j, k;
+        ut9_inv(el, j, k);
+        double acc = 0.0;
+        for (int i = g; i < n; i += kTileGroups) {
+            const double* row = sj + i * kGramStride;
+            acc += row[j] * row[k] + row[9 + j] * row[9 + k];
+        }
+        red[g][el] = acc;
+    }
+    __syncthreads();
+    if (t < 45) {
+        double v = red[0][t];
+#pragma unroll
+        for (int g = 1; g < kTileGroups; ++g) v += red[g][t];
+        part[45L * blockIdx.x + t] = v;
+    }
+}
+
+// One warp per camera: U = sum of the camera's tile partials, column norms
+// s = sqrt(diag U), scaled block U/(s s) written into the diagonal block of Z
+// (both triangles). J <- J diag(1/s) skips s == 0 (ScaledSparseMatrix.cpp:352-356).
+__global__ void __launch_bounds__(128) k_camera_gram_reduce(int num_cams, const int* __restrict__ cam_ptr,
+                                                            const double* __restrict__ part,
+                                                            double* __restrict__ s_cam, double* Z, long ldz) {
+    __shared__ double sh[4][45];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cam = blockIdx.x * 4 + w;
+    if (cam >= num_cams) return;
+    const int k0 = tile_base(cam_ptr, cam), k1 = tile_base(cam_ptr, cam + 1);
+    double a0 = 0.0, a1 = 0.0;
+    for (int k = k0; k < k1; ++k) {
+        a0 += part[45L * k + lane];
+        if (lane < 13) a1 += part[45L * k + 32 + lane];
+    }
+    double* u = sh[w];
+    u[lane] = a0;
+    if (lane < 13) u[32 + lane] = a1;
+    __syncwarp();
+    if (lane < 9 && s_cam) s_cam[9L * cam + lane] = sqrt(u[ut9(lane, lane)]);
+    for (int el = lane; el < 45; el += 32) {
+        int j, k;
+        ut9_inv(el, j, k);
+        const double sj = sqrt(u[ut9(j, j)]), sk = sqrt(u[ut9(k, k)]);
+        double v = u[el];
+        if (sj != 0) v *= 1.0 / sj;
+        if (sk != 0) v *= 1.0 / sk;
+        const long r = 9L * cam + j, c = 9L * cam + k;
+        Z[r + c * ldz] = v;
+        Z[c + r * ldz] = v;
+    }
+}
+
+size_t camera_tile_part_doubles(int num_cams, int num_obs) { return 45 * camera_tile_slots(num_cams, num_obs); }
 
 void launch_camera_blocks(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
     if (s.num_cams == 0) return;
-    k_camera_blocks<true><<<(s.num_cams + 3) / 4, 128, 0, st>>>(s.num_cams, s.J, s.cam_ptr,
-                                                                s.cam_obs, s.s_cam, Z, ldz);
-    count_launch();
+    const unsigned slots = (unsigned)camera_tile_slots(s.num_cams, s.num_obs);
+    k_camera_gram_tiles<<<slots, kObsTile, 0, st>>>(s.num_cams, s.J, s.cam_ptr, s.cam_obs, s.cam_part);
+    k_camera_gram_reduce<<<(s.num_cams + 3) / 4, 128, 0, st>>>(s.num_cams, s.cam_ptr, s.cam_part, s.s_cam, Z,
+                                                                ldz);
+    count_launch(2);
 }
 
 // One thread per point: V_p = sum Jp^T Jp (unscaled), s = sqrt(diag), scaled
@@ -441,159 +523,213 @@ void launch_point_blocks(const SceneDev& s, cudaStream_t st) {
     count_launch();
 }
 
-// One thread per observation: W_o = Jc^T Jp scaled by the column norms and
-// Y_o = W_o iV_p (the camera-point block of Y = W * iV, compute.cpp:108).
-__global__ void k_obs_blocks(int num_obs, const double* __restrict__ J,
-                             const int* __restrict__ obs_cam, const int* __restrict__ obs_pt,
-                             const double* __restrict__ s_cam, const double* __restrict__ s_pt,
-                             const double* __restrict__ iVs, double* __restrict__ Ws,
-                             double* __restrict__ Ys) {
-    int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= num_obs) return;
-    int c = obs_cam[o], p = obs_pt[o];
-    if (c < 0 || p < 0) return;
-    double r0[9], r1[9], a[3], b[3];
-    load_cam_rows(J, o, r0, r1);
-    load_pt_rows(J, o, a, b);
-    double sp[3], is[6];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        double v = s_pt[3L * p + k];
-        sp[k] = v != 0 ? 1.0 / v : 1.0;
+// W_o = Jc^T Jp scaled by the column norms and Y_o = W_o iV_p (the
+// camera-point block of Y = W * iV, compute.cpp:108), one camera tile per CTA,
+// fused with the tile's share of the Schur self terms sum_o Y_o W_o^T of the
+// camera's diagonal block. One thread per observation computes its two 9 x 3
+// blocks into shared memory (odd record stride 27: conflict-free); warps then
+// write whole 216-byte records, and thread (el, g) sums upper-triangle element
+// el of Y_o W_o^T over the tile's observations g, g + 5, ...
+constexpr size_t kObsTileSmem = 2ul * kObsTile * 27 * sizeof(double);  // 110,592 bytes
+
+__global__ void __launch_bounds__(kObsTile) k_camera_obs_tiles(
+    int num_cams, const double* __restrict__ J, const int* __restrict__ cam_ptr, const int* __restrict__ cam_obs,
+    const int* __restrict__ obs_pt, const double* __restrict__ s_cam, const double* __restrict__ s_pt,
+    const double* __restrict__ iVs, double* __restrict__ Ws, double* __restrict__ Ys, double* __restrict__ part) {
+    extern __shared__ double smem[];
+    double* sw = smem;                   // [kObsTile][27] W_o
+    double* sy = smem + kObsTile * 27;   // [kObsTile][27] Y_o
+    __shared__ int so[kObsTile];
+    __shared__ double isc[9];
+    ObsTile tile;
+    if (!find_tile(cam_ptr, num_cams, blockIdx.x, tile)) return;
+    const int n = tile.end - tile.begin, t = threadIdx.x;
+    if (t < 9) {
+        const double v = s_cam[9L * tile.cam + t];
+        isc[t] = v != 0 ? 1.0 / v : 1.0;
     }
-#pragma unroll
-    for (int k = 0; k < 6; ++k) is[k] = iVs[6L * p + k];
-    const double iv[3][3] = {{is[0], is[1], is[2]}, {is[1], is[3], is[4]}, {is[2], is[4], is[5]}};
-    double* W = Ws + 27L * o;
-    double* Y = Ys + 27L * o;
-#pragma unroll
-    for (int j = 0; j < 9; ++j) {
-        double sc = s_cam[9L * c + j];
-        sc = sc != 0 ? 1.0 / sc : 1.0;
-        double w[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) w[k] = (r0[j] * a[k] + r1[j] * b[k]) * sc * sp[k];
+    __syncthreads();
+    if (t < n) {
+        const int o = cam_obs[tile.begin + t];
+        const int p = obs_pt[o];
+        so[t] = o;
+        double r0[9], r1[9], a[3], b[3];
+        load_cam_rows(J, o, r0, r1);
+        load_pt_rows(J, o, a, b);
+        double sp[3], is[6];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            W[3 * j + k] = w[k];
-            Y[3 * j + k] = w[0] * iv[0][k] + w[1] * iv[1][k] + w[2] * iv[2][k];
+            const double v = s_pt[3L * p + k];
+            sp[k] = v != 0 ? 1.0 / v : 1.0;
         }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) is[k] = iVs[6L * p + k];
+        const double iv[3][3] = {{is[0], is[1], is[2]}, {is[1], is[3], is[4]}, {is[2], is[4], is[5]}};
+        double* W = sw + 27 * t;
+        double* Y = sy + 27 * t;
+#pragma unroll
+        for (int j = 0; j < 9; ++j) {
+            const double sc = isc[j];
+            double w[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) w[k] = (r0[j] * a[k] + r1[j] * b[k]) * sc * sp[k];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                W[3 * j + k] = w[k];
+                Y[3 * j + k] = w[0] * iv[0][k] + w[1] * iv[1][k] + w[2] * iv[2][k];
+            }
+        }
+    }
+    __syncthreads();
+    const int warp = t >> 5, lane = t & 31;
+    if (lane < 27)
+        for (int i = warp; i < n; i += kObsTile / 32) {
+            const long o = so[i];
+            Ws[27 * o + lane] = sw[27 * i + lane];
+            Ys[27 * o + lane] = sy[27 * i + lane];
+        }
+    double acc = 0.0;
+    const int el = t % 45, g = t / 45;
+    if (t < 45 * kTileGroups) {
+        int j, k;
+        ut9_inv(el, j, k);
+        for (int i = g; i < n; i += kTileGroups) {
+            const double* y = sy + 27 * i + 3 * j;
+            const double* w = sw + 27 * i + 3 * k;
+            acc += y[0] * w[0] + y[1] * w[1] + y[2] * w[2];
+        }
+    }
+    __syncthreads();  // the tile is consumed: its first 225 doubles take the group sums
+    if (t < 45 * kTileGroups) smem[45 * g + el] = acc;
+    __syncthreads();
+    if (t < 45) {
+        double v = smem[t];
+#pragma unroll
+        for (int q = 1; q < kTileGroups; ++q) v += smem[45 * q + t];
+        part[45L * blockIdx.x + t] = v;
     }
 }
 
 void launch_obs_blocks(const SceneDev& s, cudaStream_t st) {
-    if (s.num_obs == 0) return;
-    k_obs_blocks<<<(s.num_obs + 127) / 128, 128, 0, st>>>(s.num_obs, s.J, s.obs_cam, s.obs_pt,
-                                                          s.s_cam, s.s_pt, s.iVs, s.Ws, s.Ys);
+    if (s.num_cams == 0) return;
+    prepare_assembly_kernels();
+    const unsigned slots = (unsigned)camera_tile_slots(s.num_cams, s.num_obs);
+    k_camera_obs_tiles<<<slots, kObsTile, kObsTileSmem, st>>>(s.num_cams, s.J, s.cam_ptr, s.cam_obs, s.obs_pt,
+                                                              s.s_cam, s.s_pt, s.iVs, s.Ws, s.Ys, s.cam_part);
     count_launch();
 }
 
-// Self terms of the Schur complement: Z(c, c) -= sum over observations o of
-// camera c of Y_o W_o^T (= W_o iV_p W_o^T, symmetric). One warp per camera,
-// lanes stride over the camera's observations (ascending) and the 45 upper-
-// triangle sums are reduced across the warp in a fixed order. Only the upper
-// triangle of the diagonal block is updated (it is mirrored later).
-__global__ void __launch_bounds__(128) k_camera_self(int num_cams, const int* __restrict__ cam_ptr,
-                                                     const int* __restrict__ cam_obs,
-                                                     const double* __restrict__ Ws,
-                                                     const double* __restrict__ Ys, double* Z, long ldz) {
+// Self terms of the Schur complement, Z(c, c) -= sum over observations o of
+// camera c of Y_o W_o^T (= W_o iV_p W_o^T, symmetric): one warp per camera adds
+// the camera's tile partials in slot order. Only the upper triangle of the
+// diagonal block is updated (it is mirrored later).
+__global__ void __launch_bounds__(128) k_camera_self_reduce(int num_cams, const int* __restrict__ cam_ptr,
+                                                            const double* __restrict__ part, double* Z,
+                                                            long ldz) {
     const int cam = blockIdx.x * 4 + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (cam >= num_cams) return;
-    double acc[45];
-#pragma unroll
-    for (int t = 0; t < 45; ++t) acc[t] = 0.0;
-    for (int i = cam_ptr[cam] + lane; i < cam_ptr[cam + 1]; i += 32) {
-        const int o = cam_obs[i];
-        const double* y = Ys + 27L * o;
-        const double* w = Ws + 27L * o;
-        double yy[27], ww[27];
-#pragma unroll
-        for (int k = 0; k < 27; ++k) {
-            yy[k] = __ldg(y + k);
-            ww[k] = __ldg(w + k);
-        }
-#pragma unroll
-        for (int j = 0; j < 9; ++j)
-#pragma unroll
-            for (int k = j; k < 9; ++k)
-                acc[ut9(j, k)] += yy[3 * j] * ww[3 * k] + yy[3 * j + 1] * ww[3 * k + 1] + yy[3 * j + 2] * ww[3 * k + 2];
+    const int k0 = tile_base(cam_ptr, cam), k1 = tile_base(cam_ptr, cam + 1);
+    for (int el = lane; el < 45; el += 32) {
+        double v = 0.0;
+        for (int k = k0; k < k1; ++k) v += part[45L * k + el];
+        int j, k;
+        ut9_inv(el, j, k);
+        Z[(9L * cam + j) + (9L * cam + k) * ldz] -= v;
     }
-#pragma unroll
-    for (int t = 0; t < 45; ++t) acc[t] = warp_sum(acc[t]);
-#pragma unroll
-    for (int j = 0; j < 9; ++j)
-#pragma unroll
-        for (int k = j; k < 9; ++k)
-            if (lane == ut9(j, k) || lane + 32 == ut9(j, k)) Z[(9L * cam + j) + (9L * cam + k) * ldz] -= acc[ut9(j, k)];
 }
 
 void launch_camera_self(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
     if (s.num_cams == 0) return;
-    k_camera_self<<<(s.num_cams + 3) / 4, 128, 0, st>>>(s.num_cams, s.cam_ptr, s.cam_obs, s.Ws, s.Ys, Z, ldz);
+    k_camera_self_reduce<<<(s.num_cams + 3) / 4, 128, 0, st>>>(s.num_cams, s.cam_ptr, s.cam_part, Z, ldz);
     count_launch();
 }
 
 // Deterministic Schur scatter: Z(c, c') -= sum over points p seen by both
 // cameras of Y_o W_o'^T, for c <= c' (upper block triangle).
 //
-//  1. k_pair_enum (count / scatter): every point lists its ordered
+//  1. k_pair_enum (count / scatter): one warp per point lists its ordered
 //     observation pairs (o, o') with camera(o) <= camera(o'); pairs are
 //     counted per camera-pair block and scattered into a block-grouped list.
-//  2. the pairs of each block are sorted by (o, o') (warp rank sort, or a
+//  2. k_list_blocks collects the non-empty blocks (any order: it only
+//     distributes work).
+//  3. the pairs of each block are sorted by (o, o') (warp rank sort, or a
 //     block bitonic sort for long lists), which fixes the summation order.
-//  3. k_schur_blocks: one warp per block reduces its pairs in registers (lane
-//     l owns elements l, l+32, l+64 of the 9x9 block) and writes the block of
-//     Z once. No floating-point atomics: results are bitwise repeatable.
+//  4. k_schur_blocks: one warp per non-empty block reduces its pairs in
+//     registers and writes the block of Z once. No floating-point atomics:
+//     results are bitwise repeatable.
 template <bool kScatter>
-__global__ void k_pair_enum(int num_points, int num_cams, const int* __restrict__ pt_ptr,
-                            const int* __restrict__ pt_obs, const int* __restrict__ obs_cam,
-                            int* cnt_or_cursor, unsigned long long* __restrict__ pairs) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) k_pair_enum(int num_points, int num_cams, const int* __restrict__ pt_ptr,
+                                                   const int* __restrict__ pt_obs, const int* __restrict__ obs_cam,
+                                                   int* cnt_or_cursor, unsigned long long* __restrict__ pairs) {
+    const int p = blockIdx.x * 4 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (p >= num_points) return;
-    const int b = pt_ptr[p], e = pt_ptr[p + 1];
-    for (int i = b; i < e; ++i) {
-        const int oa = pt_obs[i], ca = obs_cam[oa];
-        for (int k = b; k < e; ++k) {
-            const int ob = pt_obs[k], cb = obs_cam[ob];
-            if (ca > cb || k == i) continue;  // self pairs are reduced per camera (k_camera_self)
-            const long key = (long)ca * num_cams + cb;
-            if (kScatter) {
-                int pos = atomicAdd(cnt_or_cursor + key, 1);
-                pairs[pos] = ((unsigned long long)(unsigned)oa << 32) | (unsigned)ob;
-            } else {
-                atomicAdd(cnt_or_cursor + key, 1);
-            }
+    const int b = pt_ptr[p], m = pt_ptr[p + 1] - b;
+    const long mm = (long)m * m;
+    for (long idx = lane; idx < mm; idx += 32) {
+        const int i = (int)(idx / m), k = (int)(idx - (long)i * m);
+        if (i == k) continue;  // self pairs are reduced per camera (k_camera_obs_tiles)
+        const int oa = pt_obs[b + i], ob = pt_obs[b + k];
+        const int ca = obs_cam[oa], cb = obs_cam[ob];
+        if (ca > cb) continue;
+        const long key = (long)ca * num_cams + cb;
+        if (kScatter) {
+            const int pos = atomicAdd(cnt_or_cursor + key, 1);
+            pairs[pos] = ((unsigned long long)(unsigned)oa << 32) | (unsigned)ob;
+        } else {
+            atomicAdd(cnt_or_cursor + key, 1);
         }
     }
 }
 
+// nz[0] = number of non-empty blocks, nz[1] = work cursor of k_schur_blocks,
+// nz[2 ...] = their ids (warp-aggregated appends).
+__global__ void k_list_blocks(long nblk, const int* __restrict__ blk_ptr, int* nz) {
+    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = k < nblk && blk_ptr[k + 1] > blk_ptr[k];
+    const unsigned mask = __ballot_sync(0xffffffffu, live);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(nz, __popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (live) nz[2 + base + __popc(mask & ((1u << lane) - 1))] = (int)k;
+}
+
 constexpr int kPairWarpCap = 1024;
-// long_list[0] counts the blocks with more than kPairWarpCap pairs; their ids
-// follow (capacity long_cap) and are sorted by k_sort_pairs_block.
-__global__ void k_sort_pairs_warp(long nseg, const int* __restrict__ ptr, unsigned long long* data,
-                                  int* long_list, int long_cap) {
-    __shared__ unsigned long long sh[4][kPairWarpCap];
+constexpr int kSortWarps = 4;
+// One warp per listed block (grid-stride over the list), rank sort through
+// shared memory. long_list[0] counts the blocks with more than kPairWarpCap
+// pairs; their ids follow (capacity long_cap) and are sorted by
+// k_sort_pairs_block.
+__global__ void __launch_bounds__(32 * kSortWarps) k_sort_pairs_warp(const int* __restrict__ nz,
+                                                                    const int* __restrict__ ptr,
+                                                                    unsigned long long* data, int* long_list,
+                                                                    int long_cap) {
+    __shared__ unsigned long long sh[kSortWarps][kPairWarpCap];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long seg = (long)blockIdx.x * 4 + w;
-    if (seg >= nseg) return;
-    const int b = ptr[seg], n = ptr[seg + 1] - b;
-    if (n <= 1) return;
-    if (n > kPairWarpCap) {
-        if (lane == 0) {
-            int i = atomicAdd(long_list, 1);
-            if (i < long_cap) long_list[1 + i] = (int)seg;
-        }
-        return;
-    }
+    const int nlist = nz[0];
     unsigned long long* s = sh[w];
-    for (int i = lane; i < n; i += 32) s[i] = data[b + i];
-    __syncwarp();
-    for (int i = lane; i < n; i += 32) {
-        unsigned long long v = s[i];
-        int r = 0;
-        for (int j = 0; j < n; ++j) r += s[j] < v;
-        data[b + r] = v;
+    for (int t = blockIdx.x * kSortWarps + w; t < nlist; t += gridDim.x * kSortWarps) {
+        const int seg = nz[2 + t];
+        const int b = ptr[seg], n = ptr[seg + 1] - b;
+        if (n <= 1) continue;
+        if (n > kPairWarpCap) {
+            if (lane == 0) {
+                const int i = atomicAdd(long_list, 1);
+                if (i < long_cap) long_list[1 + i] = seg;
+            }
+            continue;
+        }
+        for (int i = lane; i < n; i += 32) s[i] = data[b + i];
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) {
+            const unsigned long long v = s[i];
+            int r = 0;
+            for (int j = 0; j < n; ++j) r += s[j] < v;
+            data[b + r] = v;
+        }
+        __syncwarp();
     }
 }
 
@@ -634,51 +770,78 @@ __global__ void k_sort_pairs_block(const int* __restrict__ ptr, unsigned long lo
     }
 }
 
-// One CTA (8 warps) per camera-pair block. Warp w reduces pairs b+w, b+w+8,
-// ... (lane l owns elements l, l+32, l+64 of the 9x9 block); the 8 partial
-// blocks are then summed in warp order: a fixed summation order for every
-// element, so the result is bitwise repeatable.
-__global__ void __launch_bounds__(256) k_schur_blocks(int num_cams, const int* __restrict__ blk_ptr,
-                                                      const unsigned long long* __restrict__ pairs,
-                                                      const double* __restrict__ Ws,
-                                                      const double* __restrict__ Ys, double* Z, long ldz) {
-    __shared__ double part[8][81];
-    const long blk = blockIdx.x;
-    const int b = blk_ptr[blk], e = blk_ptr[blk + 1];
-    if (b == e) return;
-    const int ca = (int)(blk / num_cams), cb = (int)(blk - (long)ca * num_cams);
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r0 = lane % 9, q0 = lane / 9;
-    const int r1 = (lane + 32) % 9, q1 = (lane + 32) / 9;
-    const int r2 = (lane + 64) % 9, q2 = (lane + 64) / 9;
-    const bool has2 = lane + 64 < 81;
-    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-    for (int i = b + w; i < e; i += 8) {
-        const unsigned long long pr = __ldg(pairs + i);
-        const double* y = Ys + 27L * (int)(pr >> 32);
-        const double* x = Ws + 27L * (int)(pr & 0xffffffffu);
-        acc0 += __ldg(y + 3 * r0) * __ldg(x + 3 * q0) + __ldg(y + 3 * r0 + 1) * __ldg(x + 3 * q0 + 1) +
-                __ldg(y + 3 * r0 + 2) * __ldg(x + 3 * q0 + 2);
-        acc1 += __ldg(y + 3 * r1) * __ldg(x + 3 * q1) + __ldg(y + 3 * r1 + 1) * __ldg(x + 3 * q1 + 1) +
-                __ldg(y + 3 * r1 + 2) * __ldg(x + 3 * q1 + 2);
-        if (has2)
-            acc2 += __ldg(y + 3 * r2) * __ldg(x + 3 * q2) + __ldg(y + 3 * r2 + 1) * __ldg(x + 3 * q2 + 1) +
-                    __ldg(y + 3 * r2 + 2) * __ldg(x + 3 * q2 + 2);
-    }
-    part[w][lane] = acc0;
-    part[w][lane + 32] = acc1;
-    if (has2) part[w][lane + 64] = acc2;
-    __syncthreads();
-    if (threadIdx.x < 81) {
-        const int el = threadIdx.x, r = el % 9, q = el / 9;
-        double v = 0.0;
+// One warp per non-empty camera-pair block, persistent: warps take list
+// entries from the cursor nz[1] (the assignment of blocks to warps varies
+// from run to run; each block's arithmetic does not). A block's pairs are
+// walked in their sorted order, 8 at a time: lanes 0..26 load Y_o and W_o' as
+// two coalesced 216-byte records and element (r, q) = sum_m Y_o(r, m) W_o'(q, m)
+// takes its operands by shuffle. Lane l owns elements l, l + 32, l + 64 of the
+// 9 x 9 block (column-major: r = el % 9, q = el / 9); every element is summed
+// in pair order, so the result is bitwise repeatable.
+constexpr int kSchurWarps = 8;
+__global__ void __launch_bounds__(32 * kSchurWarps) k_schur_blocks(int num_cams, const int* __restrict__ blk_ptr,
+                                                                   int* nz,
+                                                                   const unsigned long long* __restrict__ pairs,
+                                                                   const double* __restrict__ Ws,
+                                                                   const double* __restrict__ Ys, double* Z,
+                                                                   long ldz) {
+    const int lane = threadIdx.x & 31;
+    const int nlist = *(volatile int*)nz;
+    int rr[3], qq[3];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) v += part[k][el];
-        double* z = Z + (9L * ca + r) + (9L * cb + q) * ldz;
-        if (ca == cb) {
-            if (r <= q) *z -= v;  // diagonal block holds U (scaled) already
-        } else {
-            *z = -v;
+    for (int u = 0; u < 3; ++u) {
+        const int el = min(lane + 32 * u, 80);
+        rr[u] = 3 * (el % 9);
+        qq[u] = 3 * (el / 9);
+    }
+    const bool has2 = lane + 64 < 81;
+    while (true) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(nz + 1, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= nlist) break;
+        const int blk = nz[2 + t];
+        const int b = blk_ptr[blk], e = blk_ptr[blk + 1];
+        double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+        for (int i0 = b; i0 < e; i0 += 32) {
+            const int cnt = min(32, e - i0);
+            const unsigned long long mine = lane < cnt ? __ldg(pairs + i0 + lane) : 0ull;
+            for (int j0 = 0; j0 < cnt; j0 += 8) {
+                double yv[8], wv[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const unsigned long long pr = __shfl_sync(0xffffffffu, mine, j0 + u);
+                    const bool ok = j0 + u < cnt && lane < 27;
+                    yv[u] = ok ? __ldg(Ys + 27L * (long)(pr >> 32) + lane) : 0.0;
+                    wv[u] = ok ? __ldg(Ws + 27L * (long)(pr & 0xffffffffu) + lane) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) {
+                        d0 += __shfl_sync(0xffffffffu, yv[u], rr[0] + m) * __shfl_sync(0xffffffffu, wv[u], qq[0] + m);
+                        d1 += __shfl_sync(0xffffffffu, yv[u], rr[1] + m) * __shfl_sync(0xffffffffu, wv[u], qq[1] + m);
+                        d2 += __shfl_sync(0xffffffffu, yv[u], rr[2] + m) * __shfl_sync(0xffffffffu, wv[u], qq[2] + m);
+                    }
+                    acc0 += d0;
+                    acc1 += d1;
+                    acc2 += d2;
+                }
+            }
+        }
+        const int ca = blk / num_cams, cb = blk - ca * num_cams;
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+            if (u == 2 && !has2) break;
+            const double v = u == 0 ? acc0 : (u == 1 ? acc1 : acc2);
+            const int r = rr[u] / 3, q = qq[u] / 3;
+            double* z = Z + (9L * ca + r) + (9L * cb + q) * ldz;
+            if (ca == cb) {
+                if (r <= q) *z -= v;  // the diagonal block holds U and the self terms already
+            } else {
+                *z = -v;
+            }
         }
     }
 }
@@ -689,8 +852,8 @@ void launch_schur_count(const SceneDev& s, cudaStream_t st) {
     const long nblk = (long)s.num_cams * s.num_cams;
     cudaMemsetAsync(s.blk_cnt, 0, sizeof(int) * (size_t)nblk, st);
     if (s.num_points > 0) {
-        k_pair_enum<false><<<(s.num_points + 127) / 128, 128, 0, st>>>(s.num_points, s.num_cams, s.pt_ptr,
-                                                                       s.pt_obs, s.obs_cam, s.blk_cnt, nullptr);
+        k_pair_enum<false><<<(s.num_points + 3) / 4, 128, 0, st>>>(s.num_points, s.num_cams, s.pt_ptr, s.pt_obs,
+                                                                   s.obs_cam, s.blk_cnt, nullptr);
         count_launch();
     }
     exclusive_scan(s.blk_cnt, s.blk_ptr, (int)nblk, s.scan_tmp, st);
@@ -700,8 +863,18 @@ void prepare_assembly_kernels() {
     static std::atomic<unsigned long long> attr{0};
     once_per_device(attr, [] {
         return cudaFuncSetAttribute(k_sort_pairs_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(kPairBlockCap * sizeof(unsigned long long))) == cudaSuccess;
+                                    (int)(kPairBlockCap * sizeof(unsigned long long))) == cudaSuccess &&
+               cudaFuncSetAttribute(k_camera_obs_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kObsTileSmem) == cudaSuccess &&
+               cudaFuncSetAttribute(k_camera_obs_tiles, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared) == cudaSuccess;
     });
+}
+
+// ints of the non-empty block list for a scene with npairs pairs
+size_t schur_list_ints(int num_cams, long npairs) {
+    const long upper = (long)num_cams * (num_cams + 1) / 2;
+    return (size_t)std::min(upper, npairs) + 2;
 }
 
 void launch_schur(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
@@ -709,18 +882,20 @@ void launch_schur(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
     if (nblk == 0) return;
     cudaMemcpyAsync(s.blk_cnt, s.blk_ptr, sizeof(int) * (size_t)nblk, cudaMemcpyDeviceToDevice, st);
     if (s.num_points > 0) {
-        k_pair_enum<true><<<(s.num_points + 127) / 128, 128, 0, st>>>(s.num_points, s.num_cams, s.pt_ptr,
-                                                                      s.pt_obs, s.obs_cam, s.blk_cnt, s.pairs);
+        k_pair_enum<true><<<(s.num_points + 3) / 4, 128, 0, st>>>(s.num_points, s.num_cams, s.pt_ptr, s.pt_obs,
+                                                                  s.obs_cam, s.blk_cnt, s.pairs);
         count_launch();
     }
     cudaMemsetAsync(s.long_list, 0, sizeof(int), st);
-    k_sort_pairs_warp<<<(unsigned)((nblk + 3) / 4), 128, 0, st>>>(nblk, s.blk_ptr, s.pairs, s.long_list,
-                                                                  s.long_cap);
+    cudaMemsetAsync(s.nz_list, 0, 2 * sizeof(int), st);
+    k_list_blocks<<<(unsigned)((nblk + 255) / 256), 256, 0, st>>>(nblk, s.blk_ptr, s.nz_list);
+    k_sort_pairs_warp<<<148 * 8, 32 * kSortWarps, 0, st>>>(s.nz_list, s.blk_ptr, s.pairs, s.long_list, s.long_cap);
     prepare_assembly_kernels();
     k_sort_pairs_block<<<148, 1024, kPairBlockCap * sizeof(unsigned long long), st>>>(
         s.blk_ptr, s.pairs, s.long_list, s.long_cap, s.err);
-    k_schur_blocks<<<(unsigned)nblk, 256, 0, st>>>(s.num_cams, s.blk_ptr, s.pairs, s.Ws, s.Ys, Z, ldz);
-    count_launch(3);
+    k_schur_blocks<<<148 * 8, 32 * kSchurWarps, 0, st>>>(s.num_cams, s.blk_ptr, s.nz_list, s.pairs, s.Ws, s.Ys, Z,
+                                                          ldz);
+    count_launch(4);
 }
 
 // Copy the strict upper triangle onto the lower one (32x32 tiles via smem).

@@ -93,15 +93,21 @@ struct SceneDev {
     double* iVs;          // 6*num_points upper triangle of the inverse of the scaled point block
     double* Ws;           // 27*num_obs scaled W_o = (J_c^T J_p)/(s s), 9x3 row-major
     double* Ys;           // 27*num_obs Y_o = W_o * iV_p, 9x3 row-major
+    double* cam_part;     // 45 * camera_tile_slots(): per-tile partial sums of the camera blocks
     int* blk_cnt;         // num_cams^2: pair counts, then scatter cursors, per camera-pair block
     int* blk_ptr;         // num_cams^2 + 1: pair list offsets per block
     unsigned long long* pairs;  // (o << 32 | o') per block, sorted inside a block
     int* long_list;       // [count, ids...] of blocks with more than 1024 pairs
     int long_cap;         // capacity of long_list ids
+    int* nz_list;         // [count, cursor, ids...] of the non-empty camera-pair blocks
     int* err;             // device error bits
 };
 
 void launch_validate_obs(const SceneDev& s, cudaStream_t st);
+// Camera observations are processed in tiles of 256; slots = C + num_obs/256 + 1.
+size_t camera_tile_slots(int num_cams, int num_obs);
+// ints of the non-empty camera-pair block list for npairs pairs
+size_t schur_list_ints(int num_cams, long npairs);
 void launch_build_index(SceneDev& s, cudaStream_t st);
 // U blocks (scaled) written to the diagonal blocks of Z (ldz), column norms.
 void launch_camera_blocks(const SceneDev& s, double* Z, int ldz, cudaStream_t st);

@@ -69,6 +69,10 @@ __device__ void sym3_pinv(const double in[6], double out[3][3]) {
             out[i][j] = v[i][0] * v[j][0] * iw[0] + v[i][1] * v[j][1] * iw[1] + v[i][2] * v[j][2] * iw[2];
 }
 
+// Four threads per point: thread q of the quad sums observations b + q,
+// b + q + 4, ... of the point into its S; the quad then adds its four partial
+// S in a fixed butterfly order (bitwise repeatable) and thread 0 finishes.
+constexpr int kPointLanes = 4;
 __global__ void __launch_bounds__(128) k_point_cov(int num_points, int3 fix, int has_fix,
                                                    const double* __restrict__ J,
                                                    const int* __restrict__ pt_ptr,
@@ -77,24 +81,26 @@ __global__ void __launch_bounds__(128) k_point_cov(int num_points, int3 fix, int
                                                    const double* __restrict__ Vraw,
                                                    const double* __restrict__ sig,
                                                    double* __restrict__ pt_unc) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= num_points) return;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = gt / kPointLanes, q = gt % kPointLanes;
+    const unsigned quad = 0xfu << (threadIdx.x & 28);
+    if (p >= num_points) return;  // whole quads leave together
     if (has_fix && (p == fix.x || p == fix.y || p == fix.z)) return;  // fixed points are skipped
     double* out = pt_unc + 6L * p;
-    int b = pt_ptr[p], e = pt_ptr[p + 1];
+    const int b = pt_ptr[p], e = pt_ptr[p + 1];
     if (b == e) {  // pinv of an empty A: zero covariance
-        out[0] = out[1] = out[2] = out[3] = out[4] = out[5] = 0.0;
+        if (q == 0) out[0] = out[1] = out[2] = out[3] = out[4] = out[5] = 0.0;
         return;
     }
     double S[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    for (int i = b; i < e; ++i) {
+    for (int i = b + q; i < e; i += kPointLanes) {
         int o = pt_obs[i];
         const double* r = J + 24L * o;
-        const double2* q = reinterpret_cast<const double2*>(r);
+        const double2* qv = reinterpret_cast<const double2*>(r);
         double v[24];
 #pragma unroll
         for (int k = 0; k < 12; ++k) {
-            double2 x = __ldg(q + k);
+            double2 x = __ldg(qv + k);
             v[2 * k] = x.x;
             v[2 * k + 1] = x.y;
         }
@@ -124,6 +130,14 @@ __global__ void __launch_bounds__(128) k_point_cov(int num_points, int3 fix, int
             }
         }
     }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            S[a][c] += __shfl_xor_sync(quad, S[a][c], 1);
+            S[a][c] += __shfl_xor_sync(quad, S[a][c], 2);
+        }
+    if (q != 0) return;
     double Dp[3][3];
     sym3_pinv(Vraw + 6L * p, Dp);
     // Sigma_pt = D^+ + D^+ S D^+
@@ -149,7 +163,8 @@ __global__ void __launch_bounds__(128) k_point_cov(int num_points, int3 fix, int
 void launch_point_cov(const SceneDev& s, const double* sig, double* pt_unc, cudaStream_t st) {
     if (s.num_points == 0) return;
     int3 fix = make_int3(s.fix[0], s.fix[1], s.fix[2]);
-    k_point_cov<<<(s.num_points + 127) / 128, 128, 0, st>>>(s.num_points, fix, s.has_fix, s.J,
+    const long threads = (long)s.num_points * kPointLanes;
+    k_point_cov<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(s.num_points, fix, s.has_fix, s.J,
                                                             s.pt_ptr, s.pt_obs, s.obs_cam, s.Vraw,
                                                             sig, pt_unc);
     count_launch();
