@@ -21,8 +21,9 @@
 //
 // Kernel layout: 128 threads. Warp 0 lane 0 issues the TMA loads of the S
 // slices of both operands per 64-byte K block (3-stage mbarrier pipeline);
-// warp 1 lane 0 issues the tcgen05.mma (M = 128, N = 128, K = 32 bytes) and
-// commits each stage back to the producer; all four warps then read the
+// warp 1 lane 0 issues the tcgen05.mma (M = 128, N = up to 256, K = 32 bytes:
+// one A slice against several adjacent B slices) and commits each stage back
+// to the producer; all four warps then read the
 // accumulators with tcgen05.ld and write FP64. Every mbarrier wait has an
 // iteration limit after which the kernel records ERRBIT_TIMEOUT and unwinds
 // (TMEM is always freed).
@@ -121,6 +122,7 @@ struct Shape {
     static constexpr int B_BOX = NT * BKB;                 // bytes of one B slice box
     static constexpr int STAGE = S * (A_BOX + B_BOX);
     static constexpr int LEVELS = S;                       // L = 2 .. S+1
+    static constexpr int GROUP = 256 / NT;                 // B slices per MMA (N <= 256)
     static constexpr int TMEM_COLS = LEVELS * NT <= 256 ? (LEVELS * NT <= 128 ? 128 : 256) : 512;
     static constexpr int SMEM = STAGES * STAGE + 1024 /*align*/ + 256 /*barriers*/;
     static_assert(LEVELS * NT <= 512, "TMEM holds at most 512 accumulator columns");
@@ -266,10 +268,6 @@ __global__ void __launch_bounds__(THREADS, 1)
     } else if (warp == 1) {
       if (lane == 0) {
         // MMA issuer
-        const uint32_t idesc = idesc_i8(NT);
-        bool started[S];
-#pragma unroll
-        for (int l = 0; l < S; ++l) started[l] = false;
         for (int kt = 0; kt < KT; ++kt) {
             const int s = kt % STAGES;
             if (!mbar_wait(full + s, (unsigned)(kt / STAGES) & 1u)) {
@@ -280,17 +278,21 @@ __global__ void __launch_bounds__(THREADS, 1)
             const uint8_t* st = base + s * Sh::STAGE;
 #pragma unroll
             for (int kk = 0; kk < BKB / 32; ++kk) {
+                // A slice sa meets B slices 1 .. S+1-sa, whose levels sa-1 .. S-1 are adjacent
+                // accumulators: consecutive B boxes form one taller operand, so one MMA of
+                // N = g * NT (<= 256) covers g of them and A is read once per group.
 #pragma unroll
-                for (int sa = 1; sa <= S; ++sa)
+                for (int sa = 1; sa <= S; ++sa) {
+                    const uint64_t a = desc_sw64(st + (sa - 1) * Sh::A_BOX + kk * 32);
 #pragma unroll
-                    for (int sb = 1; sb <= S; ++sb) {
-                        if (sa + sb > S + 1) continue;
-                        const int l = sa + sb - 2;
-                        const uint64_t a = desc_sw64(st + (sa - 1) * Sh::A_BOX + kk * 32);
-                        const uint64_t b = desc_sw64(st + S * Sh::A_BOX + (sb - 1) * Sh::B_BOX + kk * 32);
-                        mma_i8(tmem + (uint32_t)(l * NT), a, b, idesc, started[l]);
-                        started[l] = true;
+                    for (int sb0 = 1; sb0 <= S + 1 - sa; sb0 += Sh::GROUP) {
+                        const int g = (S + 1 - sa - sb0 + 1) < Sh::GROUP ? (S + 1 - sa - sb0 + 1) : Sh::GROUP;
+                        const int l = sa + sb0 - 2;
+                        const uint64_t b = desc_sw64(st + S * Sh::A_BOX + (sb0 - 1) * Sh::B_BOX + kk * 32);
+                        // the first A slice of the first K step opens every level
+                        mma_i8(tmem + (uint32_t)(l * NT), a, b, idesc_i8(g * NT), kt > 0 || kk > 0 || sa > 1);
                     }
+                }
             }
             mma_commit(empty + s);  // stage free once these MMAs completed
         }
