@@ -81,6 +81,7 @@ struct Buffers {
     double *cam_out, *pt_out;
     SceneDev s;
     double *Z, *iZ, *add, *tmp, *e, *gjws, *sig;
+    int* dag_state;  // counters of the tile-task inverse
     unsigned long long* amax;
     TeState* te;
     PinvBuffers pb;  // UNC_SVD_SCHUR only
@@ -125,6 +126,7 @@ size_t carve(char* base, const Plan& pl, bool host_io, long long nnz, int nrows,
     b.tmp = c.take<double>(nn);
     b.e = c.take<double>(pl.N);
     b.gjws = c.take<double>(chol_small_doubles(pl.N));
+    b.dag_state = c.take<int>(spd_task_state_ints(pl.N));
     b.sig = c.take<double>((size_t)pl.C * 81);
     if (pl.svd_schur) {
         const size_t used = (c.off + 255) & ~size_t(255);
@@ -413,10 +415,19 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     // The stop rule runs on the device (k_te_decide): all 19 iterations are
     // launched and, once the rule fires, the remaining kernels return at once;
     // k = lambda^i / factorial(i-1) is evaluated here (32-bit factorial wrap).
+    // moderate sizes: the tile-task inverse (one persistent kernel); larger: the recursive form
+    const bool tasks = spd_tasks_apply(N);
+    if (tasks)
+        if (int r = spd_tasks_prepare(N)) return fail(r, "tile-task inverse: cannot upload the task list");
     auto inverse_stage = [&]() -> int {
         launch_shift_equilibrate(b.Z, N, ld, lambda, b.e, s.err, sm);
-        chol_inverse(b.Z, N, ld, b.iZ, b.add, b.tmp, b.gjws, s.err, sm);
-        launch_unequilibrate(b.Z, N, ld, b.e, b.iZ, sm);  // X in Z, iZ = X
+        if (tasks) {
+            if (int r = chol_inverse_tasks(b.Z, N, ld, b.iZ, b.add, b.dag_state, s.err, sm)) return r;
+            launch_unequilibrate_from(b.add, b.Z, N, ld, b.e, b.iZ, sm);  // X in Z, iZ = X
+        } else {
+            chol_inverse(b.Z, N, ld, b.iZ, b.add, b.tmp, b.gjws, s.err, sm);
+            launch_unequilibrate(b.Z, N, ld, b.e, b.iZ, sm);  // X in Z, iZ = X
+        }
         return UNC_OK;
     };
     auto taylor_stage = [&]() -> int {
@@ -503,7 +514,8 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         return fail(UNC_ERR_LAYOUT, "Jacobian rows are not in the 2 x (9 camera + 3 point) observation layout");
     if (err & (ERRBIT_SINGULAR | ERRBIT_NONFINITE))
         return fail(UNC_ERR_SINGULAR, "non-positive pivot or non-finite value while inverting Z + lambda*I");
-    if (err & ERRBIT_TIMEOUT) return fail(UNC_ERR_CUDA, "tensor-core pipeline wait timed out");
+    if (err & ERRBIT_TIMEOUT)
+        return fail(UNC_ERR_CUDA, "a bounded device wait ran out (tensor-core pipeline or tile-task inverse)");
     if (te.bad) return fail(UNC_ERR_SINGULAR, "non-finite Taylor-series power");
     return UNC_OK;
 }
@@ -850,23 +862,35 @@ int unc_dense_inverse_device(double* d_A, int n, int lda, void* stream) {
     if (!d_A || n <= 0 || lda < n || (lda & 1)) return fail(UNC_ERR_INVALID_ARG, "bad matrix arguments");
     cudaStream_t sm = (cudaStream_t)stream;
     const size_t mat = (size_t)lda * n;
-    const size_t wsd = 3 * mat + chol_small_doubles(n) + (size_t)n + 64;
+    // n <= 3584: the tile-task inverse (one persistent kernel), else the recursive form
+    const bool tasks = spd_tasks_apply(n);
+    if (tasks)
+        if (int r = spd_tasks_prepare(n)) return fail(r, "tile-task inverse: cannot upload the task list");
+    const size_t small_d = std::max(chol_small_doubles(n), (spd_task_state_ints(n) + 1) / 2);
+    const size_t wsd = 3 * mat + small_d + (size_t)n + 64;
     double* ws = nullptr;
     CK(cudaMalloc(&ws, wsd * sizeof(double) + 256));
     double *T = ws, *W = ws + mat, *Tt = ws + 2 * mat, *small = ws + 3 * mat;
-    double* e = small + chol_small_doubles(n);
+    double* e = small + small_d;
     int* err = reinterpret_cast<int*>(ws + wsd);
     int h_err = 0;
     cudaError_t ce = cudaMemsetAsync(ws, 0, wsd * sizeof(double) + 256, sm);
     if (ce == cudaSuccess) {
         launch_shift_equilibrate(d_A, n, lda, 0.0, e, err, sm);
-        chol_inverse(d_A, n, lda, T, W, Tt, small, err, sm);
-        launch_unequilibrate(d_A, n, lda, e, nullptr, sm);
-        ce = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, sm);
+        if (tasks) {
+            if (chol_inverse_tasks(d_A, n, lda, T, W, reinterpret_cast<int*>(small), err, sm) != UNC_OK)
+                ce = cudaErrorUnknown;
+            launch_unequilibrate_from(W, d_A, n, lda, e, nullptr, sm);
+        } else {
+            chol_inverse(d_A, n, lda, T, W, Tt, small, err, sm);
+            launch_unequilibrate(d_A, n, lda, e, nullptr, sm);
+        }
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, sm);
     }
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(sm);
     cudaFree(ws);
     if (ce != cudaSuccess) return fail(UNC_ERR_CUDA, cudaGetErrorString(ce));
+    if (h_err & ERRBIT_TIMEOUT) return fail(UNC_ERR_CUDA, "a bounded device wait of the tile-task inverse ran out");
     if (h_err & (ERRBIT_SINGULAR | ERRBIT_NONFINITE)) return fail(UNC_ERR_SINGULAR, "matrix is not positive definite");
     return UNC_OK;
 }

@@ -1,0 +1,341 @@
+// dag.cu - SPD inverse A^{-1} = L^{-T} L^{-1} as a graph of 64 x 64 tile tasks
+// run by one persistent kernel (sm_100a), for the moderate sizes where the
+// recursive form (dense.cu) is bound by its ~200 dependent launches.
+//
+// Tiles (i, j), j <= i, of the lower triangle; nt = ceil(n / 64). Tasks:
+//   POTRF(k)      T(k,k) = chol(A(k,k))^{-1}                  (the 64 x 64 leaf)
+//   TRSM(i,k)     L(i,k) = A(i,k) T(k,k)^T                    (in place in A)
+//   UPDATE(i,j,k) A(i,j) -= L(i,k) L(j,k)^T                   (k < j <= i)
+//   TACC(i,j,m)   W(i,j) += L(i,m) T(m,j)                     (j <= m < i, in the T(i,j) slot)
+//   TFIN(i,j)     T(i,j) = -T(i,i) W(i,j)                     (block forward substitution)
+//   PACC(i,j,k)   O(i,j) += T(k,i)^T T(k,j)                   (k >= i >= j; the last term also
+//                                                             writes the transposed tile)
+// The host lists the tasks in a topological order that puts the next
+// diagonal factorisation right after the update it waits for (look-ahead).
+// CTAs claim tasks from a global cursor in list order, wait (thread 0, with an
+// iteration limit) on per-tile counters, run the task with all 512 threads
+// and publish its counter. Every dependency of a claimed task was claimed
+// earlier by a running CTA that waits only on still earlier tasks, so the
+// schedule completes with any number of resident CTAs; updates of one tile
+// are applied in a fixed order, so the result is bitwise repeatable. Tile data
+// written by other CTAs is read through L2 only (ld.global.cg).
+//
+// Counters (ints, zeroed before the launch): cursor, abort flag, then per
+// lower tile: ver (updates applied to A), lrdy (L final / T(k,k) ready),
+// tacc (W accumulations), trdy (T final), pacc (O accumulations).
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "chol_leaf.cuh"
+#include "internal.h"
+
+namespace unc {
+namespace {
+
+constexpr int TB = NB;                   // tile size (the leaf size)
+constexpr int DAG_THREADS = LEAF_THREADS;
+constexpr int TLD = TB + 4;              // shared tile stride: fragment reads conflict-free in both orientations
+constexpr size_t TILE_SMEM = sizeof(double) * 2 * TB * TLD;
+constexpr size_t DAG_SMEM = TILE_SMEM > LEAF_SMEM ? TILE_SMEM : LEAF_SMEM;
+constexpr long kDagSpin = 1L << 22;      // polls of one dependency before the kernel gives up
+constexpr int kMaxTilesN = 56;           // tasks are used up to n = 56 * 64
+
+enum : int { K_POTRF = 0, K_TRSM = 1, K_UPDATE = 2, K_TACC = 3, K_TFIN = 4, K_PACC = 5 };
+
+__device__ __forceinline__ int tri(int i, int j) { return i * (i + 1) / 2 + j; }
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// thread 0 only: wait until *flag >= v (or the abort flag is raised / the limit runs out)
+__device__ bool wait_ge(const int* flag, int v, const int* abort) {
+    for (long it = 0; it < kDagSpin; ++it) {
+        if (ld_acquire(flag) >= v) return true;
+        if (ld_acquire(abort)) return false;
+        __nanosleep(32);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// Tile X (column-major, leading dimension ld; rows < vr and columns < vc
+// valid, the rest read as zero) into shared memory as sm[c * TLD + r].
+__device__ __forceinline__ void load_tile(double* sm, const double* X, long ld, int vr, int vc, int tid) {
+#pragma unroll
+    for (int u = 0; u < TB * TB / 2 / DAG_THREADS; ++u) {
+        const int q = tid + u * DAG_THREADS;
+        const int c = q >> 5, r2 = (q & 31) * 2;
+        double2 v = make_double2(0.0, 0.0);
+        if (c < vc && r2 < vr) v = __ldcg(reinterpret_cast<const double2*>(X + r2 + (long)c * ld));
+        if (r2 + 1 >= vr) v.y = 0.0;
+        *reinterpret_cast<double2*>(sm + c * TLD + r2) = v;
+    }
+}
+
+// acc += op(A) op(B) over k in [kb, ke) (multiples of 4) for this warp's 16 x 16
+// block (rows wm.., columns wn..). op(A)(m, k) = kTA ? A(k, m) : A(m, k),
+// op(B)(k, n) = kTB ? B(n, k) : B(k, n), tiles as left by load_tile.
+template <bool kTA, bool kTB>
+__device__ __forceinline__ void tile_mma(const double* As, const double* Bs, int wm, int wn, int g, int t, int kb,
+                                         int ke, double (&acc)[2][2][2]) {
+    for (int kk = kb; kk < ke; kk += 4) {
+        double a[2], b[2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int m = wm + 8 * i + g, k = kk + t;
+            a[i] = kTA ? As[m * TLD + k] : As[k * TLD + m];
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int n = wn + 8 * j + g, k = kk + t;
+            b[j] = kTB ? Bs[k * TLD + n] : Bs[n * TLD + k];
+        }
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+}
+
+// X(r, c) = alpha acc + (accumulate ? X(r, c) : 0) for r < vr, c < vc; with
+// Xm, also Xm(c, r) = the same value (the transposed tile).
+__device__ __forceinline__ void store_tile(double* X, long ld, int vr, int vc, const double (&acc)[2][2][2],
+                                           double alpha, bool accumulate, double* Xm, int wm, int wn, int g,
+                                           int t) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = wm + 8 * i + g, c = wn + 8 * j + 2 * t + h;
+                if (r < vr && c < vc) {
+                    double v = alpha * acc[i][j][h];
+                    if (accumulate) v += __ldcg(X + r + (long)c * ld);
+                    X[r + (long)c * ld] = v;
+                    if (Xm) Xm[c + (long)r * ld] = v;
+                }
+            }
+}
+
+__global__ void __launch_bounds__(DAG_THREADS, 1)
+    k_spd_inverse_tasks(double* A, double* T, double* O, int n, long ld, const int4* __restrict__ tasks, int ntasks,
+                        int* state, int ntri, int* err) {
+    extern __shared__ __align__(16) double sm[];
+    __shared__ int s_task, s_ok;
+    int* const cursor = state;
+    int* const abort = state + 1;
+    int* const ver = state + 4;
+    int* const lrdy = ver + ntri;
+    int* const tacc = lrdy + ntri;
+    int* const trdy = tacc + ntri;
+    int* const pacc = trdy + ntri;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int wm = (warp & 3) * 16, wn = (warp >> 2) * 16;
+    double* As = sm;
+    double* Bs = sm + TB * TLD;
+    auto ext = [n](int b) { return min(TB, n - TB * b); };
+    auto tile = [ld](double* M, int i, int j) { return M + (long)TB * i + (long)TB * j * ld; };
+    while (true) {
+        if (tid == 0) s_task = atomicAdd(cursor, 1);
+        __syncthreads();
+        const int task = s_task;
+        if (task >= ntasks) break;
+        const int4 tk = tasks[task];
+        const int type = tk.x, i = tk.y, j = tk.z, k = tk.w;
+        if (tid == 0) {
+            bool ok = true;
+            switch (type) {
+                case K_POTRF: ok = wait_ge(ver + tri(k, k), k, abort); break;
+                case K_TRSM: ok = wait_ge(ver + tri(i, k), k, abort) && wait_ge(lrdy + tri(k, k), 1, abort); break;
+                case K_UPDATE:
+                    ok = wait_ge(ver + tri(i, j), k, abort) && wait_ge(lrdy + tri(i, k), 1, abort) &&
+                         wait_ge(lrdy + tri(j, k), 1, abort);
+                    break;
+                case K_TACC:
+                    ok = wait_ge(tacc + tri(i, j), k - j, abort) && wait_ge(lrdy + tri(i, k), 1, abort) &&
+                         wait_ge(trdy + tri(k, j), 1, abort);
+                    break;
+                case K_TFIN: ok = wait_ge(tacc + tri(i, j), i - j, abort) && wait_ge(trdy + tri(i, i), 1, abort); break;
+                default:  // K_PACC
+                    ok = wait_ge(pacc + tri(i, j), k - i, abort) && wait_ge(trdy + tri(k, i), 1, abort) &&
+                         wait_ge(trdy + tri(k, j), 1, abort);
+                    break;
+            }
+            if (!ok) {
+                atomicOr(err, ERRBIT_TIMEOUT);
+                atomicExch(abort, 1);
+            }
+            s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) break;
+        if (type == K_POTRF) {
+            chol_leaf_tile(A, ld, TB * k, ext(k), T, ld, err, sm);
+        } else {
+            double acc[2][2][2] = {};
+            switch (type) {
+                case K_TRSM:  // L(i,k) = A(i,k) T(k,k)^T; T(k,k) lower: terms k' <= n only
+                    load_tile(As, tile(A, i, k), ld, ext(i), ext(k), tid);
+                    load_tile(Bs, tile(T, k, k), ld, ext(k), ext(k), tid);
+                    __syncthreads();
+                    tile_mma<false, true>(As, Bs, wm, wn, g, t4, 0, wn + 16, acc);
+                    __syncthreads();
+                    store_tile(tile(A, i, k), ld, ext(i), ext(k), acc, 1.0, false, nullptr, wm, wn, g, t4);
+                    break;
+                case K_UPDATE:  // A(i,j) -= L(i,k) L(j,k)^T
+                    load_tile(As, tile(A, i, k), ld, ext(i), ext(k), tid);
+                    load_tile(Bs, tile(A, j, k), ld, ext(j), ext(k), tid);
+                    __syncthreads();
+                    tile_mma<false, true>(As, Bs, wm, wn, g, t4, 0, TB, acc);
+                    store_tile(tile(A, i, j), ld, ext(i), ext(j), acc, -1.0, true, nullptr, wm, wn, g, t4);
+                    break;
+                case K_TACC:  // W(i,j) += L(i,k) T(k,j); T(j,j) lower: terms k' >= n only
+                    load_tile(As, tile(A, i, k), ld, ext(i), ext(k), tid);
+                    load_tile(Bs, tile(T, k, j), ld, ext(k), ext(j), tid);
+                    __syncthreads();
+                    tile_mma<false, false>(As, Bs, wm, wn, g, t4, k == j ? wn : 0, TB, acc);
+                    store_tile(tile(T, i, j), ld, ext(i), ext(j), acc, 1.0, k > j, nullptr, wm, wn, g, t4);
+                    break;
+                case K_TFIN:  // T(i,j) = -T(i,i) W(i,j); T(i,i) lower: terms k' <= m only
+                    load_tile(As, tile(T, i, i), ld, ext(i), ext(i), tid);
+                    load_tile(Bs, tile(T, i, j), ld, ext(i), ext(j), tid);
+                    __syncthreads();
+                    tile_mma<false, false>(As, Bs, wm, wn, g, t4, 0, wm + 16, acc);
+                    __syncthreads();
+                    store_tile(tile(T, i, j), ld, ext(i), ext(j), acc, -1.0, false, nullptr, wm, wn, g, t4);
+                    break;
+                default: {  // K_PACC: O(i,j) += T(k,i)^T T(k,j); diagonal T tiles lower
+                    load_tile(As, tile(T, k, i), ld, ext(k), ext(i), tid);
+                    load_tile(Bs, tile(T, k, j), ld, ext(k), ext(j), tid);
+                    __syncthreads();
+                    int kb = 0;
+                    if (k == i) kb = wm;
+                    if (k == j) kb = max(kb, wn);
+                    tile_mma<true, false>(As, Bs, wm, wn, g, t4, kb, TB, acc);
+                    const bool last = k == (n + TB - 1) / TB - 1;
+                    store_tile(tile(O, i, j), ld, ext(i), ext(j), acc, 1.0, k > i,
+                               (last && i > j) ? tile(O, j, i) : nullptr, wm, wn, g, t4);
+                    break;
+                }
+            }
+        }
+        __threadfence();  // this thread's tile writes, before the counter is published
+        __syncthreads();
+        if (tid == 0) {
+            switch (type) {
+                case K_POTRF:
+                    atomicExch(lrdy + tri(k, k), 1);
+                    atomicExch(trdy + tri(k, k), 1);
+                    break;
+                case K_TRSM: atomicExch(lrdy + tri(i, k), 1); break;
+                case K_UPDATE: atomicAdd(ver + tri(i, j), 1); break;
+                case K_TACC: atomicAdd(tacc + tri(i, j), 1); break;
+                case K_TFIN: atomicExch(trdy + tri(i, j), 1); break;
+                default: atomicAdd(pacc + tri(i, j), 1); break;
+            }
+        }
+    }
+}
+
+// The task list of nt x nt tiles in the order described above.
+std::vector<int4> build_tasks(int nt) {
+    std::vector<int4> v;
+    auto add = [&v](int ty, int i, int j, int k) { v.push_back(make_int4(ty, i, j, k)); };
+    add(K_POTRF, 0, 0, 0);
+    for (int i = 1; i < nt; ++i) add(K_TRSM, i, 0, 0);
+    for (int s = 0; s < nt; ++s) {
+        if (s + 1 < nt) {
+            add(K_UPDATE, s + 1, s + 1, s);
+            add(K_POTRF, s + 1, s + 1, s + 1);
+            for (int i = s + 2; i < nt; ++i) {
+                add(K_UPDATE, i, s + 1, s);
+                add(K_TRSM, i, s + 1, s + 1);
+            }
+            for (int j = s + 2; j < nt; ++j)
+                for (int i = j; i < nt; ++i) add(K_UPDATE, i, j, s);
+        }
+        if (s >= 1)
+            for (int r = s; r < nt; ++r)
+                for (int c = 0; c < s; ++c) add(K_TACC, r, c, s - 1);
+        for (int c = 0; c < s; ++c) add(K_TFIN, s, c, 0);
+        for (int r = 0; r <= s; ++r)
+            for (int c = 0; c <= r; ++c) add(K_PACC, r, c, s);
+    }
+    return v;
+}
+
+struct TaskLists {
+    std::mutex mu;
+    std::map<std::pair<int, int>, std::pair<int4*, int>> lists;  // (device, nt) -> device copy
+};
+TaskLists& task_lists() {
+    static TaskLists* t = new TaskLists;  // lives until exit, like the device buffers it holds
+    return *t;
+}
+
+}  // namespace
+
+bool spd_tasks_apply(int n) { return n > 0 && (n + TB - 1) / TB <= kMaxTilesN; }
+
+size_t spd_task_state_ints(int n) {
+    const size_t nt = (size_t)(n + TB - 1) / TB;
+    return 4 + 5 * nt * (nt + 1) / 2;
+}
+
+int spd_tasks_prepare(int n) {
+    if (!spd_tasks_apply(n)) return UNC_ERR_INVALID_ARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return UNC_ERR_CUDA;
+    const int nt = (n + TB - 1) / TB;
+    TaskLists& tl = task_lists();
+    std::lock_guard<std::mutex> lock(tl.mu);
+    if (tl.lists.count({dev, nt})) return UNC_OK;
+    const std::vector<int4> h = build_tasks(nt);
+    int4* d = nullptr;
+    if (cudaMalloc(&d, sizeof(int4) * h.size()) != cudaSuccess) return UNC_ERR_OUT_OF_MEMORY;
+    if (cudaMemcpy(d, h.data(), sizeof(int4) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(d);
+        return UNC_ERR_CUDA;
+    }
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
+        return cudaFuncSetAttribute(k_spd_inverse_tasks, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)DAG_SMEM) == cudaSuccess;
+    });
+    tl.lists[{dev, nt}] = {d, (int)h.size()};
+    return UNC_OK;
+}
+
+int chol_inverse_tasks(double* A, int n, int lda, double* T, double* O, int* state, int* err, cudaStream_t st) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return UNC_ERR_CUDA;
+    const int nt = (n + TB - 1) / TB;
+    std::pair<int4*, int> list{nullptr, 0};
+    {
+        TaskLists& tl = task_lists();
+        std::lock_guard<std::mutex> lock(tl.mu);
+        auto it = tl.lists.find({dev, nt});
+        if (it == tl.lists.end()) return UNC_ERR_INVALID_ARG;  // spd_tasks_prepare first (outside any capture)
+        list = it->second;
+    }
+    const int ntri = nt * (nt + 1) / 2;
+    if (cudaMemsetAsync(state, 0, sizeof(int) * spd_task_state_ints(n), st) != cudaSuccess) return UNC_ERR_CUDA;
+    const int grid = std::min(148, list.second);
+    k_spd_inverse_tasks<<<grid, DAG_THREADS, DAG_SMEM, st>>>(A, T, O, n, lda, list.first, list.second, state, ntri,
+                                                             err);
+    count_launch();
+    return UNC_OK;
+}
+
+}  // namespace unc

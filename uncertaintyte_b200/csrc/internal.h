@@ -176,6 +176,20 @@ void launch_shift_equilibrate(double* A, int n, int lda, double lambda, double* 
                               cudaStream_t st);
 // X <- E X E (undo equilibration), also copies into Y if Y != nullptr.
 void launch_unequilibrate(double* X, int n, int lda, const double* e, double* Y, cudaStream_t st);
+// X = diag(e) S diag(e) from a separate source S, Y (optional) = X.
+void launch_unequilibrate_from(const double* S, double* X, int n, int lda, const double* e, double* Y,
+                               cudaStream_t st);
+
+// ---------------- dag.cu ----------------
+// SPD inverse as 64 x 64 tile tasks in one persistent kernel, for n <= 3584:
+// A (lower triangle) is overwritten by L, T receives L^{-1} (lower tiles) and
+// O = A^{-1} (both triangles). state: spd_task_state_ints(n) ints.
+// spd_tasks_prepare uploads the task list of this size once per device (call it
+// outside stream capture).
+bool spd_tasks_apply(int n);
+size_t spd_task_state_ints(int n);
+int spd_tasks_prepare(int n);
+int chol_inverse_tasks(double* A, int n, int lda, double* T, double* O, int* state, int* err, cudaStream_t st);
 // Y <- Y + k*X  (N x N, column-major)
 void launch_axpy(double* Y, const double* X, double k, int n, int ld, cudaStream_t st);
 
