@@ -70,8 +70,10 @@ __device__ __forceinline__ void pair_t(double* Ts, int b0, int e) {
 // The factorisation as a device function of one 512-thread CTA (lsm: LEAF_SMEM
 // bytes). A is read through L2 only (ld.global.cg), so that a persistent caller
 // never sees a stale L1 line of a tile another CTA rewrote.
+// U (optional, shared memory, U[j * uld + i]) is added to the lower triangle of
+// the block as it is loaded (a last trailing update applied by the caller).
 __device__ __forceinline__ void chol_leaf_tile(const double* A, long lda, int k0, int kb, double* T, long ldt,
-                                               int* err, double* lsm) {
+                                               int* err, double* lsm, const double* U = nullptr, int uld = 0) {
     double* S = lsm;
     double* Ts = lsm + NB * LEAF_LD;
     double* rinv = Ts + NB * LEAF_LD;
@@ -83,8 +85,9 @@ __device__ __forceinline__ void chol_leaf_tile(const double* A, long lda, int k0
 #pragma unroll
         for (int u = 0; u < kPer; ++u) {
             const int j = (tid >> 6) + u * (LEAF_THREADS / NB);
-            v[u] = (i < kb && j < kb) ? (j <= i ? __ldcg(A + (k0 + i) + (long)(k0 + j) * lda) : 0.0)
-                                 : (i == j ? 1.0 : 0.0);
+            v[u] = (i < kb && j < kb)
+                       ? (j <= i ? __ldcg(A + (k0 + i) + (long)(k0 + j) * lda) + (U ? U[j * uld + i] : 0.0) : 0.0)
+                       : (i == j ? 1.0 : 0.0);
         }
 #pragma unroll
         for (int u = 0; u < kPer; ++u) {

@@ -10,8 +10,11 @@
 //   TFIN(i,j)     T(i,j) = -T(i,i) W(i,j)                     (block forward substitution)
 //   PACC(i,j,k)   O(i,j) += T(k,i)^T T(k,j)                   (k >= i >= j; the last term also
 //                                                             writes the transposed tile)
-// The host lists the tasks in a topological order that puts the next
-// diagonal factorisation right after the update it waits for (look-ahead).
+// POTRF(k) also applies the last update of its tile (from panel k-1) before
+// factoring and computes TRSM(k+1,k) after it, so the dependent chain from one
+// diagonal tile to the next is one task. The host lists the tasks in a
+// topological order that puts each diagonal factorisation right after the
+// tasks it waits for (look-ahead).
 // CTAs claim tasks from a global cursor in list order, wait (thread 0, with an
 // iteration limit) on per-tile counters, run the task with all 512 threads
 // and publish its counter. Every dependency of a claimed task was claimed
@@ -37,7 +40,7 @@ constexpr int TB = NB;                   // tile size (the leaf size)
 constexpr int DAG_THREADS = LEAF_THREADS;
 constexpr int TLD = TB + 4;              // shared tile stride: fragment reads conflict-free in both orientations
 constexpr size_t TILE_SMEM = sizeof(double) * 2 * TB * TLD;
-constexpr size_t DAG_SMEM = TILE_SMEM > LEAF_SMEM ? TILE_SMEM : LEAF_SMEM;
+constexpr size_t DAG_SMEM = TILE_SMEM + LEAF_SMEM;  // two operand tiles, then the leaf's block
 constexpr long kDagSpin = 1L << 22;      // polls of one dependency before the kernel gives up
 constexpr int kMaxTilesN = 56;           // tasks are used up to n = 56 * 64
 
@@ -156,7 +159,9 @@ __global__ void __launch_bounds__(DAG_THREADS, 1)
         if (tid == 0) {
             bool ok = true;
             switch (type) {
-                case K_POTRF: ok = wait_ge(ver + tri(k, k), k, abort); break;
+                case K_POTRF:  // its last update (from panel k-1) is applied inside the task
+                    ok = k == 0 || (wait_ge(ver + tri(k, k), k - 1, abort) && wait_ge(lrdy + tri(k, k - 1), 1, abort));
+                    break;
                 case K_TRSM: ok = wait_ge(ver + tri(i, k), k, abort) && wait_ge(lrdy + tri(k, k), 1, abort); break;
                 case K_UPDATE:
                     ok = wait_ge(ver + tri(i, j), k, abort) && wait_ge(lrdy + tri(i, k), 1, abort) &&
@@ -181,7 +186,54 @@ __global__ void __launch_bounds__(DAG_THREADS, 1)
         __syncthreads();
         if (!s_ok) break;
         if (type == K_POTRF) {
-            chol_leaf_tile(A, ld, TB * k, ext(k), T, ld, err, sm);
+            // A(k,k) -= L(k,k-1) L(k,k-1)^T folded into the leaf's load, the leaf, T(k,k)
+            // published, then L(k+1,k) = A(k+1,k) T(k,k)^T with T(k,k) still in shared memory
+            double* lsm = sm + 2 * TB * TLD;
+            const double* U = nullptr;
+            if (k > 0) {
+                double acc[2][2][2] = {};
+                load_tile(As, tile(A, k, k - 1), ld, ext(k), ext(k - 1), tid);
+                __syncthreads();
+                tile_mma<false, true>(As, As, wm, wn, g, t4, 0, TB, acc);
+                __syncthreads();
+#pragma unroll
+                for (int a = 0; a < 2; ++a)
+#pragma unroll
+                    for (int b = 0; b < 2; ++b)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h)
+                            As[(wn + 8 * b + 2 * t4 + h) * TLD + wm + 8 * a + g] = -acc[a][b][h];
+                __syncthreads();
+                U = As;
+            }
+            chol_leaf_tile(A, ld, TB * k, ext(k), T, ld, err, lsm, U, TLD);
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) {
+                atomicExch(lrdy + tri(k, k), 1);
+                atomicExch(trdy + tri(k, k), 1);
+            }
+            if (k + 1 >= (n + TB - 1) / TB) continue;
+            if (tid == 0) {
+                const bool ok = wait_ge(ver + tri(k + 1, k), k, abort);
+                if (!ok) {
+                    atomicOr(err, ERRBIT_TIMEOUT);
+                    atomicExch(abort, 1);
+                }
+                s_ok = ok;
+            }
+            const double* Tl = lsm + NB * LEAF_LD;  // T(r, c) at Tl[r * LEAF_LD + c], lower triangle valid
+            for (int e = tid; e < TB * TB; e += DAG_THREADS) {
+                const int r = e & (TB - 1), c = e >> 6;
+                Bs[c * TLD + r] = r >= c ? Tl[r * LEAF_LD + c] : 0.0;
+            }
+            __syncthreads();
+            if (!s_ok) break;
+            load_tile(As, tile(A, k + 1, k), ld, ext(k + 1), ext(k), tid);
+            __syncthreads();
+            double acc[2][2][2] = {};
+            tile_mma<false, true>(As, Bs, wm, wn, g, t4, 0, wn + 16, acc);
+            store_tile(tile(A, k + 1, k), ld, ext(k + 1), ext(k), acc, 1.0, false, nullptr, wm, wn, g, t4);
         } else {
             double acc[2][2][2] = {};
             switch (type) {
@@ -234,10 +286,7 @@ __global__ void __launch_bounds__(DAG_THREADS, 1)
         __syncthreads();
         if (tid == 0) {
             switch (type) {
-                case K_POTRF:
-                    atomicExch(lrdy + tri(k, k), 1);
-                    atomicExch(trdy + tri(k, k), 1);
-                    break;
+                case K_POTRF: atomicExch(lrdy + tri(k + 1, k), 1); break;  // the fused L(k+1,k)
                 case K_TRSM: atomicExch(lrdy + tri(i, k), 1); break;
                 case K_UPDATE: atomicAdd(ver + tri(i, j), 1); break;
                 case K_TACC: atomicAdd(tacc + tri(i, j), 1); break;
@@ -252,13 +301,14 @@ __global__ void __launch_bounds__(DAG_THREADS, 1)
 std::vector<int4> build_tasks(int nt) {
     std::vector<int4> v;
     auto add = [&v](int ty, int i, int j, int k) { v.push_back(make_int4(ty, i, j, k)); };
+    // POTRF(k) also applies UPDATE(k,k,k-1) first and computes TRSM(k+1,k) last
     add(K_POTRF, 0, 0, 0);
-    for (int i = 1; i < nt; ++i) add(K_TRSM, i, 0, 0);
+    for (int i = 2; i < nt; ++i) add(K_TRSM, i, 0, 0);
     for (int s = 0; s < nt; ++s) {
         if (s + 1 < nt) {
-            add(K_UPDATE, s + 1, s + 1, s);
+            if (s + 2 < nt) add(K_UPDATE, s + 2, s + 1, s);  // the input of the fused TRSM(s+2,s+1)
             add(K_POTRF, s + 1, s + 1, s + 1);
-            for (int i = s + 2; i < nt; ++i) {
+            for (int i = s + 3; i < nt; ++i) {
                 add(K_UPDATE, i, s + 1, s);
                 add(K_TRSM, i, s + 1, s + 1);
             }
