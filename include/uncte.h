@@ -216,8 +216,9 @@ int unc_server_destroy(unc_server* srv);
 /* SDM::inv (src/uncertaintyTE/ScaledDenseMatrix.cpp:232-279) for a
  * symmetric positive-definite n x n matrix in device memory (column-major,
  * leading dimension lda >= n, lda even): inverted in place on the GPU
- * (equilibration, recursive Cholesky forming L^-1, then L^-T L^-1). Scratch
- * is allocated per call. */
+ * (equilibration, Cholesky with L^-1 formed on the way, then L^-T L^-1; for
+ * n <= 3584 as 64 x 64 tile tasks in one persistent kernel, above by
+ * recursion on halves). Scratch is allocated per call. */
 int unc_dense_inverse_device(double* d_A, int n, int lda, void* stream);
 
 /* The pseudo-inverse step of svdInverse (src/uncertaintyTE/compute.cpp:200-245)
@@ -231,7 +232,7 @@ int unc_dense_inverse_device(double* d_A, int n, int lda, void* stream);
  * not positive. Scratch (4 n x ld matrices) is allocated per call. */
 int unc_pinv_psd_device(double* d_M, int n, int ld, int remove_n, double epsilon, void* stream);
 
-/* The same SPD inverse as unc_dense_inverse_device, for callers that cannot
+/* The SPD inverse of unc_dense_inverse_device (its recursive form), for callers that cannot
  * let a library allocate device memory (their device memory is reserved by
  * their own pool allocator, or cudaMalloc/cudaFree would stall a latency-
  * critical loop). No counterpart in the reference. It allocates nothing: its

@@ -3,9 +3,10 @@
 unc_dense_inverse_noalloc serves callers that cannot let a library allocate
 device memory: applications whose device memory is reserved by their own pool
 allocator, and latency-critical loops where cudaMalloc / cudaFree would stall
-the device. It runs the same kernels as unc_dense_inverse_device with a fixed
-static scratch array, so its results must match that entry point's; n and lda
-are limited to 512.
+the device. It runs the recursive inverse with a fixed static scratch array,
+while unc_dense_inverse_device takes the tile-task form at these sizes, so the
+two inverse routes must agree within the dense-inverse tolerance; n and lda are
+limited to 512.
 """
 import numpy as np
 import pytest

@@ -67,36 +67,37 @@ __device__ __forceinline__ void pair_t(double* Ts, int b0, int e) {
     Ts[(b0 + 16 + i) * LEAF_LD + b0 + j] = -s;
 }
 
-// The factorisation as a device function of one 512-thread CTA (lsm: LEAF_SMEM
-// bytes). A is read through L2 only (ld.global.cg), so that a persistent caller
-// never sees a stale L1 line of a tile another CTA rewrote.
-// U (optional, shared memory, U[j * uld + i]) is added to the lower triangle of
-// the block as it is loaded (a last trailing update applied by the caller).
-__device__ __forceinline__ void chol_leaf_tile(const double* A, long lda, int k0, int kb, double* T, long ldt,
-                                               int* err, double* lsm, const double* U = nullptr, int uld = 0) {
+// Load phase: the kb x kb diagonal block of A at (k0, k0) into S (lower
+// triangle; the upper one zero; identity tail) and Ts cleared. A is read
+// through L2 only (ld.global.cg), so that a persistent caller never sees a
+// stale L1 line of a tile another CTA rewrote. The caller synchronises.
+__device__ __forceinline__ void chol_leaf_load(const double* A, long lda, int k0, int kb, double* lsm) {
+    double* S = lsm;
+    double* Ts = lsm + NB * LEAF_LD;
+    const int tid = threadIdx.x;
+    constexpr int kPer = NB * NB / LEAF_THREADS;
+    double v[kPer];
+    const int i = tid & (NB - 1);
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+        const int j = (tid >> 6) + u * (LEAF_THREADS / NB);
+        v[u] = (i < kb && j < kb) ? (j <= i ? __ldcg(A + (k0 + i) + (long)(k0 + j) * lda) : 0.0) : (i == j ? 1.0 : 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+        const int j = (tid >> 6) + u * (LEAF_THREADS / NB);
+        S[i * LEAF_LD + j] = v[u];
+        Ts[i * LEAF_LD + j] = 0.0;
+    }
+}
+
+// Factorisation of the block in S (after chol_leaf_load and a barrier), T_kk
+// written to T at (k0, k0). One 512-thread CTA, lsm: LEAF_SMEM bytes.
+__device__ __forceinline__ void chol_leaf_factor(int k0, int kb, double* T, long ldt, int* err, double* lsm) {
     double* S = lsm;
     double* Ts = lsm + NB * LEAF_LD;
     double* rinv = Ts + NB * LEAF_LD;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    {
-        constexpr int kPer = NB * NB / LEAF_THREADS;
-        double v[kPer];
-        const int i = tid & (NB - 1);
-#pragma unroll
-        for (int u = 0; u < kPer; ++u) {
-            const int j = (tid >> 6) + u * (LEAF_THREADS / NB);
-            v[u] = (i < kb && j < kb)
-                       ? (j <= i ? __ldcg(A + (k0 + i) + (long)(k0 + j) * lda) + (U ? U[j * uld + i] : 0.0) : 0.0)
-                       : (i == j ? 1.0 : 0.0);
-        }
-#pragma unroll
-        for (int u = 0; u < kPer; ++u) {
-            const int j = (tid >> 6) + u * (LEAF_THREADS / NB);
-            S[i * LEAF_LD + j] = v[u];
-            Ts[i * LEAF_LD + j] = 0.0;
-        }
-    }
-    __syncthreads();
     for (int q = 0; q < NB / LEAF_PW; ++q) {
         const int c0 = q * LEAF_PW;
         if (warp == 0) {  // (A) Cholesky of the diagonal block in registers, lane = row
@@ -223,6 +224,14 @@ __device__ __forceinline__ void chol_leaf_tile(const double* A, long lda, int k0
             if (i < kb && j < kb) T[(k0 + i) + (long)(k0 + j) * ldt] = i >= j ? Ts[i * LEAF_LD + j] : 0.0;
         }
     }
+}
+
+// The whole leaf: load, barrier, factorisation.
+__device__ __forceinline__ void chol_leaf_tile(const double* A, long lda, int k0, int kb, double* T, long ldt,
+                                               int* err, double* lsm) {
+    chol_leaf_load(A, lda, k0, kb, lsm);
+    __syncthreads();
+    chol_leaf_factor(k0, kb, T, ldt, err, lsm);
 }
 
 }  // namespace unc

@@ -186,30 +186,31 @@ __global__ void __launch_bounds__(DAG_THREADS, 1)
         __syncthreads();
         if (!s_ok) break;
         if (type == K_POTRF) {
-            // A(k,k) -= L(k,k-1) L(k,k-1)^T folded into the leaf's load, the leaf, T(k,k)
-            // published, then L(k+1,k) = A(k+1,k) T(k,k)^T with T(k,k) still in shared memory
+            // A(k,k) -= L(k,k-1) L(k,k-1)^T applied to the leaf's block (both tiles loaded
+            // together), the leaf, T(k,k) published, then L(k+1,k) = A(k+1,k) T(k,k)^T with
+            // T(k,k) still in shared memory
             double* lsm = sm + 2 * TB * TLD;
-            const double* U = nullptr;
+            chol_leaf_load(A, ld, TB * k, ext(k), lsm);
             if (k > 0) {
                 double acc[2][2][2] = {};
                 load_tile(As, tile(A, k, k - 1), ld, ext(k), ext(k - 1), tid);
                 __syncthreads();
-                tile_mma<false, true>(As, As, wm, wn, g, t4, 0, TB, acc);
-                __syncthreads();
+                if (wn <= wm) tile_mma<false, true>(As, As, wm, wn, g, t4, 0, TB, acc);  // lower blocks only
 #pragma unroll
                 for (int a = 0; a < 2; ++a)
 #pragma unroll
                     for (int b = 0; b < 2; ++b)
 #pragma unroll
-                        for (int h = 0; h < 2; ++h)
-                            As[(wn + 8 * b + 2 * t4 + h) * TLD + wm + 8 * a + g] = -acc[a][b][h];
-                __syncthreads();
-                U = As;
+                        for (int h = 0; h < 2; ++h) {
+                            const int r = wm + 8 * a + g, c = wn + 8 * b + 2 * t4 + h;
+                            if (c <= r) lsm[r * LEAF_LD + c] -= acc[a][b][h];
+                        }
             }
-            chol_leaf_tile(A, ld, TB * k, ext(k), T, ld, err, lsm, U, TLD);
-            __threadfence();
+            __syncthreads();
+            chol_leaf_factor(TB * k, ext(k), T, ld, err, lsm);
             __syncthreads();
             if (tid == 0) {
+                __threadfence();
                 atomicExch(lrdy + tri(k, k), 1);
                 atomicExch(trdy + tri(k, k), 1);
             }
@@ -282,9 +283,11 @@ __global__ void __launch_bounds__(DAG_THREADS, 1)
                 }
             }
         }
-        __threadfence();  // this thread's tile writes, before the counter is published
+        // release: the barrier orders every thread's tile writes before thread 0's
+        // gpu-scope fence, which orders them before the counter
         __syncthreads();
         if (tid == 0) {
+            __threadfence();
             switch (type) {
                 case K_POTRF: atomicExch(lrdy + tri(k + 1, k), 1); break;  // the fused L(k+1,k)
                 case K_TRSM: atomicExch(lrdy + tri(i, k), 1); break;
@@ -328,6 +331,7 @@ std::vector<int4> build_tasks(int nt) {
 struct TaskLists {
     std::mutex mu;
     std::map<std::pair<int, int>, std::pair<int4*, int>> lists;  // (device, nt) -> device copy
+    std::map<int, cudaStream_t> upload;                          // device -> upload stream
 };
 TaskLists& task_lists() {
     static TaskLists* t = new TaskLists;  // lives until exit, like the device buffers it holds
@@ -352,10 +356,22 @@ int spd_tasks_prepare(int n) {
     std::lock_guard<std::mutex> lock(tl.mu);
     if (tl.lists.count({dev, nt})) return UNC_OK;
     const std::vector<int4> h = build_tasks(nt);
+    // upload on a private non-blocking stream: a copy on the legacy default
+    // stream would wait for every other stream's work (a serving process runs
+    // several requests at once)
+    auto it = tl.upload.find(dev);
+    if (it == tl.upload.end()) {
+        cudaStream_t us = nullptr;
+        if (cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking) != cudaSuccess) return UNC_ERR_CUDA;
+        it = tl.upload.emplace(dev, us).first;
+    }
+    cudaStream_t us = it->second;
     int4* d = nullptr;
-    if (cudaMalloc(&d, sizeof(int4) * h.size()) != cudaSuccess) return UNC_ERR_OUT_OF_MEMORY;
-    if (cudaMemcpy(d, h.data(), sizeof(int4) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
-        cudaFree(d);
+    if (cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(int4) * h.size(), us) != cudaSuccess)
+        return UNC_ERR_OUT_OF_MEMORY;
+    if (cudaMemcpyAsync(d, h.data(), sizeof(int4) * h.size(), cudaMemcpyHostToDevice, us) != cudaSuccess ||
+        cudaStreamSynchronize(us) != cudaSuccess) {
+        cudaFreeAsync(d, us);
         return UNC_ERR_CUDA;
     }
     static std::atomic<unsigned long long> attr{0};
