@@ -148,6 +148,7 @@ __global__ void __launch_bounds__(DAG_THREADS, 1)
     double* As = sm;
     double* Bs = sm + TB * TLD;
     auto ext = [n](int b) { return min(TB, n - TB * b); };
+    auto kext = [n](int b) { return (min(TB, n - TB * b) + 3) & ~3; };  // K extent of a partial tile, DMMA steps
     auto tile = [ld](double* M, int i, int j) { return M + (long)TB * i + (long)TB * j * ld; };
     while (true) {
         if (tid == 0) s_task = atomicAdd(cursor, 1);
@@ -242,7 +243,7 @@ __global__ void __launch_bounds__(DAG_THREADS, 1)
                     load_tile(As, tile(A, i, k), ld, ext(i), ext(k), tid);
                     load_tile(Bs, tile(T, k, k), ld, ext(k), ext(k), tid);
                     __syncthreads();
-                    tile_mma<false, true>(As, Bs, wm, wn, g, t4, 0, wn + 16, acc);
+                    tile_mma<false, true>(As, Bs, wm, wn, g, t4, 0, min(wn + 16, kext(k)), acc);
                     __syncthreads();
                     store_tile(tile(A, i, k), ld, ext(i), ext(k), acc, 1.0, false, nullptr, wm, wn, g, t4);
                     break;
@@ -250,21 +251,21 @@ __global__ void __launch_bounds__(DAG_THREADS, 1)
                     load_tile(As, tile(A, i, k), ld, ext(i), ext(k), tid);
                     load_tile(Bs, tile(A, j, k), ld, ext(j), ext(k), tid);
                     __syncthreads();
-                    tile_mma<false, true>(As, Bs, wm, wn, g, t4, 0, TB, acc);
+                    tile_mma<false, true>(As, Bs, wm, wn, g, t4, 0, kext(k), acc);
                     store_tile(tile(A, i, j), ld, ext(i), ext(j), acc, -1.0, true, nullptr, wm, wn, g, t4);
                     break;
                 case K_TACC:  // W(i,j) += L(i,k) T(k,j); T(j,j) lower: terms k' >= n only
                     load_tile(As, tile(A, i, k), ld, ext(i), ext(k), tid);
                     load_tile(Bs, tile(T, k, j), ld, ext(k), ext(j), tid);
                     __syncthreads();
-                    tile_mma<false, false>(As, Bs, wm, wn, g, t4, k == j ? wn : 0, TB, acc);
+                    tile_mma<false, false>(As, Bs, wm, wn, g, t4, k == j ? wn : 0, kext(k), acc);
                     store_tile(tile(T, i, j), ld, ext(i), ext(j), acc, 1.0, k > j, nullptr, wm, wn, g, t4);
                     break;
                 case K_TFIN:  // T(i,j) = -T(i,i) W(i,j); T(i,i) lower: terms k' <= m only
                     load_tile(As, tile(T, i, i), ld, ext(i), ext(i), tid);
                     load_tile(Bs, tile(T, i, j), ld, ext(i), ext(j), tid);
                     __syncthreads();
-                    tile_mma<false, false>(As, Bs, wm, wn, g, t4, 0, wm + 16, acc);
+                    tile_mma<false, false>(As, Bs, wm, wn, g, t4, 0, min(wm + 16, kext(i)), acc);
                     __syncthreads();
                     store_tile(tile(T, i, j), ld, ext(i), ext(j), acc, -1.0, false, nullptr, wm, wn, g, t4);
                     break;
@@ -275,7 +276,7 @@ __global__ void __launch_bounds__(DAG_THREADS, 1)
                     int kb = 0;
                     if (k == i) kb = wm;
                     if (k == j) kb = max(kb, wn);
-                    tile_mma<true, false>(As, Bs, wm, wn, g, t4, kb, TB, acc);
+                    tile_mma<true, false>(As, Bs, wm, wn, g, t4, kb, kext(k), acc);
                     const bool last = k == (n + TB - 1) / TB - 1;
                     store_tile(tile(O, i, j), ld, ext(i), ext(j), acc, 1.0, k > i,
                                (last && i > j) ? tile(O, j, i) : nullptr, wm, wn, g, t4);
