@@ -43,6 +43,10 @@ struct unc_context {
     size_t jac_bytes = 0;
     cudaEvent_t ev[12] = {};
     int priority = 0;  // of `stream` (0: the default priority)
+    // grid bound of the tile-task inverse: a server running requests side by side
+    // lowers it, so that one request's persistent kernel (its CTAs wait on
+    // dependencies in place) leaves SMs to the other requests' kernels
+    int task_ctas = 148;
     // dense-stage graphs: a stage seen twice with the same key is captured and
     // replayed (kStageGraphs most recent kept)
     std::vector<StageGraph> graphs;
@@ -53,6 +57,13 @@ struct unc_context {
     long long prof_launches = 0;
     double prof_seconds = 0, prof_flops = 0;
 };
+
+namespace unc {
+// (declared in internal.h)
+void context_set_task_ctas(unc_context* c, int max_ctas) {
+    if (c) c->task_ctas = std::max(1, std::min(148, max_ctas));
+}
+}  // namespace unc
 
 namespace {
 
@@ -422,7 +433,8 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     auto inverse_stage = [&]() -> int {
         launch_shift_equilibrate(b.Z, N, ld, lambda, b.e, s.err, sm);
         if (tasks) {
-            if (int r = chol_inverse_tasks(b.Z, N, ld, b.iZ, b.add, b.dag_state, s.err, sm)) return r;
+            if (int r = chol_inverse_tasks(b.Z, N, ld, b.iZ, b.add, b.dag_state, s.err, sm, ctx->task_ctas))
+                return r;
             launch_unequilibrate_from(b.add, b.Z, N, ld, b.e, b.iZ, sm);  // X in Z, iZ = X
         } else {
             chol_inverse(b.Z, N, ld, b.iZ, b.add, b.tmp, b.gjws, s.err, sm);

@@ -189,7 +189,13 @@ void launch_unequilibrate_from(const double* S, double* X, int n, int lda, const
 bool spd_tasks_apply(int n);
 size_t spd_task_state_ints(int n);
 int spd_tasks_prepare(int n);
-int chol_inverse_tasks(double* A, int n, int lda, double* T, double* O, int* state, int* err, cudaStream_t st);
+// max_ctas bounds the persistent grid (at most one CTA per SM is used anyway);
+// the task order and every tile's update order do not depend on it, so neither
+// do the results.
+int chol_inverse_tasks(double* A, int n, int lda, double* T, double* O, int* state, int* err, cudaStream_t st,
+                       int max_ctas = 148);
+// per context: the largest grid of the tile-task inverse (148 unless set)
+void context_set_task_ctas(unc_context* c, int max_ctas);
 // Y <- Y + k*X  (N x N, column-major)
 void launch_axpy(double* Y, const double* X, double k, int n, int ld, cudaStream_t st);
 

@@ -127,6 +127,8 @@ std::shared_ptr<Request> pick(unc_server* s, Worker* w) {
 void worker_loop(unc_server* s, Worker* w) {
     cudaSetDevice(s->device);
     if (unc_context_create(s->device, &w->ctx) != UNC_OK) w->ctx = nullptr;
+    // requests run side by side: each tile-task inverse takes about two workers' share of the SMs
+    if (w->ctx) unc::context_set_task_ctas(w->ctx, (2 * 148 + (int)s->workers.size() - 1) / (int)s->workers.size());
     std::unique_lock<std::mutex> lk(s->mu);
     for (;;) {
         std::shared_ptr<Request> r;
