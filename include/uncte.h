@@ -243,6 +243,16 @@ int unc_pinv_psd_device(double* d_M, int n, int ld, int remove_n, double epsilon
  * before any stream capture. Synchronous, like unc_dense_inverse_device. */
 int unc_dense_inverse_noalloc(double* d_A, int n, int lda, void* stream);
 
+/* The order in which the tile-task form of unc_dense_inverse_device (n <= 3584)
+ * runs its 64 x 64 tile tasks; no counterpart in the reference (its inverse is
+ * LAPACK's). For tools that check or draw the schedule. Returns the number of
+ * tasks (UNC_ERR_INVALID_ARG outside 1..3584); when out is non-NULL and
+ * capacity is at least that number, out receives 4 ints per task: the kind
+ * (0 diagonal factorisation with its fused update and next solve, 1 triangular
+ * solve, 2 trailing update, 3 inverse accumulation, 4 inverse finish, 5 product
+ * accumulation) and the tile indices i, j, k. Host only; needs no GPU. */
+int unc_spd_task_list(int n, int* out, int capacity);
+
 /* SSM J^T J (trn() then operator*, ScaledSparseMatrix.cpp:384-388,517-539)
  * computed by the GPU block-assembly kernels and returned as host CRS in the
  * reference's pattern. Observations may have 12-entry rows (camera + point)

@@ -407,3 +407,24 @@ int chol_inverse_tasks(double* A, int n, int lda, double* T, double* O, int* sta
 }
 
 }  // namespace unc
+
+// The task order of the tile-task inverse for an n x n matrix, for tools that
+// check or draw the schedule: returns the number of tasks; with out != NULL and
+// capacity >= that number, out receives 4 ints per task (kind 0..5 = POTRF,
+// TRSM, UPDATE, TACC, TFIN, PACC; then i, j, k as in the kernel). Host only.
+extern "C" int unc_spd_task_list(int n, int* out, int capacity) {
+    unc::g_last_error.clear();
+    if (!unc::spd_tasks_apply(n)) {
+        unc::g_last_error = "unc_spd_task_list: n must be in 1..3584";
+        return UNC_ERR_INVALID_ARG;
+    }
+    const std::vector<int4> v = unc::build_tasks((n + unc::NB - 1) / unc::NB);
+    if (out && capacity >= (int)v.size())
+        for (size_t q = 0; q < v.size(); ++q) {
+            out[4 * q] = v[q].x;
+            out[4 * q + 1] = v[q].y;
+            out[4 * q + 2] = v[q].z;
+            out[4 * q + 3] = v[q].w;
+        }
+    return (int)v.size();
+}

@@ -80,7 +80,7 @@ class UncStatistic(C.Structure):
 EXPORTS = ("unc_options_init", "unc_context_create", "unc_context_destroy", "unc_compute",
            "unc_context_set_profiling", "unc_context_profile",
            "unc_compute_device", "unc_workspace_bytes", "unc_dense_inverse_device",
-           "unc_dense_inverse_noalloc", "unc_pinv_psd_device", "unc_jtj_crs",
+           "unc_dense_inverse_noalloc", "unc_spd_task_list", "unc_pinv_psd_device", "unc_jtj_crs",
            "unc_gemm_f64_device", "unc_gemm_mixed_device", "unc_status_string", "unc_last_error",
            "unc_kernel_launches", "unc_request_bytes", "unc_context_device_bytes", "unc_context_release",
            "unc_context_set_priority", "unc_jacobian_device", "unc_compute_scene",
@@ -114,6 +114,7 @@ def lib():
     L.unc_workspace_bytes.restype = C.c_longlong
     L.unc_dense_inverse_device.argtypes = [vp, C.c_int, C.c_int, vp]
     L.unc_dense_inverse_noalloc.argtypes = [vp, C.c_int, C.c_int, vp]
+    L.unc_spd_task_list.argtypes = [C.c_int, vp, C.c_int]
     L.unc_pinv_psd_device.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, vp]
     L.unc_request_bytes.argtypes = [P(UncOptions), C.c_int, C.c_int, vp, vp]
     L.unc_request_bytes.restype = C.c_longlong
@@ -373,6 +374,22 @@ def dense_inverse_device(d_ptr: int, n: int, lda: int, stream: int = 0) -> None:
 def dense_inverse_noalloc(d_ptr: int, n: int, lda: int, stream: int = 0) -> None:
     """In-place SPD inverse with no device allocation (static scratch, n and lda <= 512)."""
     _check(lib().unc_dense_inverse_noalloc(d_ptr, n, lda, stream or None))
+
+
+SPD_TASK_KINDS = ("POTRF", "TRSM", "UPDATE", "TACC", "TFIN", "PACC")
+
+
+def spd_task_list(n: int):
+    """The tile-task order of the n x n SPD inverse (n <= 3584) as an int array
+    of shape (tasks, 4): kind (index into SPD_TASK_KINDS), i, j, k. Host only."""
+    import numpy as np
+    L = lib()
+    count = L.unc_spd_task_list(n, None, 0)
+    if count < 0:
+        _check(count)
+    out = np.zeros((count, 4), dtype=np.int32)
+    _check(0 if L.unc_spd_task_list(n, out.ctypes.data, count) == count else -1)
+    return out
 
 
 def pinv_psd_device(d_ptr: int, n: int, ld: int, remove_n: int = 7, epsilon: float = 1e-10,
