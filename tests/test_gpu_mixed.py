@@ -1,7 +1,7 @@
 """Mixed-precision Taylor products (int8-sliced tcgen05 GEMMs) against the
 FP64 GPU path and against torch FP64 products (needs a B200).
 
-Tolerance: the north-star bar for the mixed path is a maximum relative
+Tolerance: the accuracy target of the mixed path is a maximum relative
 Frobenius error of 1e-6 per camera 9x9 block and per point 3x3 block against
 the FP64 result; MIXED_TOL below is that bar.
 """
