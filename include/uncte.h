@@ -239,8 +239,9 @@ int unc_pinv_psd_device(double* d_M, int n, int ld, int remove_n, double epsilon
  * scratch is a fixed __device__ array of about 6.3 MB held by every device the
  * library is loaded on, so n and lda are limited to 512 (UNC_ERR_TOO_LARGE
  * beyond). All calls on a device share that array; calls that overlap on the
- * GPU race. The first call on a device looks up the array's address; make it
- * before any stream capture. Synchronous, like unc_dense_inverse_device. */
+ * GPU race. The first call on a device looks up the array's address (again
+ * after a device reset); make it before any stream capture. Synchronous, like
+ * unc_dense_inverse_device. */
 int unc_dense_inverse_noalloc(double* d_A, int n, int lda, void* stream);
 
 /* The order in which the tile-task form of unc_dense_inverse_device (n <= 3584)

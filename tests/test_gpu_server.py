@@ -81,3 +81,38 @@ def test_wait_timeout_and_single_collection():
     with pytest.raises(native.UncError):
         srv.wait(rid)  # already collected
     srv.close()
+
+
+def test_waiters_survive_concurrent_submits():
+    """One thread waits on a long request while the main thread submits enough
+    requests to make the server's id table grow (rehash) several times; a second
+    waiter on the same id fails cleanly instead of sharing the result."""
+    import threading
+    big = scenes.scene_jacobian(scenes.make_sized_scene(600, 100, 4, seed=21))
+    tiny = scenes.scene_jacobian(scenes.make_sized_scene(8, 20, 3, seed=22))
+    srv = native.Server(max_inflight=2)
+    rid = srv.submit(big, precision="fp64")
+    outcome = {}
+
+    def waiter(name):
+        try:
+            outcome[name] = srv.wait(rid)
+        except native.UncError as e:
+            outcome[name] = e
+
+    threads = [threading.Thread(target=waiter, args=(k,)) for k in ("a", "b")]
+    for t in threads:
+        t.start()
+    ids = [srv.submit(tiny, precision="mixed") for _ in range(600)]
+    for t in threads:
+        t.join(timeout=600)
+    got = [srv.wait(i)[:2] for i in ids]
+    srv.close()
+    ok = [v for v in outcome.values() if isinstance(v, tuple)]
+    bad = [v for v in outcome.values() if isinstance(v, native.UncError)]
+    assert len(ok) == 1 and len(bad) == 1, outcome
+    assert bad[0].status == -1  # UNC_ERR_INVALID_ARG: waited for or collected by the other thread
+    assert np.isfinite(ok[0][0]).all() and ok[0][2]["te_iterations"] > 0
+    for c, p in got[1:]:
+        np.testing.assert_array_equal(c, got[0][0])
+        np.testing.assert_array_equal(p, got[0][1])

@@ -51,3 +51,28 @@ def test_noalloc_rejects_sizes_beyond_the_static_scratch():
     with pytest.raises(native.UncError) as e:
         native.dense_inverse_noalloc(buf.data_ptr(), 513, 520)
     assert e.value.status == -8  # UNC_ERR_TOO_LARGE
+
+
+def test_noalloc_call_allocates_no_device_memory():
+    """The property the entry point exists for: after a first call (which loads
+    the kernels and looks up the array's address), a call leaves the device's
+    free memory and the caching allocator's allocation count unchanged."""
+    import torch
+    n, lda = 300, 304
+    A = _spd(n, 7)
+    src = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+    buf = torch.zeros((n, lda), dtype=torch.float64, device="cuda")
+    buf[:, :n] = src
+    native.dense_inverse_noalloc(buf.data_ptr(), n, lda)  # warm-up
+    buf[:, :n] = src
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    allocs0 = torch.cuda.memory_stats().get("allocation.all.allocated", 0)
+    native.dense_inverse_noalloc(buf.data_ptr(), n, lda)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    allocs1 = torch.cuda.memory_stats().get("allocation.all.allocated", 0)
+    assert free1 == free0, (free0, free1)
+    assert allocs1 == allocs0
+    got = buf[:, :n].cpu().numpy().T
+    assert np.max(np.abs(got @ A - np.eye(n))) < 1e-10

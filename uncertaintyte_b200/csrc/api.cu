@@ -18,6 +18,23 @@ namespace unc {
 thread_local std::string g_last_error;
 long long g_launches = 0;
 thread_local long long g_thread_launches = 0;
+
+int device_sms() {
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return 148;
+    }
+    int v = cache[dev].load(std::memory_order_relaxed);
+    if (v > 0) return v;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
+        cudaGetLastError();
+        v = 148;
+    }
+    cache[dev].store(v, std::memory_order_relaxed);
+    return v;
+}
 }  // namespace unc
 
 using namespace unc;
@@ -43,10 +60,11 @@ struct unc_context {
     size_t jac_bytes = 0;
     cudaEvent_t ev[12] = {};
     int priority = 0;  // of `stream` (0: the default priority)
+    int sm_count = 148;  // of `device`
     // grid bound of the tile-task inverse: a server running requests side by side
     // lowers it, so that one request's persistent kernel (its CTAs wait on
     // dependencies in place) leaves SMs to the other requests' kernels
-    int task_ctas = 148;
+    int task_ctas = 148;  // set to the device's SM count at creation
     // dense-stage graphs: a stage seen twice with the same key is captured and
     // replayed (kStageGraphs most recent kept)
     std::vector<StageGraph> graphs;
@@ -61,7 +79,7 @@ struct unc_context {
 namespace unc {
 // (declared in internal.h)
 void context_set_task_ctas(unc_context* c, int max_ctas) {
-    if (c) c->task_ctas = std::max(1, std::min(148, max_ctas));
+    if (c) c->task_ctas = std::max(1, std::min(c->sm_count, max_ctas));
 }
 }  // namespace unc
 
@@ -569,6 +587,8 @@ int unc_context_create(int device, unc_context** out) {
     c->device = device;
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) {  // kernel attributes now, never inside a stream capture
+        c->sm_count = device_sms();
+        c->task_ctas = c->sm_count;
         prepare_assembly_kernels();
         prepare_dense_kernels();
         prepare_mixed_kernels();

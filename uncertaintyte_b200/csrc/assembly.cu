@@ -889,11 +889,12 @@ void launch_schur(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
     cudaMemsetAsync(s.long_list, 0, sizeof(int), st);
     cudaMemsetAsync(s.nz_list, 0, 2 * sizeof(int), st);
     k_list_blocks<<<(unsigned)((nblk + 255) / 256), 256, 0, st>>>(nblk, s.blk_ptr, s.nz_list);
-    k_sort_pairs_warp<<<148 * 8, 32 * kSortWarps, 0, st>>>(s.nz_list, s.blk_ptr, s.pairs, s.long_list, s.long_cap);
+    const unsigned sms = (unsigned)device_sms();
+    k_sort_pairs_warp<<<sms * 8, 32 * kSortWarps, 0, st>>>(s.nz_list, s.blk_ptr, s.pairs, s.long_list, s.long_cap);
     prepare_assembly_kernels();
-    k_sort_pairs_block<<<148, 1024, kPairBlockCap * sizeof(unsigned long long), st>>>(
+    k_sort_pairs_block<<<sms, 1024, kPairBlockCap * sizeof(unsigned long long), st>>>(
         s.blk_ptr, s.pairs, s.long_list, s.long_cap, s.err);
-    k_schur_blocks<<<148 * 8, 32 * kSchurWarps, 0, st>>>(s.num_cams, s.blk_ptr, s.nz_list, s.pairs, s.Ws, s.Ys, Z,
+    k_schur_blocks<<<sms * 8, 32 * kSchurWarps, 0, st>>>(s.num_cams, s.blk_ptr, s.nz_list, s.pairs, s.Ws, s.Ys, Z,
                                                           ldz);
     count_launch(4);
 }

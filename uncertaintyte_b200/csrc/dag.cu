@@ -399,7 +399,7 @@ int chol_inverse_tasks(double* A, int n, int lda, double* T, double* O, int* sta
     }
     const int ntri = nt * (nt + 1) / 2;
     if (cudaMemsetAsync(state, 0, sizeof(int) * spd_task_state_ints(n), st) != cudaSuccess) return UNC_ERR_CUDA;
-    const int grid = std::max(1, std::min(std::min(148, max_ctas), list.second));
+    const int grid = std::max(1, std::min(std::min(device_sms(), max_ctas), list.second));
     k_spd_inverse_tasks<<<grid, DAG_THREADS, DAG_SMEM, st>>>(A, T, O, n, lda, list.first, list.second, state, ntri,
                                                              err);
     count_launch();

@@ -29,6 +29,10 @@ inline int ld_of(int n) { return (n + 7) & ~7; }
 
 extern thread_local std::string g_last_error;
 
+// Streaming multiprocessors of the current device (queried once per device;
+// 148 on a B200, fewer on a partitioned GPU).
+int device_sms();
+
 // Runs f() (returning true on success) until it succeeds once per device
 // (ordinal < 64) for one call site, from any thread: per-function CUDA
 // attributes are per device, and several host threads (one per context) may

@@ -18,7 +18,8 @@
 //     respect to each other) race on the array and give wrong results.
 //   * The first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress, with that device current); make that first call
-//     before any stream capture.
+//     before any stream capture. The lookup is repeated after a device reset
+//     (the CUDA context changed), so the library may outlive a reset.
 #include <mutex>
 
 #include "../../include/uncte.h"
@@ -37,8 +38,28 @@ constexpr size_t kScratchDoubles = 3 * kMat + kSmall + kEq + 8;      // + the er
 __device__ __align__(256) double g_inverse_scratch[kScratchDoubles];
 
 constexpr int kMaxDevices = 64;
+// Per device: the array's device address and the CUDA context it was looked
+// up in. A device reset (cudaDeviceReset, or a primary-context reset by other
+// code in the process) unloads the module; the next context loads it again,
+// possibly at another address, so the lookup is repeated when the current
+// context is not the one recorded.
 double* g_scratch_addr[kMaxDevices] = {};
+CUcontext g_scratch_ctx[kMaxDevices] = {};
 std::mutex g_scratch_mu;
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {
+    static const CtxGetCurrentFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            return reinterpret_cast<CtxGetCurrentFn>(p);
+        cudaGetLastError();
+        return (CtxGetCurrentFn) nullptr;
+    }();
+    return fn;
+}
 
 int scratch_for_current_device(double** out) {
     int dev = 0;
@@ -51,15 +72,29 @@ int scratch_for_current_device(double** out) {
         g_last_error = "device index above the supported range";
         return UNC_ERR_UNSUPPORTED;
     }
+    CtxGetCurrentFn get = ctx_get_current();
+    if (!get) {
+        g_last_error = "cuCtxGetCurrent is unavailable";
+        return UNC_ERR_CUDA;
+    }
+    // before the runtime has set up the device no context is current yet; the
+    // symbol lookup below does that set-up
+    CUcontext ctx = nullptr;
+    if (get(&ctx) != CUDA_SUCCESS) ctx = nullptr;
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
+    if (!g_scratch_addr[dev] || !ctx || g_scratch_ctx[dev] != ctx) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_inverse_scratch);
         if (e != cudaSuccess || !p) {
             g_last_error = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
             return UNC_ERR_CUDA;
         }
+        if (get(&ctx) != CUDA_SUCCESS || !ctx) {
+            g_last_error = "no current CUDA context after the symbol lookup";
+            return UNC_ERR_CUDA;
+        }
         g_scratch_addr[dev] = static_cast<double*>(p);
+        g_scratch_ctx[dev] = ctx;
     }
     *out = g_scratch_addr[dev];
     return UNC_OK;

@@ -56,6 +56,7 @@ struct Request {
     bool small = false;
     int bypassed = 0;
     bool done = false;
+    bool waited = false;  // a thread is inside unc_server_wait for this request
     int status = UNC_OK;
     std::string error;
     unc_statistic st{};
@@ -128,7 +129,8 @@ void worker_loop(unc_server* s, Worker* w) {
     cudaSetDevice(s->device);
     if (unc_context_create(s->device, &w->ctx) != UNC_OK) w->ctx = nullptr;
     // requests run side by side: each tile-task inverse takes about two workers' share of the SMs
-    if (w->ctx) unc::context_set_task_ctas(w->ctx, (2 * 148 + (int)s->workers.size() - 1) / (int)s->workers.size());
+    const int sms = unc::device_sms();
+    if (w->ctx) unc::context_set_task_ctas(w->ctx, (2 * sms + (int)s->workers.size() - 1) / (int)s->workers.size());
     std::unique_lock<std::mutex> lk(s->mu);
     for (;;) {
         std::shared_ptr<Request> r;
@@ -238,15 +240,23 @@ int unc_server_wait(unc_server* s, long long id, double timeout_s, int* status, 
         unc::g_last_error = "unc_server_wait: unknown request id (or already collected)";
         return UNC_ERR_INVALID_ARG;
     }
+    // Only the shared_ptr is kept across the wait: submits from other threads
+    // insert into `all` meanwhile, and a rehash invalidates every iterator.
     std::shared_ptr<Request> r = it->second;
+    if (r->waited) {
+        unc::g_last_error = "unc_server_wait: another thread is already waiting for this request";
+        return UNC_ERR_INVALID_ARG;
+    }
+    r->waited = true;
     auto ready = [&] { return r->done; };
     if (timeout_s < 0) {
         s->cv_done.wait(lk, ready);
     } else if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), ready)) {
+        r->waited = false;
         unc::g_last_error = "unc_server_wait: request still running";
         return UNC_ERR_TIMEOUT;
     }
-    s->all.erase(it);
+    s->all.erase(id);
     if (status) *status = r->status;
     if (st) *st = r->st;
     if (latency_s) *latency_s = std::chrono::duration<double>(r->t_end - r->t_submit).count();
