@@ -14,7 +14,12 @@
  *   - getCovariances(..., points3D, ...) picks the fixed points
  *     deterministically (the reference samples 100k random triples);
  *   - Options::_debug does not dump matrices;
- *   - times in Statistic are true seconds (the reference stores ms/100).
+ *   - times in Statistic are true seconds (the reference stores ms/100);
+ *   - getCamerasCentersUncEigVec / getPointsUncEigVectors return the
+ *     eigenvectors in descending eigenvalue order, the order of the eigenvalue
+ *     accessors (the reference returns them in Eigen::EigenSolver's unspecified
+ *     order, uncertainty.cpp:92-115,164-183); each vector's sign is arbitrary in
+ *     both.
  */
 #pragma once
 #include <cmath>

@@ -244,6 +244,17 @@ int unc_pinv_psd_device(double* d_M, int n, int ld, int remove_n, double epsilon
  * unc_dense_inverse_device. */
 int unc_dense_inverse_noalloc(double* d_A, int n, int lda, void* stream);
 
+/* Diagnostics of the tile-task form of unc_dense_inverse_device (n <= 3584):
+ * the same inverse with the dependency waits limited to poll_limit polls each
+ * (1..2^22; the regular calls use 2^22) and, when skip_task >= 0, that task
+ * (an index of the unc_spd_task_list order) left out of the schedule. Every
+ * wait of the persistent kernel is bounded: a wait that runs out raises an
+ * abort flag that all CTAs check, the launch drains and the call returns
+ * UNC_ERR_CUDA ("bounded device wait ... ran out") instead of hanging, and the
+ * device stays usable. A schedule with a task left out cannot complete, which
+ * is how a test makes a wait run out. No counterpart in the reference. */
+int unc_spd_inverse_tasks_bounded(double* d_A, int n, int lda, long long poll_limit, int skip_task, void* stream);
+
 /* The order in which the tile-task form of unc_dense_inverse_device (n <= 3584)
  * runs its 64 x 64 tile tasks; no counterpart in the reference (its inverse is
  * LAPACK's). For tools that check or draw the schedule. Returns the number of

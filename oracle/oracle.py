@@ -32,6 +32,9 @@ class OracleOptions(C.Structure):
         ("has_pts2fix", C.c_int),
         ("faithful_point_scan", C.c_int),
         ("threads", C.c_int),
+        ("inverse_route", C.c_int),
+        ("z_perturb", C.c_double),
+        ("skip_dense", C.c_int),
     ]
 
 
@@ -81,6 +84,12 @@ def lib():
         L.oracle_dense_inv.restype = C.c_int
         L.oracle_te_inverse.argtypes = [C.c_int, P(C.c_double), C.c_double, P(OracleStats)]
         L.oracle_te_inverse.restype = C.c_int
+        L.oracle_te_inverse_route.argtypes = [C.c_int, P(C.c_double), C.c_double, C.c_int, P(OracleStats)]
+        L.oracle_te_inverse_route.restype = C.c_int
+        L.oracle_dense_inv_cholesky.argtypes = [C.c_int, P(C.c_double)]
+        L.oracle_dense_inv_cholesky.restype = C.c_int
+        L.oracle_gemm.argtypes = [C.c_int, P(C.c_double), P(C.c_double), P(C.c_double)]
+        L.oracle_gemm.restype = None
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_set_threads.restype = C.c_int
         _LIB = L
@@ -92,10 +101,16 @@ def _p(a, t):
 
 
 def compute(jac, algorithm=2, lam=-1.0, epsilon=1e-10, svd_remove_n=-1, faithful_point_scan=False,
-            threads=0, debug=False, cam_init=None, pt_init=None):
+            threads=0, debug=False, cam_init=None, pt_init=None, route="lu", z_perturb=0.0,
+            skip_dense=False):
     """Run the oracle on a Jacobian (uncertaintyte_b200.jacob.Jacobian-like object).
 
-    Returns dict(cam, pt, stats[, Z, iZ, d])."""
+    route: "lu" (the reference's ScaledDenseMatrix::inv) or "cholesky" (the
+    Jacobi-equilibrated Cholesky inverse, the CUDA path's route) for the dense
+    inverse of the Taylor path. z_perturb: relative rounding-level perturbation
+    of the Schur complement (see uncte_oracle.h), 0 for none. skip_dense:
+    timing samples only (the dense inverse and Taylor loop are skipped, the
+    outputs are meaningless). Returns dict(cam, pt, stats[, Z, iZ, d])."""
     o = OracleOptions()
     o.algorithm = algorithm
     o.epsilon = epsilon
@@ -108,6 +123,9 @@ def compute(jac, algorithm=2, lam=-1.0, epsilon=1e-10, svd_remove_n=-1, faithful
         o.has_pts2fix = 1
     o.faithful_point_scan = int(bool(faithful_point_scan))
     o.threads = threads
+    o.inverse_route = {"lu": 0, "cholesky": 1}[route]
+    o.z_perturb = z_perturb
+    o.skip_dense = int(bool(skip_dense))
     ncam = jac.num_cams * jac.cam_params * (jac.cam_params + 1) // 2
     cam = np.zeros(ncam) if cam_init is None else np.array(cam_init, dtype=np.float64)
     pt = np.zeros(jac.num_points * 6) if pt_init is None else np.array(pt_init, dtype=np.float64)
@@ -162,12 +180,30 @@ def dense_inv(A):
     return F, info
 
 
-def te_inverse(Z, lam):
+def te_inverse(Z, lam, route="lu"):
     n = Z.shape[0]
     F = np.array(Z, dtype=np.float64, order="F")
     st = OracleStats()
-    lib().oracle_te_inverse(n, _p(F, C.c_double), lam, C.byref(st))
+    lib().oracle_te_inverse_route(n, _p(F, C.c_double), lam, {"lu": 0, "cholesky": 1}[route], C.byref(st))
     return F, st
+
+
+def dense_inv_cholesky(A):
+    """The Jacobi-equilibrated Cholesky inverse (the CUDA path's route)."""
+    n = A.shape[0]
+    F = np.array(A, dtype=np.float64, order="F")
+    info = lib().oracle_dense_inv_cholesky(n, _p(F, C.c_double))
+    return F, info
+
+
+def gemm(A, B):
+    """One dense product of the Taylor loop (operator*=): A * B."""
+    n = A.shape[0]
+    Af = np.asfortranarray(A, dtype=np.float64)
+    Bf = np.asfortranarray(B, dtype=np.float64)
+    Cf = np.zeros((n, n), order="F")
+    lib().oracle_gemm(n, _p(Af, C.c_double), _p(Bf, C.c_double), _p(Cf, C.c_double))
+    return Cf
 
 
 def set_threads(n: int) -> int:

@@ -43,6 +43,8 @@ void scipy_dgesvd_(const char*, const char*, const int*, const int*, double*, co
                    double*, const int*, double*, const int*, double*, const int*, int*);
 void scipy_dgesdd_(const char*, const int*, const int*, double*, const int*, double*, double*,
                    const int*, double*, const int*, double*, const int*, int*, int*);
+void scipy_dpotrf_(const char*, const int*, double*, const int*, int*);
+void scipy_dpotri_(const char*, const int*, double*, const int*, int*);
 void scipy_openblas_set_num_threads(int);
 int scipy_openblas_get_num_threads(void);
 }
@@ -272,11 +274,41 @@ int oracle_dense_inv(int n, double* A) {
     return info;
 }
 
+/* Cholesky route (not the reference's): symmetric Jacobi equilibration,
+ * dpotrf/dpotri, unscale. The same mathematics as the CUDA path's SPD inverse,
+ * with LAPACK's blocking and summation order. */
+int oracle_dense_inv_cholesky(int n, double* A) {
+    std::vector<double> e(n);
+    for (int i = 0; i < n; ++i) {
+        const double d = A[i + (size_t)i * n];
+        if (!(d > 0)) return i + 1;
+        e[i] = 1.0 / std::sqrt(d);
+    }
+#pragma omp parallel for
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < n; ++r) A[r + (size_t)c * n] *= e[r] * e[c];
+    int info = 0;
+    scipy_dpotrf_("L", &n, A, &n, &info);
+    if (info == 0) scipy_dpotri_("L", &n, A, &n, &info);
+#pragma omp parallel for
+    for (int c = 0; c < n; ++c)
+        for (int r = c; r < n; ++r) {
+            const double v = A[r + (size_t)c * n] * e[r] * e[c];
+            A[r + (size_t)c * n] = v;
+            A[c + (size_t)r * n] = v;
+        }
+    return info;
+}
+
 /* teInverse: compute.cpp:121-166 (iZupdate :64-71, operator*= :314-353). */
 int oracle_te_inverse(int n, double* Z, double lambda, oracle_stats* st) {
+    return oracle_te_inverse_route(n, Z, lambda, 0, st);
+}
+
+int oracle_te_inverse_route(int n, double* Z, double lambda, int route, oracle_stats* st) {
     auto t0 = Clock::now();
     for (int i = 0; i < n; ++i) Z[i + (size_t)i * n] += lambda;
-    int info = oracle_dense_inv(n, Z);
+    int info = route == 1 ? oracle_dense_inv_cholesky(n, Z) : oracle_dense_inv(n, Z);
     auto t1 = Clock::now();
     const size_t nn = (size_t)n * n;
     std::vector<double> X(Z, Z + nn), add(nn), tmp(nn);
@@ -304,6 +336,29 @@ int oracle_te_inverse(int n, double* Z, double lambda, oracle_stats* st) {
         st->t_te = secs(t1, t2);
     }
     return info;
+}
+
+void oracle_gemm(int n, const double* A, const double* B, double* C) {
+    /* operator*=: rows of A scaled by their 2-norms (scaleMat LEFT), columns of
+     * B by theirs (scaleMat RIGHT), dgemm, the product unscaled by both */
+    std::vector<double> As(A, A + (size_t)n * n), Bs(B, B + (size_t)n * n), sl(n, 0.0), sr(n, 0.0);
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < n; ++r) sl[r] += As[r + (size_t)c * n] * As[r + (size_t)c * n];
+    for (int r = 0; r < n; ++r) sl[r] = std::sqrt(sl[r]);
+#pragma omp parallel for
+    for (int c = 0; c < n; ++c) {
+        double t = 0;
+        for (int r = 0; r < n; ++r) t += Bs[r + (size_t)c * n] * Bs[r + (size_t)c * n];
+        sr[c] = std::sqrt(t);
+        for (int r = 0; r < n; ++r) {
+            As[r + (size_t)c * n] *= 1 / sl[r];
+            Bs[r + (size_t)c * n] *= 1 / sr[c];
+        }
+    }
+    gemm_nn(n, As.data(), Bs.data(), C);
+#pragma omp parallel for
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < n; ++r) C[r + (size_t)c * n] *= sl[r] * sr[c];
 }
 
 long oracle_jtj(int nrows, int ncols, const int* rows, const int* cols, const double* vals,
@@ -751,13 +806,32 @@ extern "C" int oracle_compute(const oracle_options* opt, int nrows, int ncols, c
     dense_sub(U, YWt, Z.data());
     auto t6 = Clock::now();
     st->t_compose_z = secs(t5, t6);
+    if (opt->z_perturb != 0) {
+        /* rounding-level perturbation (test infrastructure, not reference behaviour) */
+        for (int c = 0; c < N; ++c)
+            for (int r = c; r < N; ++r) {
+                uint64_t h = ((uint64_t)r << 32 | (uint32_t)c) * 0x9E3779B97F4A7C15ull;
+                h ^= h >> 29;
+                h *= 0xBF58476D1CE4E5B9ull;
+                h ^= h >> 32;
+                const double u = (double)(h >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+                const double f = 1.0 + opt->z_perturb * u;
+                Z[r + (size_t)c * N] *= f;
+                if (r != c) Z[c + (size_t)r * N] = Z[r + (size_t)c * N];
+            }
+    }
     if (dbg_Z) std::copy(Z.begin(), Z.end(), dbg_Z);
     if (dbg_d) std::copy(d.begin(), d.begin() + N, dbg_d);
 
     /* teInverse: compute.cpp:121-166 */
     double lambda = opt->lambda;
     if (lambda == -1) lambda = std::pow(10, -1.2653 * std::log10(N) - 2.9415);
-    oracle_te_inverse(N, Z.data(), lambda, st);
+    if (opt->skip_dense) {
+        for (int i = 0; i < N; ++i) Z[i + (size_t)i * N] += lambda;  /* timing sample: no inverse */
+        st->lambda = lambda;
+    } else {
+        oracle_te_inverse_route(N, Z.data(), lambda, opt->inverse_route, st);
+    }
     if (dbg_iZ) std::copy(Z.begin(), Z.end(), dbg_iZ);
 
     auto t7 = Clock::now();

@@ -29,6 +29,16 @@ typedef struct {
     int has_pts2fix;
     int faithful_point_scan;  /* 1: per point, scan every J row as compute.cpp:393 does */
     int threads;              /* OpenMP + BLAS threads; 0 = leave as is */
+    int inverse_route;        /* 0: LU as the reference (ScaledDenseMatrix::inv); 1: Cholesky on the
+                                 Jacobi-equilibrated matrix (the CUDA path's route), see below */
+    double z_perturb;         /* 0: none. Otherwise every entry of the Schur complement Z is multiplied
+                                 by (1 + z_perturb * r), r in [-1, 1) from a fixed hash of (row, col),
+                                 symmetric. At z_perturb = 2^-53 this measures how far the results move
+                                 under a rounding-level change of Z (cond(Z + lambda*I) * eps): the
+                                 floor below which two correct FP64 implementations cannot agree. */
+    int skip_dense;           /* timing samples only: 1 skips the dense inverse and the Taylor loop (iZ is
+                                 left as Z + lambda*I), so every sparse stage runs at full size but the
+                                 outputs are meaningless. 0 for results. */
 } oracle_options;
 
 typedef struct {
@@ -68,6 +78,21 @@ int oracle_dense_inv(int n, double* A);
  * Z <- Z + lambda*I, X = inv(Z), iZ = X + sum_i lambda^i/(i-1)! X^(i+1).
  * Z is overwritten with iZ. */
 int oracle_te_inverse(int n, double* Z, double lambda, oracle_stats* st);
+
+/* Cholesky route of the dense inverse (not in the reference; a second FP64
+ * route that measures how far two correct inverses of the same ill-conditioned
+ * Z + lambda*I lie apart): E = diag(A)^-1/2, A_s = E A E, dpotrf + dpotri,
+ * A^-1 = E A_s^-1 E. A is n*n column-major, in place (both triangles).
+ * Returns the LAPACK info. */
+int oracle_dense_inv_cholesky(int n, double* A);
+
+/* oracle_te_inverse with the inverse route chosen (0 LU, 1 Cholesky). */
+int oracle_te_inverse_route(int n, double* Z, double lambda, int route, oracle_stats* st);
+
+/* One dense product of the Taylor loop (operator*=, ScaledDenseMatrix.cpp:314-353:
+ * row and column scaling of A, dgemm, unscaling): C = A * B, all n*n
+ * column-major. For timing samples of the dense stage. */
+void oracle_gemm(int n, const double* A, const double* B, double* C);
 
 /* Number of BLAS threads used by the oracle after set-up. */
 int oracle_set_threads(int threads);

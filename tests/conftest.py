@@ -49,3 +49,28 @@ def block_rel_err(a, b, width):
     den = np.linalg.norm(b, axis=1)
     r = np.where(den > 0, num / np.where(den > 0, den, 1), num)
     return float(r.max()) if r.size else 0.0
+
+
+def fp64_floor(jac, ref_lu, threads=8):
+    """How far two correct FP64 computations of this scene lie apart.
+
+    Z + lambda*I is ill-conditioned (the gauge is fixed only by lambda), so
+    FP64 results are determined only to about cond * eps. Measured on the CPU
+    oracle: the Cholesky inverse route against the LU route (same Z), and the
+    LU route on the Jacobian with every value moved by at most one ulp (two
+    seeds): rounding-level input noise, which is what a different summation
+    order in the assembly amounts to. Returns (camera floor, point floor,
+    details)."""
+    import copy
+
+    import oracle
+    det = {}
+    chol = oracle.compute(jac, threads=threads, route="cholesky")
+    det["cholesky"] = (block_rel_err(chol["cam"], ref_lu["cam"], 45), block_rel_err(chol["pt"], ref_lu["pt"], 6))
+    for seed in (1, 2):
+        j2 = copy.copy(jac)
+        r = np.random.default_rng(seed).uniform(-1.0, 1.0, jac.values.size)
+        j2.values = jac.values * (1.0 + 2.0 ** -52 * r)
+        o = oracle.compute(j2, threads=threads)
+        det[f"ulp{seed}"] = (block_rel_err(o["cam"], ref_lu["cam"], 45), block_rel_err(o["pt"], ref_lu["pt"], 6))
+    return max(v[0] for v in det.values()), max(v[1] for v in det.values()), det, chol

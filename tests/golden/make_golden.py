@@ -1,9 +1,9 @@
 """Generate the golden fixtures in this folder from the reference's own test data.
 
-Run once in a checkout that has the uncertaintyTE sources (read-only) at
-REFERENCE_ROOT (default /root/reference):
+Run once with the uncertaintyTE source tree (read-only) named by the
+REFERENCE_ROOT environment variable:
 
-    python tests/golden/make_golden.py
+    REFERENCE_ROOT=<uncertaintyTE checkout> python tests/golden/make_golden.py
 
 It converts the reference's text fixtures into compressed .npz files so the
 tests do not need the reference tree at run time:
@@ -15,6 +15,9 @@ tests do not need the reference tree at run time:
   multipl_01.npz  test/SparseMatrix/multipl_in_01.txt -> multipl_out_01.txt (J^T J)
   inv_sparse_01.npz, inv_dense_01.npz
                   test/{SparseMatrix,DenseMatrix}/inv_in_01.txt -> inv_out_01.txt
+  eigvalues.npz   the expected arrays of src/test_eigValues/covarianceEigenValues_test.cpp
+                  (Uncertainty accessors on test/EigValues/output.cov): camera #5 and point
+                  #143 matrices, all camera / point matrices, all camera / point eigenvalues
 """
 from __future__ import annotations
 
@@ -28,7 +31,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from uncertaintyte_b200.jacob import load_cov, load_jacob  # noqa: E402
 
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("REFERENCE_ROOT", "")
 
 
 def _jac_arrays(j):
@@ -60,7 +63,17 @@ def _dense(path, header):
     return t.reshape(n, m)
 
 
+def _res_arrays(path):
+    """The `static const double res[] = { ... };` arrays of a test source, in order."""
+    import re
+    txt = open(path).read()
+    return [np.array([float(x) for x in body.replace("\n", " ").split(",") if x.strip()])
+            for body in re.findall(r"static const double res\[\]\s*=\s*\{(.*?)\};", txt, flags=re.S)]
+
+
 def main():
+    if not REF:
+        sys.exit("set REFERENCE_ROOT to the uncertaintyTE source tree")
     T = os.path.join(REF, "test")
     j = load_jacob(os.path.join(T, "input_jacobians/04_Daliborka.jacob"))
     hdr, cam, pt = load_cov(os.path.join(T, "EigValues/output.cov"), j.num_cams, j.cam_params)
@@ -79,6 +92,11 @@ def main():
         A = _dense(os.path.join(T, d, "inv_in_01.txt"), h)
         B = _dense(os.path.join(T, d, "inv_out_01.txt"), h)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), A=A, Ainv=B)
+    cam5, pt143, cams, pts, cam_eig, pt_eig = _res_arrays(
+        os.path.join(REF, "src", "test_eigValues", "covarianceEigenValues_test.cpp"))
+    np.savez_compressed(os.path.join(HERE, "eigvalues.npz"), cam5=cam5.reshape(9, 9), pt143=pt143.reshape(3, 3),
+                        cams=cams.reshape(-1, 9, 9), pts=pts.reshape(-1, 3, 3), cam_eig=cam_eig.reshape(-1, 9),
+                        pt_eig=pt_eig.reshape(-1, 3))
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

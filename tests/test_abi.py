@@ -81,3 +81,14 @@ def test_workspace_estimate_scales_with_cameras():
     b = native.workspace_bytes(jac)
     n = 9 * jac.num_cams
     assert b > 4 * n * n * 8  # four dense N x N buffers
+
+
+def test_cpp_dropin_caller_compiles_and_links(tmp_path):
+    """A C++ caller of include/uncertainty.h builds against libuncte.so (the GPU
+    tests run it)."""
+    exe = str(tmp_path / "dropin_check")
+    libdir = os.path.join(ROOT, "uncertaintyte_b200")
+    subprocess.run(["g++", "-O1", "-std=c++17", "-Wall", "-Werror", "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "dropin_check.cpp"), "-o", exe, "-L" + libdir, "-luncte",
+                    "-Wl,-rpath," + libdir], check=True)
+    assert os.path.exists(exe)

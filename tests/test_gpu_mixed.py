@@ -1,13 +1,15 @@
 """Mixed-precision Taylor products (int8-sliced tcgen05 GEMMs) against the
-FP64 GPU path and against torch FP64 products (needs a B200).
+FP64 CPU oracle, the FP64 GPU path and torch FP64 products (needs a B200).
 
 Tolerance: the accuracy target of the mixed path is a maximum relative
 Frobenius error of 1e-6 per camera 9x9 block and per point 3x3 block against
-the FP64 result; MIXED_TOL below is that bar.
+the FP64 oracle (the reference's algorithm on the CPU); MIXED_TOL below is that
+bar. The mixed path is also held to it against the FP64 GPU path.
 """
 import numpy as np
 import pytest
 
+import oracle
 from conftest import block_rel_err, golden_jacobian
 from uncertaintyte_b200 import native, scenes
 
@@ -30,7 +32,11 @@ def _mixed_vs_fp64(jac, ctx, precision="mixed"):
     # the stop-rule values come from the products' max |entry|: same ~1e-8..1e-6 agreement
     np.testing.assert_allclose(smp["cycle_change"], s64["cycle_change"], rtol=1e-5)
     ec, ep = block_rel_err(cmp_, c64, 45), block_rel_err(pmp, p64, 6)
-    print(f"{precision}: cams {ec:.3e} points {ep:.3e}")
+    ref = oracle.compute(jac, threads=8)
+    oc, op = block_rel_err(cmp_, ref["cam"], 45), block_rel_err(pmp, ref["pt"], 6)
+    assert smp["te_iterations"] == ref["stats"].te_iterations
+    print(f"{precision}: vs FP64 GPU cams {ec:.3e} points {ep:.3e}; vs FP64 oracle cams {oc:.3e} points {op:.3e}")
+    assert oc < MIXED_TOL and op < MIXED_TOL
     return ec, ep
 
 

@@ -56,3 +56,39 @@ def test_task_inverse_reports_indefinite_input():
     # the schedule drained: the next call on the device works
     A = _spd(200, 4)
     assert np.max(np.abs(_inverse(A) @ A - np.eye(200))) < 1e-10
+
+
+def _bounded(A, poll_limit, skip_task):
+    import torch
+    n = A.shape[0]
+    lda = (n + 7) & ~7
+    buf = torch.zeros((n, lda), dtype=torch.float64, device="cuda")
+    buf[:, :n] = torch.from_numpy(np.ascontiguousarray(A.T))
+    native.spd_inverse_tasks_bounded(buf.data_ptr(), n, lda, poll_limit, skip_task)
+    torch.cuda.synchronize()
+    return buf[:, :n].cpu().numpy().T
+
+
+def test_bounded_wait_runs_out_and_the_device_stays_usable():
+    """A schedule with one update task left out can never publish that tile's
+    counter, so the tasks after it wait on a flag that nothing sets. With the
+    waits limited to a few polls the launch must drain and the call return
+    UNC_ERR_CUDA (a bounded wait ran out); the next calls on the device work."""
+    import ctypes
+    n = 640  # 10 x 10 tiles
+    cnt = native.lib().unc_spd_task_list(n, None, 0)
+    tasks = (ctypes.c_int * (4 * cnt))()
+    native.lib().unc_spd_task_list(n, tasks, cnt)
+    kinds = np.frombuffer(tasks, dtype=np.int32).reshape(-1, 4)[:, 0]
+    skip = int(np.flatnonzero(kinds == 2)[0])  # the first trailing update
+    A = _spd(n, 11)
+    with pytest.raises(native.UncError) as e:
+        _bounded(A, 2000, skip)
+    assert e.value.status == -4  # UNC_ERR_CUDA
+    assert "ran out" in str(e.value)
+    # the same entry point with the full schedule, then the regular inverse
+    ref = np.linalg.inv(A)
+    got = _bounded(A, 1 << 22, -1)
+    assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < TOL
+    got = _inverse(A)
+    assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < TOL

@@ -93,3 +93,24 @@ def test_oracle_svd_path_runs_on_toy():
     # next few all at the FP64 noise floor (~1e-15 of the largest), so the two
     # LAPACK SVD drivers only agree to a few 1e-3 on the pseudo-inverse.
     assert block_rel_err(out1["cam"], out["cam"], 45) < 1e-2
+
+
+def test_oracle_gemm_and_cholesky_route():
+    """The dense product restated from operator*= (scaling, dgemm, unscaling) and
+    the Cholesky route of the inverse agree with numpy; on Daliborka the two
+    inverse routes give the same iteration count and results at the FP64 floor."""
+    import oracle
+    rng = np.random.default_rng(5)
+    A, B = rng.standard_normal((300, 300)), rng.standard_normal((300, 300))
+    C = oracle.gemm(A, B)
+    assert np.max(np.abs(C - A @ B)) / np.max(np.abs(A @ B)) < 1e-13
+    S = A @ A.T + 300 * np.eye(300)
+    Si, info = oracle.dense_inv_cholesky(S)
+    assert info == 0 and np.max(np.abs(Si - np.linalg.inv(S))) / np.max(np.abs(np.linalg.inv(S))) < 1e-13
+    from conftest import block_rel_err, golden_jacobian
+    jac = golden_jacobian("daliborka")
+    lu = oracle.compute(jac, threads=8)
+    ch = oracle.compute(jac, threads=8, route="cholesky")
+    assert ch["stats"].te_iterations == lu["stats"].te_iterations == 14
+    assert block_rel_err(ch["cam"], lu["cam"], 45) < 1e-8
+    assert block_rel_err(ch["pt"], lu["pt"], 6) < 1e-8

@@ -550,6 +550,47 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     return UNC_OK;
 }
 
+// SDM::inv on the GPU (unc_dense_inverse_device). poll_limit / skip_task are
+// passed to the tile-task form (n <= 3584): 0 / -1 for the regular schedule.
+int dense_inverse(double* d_A, int n, int lda, void* stream, long long poll_limit, int skip_task) {
+    g_last_error.clear();
+    if (!d_A || n <= 0 || lda < n || (lda & 1)) return fail(UNC_ERR_INVALID_ARG, "bad matrix arguments");
+    cudaStream_t sm = (cudaStream_t)stream;
+    const size_t mat = (size_t)lda * n;
+    // n <= 3584: the tile-task inverse (one persistent kernel), else the recursive form
+    const bool tasks = spd_tasks_apply(n);
+    if (tasks)
+        if (int r = spd_tasks_prepare(n)) return fail(r, "tile-task inverse: cannot upload the task list");
+    const size_t small_d = std::max(chol_small_doubles(n), (spd_task_state_ints(n) + 1) / 2);
+    const size_t wsd = 3 * mat + small_d + (size_t)n + 64;
+    double* ws = nullptr;
+    CK(cudaMalloc(&ws, wsd * sizeof(double) + 256));
+    double *T = ws, *W = ws + mat, *Tt = ws + 2 * mat, *small = ws + 3 * mat;
+    double* e = small + small_d;
+    int* err = reinterpret_cast<int*>(ws + wsd);
+    int h_err = 0;
+    cudaError_t ce = cudaMemsetAsync(ws, 0, wsd * sizeof(double) + 256, sm);
+    if (ce == cudaSuccess) {
+        launch_shift_equilibrate(d_A, n, lda, 0.0, e, err, sm);
+        if (tasks) {
+            if (chol_inverse_tasks(d_A, n, lda, T, W, reinterpret_cast<int*>(small), err, sm, device_sms(),
+                                   poll_limit, skip_task) != UNC_OK)
+                ce = cudaErrorUnknown;
+            launch_unequilibrate_from(W, d_A, n, lda, e, nullptr, sm);
+        } else {
+            chol_inverse(d_A, n, lda, T, W, Tt, small, err, sm);
+            launch_unequilibrate(d_A, n, lda, e, nullptr, sm);
+        }
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, sm);
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(sm);
+    cudaFree(ws);
+    if (ce != cudaSuccess) return fail(UNC_ERR_CUDA, cudaGetErrorString(ce));
+    if (h_err & ERRBIT_TIMEOUT) return fail(UNC_ERR_CUDA, "a bounded device wait of the tile-task inverse ran out");
+    if (h_err & (ERRBIT_SINGULAR | ERRBIT_NONFINITE)) return fail(UNC_ERR_SINGULAR, "matrix is not positive definite");
+    return UNC_OK;
+}
+
 Plan make_plan(const unc_options* o, int num_rows) {
     Plan pl;
     pl.C = o->num_cams;
@@ -890,41 +931,14 @@ int unc_compute_scene(unc_context* ctx, const unc_options* o, const double* cams
 }
 
 int unc_dense_inverse_device(double* d_A, int n, int lda, void* stream) {
+    return dense_inverse(d_A, n, lda, stream, 0, -1);
+}
+
+int unc_spd_inverse_tasks_bounded(double* d_A, int n, int lda, long long poll_limit, int skip_task, void* stream) {
     g_last_error.clear();
-    if (!d_A || n <= 0 || lda < n || (lda & 1)) return fail(UNC_ERR_INVALID_ARG, "bad matrix arguments");
-    cudaStream_t sm = (cudaStream_t)stream;
-    const size_t mat = (size_t)lda * n;
-    // n <= 3584: the tile-task inverse (one persistent kernel), else the recursive form
-    const bool tasks = spd_tasks_apply(n);
-    if (tasks)
-        if (int r = spd_tasks_prepare(n)) return fail(r, "tile-task inverse: cannot upload the task list");
-    const size_t small_d = std::max(chol_small_doubles(n), (spd_task_state_ints(n) + 1) / 2);
-    const size_t wsd = 3 * mat + small_d + (size_t)n + 64;
-    double* ws = nullptr;
-    CK(cudaMalloc(&ws, wsd * sizeof(double) + 256));
-    double *T = ws, *W = ws + mat, *Tt = ws + 2 * mat, *small = ws + 3 * mat;
-    double* e = small + small_d;
-    int* err = reinterpret_cast<int*>(ws + wsd);
-    int h_err = 0;
-    cudaError_t ce = cudaMemsetAsync(ws, 0, wsd * sizeof(double) + 256, sm);
-    if (ce == cudaSuccess) {
-        launch_shift_equilibrate(d_A, n, lda, 0.0, e, err, sm);
-        if (tasks) {
-            if (chol_inverse_tasks(d_A, n, lda, T, W, reinterpret_cast<int*>(small), err, sm) != UNC_OK)
-                ce = cudaErrorUnknown;
-            launch_unequilibrate_from(W, d_A, n, lda, e, nullptr, sm);
-        } else {
-            chol_inverse(d_A, n, lda, T, W, Tt, small, err, sm);
-            launch_unequilibrate(d_A, n, lda, e, nullptr, sm);
-        }
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, sm);
-    }
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(sm);
-    cudaFree(ws);
-    if (ce != cudaSuccess) return fail(UNC_ERR_CUDA, cudaGetErrorString(ce));
-    if (h_err & ERRBIT_TIMEOUT) return fail(UNC_ERR_CUDA, "a bounded device wait of the tile-task inverse ran out");
-    if (h_err & (ERRBIT_SINGULAR | ERRBIT_NONFINITE)) return fail(UNC_ERR_SINGULAR, "matrix is not positive definite");
-    return UNC_OK;
+    if (!spd_tasks_apply(n)) return fail(UNC_ERR_INVALID_ARG, "the tile-task inverse takes n in 1..3584");
+    if (poll_limit < 1 || poll_limit > (1LL << 22)) return fail(UNC_ERR_INVALID_ARG, "poll_limit must be in 1..2^22");
+    return dense_inverse(d_A, n, lda, stream, poll_limit, skip_task);
 }
 
 int unc_jtj_crs(int num_rows, int num_cols, const int* rows, const int* cols, const double* values,

@@ -20,8 +20,6 @@
 
 namespace {
 
-// JacobianIO::loadJacobian (JacobianIO.cpp:32-63) with a fast tokenizer;
-// '#' starts a comment (the documented template carries some).
 // JacobianIO::loadJacobian (JacobianIO.cpp:32-63) through the library's
 // parser: text (all host threads) or this library's binary form.
 bool load_jacob(const std::string& path, cov::Options& opt, ceres::CRSMatrix& J) {

@@ -26,6 +26,7 @@
 // Counters (ints, zeroed before the launch): cursor, abort flag, then per
 // lower tile: ver (updates applied to A), lrdy (L final / T(k,k) ready),
 // tacc (W accumulations), trdy (T final), pacc (O accumulations).
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -54,9 +55,10 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
     return v;
 }
 
-// thread 0 only: wait until *flag >= v (or the abort flag is raised / the limit runs out)
-__device__ bool wait_ge(const int* flag, int v, const int* abort) {
-    for (long it = 0; it < kDagSpin; ++it) {
+// thread 0 only: wait until *flag >= v (or the abort flag is raised / the
+// limit of `spin` polls runs out)
+__device__ bool wait_ge(const int* flag, int v, const int* abort, long spin) {
+    for (long it = 0; it < spin; ++it) {
         if (ld_acquire(flag) >= v) return true;
         if (ld_acquire(abort)) return false;
         __nanosleep(32);
@@ -130,13 +132,14 @@ __device__ __forceinline__ void store_tile(double* X, long ld, int vr, int vc, c
             }
 }
 
-__global__ void __launch_bounds__(DAG_THREADS, 1)
-    k_spd_inverse_tasks(double* A, double* T, double* O, int n, long ld, const int4* __restrict__ tasks, int ntasks,
-                        int* state, int ntri, int* err) {
-    extern __shared__ __align__(16) double sm[];
-    __shared__ int s_task, s_ok;
-    int* const cursor = state;
-    int* const abort = state + 1;
+// One tile task (type, i, j, k) of the n x n matrix whose tiles A, T, O and
+// counters (`state`, laid out as described at the top) are given, run by all
+// DAG_THREADS threads of the block; thread 0 waits for its dependencies first.
+// Returns false when a wait gave up (ERRBIT_TIMEOUT and the abort flag are
+// set): the caller stops taking tasks.
+__device__ __forceinline__ bool run_task(double* A, double* T, double* O, int n, long ld, int* state, int ntri,
+                                         int* err, int* abort, long spin, int type, int i, int j, int k, double* sm,
+                                         int& s_ok) {
     int* const ver = state + 4;
     int* const lrdy = ver + ntri;
     int* const tacc = lrdy + ntri;
@@ -150,154 +153,195 @@ __global__ void __launch_bounds__(DAG_THREADS, 1)
     auto ext = [n](int b) { return min(TB, n - TB * b); };
     auto kext = [n](int b) { return (min(TB, n - TB * b) + 3) & ~3; };  // K extent of a partial tile, DMMA steps
     auto tile = [ld](double* M, int i, int j) { return M + (long)TB * i + (long)TB * j * ld; };
-    while (true) {
-        if (tid == 0) s_task = atomicAdd(cursor, 1);
+    if (tid == 0) {
+        bool ok = true;
+        switch (type) {
+            case K_POTRF:  // its last update (from panel k-1) is applied inside the task
+                ok = k == 0 || (wait_ge(ver + tri(k, k), k - 1, abort, spin) &&
+                                wait_ge(lrdy + tri(k, k - 1), 1, abort, spin));
+                break;
+            case K_TRSM:
+                ok = wait_ge(ver + tri(i, k), k, abort, spin) && wait_ge(lrdy + tri(k, k), 1, abort, spin);
+                break;
+            case K_UPDATE:
+                ok = wait_ge(ver + tri(i, j), k, abort, spin) && wait_ge(lrdy + tri(i, k), 1, abort, spin) &&
+                     wait_ge(lrdy + tri(j, k), 1, abort, spin);
+                break;
+            case K_TACC:
+                ok = wait_ge(tacc + tri(i, j), k - j, abort, spin) && wait_ge(lrdy + tri(i, k), 1, abort, spin) &&
+                     wait_ge(trdy + tri(k, j), 1, abort, spin);
+                break;
+            case K_TFIN:
+                ok = wait_ge(tacc + tri(i, j), i - j, abort, spin) && wait_ge(trdy + tri(i, i), 1, abort, spin);
+                break;
+            default:  // K_PACC
+                ok = wait_ge(pacc + tri(i, j), k - i, abort, spin) && wait_ge(trdy + tri(k, i), 1, abort, spin) &&
+                     wait_ge(trdy + tri(k, j), 1, abort, spin);
+                break;
+        }
+        if (!ok) {
+            atomicOr(err, ERRBIT_TIMEOUT);
+            atomicExch(abort, 1);
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    if (!s_ok) return false;
+    if (type == K_POTRF) {
+        // A(k,k) -= L(k,k-1) L(k,k-1)^T applied to the leaf's block (both tiles loaded
+        // together), the leaf, T(k,k) published, then L(k+1,k) = A(k+1,k) T(k,k)^T with
+        // T(k,k) still in shared memory
+        double* lsm = sm + 2 * TB * TLD;
+        chol_leaf_load(A, ld, TB * k, ext(k), lsm);
+        if (k > 0) {
+            double acc[2][2][2] = {};
+            load_tile(As, tile(A, k, k - 1), ld, ext(k), ext(k - 1), tid);
+            __syncthreads();
+            if (wn <= wm) tile_mma<false, true>(As, As, wm, wn, g, t4, 0, TB, acc);  // lower blocks only
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int r = wm + 8 * a + g, c = wn + 8 * b + 2 * t4 + h;
+                        if (c <= r) lsm[r * LEAF_LD + c] -= acc[a][b][h];
+                    }
+        }
         __syncthreads();
-        const int task = s_task;
-        if (task >= ntasks) break;
-        const int4 tk = tasks[task];
-        const int type = tk.x, i = tk.y, j = tk.z, k = tk.w;
+        chol_leaf_factor(TB * k, ext(k), T, ld, err, lsm);
+        __syncthreads();
         if (tid == 0) {
-            bool ok = true;
-            switch (type) {
-                case K_POTRF:  // its last update (from panel k-1) is applied inside the task
-                    ok = k == 0 || (wait_ge(ver + tri(k, k), k - 1, abort) && wait_ge(lrdy + tri(k, k - 1), 1, abort));
-                    break;
-                case K_TRSM: ok = wait_ge(ver + tri(i, k), k, abort) && wait_ge(lrdy + tri(k, k), 1, abort); break;
-                case K_UPDATE:
-                    ok = wait_ge(ver + tri(i, j), k, abort) && wait_ge(lrdy + tri(i, k), 1, abort) &&
-                         wait_ge(lrdy + tri(j, k), 1, abort);
-                    break;
-                case K_TACC:
-                    ok = wait_ge(tacc + tri(i, j), k - j, abort) && wait_ge(lrdy + tri(i, k), 1, abort) &&
-                         wait_ge(trdy + tri(k, j), 1, abort);
-                    break;
-                case K_TFIN: ok = wait_ge(tacc + tri(i, j), i - j, abort) && wait_ge(trdy + tri(i, i), 1, abort); break;
-                default:  // K_PACC
-                    ok = wait_ge(pacc + tri(i, j), k - i, abort) && wait_ge(trdy + tri(k, i), 1, abort) &&
-                         wait_ge(trdy + tri(k, j), 1, abort);
-                    break;
-            }
+            __threadfence();
+            atomicExch(lrdy + tri(k, k), 1);
+            atomicExch(trdy + tri(k, k), 1);
+        }
+        if (k + 1 >= (n + TB - 1) / TB) return true;
+        if (tid == 0) {
+            const bool ok = wait_ge(ver + tri(k + 1, k), k, abort, spin);
             if (!ok) {
                 atomicOr(err, ERRBIT_TIMEOUT);
                 atomicExch(abort, 1);
             }
             s_ok = ok;
         }
+        const double* Tl = lsm + NB * LEAF_LD;  // T(r, c) at Tl[r * LEAF_LD + c], lower triangle valid
+        for (int e = tid; e < TB * TB; e += DAG_THREADS) {
+            const int r = e & (TB - 1), c = e >> 6;
+            Bs[c * TLD + r] = r >= c ? Tl[r * LEAF_LD + c] : 0.0;
+        }
         __syncthreads();
-        if (!s_ok) break;
-        if (type == K_POTRF) {
-            // A(k,k) -= L(k,k-1) L(k,k-1)^T applied to the leaf's block (both tiles loaded
-            // together), the leaf, T(k,k) published, then L(k+1,k) = A(k+1,k) T(k,k)^T with
-            // T(k,k) still in shared memory
-            double* lsm = sm + 2 * TB * TLD;
-            chol_leaf_load(A, ld, TB * k, ext(k), lsm);
-            if (k > 0) {
-                double acc[2][2][2] = {};
-                load_tile(As, tile(A, k, k - 1), ld, ext(k), ext(k - 1), tid);
+        if (!s_ok) return false;
+        load_tile(As, tile(A, k + 1, k), ld, ext(k + 1), ext(k), tid);
+        __syncthreads();
+        double acc[2][2][2] = {};
+        tile_mma<false, true>(As, Bs, wm, wn, g, t4, 0, wn + 16, acc);
+        store_tile(tile(A, k + 1, k), ld, ext(k + 1), ext(k), acc, 1.0, false, nullptr, wm, wn, g, t4);
+    } else {
+        double acc[2][2][2] = {};
+        switch (type) {
+            case K_TRSM:  // L(i,k) = A(i,k) T(k,k)^T; T(k,k) lower: terms k' <= n only
+                load_tile(As, tile(A, i, k), ld, ext(i), ext(k), tid);
+                load_tile(Bs, tile(T, k, k), ld, ext(k), ext(k), tid);
                 __syncthreads();
-                if (wn <= wm) tile_mma<false, true>(As, As, wm, wn, g, t4, 0, TB, acc);  // lower blocks only
-#pragma unroll
-                for (int a = 0; a < 2; ++a)
-#pragma unroll
-                    for (int b = 0; b < 2; ++b)
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            const int r = wm + 8 * a + g, c = wn + 8 * b + 2 * t4 + h;
-                            if (c <= r) lsm[r * LEAF_LD + c] -= acc[a][b][h];
-                        }
-            }
-            __syncthreads();
-            chol_leaf_factor(TB * k, ext(k), T, ld, err, lsm);
-            __syncthreads();
-            if (tid == 0) {
-                __threadfence();
-                atomicExch(lrdy + tri(k, k), 1);
-                atomicExch(trdy + tri(k, k), 1);
-            }
-            if (k + 1 >= (n + TB - 1) / TB) continue;
-            if (tid == 0) {
-                const bool ok = wait_ge(ver + tri(k + 1, k), k, abort);
-                if (!ok) {
-                    atomicOr(err, ERRBIT_TIMEOUT);
-                    atomicExch(abort, 1);
-                }
-                s_ok = ok;
-            }
-            const double* Tl = lsm + NB * LEAF_LD;  // T(r, c) at Tl[r * LEAF_LD + c], lower triangle valid
-            for (int e = tid; e < TB * TB; e += DAG_THREADS) {
-                const int r = e & (TB - 1), c = e >> 6;
-                Bs[c * TLD + r] = r >= c ? Tl[r * LEAF_LD + c] : 0.0;
-            }
-            __syncthreads();
-            if (!s_ok) break;
-            load_tile(As, tile(A, k + 1, k), ld, ext(k + 1), ext(k), tid);
-            __syncthreads();
-            double acc[2][2][2] = {};
-            tile_mma<false, true>(As, Bs, wm, wn, g, t4, 0, wn + 16, acc);
-            store_tile(tile(A, k + 1, k), ld, ext(k + 1), ext(k), acc, 1.0, false, nullptr, wm, wn, g, t4);
-        } else {
-            double acc[2][2][2] = {};
-            switch (type) {
-                case K_TRSM:  // L(i,k) = A(i,k) T(k,k)^T; T(k,k) lower: terms k' <= n only
-                    load_tile(As, tile(A, i, k), ld, ext(i), ext(k), tid);
-                    load_tile(Bs, tile(T, k, k), ld, ext(k), ext(k), tid);
-                    __syncthreads();
-                    tile_mma<false, true>(As, Bs, wm, wn, g, t4, 0, min(wn + 16, kext(k)), acc);
-                    __syncthreads();
-                    store_tile(tile(A, i, k), ld, ext(i), ext(k), acc, 1.0, false, nullptr, wm, wn, g, t4);
-                    break;
-                case K_UPDATE:  // A(i,j) -= L(i,k) L(j,k)^T
-                    load_tile(As, tile(A, i, k), ld, ext(i), ext(k), tid);
-                    load_tile(Bs, tile(A, j, k), ld, ext(j), ext(k), tid);
-                    __syncthreads();
-                    tile_mma<false, true>(As, Bs, wm, wn, g, t4, 0, kext(k), acc);
-                    store_tile(tile(A, i, j), ld, ext(i), ext(j), acc, -1.0, true, nullptr, wm, wn, g, t4);
-                    break;
-                case K_TACC:  // W(i,j) += L(i,k) T(k,j); T(j,j) lower: terms k' >= n only
-                    load_tile(As, tile(A, i, k), ld, ext(i), ext(k), tid);
-                    load_tile(Bs, tile(T, k, j), ld, ext(k), ext(j), tid);
-                    __syncthreads();
-                    tile_mma<false, false>(As, Bs, wm, wn, g, t4, k == j ? wn : 0, kext(k), acc);
-                    store_tile(tile(T, i, j), ld, ext(i), ext(j), acc, 1.0, k > j, nullptr, wm, wn, g, t4);
-                    break;
-                case K_TFIN:  // T(i,j) = -T(i,i) W(i,j); T(i,i) lower: terms k' <= m only
-                    load_tile(As, tile(T, i, i), ld, ext(i), ext(i), tid);
-                    load_tile(Bs, tile(T, i, j), ld, ext(i), ext(j), tid);
-                    __syncthreads();
-                    tile_mma<false, false>(As, Bs, wm, wn, g, t4, 0, min(wm + 16, kext(i)), acc);
-                    __syncthreads();
-                    store_tile(tile(T, i, j), ld, ext(i), ext(j), acc, -1.0, false, nullptr, wm, wn, g, t4);
-                    break;
-                default: {  // K_PACC: O(i,j) += T(k,i)^T T(k,j); diagonal T tiles lower
-                    load_tile(As, tile(T, k, i), ld, ext(k), ext(i), tid);
-                    load_tile(Bs, tile(T, k, j), ld, ext(k), ext(j), tid);
-                    __syncthreads();
-                    int kb = 0;
-                    if (k == i) kb = wm;
-                    if (k == j) kb = max(kb, wn);
-                    tile_mma<true, false>(As, Bs, wm, wn, g, t4, kb, kext(k), acc);
-                    const bool last = k == (n + TB - 1) / TB - 1;
-                    store_tile(tile(O, i, j), ld, ext(i), ext(j), acc, 1.0, k > i,
-                               (last && i > j) ? tile(O, j, i) : nullptr, wm, wn, g, t4);
-                    break;
-                }
+                tile_mma<false, true>(As, Bs, wm, wn, g, t4, 0, min(wn + 16, kext(k)), acc);
+                __syncthreads();
+                store_tile(tile(A, i, k), ld, ext(i), ext(k), acc, 1.0, false, nullptr, wm, wn, g, t4);
+                break;
+            case K_UPDATE:  // A(i,j) -= L(i,k) L(j,k)^T
+                load_tile(As, tile(A, i, k), ld, ext(i), ext(k), tid);
+                load_tile(Bs, tile(A, j, k), ld, ext(j), ext(k), tid);
+                __syncthreads();
+                tile_mma<false, true>(As, Bs, wm, wn, g, t4, 0, kext(k), acc);
+                store_tile(tile(A, i, j), ld, ext(i), ext(j), acc, -1.0, true, nullptr, wm, wn, g, t4);
+                break;
+            case K_TACC:  // W(i,j) += L(i,k) T(k,j); T(j,j) lower: terms k' >= n only
+                load_tile(As, tile(A, i, k), ld, ext(i), ext(k), tid);
+                load_tile(Bs, tile(T, k, j), ld, ext(k), ext(j), tid);
+                __syncthreads();
+                tile_mma<false, false>(As, Bs, wm, wn, g, t4, k == j ? wn : 0, kext(k), acc);
+                store_tile(tile(T, i, j), ld, ext(i), ext(j), acc, 1.0, k > j, nullptr, wm, wn, g, t4);
+                break;
+            case K_TFIN:  // T(i,j) = -T(i,i) W(i,j); T(i,i) lower: terms k' <= m only
+                load_tile(As, tile(T, i, i), ld, ext(i), ext(i), tid);
+                load_tile(Bs, tile(T, i, j), ld, ext(i), ext(j), tid);
+                __syncthreads();
+                tile_mma<false, false>(As, Bs, wm, wn, g, t4, 0, min(wm + 16, kext(i)), acc);
+                __syncthreads();
+                store_tile(tile(T, i, j), ld, ext(i), ext(j), acc, -1.0, false, nullptr, wm, wn, g, t4);
+                break;
+            default: {  // K_PACC: O(i,j) += T(k,i)^T T(k,j); diagonal T tiles lower
+                load_tile(As, tile(T, k, i), ld, ext(k), ext(i), tid);
+                load_tile(Bs, tile(T, k, j), ld, ext(k), ext(j), tid);
+                __syncthreads();
+                int kb = 0;
+                if (k == i) kb = wm;
+                if (k == j) kb = max(kb, wn);
+                tile_mma<true, false>(As, Bs, wm, wn, g, t4, kb, kext(k), acc);
+                const bool last = k == (n + TB - 1) / TB - 1;
+                store_tile(tile(O, i, j), ld, ext(i), ext(j), acc, 1.0, k > i,
+                           (last && i > j) ? tile(O, j, i) : nullptr, wm, wn, g, t4);
+                break;
             }
         }
-        // release: the barrier orders every thread's tile writes before thread 0's
-        // gpu-scope fence, which orders them before the counter
+    }
+    // release: the barrier orders every thread's tile writes before thread 0's
+    // gpu-scope fence, which orders them before the counter
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        switch (type) {
+            case K_POTRF: atomicExch(lrdy + tri(k + 1, k), 1); break;  // the fused L(k+1,k)
+            case K_TRSM: atomicExch(lrdy + tri(i, k), 1); break;
+            case K_UPDATE: atomicAdd(ver + tri(i, j), 1); break;
+            case K_TACC: atomicAdd(tacc + tri(i, j), 1); break;
+            case K_TFIN: atomicExch(trdy + tri(i, j), 1); break;
+            default: atomicAdd(pacc + tri(i, j), 1); break;
+        }
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(DAG_THREADS, 1)
+    k_spd_inverse_tasks(double* A, double* T, double* O, int n, long ld, const int4* __restrict__ tasks, int ntasks,
+                        int* state, int ntri, int* err, long spin) {
+    extern __shared__ __align__(16) double sm[];
+    __shared__ int s_task, s_ok;
+    int* const cursor = state;
+    int* const abort = state + 1;
+    while (true) {
+        if (threadIdx.x == 0) s_task = atomicAdd(cursor, 1);
         __syncthreads();
-        if (tid == 0) {
-            __threadfence();
-            switch (type) {
-                case K_POTRF: atomicExch(lrdy + tri(k + 1, k), 1); break;  // the fused L(k+1,k)
-                case K_TRSM: atomicExch(lrdy + tri(i, k), 1); break;
-                case K_UPDATE: atomicAdd(ver + tri(i, j), 1); break;
-                case K_TACC: atomicAdd(tacc + tri(i, j), 1); break;
-                case K_TFIN: atomicExch(trdy + tri(i, j), 1); break;
-                default: atomicAdd(pacc + tri(i, j), 1); break;
-            }
-        }
+        const int task = s_task;
+        if (task >= ntasks) break;
+        const int4 tk = tasks[task];
+        if (!run_task(A, T, O, n, ld, state, ntri, err, abort, spin, tk.x, tk.y, tk.z, tk.w, sm, s_ok)) break;
+    }
+}
+
+// The same schedule over the tile tasks of many matrices (a batch of
+// reconstructions) in one persistent launch: task.x = type + 8 * matrix, the
+// matrices' descriptors in `mats`, their counters at mats[m].state, one cursor
+// and one abort flag (ctl[0], ctl[1]) for the whole list. The list interleaves
+// the matrices' own topological orders, so every dependency of a task is still
+// earlier in the list and the launch completes with any number of resident
+// CTAs; each task does exactly the arithmetic of the single-matrix kernel, so
+// the results are bitwise those of one launch per matrix.
+__global__ void __launch_bounds__(DAG_THREADS, 1)
+    k_spd_inverse_tasks_grouped(const SpdTaskMatrix* __restrict__ mats, const int4* __restrict__ tasks, int ntasks,
+                                int* ctl, long spin) {
+    extern __shared__ __align__(16) double sm[];
+    __shared__ int s_task, s_ok;
+    while (true) {
+        if (threadIdx.x == 0) s_task = atomicAdd(ctl, 1);
+        __syncthreads();
+        const int task = s_task;
+        if (task >= ntasks) break;
+        const int4 tk = tasks[task];
+        const SpdTaskMatrix& m = mats[tk.x >> 3];
+        if (!run_task(m.A, m.T, m.O, m.n, m.ld, m.state, m.ntri, m.err, ctl + 1, spin, tk.x & 7, tk.y, tk.z, tk.w, sm,
+                      s_ok))
+            break;
     }
 }
 
@@ -385,7 +429,7 @@ int spd_tasks_prepare(int n) {
 }
 
 int chol_inverse_tasks(double* A, int n, int lda, double* T, double* O, int* state, int* err, cudaStream_t st,
-                       int max_ctas) {
+                       int max_ctas, long long poll_limit, int skip_task) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return UNC_ERR_CUDA;
     const int nt = (n + TB - 1) / TB;
@@ -399,9 +443,65 @@ int chol_inverse_tasks(double* A, int n, int lda, double* T, double* O, int* sta
     }
     const int ntri = nt * (nt + 1) / 2;
     if (cudaMemsetAsync(state, 0, sizeof(int) * spd_task_state_ints(n), st) != cudaSuccess) return UNC_ERR_CUDA;
+    const long spin = poll_limit > 0 ? (long)std::min<long long>(poll_limit, kDagSpin) : kDagSpin;
+    int4* own = nullptr;  // a schedule with one task left out (tests of the bounded waits)
+    if (skip_task >= 0 && skip_task < list.second) {
+        std::vector<int4> h = build_tasks(nt);
+        h.erase(h.begin() + skip_task);
+        if (cudaMallocAsync(reinterpret_cast<void**>(&own), sizeof(int4) * h.size(), st) != cudaSuccess)
+            return UNC_ERR_OUT_OF_MEMORY;
+        if (cudaMemcpyAsync(own, h.data(), sizeof(int4) * h.size(), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            cudaFreeAsync(own, st);
+            return UNC_ERR_CUDA;
+        }
+        list = {own, (int)h.size()};
+    }
     const int grid = std::max(1, std::min(std::min(device_sms(), max_ctas), list.second));
     k_spd_inverse_tasks<<<grid, DAG_THREADS, DAG_SMEM, st>>>(A, T, O, n, lda, list.first, list.second, state, ntri,
-                                                             err);
+                                                             err, spin);
+    count_launch();
+    if (own && cudaFreeAsync(own, st) != cudaSuccess) return UNC_ERR_CUDA;
+    return UNC_OK;
+}
+
+std::vector<int4> spd_tasks_grouped_list(const std::vector<int>& ns) {
+    struct Item {
+        double key;
+        int m, q;
+        int4 t;
+    };
+    std::vector<Item> items;
+    for (int m = 0; m < (int)ns.size(); ++m) {
+        const std::vector<int4> v = build_tasks((ns[m] + TB - 1) / TB);
+        for (int q = 0; q < (int)v.size(); ++q) {
+            int4 t = v[q];
+            t.x += 8 * m;
+            items.push_back({(q + 1.0) / (double)v.size(), m, q, t});
+        }
+    }
+    // stable in (key, matrix, position): a matrix's own order is kept
+    std::sort(items.begin(), items.end(), [](const Item& a, const Item& b) {
+        if (a.key != b.key) return a.key < b.key;
+        if (a.m != b.m) return a.m < b.m;
+        return a.q < b.q;
+    });
+    std::vector<int4> out(items.size());
+    for (size_t i = 0; i < items.size(); ++i) out[i] = items[i].t;
+    return out;
+}
+
+int chol_inverse_tasks_grouped(const SpdTaskMatrix* d_mats, const int4* d_tasks, int ntasks, int* ctl,
+                               cudaStream_t st, int max_ctas, long long poll_limit) {
+    if (ntasks <= 0) return UNC_OK;
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
+        return cudaFuncSetAttribute(k_spd_inverse_tasks_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)DAG_SMEM) == cudaSuccess;
+    });
+    const long spin = poll_limit > 0 ? (long)std::min<long long>(poll_limit, kDagSpin) : kDagSpin;
+    const int grid = std::max(1, std::min(std::min(device_sms(), max_ctas), ntasks));
+    k_spd_inverse_tasks_grouped<<<grid, DAG_THREADS, DAG_SMEM, st>>>(d_mats, d_tasks, ntasks, ctl, spin);
     count_launch();
     return UNC_OK;
 }

@@ -7,6 +7,7 @@
 #include <atomic>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/uncte.h"
 
@@ -196,8 +197,29 @@ int spd_tasks_prepare(int n);
 // max_ctas bounds the persistent grid (at most one CTA per SM is used anyway);
 // the task order and every tile's update order do not depend on it, so neither
 // do the results.
+// poll_limit (> 0): polls of one dependency before a wait gives up (default
+// and maximum 2^22); skip_task >= 0 leaves that task out of the schedule, which
+// can then not complete: only for tests of the bounded waits.
 int chol_inverse_tasks(double* A, int n, int lda, double* T, double* O, int* state, int* err, cudaStream_t st,
-                       int max_ctas = 148);
+                       int max_ctas = 148, long long poll_limit = 0, int skip_task = -1);
+// One matrix of a grouped tile-task inverse: A (lower triangle) becomes L, T
+// receives L^{-1}, O = A^{-1}; state: spd_task_state_ints(n) zeroed ints; err:
+// the matrix's error word.
+struct SpdTaskMatrix {
+    double *A, *T, *O;
+    long ld;
+    int n, ntri;
+    int* state;
+    int* err;
+};
+// The interleaved task list of matrices of sizes ns (each <= 3584): every
+// matrix's own order kept, merged by fractional position so that all matrices
+// progress together; task.x = type + 8 * matrix index.
+std::vector<int4> spd_tasks_grouped_list(const std::vector<int>& ns);
+// One persistent launch over the list (d_mats / d_tasks in device memory; ctl:
+// 2 ints, zeroed by the caller in stream order, as is every matrix's state).
+int chol_inverse_tasks_grouped(const SpdTaskMatrix* d_mats, const int4* d_tasks, int ntasks, int* ctl,
+                               cudaStream_t st, int max_ctas, long long poll_limit = 0);
 // per context: the largest grid of the tile-task inverse (148 unless set)
 void context_set_task_ctas(unc_context* c, int max_ctas);
 // Y <- Y + k*X  (N x N, column-major)

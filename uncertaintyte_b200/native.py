@@ -80,7 +80,7 @@ class UncStatistic(C.Structure):
 EXPORTS = ("unc_options_init", "unc_context_create", "unc_context_destroy", "unc_compute",
            "unc_context_set_profiling", "unc_context_profile",
            "unc_compute_device", "unc_workspace_bytes", "unc_dense_inverse_device",
-           "unc_dense_inverse_noalloc", "unc_spd_task_list", "unc_pinv_psd_device", "unc_jtj_crs",
+           "unc_dense_inverse_noalloc", "unc_spd_task_list", "unc_spd_inverse_tasks_bounded", "unc_pinv_psd_device", "unc_jtj_crs",
            "unc_gemm_f64_device", "unc_gemm_mixed_device", "unc_status_string", "unc_last_error",
            "unc_kernel_launches", "unc_request_bytes", "unc_context_device_bytes", "unc_context_release",
            "unc_context_set_priority", "unc_jacobian_device", "unc_compute_scene",
@@ -115,6 +115,7 @@ def lib():
     L.unc_dense_inverse_device.argtypes = [vp, C.c_int, C.c_int, vp]
     L.unc_dense_inverse_noalloc.argtypes = [vp, C.c_int, C.c_int, vp]
     L.unc_spd_task_list.argtypes = [C.c_int, vp, C.c_int]
+    L.unc_spd_inverse_tasks_bounded.argtypes = [vp, C.c_int, C.c_int, C.c_longlong, C.c_int, vp]
     L.unc_pinv_psd_device.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, vp]
     L.unc_request_bytes.argtypes = [P(UncOptions), C.c_int, C.c_int, vp, vp]
     L.unc_request_bytes.restype = C.c_longlong
@@ -369,6 +370,14 @@ def workspace_bytes(jac: Jacobian) -> int:
 
 def dense_inverse_device(d_ptr: int, n: int, lda: int, stream: int = 0) -> None:
     _check(lib().unc_dense_inverse_device(d_ptr, n, lda, stream or None))
+
+
+def spd_inverse_tasks_bounded(d_ptr: int, n: int, lda: int, poll_limit: int, skip_task: int = -1,
+                              stream: int = 0) -> None:
+    """The tile-task inverse with its dependency waits limited to poll_limit
+    polls, optionally with one task left out of the schedule (a test of the
+    bounded waits: the call must then fail with UNC_ERR_CUDA, not hang)."""
+    _check(lib().unc_spd_inverse_tasks_bounded(d_ptr, n, lda, poll_limit, skip_task, stream or None))
 
 
 def dense_inverse_noalloc(d_ptr: int, n: int, lda: int, stream: int = 0) -> None:
