@@ -73,7 +73,11 @@ def _args():
     ap.add_argument("--scenes", type=int, default=256, help="batch: number of scenes")
     ap.add_argument("--requests", type=int, default=200, help="serve: requests per precision")
     ap.add_argument("--rate", type=float, default=10.0, help="serve: Poisson arrival rate (requests/s)")
-    ap.add_argument("--pool", type=int, default=32, help="serve: distinct scenes the requests draw from")
+    ap.add_argument("--pool", type=int, default=32,
+                    help="serve: distinct scenes the requests draw from (0: every request its own scene)")
+    ap.add_argument("--serve-precisions", default="mixed,fp64", help="serve: precisions streamed, comma-separated")
+    ap.add_argument("--serve-requests", type=int, default=60,
+                    help="large/medium: requests of the bounded serving stream in the line (0: none)")
     ap.add_argument("--inflight", type=int, default=8, help="batch/serve: concurrent requests on the GPU")
     return ap.parse_args()
 
@@ -665,8 +669,18 @@ def run_ours(a):
                                                         "time_inv_z", "time_te", "time_pts_unc",
                                                         "time_all")}}
         line.update(stage_rooflines(stats, jac.num_cams, jac.num_points, jac.num_obs))
-        print(json.dumps(line), flush=True)
     ctx.close()
+    if a.serve_requests > 0 and ws == 1:
+        # a bounded serving stream of the serving configuration (Poisson arrivals,
+        # continuous batching on this GPU): p50/p99 and throughput, mixed and FP64
+        d_rows = d_cols = d_vals = flush = None
+        torch.cuda.empty_cache()
+        sv = serve_stream(local, a.serve_requests, a.rate, 12, a.inflight, 0, clocks=False)
+        if rank == 0:
+            line["serve"] = {"workload": WORKLOADS["serve"].replace("a seeded pool of 32", "a seeded pool of 12"),
+                             **sv}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if ws > 1:
         dist.destroy_process_group()
     return 0
@@ -707,6 +721,9 @@ def _dist_ms(x):
 
 
 def run_batch(a):
+    """256 uneven scenes: the grouped batch (unc_batch_compute: one launch
+    sequence, graph-replayed, host arrays in and out) against a per-scene
+    sequential loop through unc_compute; results compared bitwise."""
     ws, rank, local = _dist()
     counts, jacs = _scene_set("batch", a.scenes, seed=rank)
     from uncertaintyte_b200 import native
@@ -714,7 +731,6 @@ def run_batch(a):
     ctx = native.Context(local)
     for j in jacs[:4]:
         native.compute_covariances(j, ctx, precision=prec)
-    # per-scene sequential loop through the public host API
     seq_t, seq_res = [], []
     l0 = native.kernel_launches()
     t0 = time.perf_counter()
@@ -724,106 +740,180 @@ def run_batch(a):
         seq_t.append(time.perf_counter() - ts)
         seq_res.append((c, p))
     t_seq = time.perf_counter() - t0
+    seq_launches = native.kernel_launches() - l0
     ctx.close()
-    # the same scenes submitted at once to the request server
-    srv = native.Server(local, 0, a.inflight)
-    for rid in [srv.submit(j, precision=prec) for j in jacs[:a.inflight]]:
-        srv.wait(rid)
+    bt = native.Batch(local)
+    first = bt.compute(jacs, precision=prec)  # tile-width trials, direct launches
+    tuned = bt.last_timing()
+    for _ in range(max(a.warmup, 2)):  # the second call captures the graph, later ones replay it
+        bt.compute(jacs, precision=prec)
     clocks = ClockSampler(local)
     clocks.start()
     clocks.mark(True)
     l1 = native.kernel_launches()
-    t0 = time.perf_counter()
-    ids = [srv.submit(j, precision=prec) for j in jacs]
-    out = [srv.wait(i) for i in ids]
-    t_b = time.perf_counter() - t0
-    launches = native.kernel_launches() - l1
+    steps = max(1, a.steps)
+    wall, dev, h2d, d2h, out = [], [], [], [], None
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        out = bt.compute(jacs, precision=prec)
+        wall.append(time.perf_counter() - t0)
+        tm = bt.last_timing()
+        dev.append(tm["device_s"])
+        h2d.append(tm["h2d_s"])
+        d2h.append(tm["d2h_s"])
+    launches = (native.kernel_launches() - l1) // steps
     clocks.mark(False)
     clk = clocks.stop()
-    srv.close()
-    identical = all(np.array_equal(c0, o[0]) and np.array_equal(p0, o[1]) for (c0, p0), o in zip(seq_res, out))
+    bt.close()
+    identical = all(np.array_equal(c0, o[0]) and np.array_equal(p0, o[1]) and o[3] == 0
+                    for (c0, p0), o in zip(seq_res, out))
+    identical_first = all(np.array_equal(c0, o[0]) and np.array_equal(p0, o[1]) for (c0, p0), o in zip(seq_res, first))
     n = len(jacs)
-    h2d = sum(j.rows.nbytes + j.cols.nbytes + j.values.nbytes for j in jacs)
-    d2h = sum(8 * (45 * j.num_cams + 6 * j.num_points) for j in jacs)
+    t_b = float(np.median(wall))
+    t_dev = float(np.median(dev))
+    h2d_b = sum(j.rows.nbytes + j.cols.nbytes + j.values.nbytes for j in jacs)
+    d2h_b = sum(8 * (45 * j.num_cams + 6 * j.num_points) for j in jacs)
     line = {"metric": "batched covariance solves (256 uneven scenes)", "value": n / t_b, "unit": "scenes/s",
-            "n_gpus": ws, "steps": 1, "warmup": 1, "ms_per_step": 1e3 * t_b, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
+            "n_gpus": ws, "steps": steps, "warmup": max(a.warmup, 2) + 1, "ms_per_step": 1e3 * t_b,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if prec == "fp64" else "i8-sliced products, f64 elsewhere",
             "data": "synthetic (seeded generator with the configuration's shapes; no public dataset)",
-            "config": {"workload": WORKLOADS["batch"], "precision": prec, "inflight": a.inflight,
+            "config": {"workload": WORKLOADS["batch"], "precision": prec,
                        "cams_total": int(np.sum(counts)), "cams_median": float(np.median(counts)),
-                       "timing": "host wall clock, host arrays in and out (end to end)"},
+                       "cams_max": int(np.max(counts)),
+                       "timing": "host wall clock per batch (median), host arrays in and out"},
+            "grouped": {"scenes_per_s_end_to_end": n / t_b, "seconds_end_to_end": t_b,
+                        "device_seconds": t_dev, "scenes_per_s_device": n / t_dev if t_dev > 0 else None,
+                        "h2d_seconds": float(np.median(h2d)), "d2h_seconds": float(np.median(d2h)),
+                        "grouped_scenes": tuned["grouped_scenes"], "tile_n_autotuned": tuned["tile_n"],
+                        "gpu_launches_per_batch": int(launches),
+                        "per_scene_completion_ms": 1e3 * t_b,
+                        "note": "every scene of a batch completes with the batch (one launch sequence)"},
             "sequential_loop": {"seconds": t_seq, "scenes_per_s": n / t_seq, "per_scene_ms": _dist_ms(seq_t),
-                                "gpu_launches": int(l1 - l0)},
-            "batched": {"seconds": t_b, "speedup_vs_sequential": t_seq / t_b,
-                        "completion_latency_ms": _dist_ms([o[3] for o in out]),
-                        "identical_to_sequential": bool(identical)},
-            "e2e": {"value": n / t_b, "unit": "scenes/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
+                                "gpu_launches": int(seq_launches)},
+            "speedup_grouped_over_sequential": t_seq / t_b,
+            "identical_to_per_scene": bool(identical and identical_first),
+            "e2e": {"value": n / t_b, "unit": "scenes/s", "h2d_bytes_per_step": int(h2d_b),
+                    "d2h_bytes_per_step": int(d2h_b)},
             "gpu_launches": int(launches), "clocks": clk}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
 
 
-def run_serve(a):
-    ws, rank, local = _dist()
-    counts, jacs = _scene_set("serve", a.pool, seed=1 + rank)
-    from uncertaintyte_b200 import native
+class _SceneStream:
+    """Distinct serving scenes generated just in time in spawned processes
+    (the scenes of a 10k-request run do not fit in host memory together)."""
+
+    def __init__(self, counts, ppc, lam, seed, lookahead=48):
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        self.jobs = [(int(C), ppc, lam, seed * 100003 + i) for i, C in enumerate(counts)]
+        self.ex = ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1), mp_context=mp.get_context("spawn"))
+        self.fut = {}
+        self.next = 0
+        self.lookahead = lookahead
+
+    def get(self, k):
+        while self.next < len(self.jobs) and self.next <= k + self.lookahead:
+            self.fut[self.next] = self.ex.submit(_gen_scene, self.jobs[self.next])
+            self.next += 1
+        return self.fut.pop(k).result()
+
+    def close(self):
+        self.ex.shutdown(cancel_futures=True)
+
+
+def serve_stream(local, requests, rate, pool, inflight, seed, precisions=("mixed", "fp64"), clocks=True):
+    """A Poisson request stream through the request server (unc_server_*):
+    latency from submit to result, host arrays in and out. pool > 0: the
+    requests draw from that many distinct seeded scenes (each solved once,
+    untimed, before the stream); pool == 0: every request is its own scene,
+    generated while the stream runs."""
+    from uncertaintyte_b200 import native, scenes
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    rng = np.random.default_rng(2 + rank)
-    picks = rng.integers(0, len(jacs), a.requests)
-    gaps = rng.exponential(1.0 / a.rate, a.requests)
-    res, first = {}, {}
-    clk = None
-    for prec in ("mixed", "fp64"):
-        srv = native.Server(local, 0, a.inflight)
-        warm = [srv.submit(j, precision=prec) for j in jacs]  # every pool scene once, untimed
-        first[prec] = [srv.wait(i)[:2] for i in warm]
-        clocks = ClockSampler(local) if prec == "mixed" else None
-        if clocks:
-            clocks.start()
-            clocks.mark(True)
-        ids = []
+    rng = np.random.default_rng(2 + seed)
+    gaps = rng.exponential(1.0 / rate, requests)
+    if pool > 0:
+        counts, jacs = _scene_set("serve", pool, seed=1 + seed)
+        picks = rng.integers(0, len(jacs), requests)
+    else:
+        counts = scenes.sample_camera_counts(requests, 150, 1.2, 8, 3000, 1 + seed)
+        jacs, picks = None, None
+    res, first, clk = {}, {}, None
+    h2d = d2h = 0
+    for prec in precisions:
+        srv = native.Server(local, 0, inflight)
+        if jacs is not None:
+            warm = [srv.submit(j, precision=prec) for j in jacs]  # every pool scene once, untimed
+            first[prec] = [srv.wait(i)[:2] for i in warm]
+        stream = _SceneStream(counts, 200, 5, 1 + seed) if jacs is None else None
+        sampler = ClockSampler(local) if (clocks and prec == precisions[0]) else None
+        if sampler:
+            sampler.start()
+            sampler.mark(True)
+        ids, late = [], 0
+        h2d = d2h = 0
         t0 = time.perf_counter()
         due = t0
-        for k in range(a.requests):
+        for k in range(requests):
+            j = jacs[picks[k]] if jacs is not None else stream.get(k)
             due += gaps[k]
             wait = due - time.perf_counter()
             if wait > 0:
                 time.sleep(wait)
-            ids.append(srv.submit(jacs[picks[k]], precision=prec))
+            elif wait < -0.05:
+                late += 1
+            ids.append(srv.submit(j, precision=prec))
+            h2d += j.values.nbytes + j.cols.nbytes + j.rows.nbytes
+            d2h += 8 * (45 * j.num_cams + 6 * j.num_points)
         out = [srv.wait(i) for i in ids]
         t1 = time.perf_counter()
-        if clocks:
-            clocks.mark(False)
-            clk = clocks.stop()
+        if stream:
+            stream.close()
+        if sampler:
+            sampler.mark(False)
+            clk = sampler.stop()
         srv.close()
         lat, que = [o[3] for o in out], [o[4] for o in out]
         res[prec] = {"latency_ms": _dist_ms(lat), "queue_ms": _dist_ms(que),
-                     "throughput_req_s": a.requests / (t1 - t0), "seconds": t1 - t0}
-    from conftest import block_rel_err
-    ec = max(block_rel_err(m[0], f[0], 45) for m, f in zip(first["mixed"], first["fp64"]))
-    ep = max(block_rel_err(m[1], f[1], 6) for m, f in zip(first["mixed"], first["fp64"]))
-    m = res["mixed"]
-    line = {"metric": "served latency p50/p99 and throughput (mixed precision)", "value": m["latency_ms"]["p50"],
-            "unit": "ms (p50 latency)", "p99_ms": m["latency_ms"]["p99"],
+                     "throughput_req_s": requests / (t1 - t0), "seconds": t1 - t0,
+                     "submitted_late": late}
+    out = {"requests": requests, "rate_req_s": rate, "inflight": inflight,
+           "scenes": f"pool of {pool} distinct scenes" if pool > 0 else "every request a distinct scene",
+           "cams_max": int(np.max(counts)), "cams_median": float(np.median(counts)), "clocks": clk,
+           "h2d_bytes_per_request": int(h2d / requests), "d2h_bytes_per_request": int(d2h / requests)}
+    out.update(res)
+    if "mixed" in res and "fp64" in res:
+        out["p50_speedup_mixed_over_fp64"] = res["fp64"]["latency_ms"]["p50"] / res["mixed"]["latency_ms"]["p50"]
+        out["p99_speedup_mixed_over_fp64"] = res["fp64"]["latency_ms"]["p99"] / res["mixed"]["latency_ms"]["p99"]
+    if first.get("mixed") and first.get("fp64"):
+        from conftest import block_rel_err
+        out["mixed_vs_fp64_max_rel_err"] = {
+            "camera_9x9": max(block_rel_err(m[0], f[0], 45) for m, f in zip(first["mixed"], first["fp64"])),
+            "point_3x3": max(block_rel_err(m[1], f[1], 6) for m, f in zip(first["mixed"], first["fp64"])),
+            "bar": 1e-6}
+    return out
+
+
+def run_serve(a):
+    ws, rank, local = _dist()
+    precs = tuple(a.serve_precisions.split(","))
+    r = serve_stream(local, a.requests, a.rate, a.pool, a.inflight, rank, precs)
+    m = r[precs[0]]
+    line = {"metric": f"served latency p50/p99 and throughput ({precs[0]} precision)",
+            "value": m["latency_ms"]["p50"], "unit": "ms (p50 latency)", "p99_ms": m["latency_ms"]["p99"],
             "throughput_req_s": m["throughput_req_s"], "n_gpus": ws, "steps": a.requests, "warmup": a.pool,
             "ms_per_step": 1e3 * m["seconds"] / a.requests, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "i8-sliced products, f64 elsewhere",
-            "data": "synthetic (seeded pool of scenes with the configuration's shapes; no public dataset)",
+            "data": "synthetic (seeded scenes with the configuration's shapes; no public dataset)",
             "config": {"workload": WORKLOADS["serve"], "requests": a.requests, "rate_req_s": a.rate,
-                       "inflight": a.inflight, "pool_cams": sorted(int(c) for c in counts),
+                       "inflight": a.inflight, "scenes": r["scenes"],
                        "timing": "submit to result, host wall clock, host arrays in and out"},
-            "mixed": m, "fp64": res["fp64"],
-            "p99_speedup_mixed_over_fp64": res["fp64"]["latency_ms"]["p99"] / m["latency_ms"]["p99"],
-            "mixed_vs_fp64_max_rel_err": {"camera_9x9": ec, "point_3x3": ep, "bar": 1e-6},
+            "serve": r,
             "e2e": {"value": m["latency_ms"]["p50"], "unit": "ms (p50 latency)",
-                    "h2d_bytes_per_step": int(np.mean([jacs[k].values.nbytes + jacs[k].cols.nbytes
-                                                        + jacs[k].rows.nbytes for k in picks])),
-                    "d2h_bytes_per_step": int(np.mean([8 * (45 * jacs[k].num_cams + 6 * jacs[k].num_points)
-                                                       for k in picks]))},
-            "clocks": clk}
+                    "h2d_bytes_per_step": r["h2d_bytes_per_request"], "d2h_bytes_per_step": r["d2h_bytes_per_request"]},
+            "clocks": r["clocks"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0

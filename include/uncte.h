@@ -213,6 +213,43 @@ int unc_server_wait(unc_server* srv, long long id, double timeout_s, int* status
 /* Finish every queued and running request, then stop the workers. */
 int unc_server_destroy(unc_server* srv);
 
+/* ---- Batches: many reconstructions in one grouped launch sequence. No
+ * counterpart in the reference, whose computeCovariances
+ * (src/uncertaintyTE/compute.cpp:458-540) solves one reconstruction per call
+ * and is not re-entrant; unc_batch_compute is that call over num_scenes scenes
+ * at once. The inputs of all scenes go to the device in one copy; the sparse
+ * stages of the scenes run as parallel branches, the dense stage is grouped
+ * (one persistent tile-task kernel inverts every scene's Schur complement,
+ * each Taylor-series step is one launch over all scenes' product tiles); the
+ * sequence of a batch shape (sizes, fixed points, lambda) is captured in a
+ * CUDA graph the second time it is seen and replayed after. The product tile
+ * width is chosen by timing the candidates on the first batch of a size class.
+ * Each scene's result is bitwise the one unc_compute gives for it alone.
+ * Scenes outside the grouped path (the SVD algorithms, UNC_PRECISION_FP64,
+ * 9 * num_cams above 3584, Jacobians not in the 24-entries-per-observation
+ * layout) are computed with unc_compute in the same call.
+ * Per scene i: opts[i], the host CRS arrays and the host outputs as for
+ * unc_compute; status[i] receives the scene's own status code; stats (NULL or
+ * num_scenes entries) the statistics (time_all: the whole batch's time). The
+ * call returns UNC_OK unless the batch itself could not run. A batch object is
+ * not thread-safe. */
+typedef struct unc_batch unc_batch;
+int unc_batch_create(int device, unc_batch** out);
+int unc_batch_destroy(unc_batch* batch);
+int unc_batch_compute(unc_batch* batch, int num_scenes, const unc_options* opts, const int* num_rows,
+                      const int* num_cols, const int* const* rows, const int* const* cols,
+                      const double* const* values, double* const* cam_unc, double* const* pt_unc, int* status,
+                      unc_statistic* stats);
+/* Times of the last unc_batch_compute (seconds): the input copy, the device
+ * work of the grouped scenes, the output copy; how many scenes were grouped
+ * and the product tile width used. */
+int unc_batch_last_timing(const unc_batch* batch, double* h2d_s, double* device_s, double* d2h_s,
+                          int* grouped_scenes, int* tile_n);
+/* Device bytes a batch object keeps between calls, and their release (the
+ * next call allocates again). */
+long long unc_batch_device_bytes(const unc_batch* batch);
+int unc_batch_release(unc_batch* batch);
+
 /* SDM::inv (src/uncertaintyTE/ScaledDenseMatrix.cpp:232-279) for a
  * symmetric positive-definite n x n matrix in device memory (column-major,
  * leading dimension lda >= n, lda even): inverted in place on the GPU

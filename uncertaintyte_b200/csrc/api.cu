@@ -13,6 +13,7 @@
 
 #include "../../include/uncte.h"
 #include "internal.h"
+#include "pipeline.h"
 
 namespace unc {
 thread_local std::string g_last_error;
@@ -99,22 +100,9 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
-struct Plan {
-    int C, P, nobs, N, ld;
-    bool svd_schur;  // UNC_SVD_SCHUR: pseudo-inverse of the camera Schur complement
-};
+}  // namespace
 
-struct Buffers {
-    int *rows, *cols;
-    double* vals;
-    double *cam_out, *pt_out;
-    SceneDev s;
-    double *Z, *iZ, *add, *tmp, *e, *gjws, *sig;
-    int* dag_state;  // counters of the tile-task inverse
-    unsigned long long* amax;
-    TeState* te;
-    PinvBuffers pb;  // UNC_SVD_SCHUR only
-};
+namespace unc {
 
 // Lay out the workspace; with base == nullptr only the size is computed.
 size_t carve(char* base, const Plan& pl, bool host_io, long long nnz, int nrows, Buffers& b) {
@@ -219,6 +207,123 @@ bool is_svd(const unc_options* o) {
     return o->algorithm == UNC_SVD_QR_ITERATION || o->algorithm == UNC_SVD_DEVIDE_AND_CONQUER;
 }
 
+size_t schur_pair_bytes(int C, long long npairs) {
+    const size_t long_cap = (size_t)npairs / 1025 + 1;
+    const size_t nz_ints = schur_list_ints(C, (long)npairs);
+    return (size_t)npairs * 8 + (long_cap + 1 + nz_ints) * sizeof(int) + 64;
+}
+
+long long schur_pairs_bound(const unc_options* o, int num_rows, long long nnz, const int* cols) {
+    const int C = o->num_cams, P = o->num_points, nobs = num_rows / 2;
+    const long long cam_off = 9LL * C;
+    std::vector<int> m(P > 0 ? P : 1, 0);
+    for (int ob = 0; ob < nobs; ++ob) {
+        const long long k = 24LL * ob + 9;  // the point column the device reads (k_validate_obs)
+        if (k >= nnz) break;
+        const long long c = cols[k];
+        if (c < cam_off) continue;
+        const long long pt = (c - cam_off) / 3;
+        if (pt < P) ++m[pt];
+    }
+    long long pairs = 0;
+    for (int v : m) pairs += (long long)v * (v - 1);
+    return pairs;
+}
+
+double auto_lambda(int N) { return pow(10, -1.2653 * log10((double)N) - 2.9415); }
+
+int32_t factorial_i32(int n) {
+    uint32_t f = 1;
+    for (int i = 2; i <= n; ++i) f *= (uint32_t)i;
+    return (int32_t)f;
+}
+
+Plan make_plan(const unc_options* o, int num_rows) {
+    Plan pl;
+    pl.C = o->num_cams;
+    pl.P = o->num_points;
+    pl.nobs = num_rows / 2;
+    pl.N = 9 * pl.C;
+    pl.ld = ld_of(pl.N);
+    pl.svd_schur = o->algorithm == UNC_SVD_SCHUR;
+    return pl;
+}
+
+int sparse_stage(const unc_options* o, const Plan& pl, long long nnz, const int* rows, const int* cols,
+                 const double* vals, Buffers& b, int fx[3], cudaEvent_t* ev, cudaStream_t sm, void** pair_buf,
+                 size_t* pair_bytes, long long pairs_cap) {
+    SceneDev& s = b.s;
+    s.nnz = (long)nnz;
+    s.num_cams = pl.C;
+    s.num_points = pl.P;
+    s.num_obs = pl.nobs;
+    s.rows = rows;
+    s.cols = cols;
+    s.J = vals;
+    fx[0] = o->pts2fix[0];
+    fx[1] = o->pts2fix[1];
+    fx[2] = o->pts2fix[2];
+    std::sort(fx, fx + 2);  // the reference sorts only the first two ids (compute.cpp:285)
+    s.has_fix = pl.svd_schur ? 0 : 1;  // the SVD on Z keeps every point
+    if (pl.svd_schur) fx[0] = fx[1] = fx[2] = -1;
+    for (int i = 0; i < 3; ++i) s.fix[i] = fx[i];
+    const int N = pl.N, ld = pl.ld;
+    auto mark = [&](int i) -> int {
+        if (ev) CK(cudaEventRecord(ev[i], sm));
+        return UNC_OK;
+    };
+
+    if (int r = mark(0)) return r;
+    CK(cudaMemsetAsync(s.err, 0, 16, sm));
+    launch_validate_obs(s, sm);
+    if (int r = mark(1)) return r;
+    launch_build_index(s, sm);
+    if (int r = mark(2)) return r;
+    // zero the dense buffers once (padding rows must stay finite for the GEMM loads)
+    CK(cudaMemsetAsync(b.Z, 0, (size_t)((char*)(b.tmp + (size_t)ld * N) - (char*)b.Z), sm));
+    launch_camera_blocks(s, b.Z, ld, sm);
+    launch_point_blocks(s, sm);
+    if (int r = mark(3)) return r;
+    launch_obs_blocks(s, sm);
+    launch_schur_count(s, sm);
+    long long npairs = pairs_cap;
+    if (pairs_cap < 0) {
+        int dev_pairs = 0;
+        CK(cudaMemcpyAsync(&dev_pairs, s.blk_ptr + (size_t)pl.C * pl.C, sizeof(int), cudaMemcpyDeviceToHost, sm));
+        if (int r = mark(4)) return r;
+        CK(cudaStreamSynchronize(sm));
+        if (dev_pairs < 0) return fail(UNC_ERR_TOO_LARGE, "more than 2^31 co-visible observation pairs");
+        npairs = dev_pairs;
+        const size_t need = schur_pair_bytes(pl.C, npairs);
+        // headroom for the next scene
+        if (int r = grow_buffer(pair_buf, pair_bytes, need, need + need / 4, sm)) return r;
+    } else {
+        if (int r = mark(4)) return r;
+        if (*pair_bytes < schur_pair_bytes(pl.C, npairs)) return fail(UNC_ERR_INVALID_ARG, "pair list too small");
+    }
+    const size_t long_cap = (size_t)npairs / 1025 + 1;
+    s.pairs = reinterpret_cast<unsigned long long*>(*pair_buf);
+    s.pair_cap = (long)npairs;
+    s.long_list = reinterpret_cast<int*>(s.pairs + npairs + 1);
+    s.long_cap = (int)long_cap;
+    s.nz_list = s.long_list + long_cap + 1;
+    launch_camera_self(s, b.Z, ld, sm);
+    launch_schur(s, b.Z, ld, sm);
+    launch_mirror_upper(b.Z, N, ld, sm);
+    if (int r = mark(5)) return r;
+    return UNC_OK;
+}
+
+void output_stage(const Plan& pl, Buffers& b, double* cam_out, double* pt_out, cudaStream_t sm) {
+    launch_camera_output(b.iZ, pl.ld, b.s.s_cam, pl.C, cam_out, b.sig, sm);
+    if (pl.P > 3) cudaMemsetAsync(pt_out, 0, sizeof(double) * 6 * ((size_t)pl.P - 3), sm);
+    launch_point_cov(b.s, b.sig, pt_out, sm);
+}
+
+}  // namespace unc
+
+namespace {
+
 constexpr size_t kStageGraphs = 8, kSeenKeys = 16;
 
 void drop_graphs(unc_context* ctx) {
@@ -278,12 +383,6 @@ int run_stage(unc_context* ctx, const GraphKey& key, cudaStream_t sm, F&& stage,
     return UNC_OK;
 }
 
-// factorial() of compute.cpp:57-62: 32-bit signed, wraps from 13! on.
-int32_t factorial_i32(int n) {
-    uint32_t f = 1;
-    for (int i = 2; i <= n; ++i) f *= (uint32_t)i;
-    return (int32_t)f;
-}
 
 float ev_s(cudaEvent_t a, cudaEvent_t b) {
     float ms = 0;
@@ -299,52 +398,10 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
                  const int* cols, const double* vals, double* cam_out, double* pt_out, Buffers& b,
                  const Plan& pl, unc_statistic* st, cudaStream_t sm) {
     SceneDev& s = b.s;
-    s.nnz = (long)nnz;
-    s.num_cams = pl.C;
-    s.num_points = pl.P;
-    s.num_obs = pl.nobs;
-    s.rows = rows;
-    s.cols = cols;
-    s.J = vals;
-    int fx[3] = {o->pts2fix[0], o->pts2fix[1], o->pts2fix[2]};
-    std::sort(fx, fx + 2);  // the reference sorts only the first two ids (compute.cpp:285)
-    s.has_fix = pl.svd_schur ? 0 : 1;  // the SVD on Z keeps every point
-    if (pl.svd_schur) fx[0] = fx[1] = fx[2] = -1;
-    for (int i = 0; i < 3; ++i) s.fix[i] = fx[i];
+    int fx[3];
     const int N = pl.N, ld = pl.ld;
     cudaEvent_t* ev = ctx->ev;
-
-    CK(cudaEventRecord(ev[0], sm));
-    CK(cudaMemsetAsync(s.err, 0, 16, sm));
-    launch_validate_obs(s, sm);
-    CK(cudaEventRecord(ev[1], sm));
-    launch_build_index(s, sm);
-    CK(cudaEventRecord(ev[2], sm));
-    // zero the dense buffers once (padding rows must stay finite for the GEMM loads)
-    CK(cudaMemsetAsync(b.Z, 0, (size_t)((char*)(b.tmp + (size_t)ld * N) - (char*)b.Z), sm));
-    launch_camera_blocks(s, b.Z, ld, sm);
-    launch_point_blocks(s, sm);
-    CK(cudaEventRecord(ev[3], sm));
-    launch_obs_blocks(s, sm);
-    launch_schur_count(s, sm);
-    int npairs = 0;
-    CK(cudaMemcpyAsync(&npairs, s.blk_ptr + (size_t)pl.C * pl.C, sizeof(int), cudaMemcpyDeviceToHost, sm));
-    CK(cudaEventRecord(ev[4], sm));
-    CK(cudaStreamSynchronize(sm));
-    if (npairs < 0) return fail(UNC_ERR_TOO_LARGE, "more than 2^31 co-visible observation pairs");
-    const size_t long_cap = (size_t)npairs / 1025 + 1;
-    const size_t nz_ints = schur_list_ints(pl.C, npairs);
-    const size_t need = (size_t)npairs * 8 + (long_cap + 1 + nz_ints) * sizeof(int) + 64;
-    // headroom for the next scene
-    if (int r = grow_buffer(&ctx->tup, &ctx->tup_bytes, need, need + need / 4, sm)) return r;
-    s.pairs = reinterpret_cast<unsigned long long*>(ctx->tup);
-    s.long_list = reinterpret_cast<int*>(s.pairs + npairs + 1);
-    s.long_cap = (int)long_cap;
-    s.nz_list = s.long_list + long_cap + 1;
-    launch_camera_self(s, b.Z, ld, sm);
-    launch_schur(s, b.Z, ld, sm);
-    launch_mirror_upper(b.Z, N, ld, sm);
-    CK(cudaEventRecord(ev[5], sm));
+    if (int r = sparse_stage(o, pl, nnz, rows, cols, vals, b, fx, ev, sm, &ctx->tup, &ctx->tup_bytes, -1)) return r;
 
     PinvInfo pinfo{};
     if (pl.svd_schur) {
@@ -386,7 +443,7 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     }
 
     double lambda = o->lambda;
-    if (lambda == -1) lambda = pow(10, -1.2653 * log10((double)N) - 2.9415);  // compute.cpp:124-125
+    if (lambda == -1) lambda = auto_lambda(N);  // compute.cpp:124-125
 
     // Every power X^(i+1) is symmetric: only the lower-triangle tiles of each
     // product are computed (half the flops), then mirrored for the next product.
@@ -504,9 +561,7 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         CK(cudaEventRecord(ev[7], sm));
     }
 
-    launch_camera_output(b.iZ, ld, s.s_cam, pl.C, cam_out, b.sig, sm);
-    if (pl.P > 3) CK(cudaMemsetAsync(pt_out, 0, sizeof(double) * 6 * ((size_t)pl.P - 3), sm));
-    launch_point_cov(s, b.sig, pt_out, sm);
+    output_stage(pl, b, cam_out, pt_out, sm);
     CK(cudaEventRecord(ev[8], sm));
 
     int err = 0;
@@ -589,17 +644,6 @@ int dense_inverse(double* d_A, int n, int lda, void* stream, long long poll_limi
     if (h_err & ERRBIT_TIMEOUT) return fail(UNC_ERR_CUDA, "a bounded device wait of the tile-task inverse ran out");
     if (h_err & (ERRBIT_SINGULAR | ERRBIT_NONFINITE)) return fail(UNC_ERR_SINGULAR, "matrix is not positive definite");
     return UNC_OK;
-}
-
-Plan make_plan(const unc_options* o, int num_rows) {
-    Plan pl;
-    pl.C = o->num_cams;
-    pl.P = o->num_points;
-    pl.nobs = num_rows / 2;
-    pl.N = 9 * pl.C;
-    pl.ld = ld_of(pl.N);
-    pl.svd_schur = o->algorithm == UNC_SVD_SCHUR;
-    return pl;
 }
 
 }  // namespace

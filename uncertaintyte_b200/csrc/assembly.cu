@@ -661,7 +661,8 @@ void launch_camera_self(const SceneDev& s, double* Z, int ldz, cudaStream_t st) 
 template <bool kScatter>
 __global__ void __launch_bounds__(128) k_pair_enum(int num_points, int num_cams, const int* __restrict__ pt_ptr,
                                                    const int* __restrict__ pt_obs, const int* __restrict__ obs_cam,
-                                                   int* cnt_or_cursor, unsigned long long* __restrict__ pairs) {
+                                                   int* cnt_or_cursor, unsigned long long* __restrict__ pairs,
+                                                   long cap) {
     const int p = blockIdx.x * 4 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (p >= num_points) return;
     const int b = pt_ptr[p], m = pt_ptr[p + 1] - b;
@@ -675,7 +676,7 @@ __global__ void __launch_bounds__(128) k_pair_enum(int num_points, int num_cams,
         const long key = (long)ca * num_cams + cb;
         if (kScatter) {
             const int pos = atomicAdd(cnt_or_cursor + key, 1);
-            pairs[pos] = ((unsigned long long)(unsigned)oa << 32) | (unsigned)ob;
+            if (pos < cap) pairs[pos] = ((unsigned long long)(unsigned)oa << 32) | (unsigned)ob;
         } else {
             atomicAdd(cnt_or_cursor + key, 1);
         }
@@ -853,7 +854,7 @@ void launch_schur_count(const SceneDev& s, cudaStream_t st) {
     cudaMemsetAsync(s.blk_cnt, 0, sizeof(int) * (size_t)nblk, st);
     if (s.num_points > 0) {
         k_pair_enum<false><<<(s.num_points + 3) / 4, 128, 0, st>>>(s.num_points, s.num_cams, s.pt_ptr, s.pt_obs,
-                                                                   s.obs_cam, s.blk_cnt, nullptr);
+                                                                   s.obs_cam, s.blk_cnt, nullptr, 0);
         count_launch();
     }
     exclusive_scan(s.blk_cnt, s.blk_ptr, (int)nblk, s.scan_tmp, st);
@@ -877,13 +878,29 @@ size_t schur_list_ints(int num_cams, long npairs) {
     return (size_t)std::min(upper, npairs) + 2;
 }
 
+// A pair list sized from a host-side count (a captured launch sequence cannot
+// read the device count back) that the device count exceeds: the error bit is
+// set and every block is emptied, so that nothing reads or writes past the list.
+__global__ void k_pair_capacity(int* blk_ptr, long nblk, long cap, int* err) {
+    __shared__ int over;
+    if (threadIdx.x == 0) {
+        over = blk_ptr[nblk] > cap;
+        if (over) atomicOr(err, ERRBIT_PAIR_CAP);
+    }
+    __syncthreads();  // every thread has the decision before any entry is cleared
+    if (!over) return;
+    for (long k = threadIdx.x; k <= nblk; k += blockDim.x) blk_ptr[k] = 0;
+}
+
 void launch_schur(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
     const long nblk = (long)s.num_cams * s.num_cams;
     if (nblk == 0) return;
+    k_pair_capacity<<<1, 256, 0, st>>>(s.blk_ptr, nblk, s.pair_cap, s.err);
+    count_launch();
     cudaMemcpyAsync(s.blk_cnt, s.blk_ptr, sizeof(int) * (size_t)nblk, cudaMemcpyDeviceToDevice, st);
     if (s.num_points > 0) {
         k_pair_enum<true><<<(s.num_points + 3) / 4, 128, 0, st>>>(s.num_points, s.num_cams, s.pt_ptr, s.pt_obs,
-                                                                  s.obs_cam, s.blk_cnt, s.pairs);
+                                                                  s.obs_cam, s.blk_cnt, s.pairs, s.pair_cap);
         count_launch();
     }
     cudaMemsetAsync(s.long_list, 0, sizeof(int), st);

@@ -1,0 +1,736 @@
+// batch.cu - many reconstructions solved together: one grouped launch
+// sequence over a batch of scenes (host code).
+//
+// The reference computes one reconstruction per call (computeCovariances,
+// compute.cpp:458-540) and is not re-entrant; this is the batched form of that
+// call, with no counterpart there. Per batch:
+//
+//   * inputs of all scenes packed into one pinned staging area and copied to
+//     the device in one transfer; outputs come back the same way;
+//   * the sparse stages (validation, J^T J blocks, Schur complement) of every
+//     scene as parallel branches of one launch sequence;
+//   * the dense stage grouped across scenes: one persistent tile-task kernel
+//     runs the SPD inverses of all scenes from one interleaved work list, and
+//     every Taylor-series step (stop rule, slicing, int8 tensor-core product)
+//     is one launch over the tiles / rows of all scenes;
+//   * the camera and point outputs again as parallel branches.
+//
+// The sequence for a given batch shape (sizes, fixed points, lambda, buffer
+// addresses) is captured in a CUDA graph the second time the shape is seen and
+// replayed from then on. The product's tile width is chosen by timing the
+// candidates on the first batch of a size class (an autotuner, cached per size
+// class); the products' per-element arithmetic does not depend on it.
+// Every grouped kernel performs, per element, exactly the arithmetic of its
+// per-scene counterpart, so each scene's result is bitwise the one
+// unc_compute gives for it alone.
+//
+// Scenes the grouped path does not cover (the SVD algorithms, the FP64
+// precision, N = 9 cameras above 3584) are computed one after another with
+// unc_compute in the same call.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <thread>
+#include <vector>
+
+#include "../../include/uncte.h"
+#include "pipeline.h"
+
+using namespace unc;
+
+namespace {
+
+#define BCK(call)                                                                                 \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) {                                                                  \
+            g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);                    \
+            return e_ == cudaErrorMemoryAllocation ? UNC_ERR_OUT_OF_MEMORY : UNC_ERR_CUDA;        \
+        }                                                                                         \
+    } while (0)
+
+int bfail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+constexpr int kBranches = 8;      // parallel streams for the per-scene stages
+constexpr int kGraphs = 4;        // batch-shape graphs kept
+constexpr int kTaylorIters = 19;  // iterations launched after the first product (compute.cpp:145)
+
+struct Scene {
+    int idx;  // position in the caller's arrays
+    unc_options opt;
+    Plan pl;
+    long long nnz;
+    long long pairs_cap;
+    int fx[3];
+    double lambda;
+    Buffers b;
+    void* pair_buf;
+    size_t pair_bytes;
+    int* in_rows;
+    int* in_cols;
+    double* in_vals;
+    double* out_cam;
+    double* out_pt;
+    size_t in_off[3], out_off[2];  // byte offsets in the staging areas
+    int8_t *bufX, *bufP;
+    int *eX, *eP;
+};
+
+struct Layout {
+    size_t in_bytes = 0, out_bytes = 0, total = 0;
+    // device regions (offsets)
+    size_t mixed_off = 0, mixed_bytes = 0;
+    size_t zero_off = 0, zero_bytes = 0;  // dag states + control words
+    size_t amax_off = 0, amax_bytes = 0;
+    size_t stat_off = 0, stat_bytes = 0;  // error words + Taylor states
+    size_t desc_off = 0, desc_bytes = 0;  // descriptors uploaded from the host
+};
+
+struct Graph {
+    std::vector<unsigned long long> key;
+    cudaGraphExec_t exec = nullptr;
+    long long launches = 0;
+};
+
+}  // namespace
+
+struct unc_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t branch[kBranches] = {};
+    cudaEvent_t fork = nullptr, join[kBranches] = {}, ev[6] = {};
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    void* host = nullptr;  // pinned staging: inputs, outputs, descriptors, status words
+    size_t host_bytes = 0;
+    std::vector<Graph> graphs;
+    std::vector<std::vector<unsigned long long>> seen;
+    std::map<std::pair<int, int>, int> tile_choice;  // (slices, size class) -> tile width
+    unc_context* single = nullptr;                  // scenes outside the grouped path
+    double t_h2d = 0, t_dev = 0, t_d2h = 0;
+    int grouped = 0, tile_n = 0;
+};
+
+namespace {
+
+struct Copy {
+    void* dst;
+    const void* src;
+    size_t bytes;
+};
+
+// Host-side copies with several threads (the staging area is pinned; the
+// caller's arrays are ordinary host memory).
+void parallel_copy(const std::vector<Copy>& jobs) {
+    const int nt = (int)std::min<size_t>(16, std::max<size_t>(1, std::thread::hardware_concurrency()));
+    size_t total = 0;
+    for (auto& j : jobs) total += j.bytes;
+    if (total < (64u << 20) || nt == 1) {
+        for (auto& j : jobs) memcpy(j.dst, j.src, j.bytes);
+        return;
+    }
+    // split every copy into pieces of at most 8 MB and deal them out
+    struct Piece {
+        char* d;
+        const char* s;
+        size_t n;
+    };
+    std::vector<Piece> pieces;
+    for (auto& j : jobs)
+        for (size_t o = 0; o < j.bytes; o += (8u << 20))
+            pieces.push_back({(char*)j.dst + o, (const char*)j.src + o, std::min<size_t>(8u << 20, j.bytes - o)});
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+        th.emplace_back([&, t] {
+            for (size_t p = t; p < pieces.size(); p += nt) memcpy(pieces[p].d, pieces[p].s, pieces[p].n);
+        });
+    for (auto& x : th) x.join();
+}
+
+int slices_of(int precision) {
+    return precision == UNC_PRECISION_MIXED4 ? 4 : (precision == UNC_PRECISION_MIXED3 ? 3 : 5);
+}
+
+int lower_tile_count(int n, int nt) {
+    std::vector<int4> t;
+    mixed_lower_tiles(0, n, nt, t);
+    return (int)t.size();
+}
+
+// Lay out the device workspace of a group for tile width nt (base == nullptr:
+// sizes only). Fills the per-scene pointers.
+void lay_out(char* base, std::vector<Scene>& sc, int slices, int nt, Layout& L, size_t ntasks, size_t ntiles) {
+    Carver c{base};
+    const size_t in0 = c.off;
+    for (auto& s : sc) {
+        s.in_rows = c.take<int>((size_t)s.pl.nobs * 2 + 1);
+        s.in_off[0] = (char*)s.in_rows - base;
+        s.in_cols = c.take<int>((size_t)s.nnz);
+        s.in_off[1] = (char*)s.in_cols - base;
+        s.in_vals = c.take<double>((size_t)s.nnz);
+        s.in_off[2] = (char*)s.in_vals - base;
+    }
+    c.off = (c.off + 255) & ~size_t(255);
+    L.in_bytes = c.off - in0;
+    const size_t out0 = c.off;
+    for (auto& s : sc) {
+        s.out_cam = c.take<double>((size_t)s.pl.C * 45);
+        s.out_off[0] = (char*)s.out_cam - base;
+        s.out_pt = c.take<double>((size_t)s.pl.P * 6);
+        s.out_off[1] = (char*)s.out_pt - base;
+    }
+    c.off = (c.off + 255) & ~size_t(255);
+    L.out_bytes = c.off - out0;
+    for (auto& s : sc) {
+        const size_t need = carve(nullptr, s.pl, false, 0, s.pl.nobs * 2, s.b);
+        char* at = c.take<char>(need);
+        carve(base ? at : nullptr, s.pl, false, 0, s.pl.nobs * 2, s.b);
+        s.pair_bytes = schur_pair_bytes(s.pl.C, s.pairs_cap);
+        s.pair_buf = c.take<char>(s.pair_bytes);
+    }
+    c.off = (c.off + 255) & ~size_t(255);
+    L.mixed_off = c.off;
+    for (auto& s : sc) {
+        const size_t sb = mixed_slice_bytes_nt(s.pl.N, slices, nt);
+        s.bufX = c.take<int8_t>(sb);
+        s.bufP = c.take<int8_t>(sb);
+        s.eX = c.take<int>((size_t)s.pl.N + 64);
+        s.eP = c.take<int>((size_t)s.pl.N + 64);
+    }
+    c.off = (c.off + 255) & ~size_t(255);
+    L.mixed_bytes = c.off - L.mixed_off;
+    // zero at the start of the dense stage: tile-task counters of every scene, control words
+    L.zero_off = c.off;
+    for (auto& s : sc) s.b.dag_state = c.take<int>(spd_task_state_ints(s.pl.N));
+    c.take<int>(4);
+    c.off = (c.off + 255) & ~size_t(255);
+    L.zero_bytes = c.off - L.zero_off;
+    L.amax_off = c.off;
+    for (auto& s : sc) s.b.amax = c.take<unsigned long long>(4);
+    c.off = (c.off + 255) & ~size_t(255);
+    L.amax_bytes = c.off - L.amax_off;
+    // status words read back at the end: error words, then Taylor states
+    L.stat_off = c.off;
+    int* errs = c.take<int>(4 * sc.size());
+    TeState* te = c.take<TeState>(sc.size());
+    c.off = (c.off + 255) & ~size_t(255);
+    L.stat_bytes = c.off - L.stat_off;
+    for (size_t i = 0; i < sc.size(); ++i) {
+        sc[i].b.s.err = base ? errs + 4 * i : nullptr;
+        sc[i].b.te = base ? te + i : nullptr;
+    }
+    // descriptors (host-filled, one upload)
+    L.desc_off = c.off;
+    const size_t n = sc.size();
+    c.take<SpdTaskMatrix>(n);
+    c.take<int4>(ntasks);
+    c.take<CUtensorMap>(3 * n);
+    c.take<DenseJob>(n);
+    c.take<long>(n + 1);
+    c.take<long>(n + 1);
+    c.take<MixedSliceJob>(3 * n);
+    c.take<int>(n + 1);
+    c.take<MixedGemmJob>(3 * n);
+    c.take<int4>(ntiles);
+    c.take<double>((size_t)kTaylorIters * n);
+    c.off = (c.off + 255) & ~size_t(255);
+    L.desc_bytes = c.off - L.desc_off;
+    L.total = c.off + 256;
+}
+
+// Device addresses of the descriptor region, in lay_out's order.
+struct Desc {
+    SpdTaskMatrix* mats;
+    int4* tasks;
+    CUtensorMap* maps;
+    DenseJob* dense;
+    long* blk_rows;
+    long* blk_elems;
+    MixedSliceJob* slice;  // [X | P odd | P even]
+    int* row_start;
+    MixedGemmJob* gemm;    // [first | odd | even]
+    int4* tiles;
+    double* kvals;
+};
+
+Desc desc_at(char* base, size_t n, size_t ntasks, size_t ntiles) {
+    Carver c{base};
+    Desc d;
+    d.mats = c.take<SpdTaskMatrix>(n);
+    d.tasks = c.take<int4>(ntasks);
+    d.maps = c.take<CUtensorMap>(3 * n);
+    d.dense = c.take<DenseJob>(n);
+    d.blk_rows = c.take<long>(n + 1);
+    d.blk_elems = c.take<long>(n + 1);
+    d.slice = c.take<MixedSliceJob>(3 * n);
+    d.row_start = c.take<int>(n + 1);
+    d.gemm = c.take<MixedGemmJob>(3 * n);
+    d.tiles = c.take<int4>(ntiles);
+    d.kvals = c.take<double>((size_t)kTaylorIters * n);
+    return d;
+}
+
+struct GroupRun {
+    std::vector<Scene> sc;
+    int slices = 5, nt = 96;
+    Layout L;
+    size_t ntasks = 0, ntiles = 0;
+    long nblk_rows = 0, nblk_elems = 0;
+    int total_rows = 0;
+    Desc dd{};  // device descriptors
+    char* dbase = nullptr;
+    char* hbase = nullptr;  // staging: [IN | OUT | descriptors | status]
+    size_t h_in = 0, h_out = 0, h_desc = 0, h_stat = 0;
+};
+
+// The launch sequence of a group on b->stream (captured or direct).
+int launch_group(unc_batch* b, GroupRun& g, cudaEvent_t taylor0, cudaEvent_t taylor1) {
+    cudaStream_t sm = b->stream;
+    const int n = (int)g.sc.size();
+    BCK(cudaEventRecord(b->fork, sm));
+    for (int k = 0; k < kBranches; ++k) BCK(cudaStreamWaitEvent(b->branch[k], b->fork, 0));
+    for (int i = 0; i < n; ++i) {
+        Scene& s = g.sc[i];
+        cudaStream_t br = b->branch[i % kBranches];
+        int fx[3];
+        if (int r = sparse_stage(&s.opt, s.pl, s.nnz, s.in_rows, s.in_cols, s.in_vals, s.b, fx, nullptr, br,
+                                 &s.pair_buf, &s.pair_bytes, s.pairs_cap))
+            return r;
+    }
+    for (int k = 0; k < kBranches; ++k) {
+        BCK(cudaEventRecord(b->join[k], b->branch[k]));
+        BCK(cudaStreamWaitEvent(sm, b->join[k], 0));
+    }
+    // the dense stage, grouped (compute.cpp:121-166)
+    BCK(cudaMemsetAsync(g.dbase + g.L.mixed_off, 0, g.L.mixed_bytes, sm));  // slice padding must be zero
+    BCK(cudaMemsetAsync(g.dbase + g.L.zero_off, 0, g.L.zero_bytes, sm));
+    launch_shift_equilibrate_grouped(g.dd.dense, n, g.dd.blk_rows, g.nblk_rows, g.dd.blk_elems, g.nblk_elems, sm);
+    int* ctl = reinterpret_cast<int*>(g.dbase + g.L.zero_off + g.L.zero_bytes - 256);
+    if (int r = chol_inverse_tasks_grouped(g.dd.mats, g.dd.tasks, (int)g.ntasks, ctl, sm, device_sms())) return r;
+    launch_unequilibrate_grouped(g.dd.dense, n, g.dd.blk_elems, g.nblk_elems, sm);  // X in Z, iZ = X
+    if (taylor0) BCK(cudaEventRecord(taylor0, sm));
+    mixed_slice_grouped(g.dd.slice, n, g.dd.row_start, g.total_rows, sm);  // X
+    launch_te_init_grouped(g.dd.dense, n, sm);
+    BCK(cudaMemsetAsync(g.dbase + g.L.amax_off, 0, g.L.amax_bytes, sm));
+    mixed_gemm_grouped(g.slices, g.nt, g.dd.gemm, g.dd.tiles, (int)g.ntiles, sm);  // X X -> add
+    for (int it = 1; it <= kTaylorIters; ++it) {
+        const int par = 1 + ((it - 1) & 1);  // odd iterations: add -> tmp, even: tmp -> add
+        launch_te_decide_grouped(g.dd.dense, n, g.dd.kvals + (size_t)(it - 1) * n, sm);
+        BCK(cudaMemsetAsync(g.dbase + g.L.amax_off, 0, g.L.amax_bytes, sm));
+        mixed_slice_grouped(g.dd.slice + (size_t)par * n, n, g.dd.row_start, g.total_rows, sm);
+        mixed_gemm_grouped(g.slices, g.nt, g.dd.gemm + (size_t)par * n, g.dd.tiles, (int)g.ntiles, sm);
+    }
+    if (taylor1) BCK(cudaEventRecord(taylor1, sm));
+    // outputs (compute.cpp:168-183, 370-455)
+    BCK(cudaEventRecord(b->fork, sm));
+    for (int k = 0; k < kBranches; ++k) BCK(cudaStreamWaitEvent(b->branch[k], b->fork, 0));
+    for (int i = 0; i < n; ++i) output_stage(g.sc[i].pl, g.sc[i].b, g.sc[i].out_cam, g.sc[i].out_pt,
+                                             b->branch[i % kBranches]);
+    for (int k = 0; k < kBranches; ++k) {
+        BCK(cudaEventRecord(b->join[k], b->branch[k]));
+        BCK(cudaStreamWaitEvent(sm, b->join[k], 0));
+    }
+    return UNC_OK;
+}
+
+// Prepare a group for tile width nt: layout, buffers, descriptors uploaded.
+int prepare_group(unc_batch* b, GroupRun& g, int nt) {
+    g.nt = nt;
+    const int n = (int)g.sc.size();
+    std::vector<int> ns(n);
+    for (int i = 0; i < n; ++i) ns[i] = g.sc[i].pl.N;
+    const std::vector<int4> tasks = spd_tasks_grouped_list(ns);
+    g.ntasks = tasks.size();
+    // product tiles, larger K first (longer tiles start early)
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return ns[a] > ns[c]; });
+    std::vector<int4> tiles;
+    for (int i : order) mixed_lower_tiles(i, ns[i], nt, tiles);
+    g.ntiles = tiles.size();
+    lay_out(nullptr, g.sc, g.slices, nt, g.L, g.ntasks, g.ntiles);
+    cudaStream_t sm = b->stream;
+    if (b->ws_bytes < g.L.total) {
+        if (b->ws) BCK(cudaFreeAsync(b->ws, sm));
+        b->ws = nullptr;
+        b->ws_bytes = 0;
+        BCK(cudaMallocAsync(&b->ws, g.L.total, sm));
+        b->ws_bytes = g.L.total;
+        for (auto& gr : b->graphs) cudaGraphExecDestroy(gr.exec);  // they name the old addresses
+        b->graphs.clear();
+    }
+    g.dbase = (char*)b->ws;
+    lay_out(g.dbase, g.sc, g.slices, nt, g.L, g.ntasks, g.ntiles);
+    // pinned staging: [IN | OUT | descriptors | status]
+    g.h_in = 0;
+    g.h_out = g.L.in_bytes;
+    g.h_desc = g.h_out + g.L.out_bytes;
+    g.h_stat = g.h_desc + g.L.desc_bytes;
+    const size_t hneed = g.h_stat + g.L.stat_bytes + 256;
+    if (b->host_bytes < hneed) {
+        BCK(cudaStreamSynchronize(sm));
+        if (b->host) cudaFreeHost(b->host);
+        b->host = nullptr;
+        b->host_bytes = 0;
+        BCK(cudaMallocHost(&b->host, hneed));
+        b->host_bytes = hneed;
+    }
+    g.hbase = (char*)b->host;
+    // descriptors
+    g.dd = desc_at(g.dbase + g.L.desc_off, n, g.ntasks, g.ntiles);
+    BCK(cudaStreamSynchronize(sm));  // the staging area is reused
+    char* hd = g.hbase + g.h_desc;
+    const Desc hdd = desc_at(hd, n, g.ntasks, g.ntiles);
+    memset(hd, 0, g.L.desc_bytes);
+    long br = 0, be = 0;
+    int rs = 0;
+    for (int i = 0; i < n; ++i) {
+        Scene& s = g.sc[i];
+        const int N = s.pl.N;
+        const long ld = s.pl.ld;
+        hdd.mats[i] = SpdTaskMatrix{s.b.Z, s.b.iZ, s.b.add, ld, N, (N / 64 + (N % 64 != 0)) *
+                                                                        (N / 64 + (N % 64 != 0) + 1) / 2,
+                                    s.b.dag_state, s.b.s.err};
+        MixedOperand xa, xb, p;
+        if (!mixed_plan_nt(xa, s.bufX, s.eX, N, g.slices, false, nt) ||
+            !mixed_plan_nt(xb, s.bufX, s.eX, N, g.slices, true, nt) ||
+            !mixed_plan_nt(p, s.bufP, s.eP, N, g.slices, false, nt))
+            return bfail(UNC_ERR_CUDA, "tensor-map encoding failed");
+        hdd.maps[3 * i] = xa.map;
+        hdd.maps[3 * i + 1] = xb.map;
+        hdd.maps[3 * i + 2] = p.map;
+        hdd.dense[i] = DenseJob{s.b.Z, s.b.iZ, s.b.add, s.b.e, ld, N, s.lambda, s.b.s.err, s.b.te, s.b.amax};
+        hdd.blk_rows[i] = br;
+        hdd.blk_elems[i] = be;
+        br += (N + 255) / 256;
+        be += ((long)N * N + 255) / 256;
+        hdd.row_start[i] = rs;
+        rs += N;
+        // slicing: X (no update), then the power of odd / even iterations with the Taylor update
+        hdd.slice[i] = MixedSliceJob{s.b.Z, ld, N, g.slices, s.bufX, xa.rows, xa.kp, s.eX, nullptr, nullptr, nullptr};
+        hdd.slice[n + i] = MixedSliceJob{s.b.add, ld, N, g.slices, s.bufP, p.rows, p.kp, s.eP, s.b.iZ, s.b.te,
+                                         &s.b.te->done};
+        hdd.slice[2 * n + i] = MixedSliceJob{s.b.tmp, ld, N, g.slices, s.bufP, p.rows, p.kp, s.eP, s.b.iZ, s.b.te,
+                                             &s.b.te->done};
+        const CUtensorMap* dm = g.dd.maps + 3 * i;
+        hdd.gemm[i] = MixedGemmJob{dm, dm + 1, N, xa.kp, xa.rows, xb.rows, s.eX, s.eX, s.b.add, ld, s.b.amax,
+                                   s.b.s.err, nullptr};
+        hdd.gemm[n + i] = MixedGemmJob{dm + 2, dm + 1, N, p.kp, p.rows, xb.rows, s.eP, s.eX, s.b.tmp, ld, s.b.amax,
+                                       s.b.s.err, &s.b.te->done};
+        hdd.gemm[2 * n + i] = MixedGemmJob{dm + 2, dm + 1, N, p.kp, p.rows, xb.rows, s.eP, s.eX, s.b.add, ld,
+                                           s.b.amax, s.b.s.err, &s.b.te->done};
+        for (int it = 1; it <= kTaylorIters; ++it)
+            hdd.kvals[(size_t)(it - 1) * n + i] = pow(s.lambda, it) / factorial_i32(it - 1);
+    }
+    hdd.blk_rows[n] = br;
+    hdd.blk_elems[n] = be;
+    hdd.row_start[n] = rs;
+    g.nblk_rows = br;
+    g.nblk_elems = be;
+    g.total_rows = rs;
+    memcpy(hdd.tasks, tasks.data(), sizeof(int4) * tasks.size());
+    memcpy(hdd.tiles, tiles.data(), sizeof(int4) * tiles.size());
+    BCK(cudaMemcpyAsync(g.dbase + g.L.desc_off, hd, g.L.desc_bytes, cudaMemcpyHostToDevice, sm));
+    return UNC_OK;
+}
+
+std::vector<unsigned long long> shape_key(const unc_batch* b, const GroupRun& g) {
+    std::vector<unsigned long long> k = {(unsigned long long)(uintptr_t)b->ws, (unsigned long long)g.sc.size(),
+                                         (unsigned long long)g.slices, (unsigned long long)g.nt};
+    for (const Scene& s : g.sc) {
+        unsigned long long lam;
+        memcpy(&lam, &s.lambda, 8);
+        k.insert(k.end(), {(unsigned long long)s.pl.C, (unsigned long long)s.pl.P, (unsigned long long)s.pl.nobs,
+                           (unsigned long long)s.nnz, (unsigned long long)s.pairs_cap,
+                           (unsigned long long)(unsigned)s.fx[0] << 32 | (unsigned)s.fx[1],
+                           (unsigned long long)(unsigned)s.fx[2], lam});
+    }
+    return k;
+}
+
+// Run the device part of a group: from the graph of its shape when there is
+// one, else directly (and capture it when the shape was seen before).
+int run_device(unc_batch* b, GroupRun& g, cudaEvent_t taylor0, cudaEvent_t taylor1) {
+    if (taylor0) return launch_group(b, g, taylor0, taylor1);  // timed runs (the autotuner) are not captured
+    const auto key = shape_key(b, g);
+    for (auto& gr : b->graphs)
+        if (gr.key == key) {
+            BCK(cudaGraphLaunch(gr.exec, b->stream));
+            count_launch((int)gr.launches);
+            return UNC_OK;
+        }
+    const bool again = std::find(b->seen.begin(), b->seen.end(), key) != b->seen.end();
+    if (!again) {
+        if (b->seen.size() >= 16) b->seen.erase(b->seen.begin());
+        b->seen.push_back(key);
+        return launch_group(b, g, nullptr, nullptr);
+    }
+    const long long l0 = g_thread_launches;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool ok = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    int rc = UNC_OK;
+    if (ok) {
+        rc = launch_group(b, g, nullptr, nullptr);
+        ok = cudaStreamEndCapture(b->stream, &graph) == cudaSuccess && rc == UNC_OK && graph;
+    }
+    if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    const long long launches = g_thread_launches - l0;  // captured, not run
+    __atomic_sub_fetch(&g_launches, launches, __ATOMIC_RELAXED);
+    g_thread_launches -= launches;
+    if (!ok) {
+        cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        return launch_group(b, g, nullptr, nullptr);
+    }
+    if (b->graphs.size() >= (size_t)kGraphs) {
+        cudaGraphExecDestroy(b->graphs.front().exec);
+        b->graphs.erase(b->graphs.begin());
+    }
+    b->graphs.push_back(Graph{key, exec, launches});
+    BCK(cudaGraphLaunch(exec, b->stream));
+    count_launch((int)launches);
+    return UNC_OK;
+}
+
+int run_group(unc_batch* b, GroupRun& g, const int* const* rows, const int* const* cols,
+              const double* const* values, double* const* cam_unc, double* const* pt_unc, int* status,
+              unc_statistic* stats) {
+    cudaStream_t sm = b->stream;
+    // tile width: the size class's cached choice, else time every candidate
+    const std::vector<int> cand = mixed_tile_candidates(g.slices);
+    long tiles96 = 0;
+    for (const Scene& s : g.sc) tiles96 += lower_tile_count(s.pl.N, 96);
+    const int size_class = (int)std::lround(2.0 * std::log2((double)std::max(1L, tiles96)));
+    const auto ck = std::make_pair(g.slices, size_class);
+    auto hit = b->tile_choice.find(ck);
+    // every candidate computes the same bytes; the last one run leaves the results
+    const std::vector<int> trials = hit != b->tile_choice.end() ? std::vector<int>{hit->second} : cand;
+    float best_ms = 0;
+    int best = trials[0];
+    for (size_t t = 0; t < trials.size(); ++t) {
+        if (int r = prepare_group(b, g, trials[t])) return r;
+        // inputs: pack and copy (one transfer)
+        std::vector<Copy> cp;
+        for (const Scene& s : g.sc) {
+            cp.push_back({g.hbase + g.h_in + s.in_off[0], rows[s.idx], sizeof(int) * ((size_t)s.pl.nobs * 2 + 1)});
+            cp.push_back({g.hbase + g.h_in + s.in_off[1], cols[s.idx], sizeof(int) * (size_t)s.nnz});
+            cp.push_back({g.hbase + g.h_in + s.in_off[2], values[s.idx], sizeof(double) * (size_t)s.nnz});
+        }
+        parallel_copy(cp);
+        BCK(cudaEventRecord(b->ev[0], sm));
+        BCK(cudaMemcpyAsync(g.dbase, g.hbase + g.h_in, g.L.in_bytes, cudaMemcpyHostToDevice, sm));
+        BCK(cudaEventRecord(b->ev[1], sm));
+        const bool timed = trials.size() > 1;
+        if (int r = run_device(b, g, timed ? b->ev[4] : nullptr, timed ? b->ev[5] : nullptr)) return r;
+        BCK(cudaEventRecord(b->ev[2], sm));
+        BCK(cudaMemcpyAsync(g.hbase + g.h_out, g.dbase + g.L.in_bytes, g.L.out_bytes, cudaMemcpyDeviceToHost, sm));
+        BCK(cudaMemcpyAsync(g.hbase + g.h_stat, g.dbase + g.L.stat_off, g.L.stat_bytes, cudaMemcpyDeviceToHost, sm));
+        BCK(cudaEventRecord(b->ev[3], sm));
+        BCK(cudaStreamSynchronize(sm));
+        BCK(cudaGetLastError());
+        if (timed) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, b->ev[4], b->ev[5]);
+            if (t == 0 || ms < best_ms) {
+                best_ms = ms;
+                best = trials[t];
+            }
+        }
+    }
+    if (hit == b->tile_choice.end()) b->tile_choice[ck] = best;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
+    b->t_h2d += ms * 1e-3;
+    cudaEventElapsedTime(&ms, b->ev[1], b->ev[2]);
+    b->t_dev += ms * 1e-3;
+    cudaEventElapsedTime(&ms, b->ev[2], b->ev[3]);
+    b->t_d2h += ms * 1e-3;
+    b->grouped += (int)g.sc.size();
+    b->tile_n = g.nt;
+    // outputs: the reference's zeroing rule as in unc_compute (fixed points past
+    // 6 (P - 3) keep the caller's values)
+    std::vector<Copy> cp;
+    const int* errs = reinterpret_cast<const int*>(g.hbase + g.h_stat);
+    const TeState* tes = reinterpret_cast<const TeState*>(g.hbase + g.h_stat + ((4 * g.sc.size() * sizeof(int) + 255) & ~size_t(255)));
+    for (size_t i = 0; i < g.sc.size(); ++i) {
+        const Scene& s = g.sc[i];
+        const int err = errs[4 * i];
+        const TeState& te = tes[i];
+        int rc = UNC_OK;
+        if (err & ERRBIT_LAYOUT) rc = UNC_ERR_LAYOUT;
+        else if (err & (ERRBIT_SINGULAR | ERRBIT_NONFINITE)) rc = UNC_ERR_SINGULAR;
+        else if (err & (ERRBIT_TIMEOUT | ERRBIT_PAIR_CAP)) rc = UNC_ERR_CUDA;
+        else if (te.bad) rc = UNC_ERR_SINGULAR;
+        status[s.idx] = rc;
+        if (stats) {
+            unc_statistic& st = stats[s.idx];
+            memset(&st, 0, sizeof(st));
+            st.lambda = s.lambda;
+            for (int k = 0; k < 3; ++k) st.fixed_pts[k] = s.fx[k];
+            st.te_iterations = te.iters;
+            for (int k = 0; k < te.iters && k < 20; ++k) st.cycle_change[k] = te.change[k];
+            st.time_all = b->t_h2d + b->t_dev + b->t_d2h;  // the batch's, shared by its scenes
+            st.device_bytes = (long long)(g.L.total / g.sc.size());
+        }
+        if (rc != UNC_OK) continue;
+        cp.push_back({cam_unc[s.idx], g.hbase + g.h_out + (s.out_off[0] - g.L.in_bytes),
+                      sizeof(double) * 45 * (size_t)s.pl.C});
+        const size_t head = s.pl.P > 3 ? (size_t)(s.pl.P - 3) : 0;
+        const char* hp = g.hbase + g.h_out + (s.out_off[1] - g.L.in_bytes);
+        if (head) cp.push_back({pt_unc[s.idx], hp, sizeof(double) * 6 * head});
+        for (int p = (int)head; p < s.pl.P; ++p) {
+            if (p == s.fx[0] || p == s.fx[1] || p == s.fx[2]) continue;
+            cp.push_back({pt_unc[s.idx] + 6L * p, hp + sizeof(double) * 6 * (size_t)p, sizeof(double) * 6});
+        }
+    }
+    parallel_copy(cp);
+    return UNC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int unc_batch_create(int device, unc_batch** out) {
+    if (!out) return bfail(UNC_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    unc_batch* b = new unc_batch();
+    b->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) {
+        prepare_assembly_kernels();
+        prepare_dense_kernels();
+        prepare_mixed_kernels();
+        prepare_task_kernels();
+        e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    }
+    for (int k = 0; k < kBranches && e == cudaSuccess; ++k) e = cudaStreamCreateWithFlags(&b->branch[k], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    for (int k = 0; k < kBranches && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming);
+    for (int k = 0; k < 6 && e == cudaSuccess; ++k) e = cudaEventCreate(&b->ev[k]);
+    if (e != cudaSuccess) {
+        g_last_error = std::string("unc_batch_create: ") + cudaGetErrorString(e);
+        unc_batch_destroy(b);
+        return UNC_ERR_CUDA;
+    }
+    *out = b;
+    return UNC_OK;
+}
+
+int unc_batch_destroy(unc_batch* b) {
+    if (!b) return UNC_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (auto& g : b->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (b->ws) cudaFree(b->ws);
+    if (b->host) cudaFreeHost(b->host);
+    if (b->single) unc_context_destroy(b->single);
+    for (int k = 0; k < 6; ++k)
+        if (b->ev[k]) cudaEventDestroy(b->ev[k]);
+    for (int k = 0; k < kBranches; ++k) {
+        if (b->join[k]) cudaEventDestroy(b->join[k]);
+        if (b->branch[k]) cudaStreamDestroy(b->branch[k]);
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return UNC_OK;
+}
+
+int unc_batch_compute(unc_batch* b, int num_scenes, const unc_options* opts, const int* num_rows,
+                      const int* num_cols, const int* const* rows, const int* const* cols,
+                      const double* const* values, double* const* cam_unc, double* const* pt_unc, int* status,
+                      unc_statistic* stats) {
+    g_last_error.clear();
+    if (!b || num_scenes < 0 || (num_scenes > 0 && (!opts || !num_rows || !num_cols || !rows || !cols || !values ||
+                                                    !cam_unc || !pt_unc || !status)))
+        return bfail(UNC_ERR_INVALID_ARG, "unc_batch_compute: null argument");
+    BCK(cudaSetDevice(b->device));
+    b->t_h2d = b->t_dev = b->t_d2h = 0;
+    b->grouped = 0;
+    std::map<int, GroupRun> groups;  // by slice count
+    std::vector<int> single;
+    for (int i = 0; i < num_scenes; ++i) {
+        const unc_options* o = opts + i;
+        status[i] = check_options(o, num_rows[i], num_cols[i]);
+        if (status[i] != UNC_OK) continue;
+        if (!rows[i] || !cols[i] || !values[i] || !cam_unc[i] || !pt_unc[i]) {
+            status[i] = UNC_ERR_INVALID_ARG;
+            continue;
+        }
+        const long long nnz = rows[i][num_rows[i]];
+        if (nnz < 0 || rows[i][0] != 0 || nnz != 24LL * (num_rows[i] / 2)) {  // the layout the grouped path stages
+            single.push_back(i);
+            continue;
+        }
+        if (o->algorithm != UNC_TAYLOR_EXPANSION || o->precision == UNC_PRECISION_FP64 ||
+            !spd_tasks_apply(9 * o->num_cams)) {
+            single.push_back(i);
+            continue;
+        }
+        Scene s{};
+        s.idx = i;
+        s.opt = *o;
+        s.pl = make_plan(o, num_rows[i]);
+        s.nnz = nnz;
+        s.pairs_cap = schur_pairs_bound(o, num_rows[i], nnz, cols[i]);
+        s.fx[0] = o->pts2fix[0];
+        s.fx[1] = o->pts2fix[1];
+        s.fx[2] = o->pts2fix[2];
+        std::sort(s.fx, s.fx + 2);  // the reference sorts only the first two ids (compute.cpp:285)
+        s.lambda = o->lambda == -1 ? auto_lambda(s.pl.N) : o->lambda;  // compute.cpp:124-125
+        GroupRun& g = groups[slices_of(o->precision)];
+        g.slices = slices_of(o->precision);
+        g.sc.push_back(s);
+    }
+    for (auto& kv : groups) {
+        if (int r = run_group(b, kv.second, rows, cols, values, cam_unc, pt_unc, status, stats)) return r;
+    }
+    for (int i : single) {
+        if (!b->single) {
+            if (int r = unc_context_create(b->device, &b->single)) return r;
+        }
+        status[i] = unc_compute(b->single, opts + i, num_rows[i], num_cols[i], rows[i], cols[i], values[i],
+                                cam_unc[i], pt_unc[i], stats ? stats + i : nullptr);
+    }
+    return UNC_OK;
+}
+
+long long unc_batch_device_bytes(const unc_batch* b) {
+    if (!b) return -1;
+    return (long long)b->ws_bytes + (b->single ? unc_context_device_bytes(b->single) : 0);
+}
+
+int unc_batch_release(unc_batch* b) {
+    if (!b) return bfail(UNC_ERR_INVALID_ARG, "batch is NULL");
+    BCK(cudaSetDevice(b->device));
+    BCK(cudaStreamSynchronize(b->stream));
+    for (auto& g : b->graphs) cudaGraphExecDestroy(g.exec);
+    b->graphs.clear();
+    b->seen.clear();
+    if (b->ws) BCK(cudaFree(b->ws));
+    b->ws = nullptr;
+    b->ws_bytes = 0;
+    if (b->single) unc_context_release(b->single);
+    return UNC_OK;
+}
+
+int unc_batch_last_timing(const unc_batch* b, double* h2d_s, double* device_s, double* d2h_s, int* grouped_scenes,
+                          int* tile_n) {
+    if (!b) return bfail(UNC_ERR_INVALID_ARG, "batch is NULL");
+    if (h2d_s) *h2d_s = b->t_h2d;
+    if (device_s) *device_s = b->t_dev;
+    if (d2h_s) *d2h_s = b->t_d2h;
+    if (grouped_scenes) *grouped_scenes = b->grouped;
+    if (tile_n) *tile_n = b->tile_n;
+    return UNC_OK;
+}
+
+}  // extern "C"

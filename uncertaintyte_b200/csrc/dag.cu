@@ -491,14 +491,20 @@ std::vector<int4> spd_tasks_grouped_list(const std::vector<int>& ns) {
     return out;
 }
 
+void prepare_task_kernels() {
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
+        return cudaFuncSetAttribute(k_spd_inverse_tasks, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)DAG_SMEM) == cudaSuccess &&
+               cudaFuncSetAttribute(k_spd_inverse_tasks_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)DAG_SMEM) == cudaSuccess;
+    });
+}
+
 int chol_inverse_tasks_grouped(const SpdTaskMatrix* d_mats, const int4* d_tasks, int ntasks, int* ctl,
                                cudaStream_t st, int max_ctas, long long poll_limit) {
     if (ntasks <= 0) return UNC_OK;
-    static std::atomic<unsigned long long> attr{0};
-    once_per_device(attr, [] {
-        return cudaFuncSetAttribute(k_spd_inverse_tasks_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)DAG_SMEM) == cudaSuccess;
-    });
+    prepare_task_kernels();
     const long spin = poll_limit > 0 ? (long)std::min<long long>(poll_limit, kDagSpin) : kDagSpin;
     const int grid = std::max(1, std::min(std::min(device_sms(), max_ctas), ntasks));
     k_spd_inverse_tasks_grouped<<<grid, DAG_THREADS, DAG_SMEM, st>>>(d_mats, d_tasks, ntasks, ctl, spin);

@@ -451,9 +451,7 @@ void chol_inverse(double* A, int n, int lda, double* T, double* W, double* Tt, d
 // ------------------------------------------------------------------------
 // elementwise helpers
 // ------------------------------------------------------------------------
-__global__ void k_shift_diag_scale(double* A, int n, long lda, double lambda, double* e, int* err) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__device__ __forceinline__ void shift_diag_one(double* A, int i, long lda, double lambda, double* e, int* err) {
     double d = A[i + i * lda] + lambda;
     A[i + i * lda] = d;
     if (!(d > 0.0 && isfinite(d))) {
@@ -464,15 +462,27 @@ __global__ void k_shift_diag_scale(double* A, int n, long lda, double lambda, do
     }
 }
 
+__global__ void k_shift_diag_scale(double* A, int n, long lda, double lambda, double* e, int* err) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    shift_diag_one(A, i, lda, lambda, e, err);
+}
+
+// element idx of a column-major n x n matrix: A <- A e_r e_c (and Y = the same)
+__device__ __forceinline__ void scale_sym_one(double* A, long idx, int n, long lda, const double* __restrict__ e,
+                                              double* Y, long ldy) {
+    int c = (int)(idx / n), r = (int)(idx - (long)c * n);
+    double v = A[r + c * lda] * e[r] * e[c];
+    A[r + c * lda] = v;
+    if (Y) Y[r + c * ldy] = v;
+}
+
 __global__ void k_scale_sym(double* A, int n, long lda, const double* __restrict__ e,
                             double* Y, long ldy) {
     long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
     long total = (long)n * n;
     if (idx >= total) return;
-    int c = (int)(idx / n), r = (int)(idx - (long)c * n);
-    double v = A[r + c * lda] * e[r] * e[c];
-    A[r + c * lda] = v;
-    if (Y) Y[r + c * ldy] = v;
+    scale_sym_one(A, idx, n, lda, e, Y, ldy);
 }
 
 void launch_shift_equilibrate(double* A, int n, int lda, double lambda, double* e, int* err,
@@ -483,15 +493,20 @@ void launch_shift_equilibrate(double* A, int n, int lda, double lambda, double* 
     count_launch(2);
 }
 
+__device__ __forceinline__ void scale_sym_from_one(const double* __restrict__ S, double* A, long idx, int n,
+                                                   long lda, const double* __restrict__ e, double* Y, long ldy) {
+    int c = (int)(idx / n), r = (int)(idx - (long)c * n);
+    double v = S[r + c * lda] * e[r] * e[c];
+    A[r + c * lda] = v;
+    if (Y) Y[r + c * ldy] = v;
+}
+
 __global__ void k_scale_sym_from(const double* __restrict__ S, double* A, int n, long lda,
                                  const double* __restrict__ e, double* Y, long ldy) {
     long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
     long total = (long)n * n;
     if (idx >= total) return;
-    int c = (int)(idx / n), r = (int)(idx - (long)c * n);
-    double v = S[r + c * lda] * e[r] * e[c];
-    A[r + c * lda] = v;
-    if (Y) Y[r + c * ldy] = v;
+    scale_sym_from_one(S, A, idx, n, lda, e, Y, ldy);
 }
 
 void launch_unequilibrate_from(const double* S, double* X, int n, int lda, const double* e, double* Y,
@@ -522,8 +537,8 @@ void launch_axpy(double* Y, const double* X, double k, int n, int ld, cudaStream
     count_launch();
 }
 
-__global__ void k_te_decide(TeState* s, const unsigned long long* amax_bits, double k) {
-    if (threadIdx.x != 0 || blockIdx.x != 0 || s->done) return;
+__device__ __forceinline__ void te_decide_one(TeState* s, const unsigned long long* amax_bits, double k) {
+    if (s->done) return;
     double amax = __longlong_as_double((long long)*amax_bits);
     amax = fmax(amax, 2.2250738585072014e-308);  // absMax starts at DBL_MIN (ScaledDenseMatrix.cpp:208)
     if (!(amax <= 1.7976931348623157e308)) s->bad = 1;
@@ -538,14 +553,92 @@ __global__ void k_te_decide(TeState* s, const unsigned long long* amax_bits, dou
     s->coef = k;
 }
 
-__global__ void k_te_init(TeState* s) {
+__global__ void k_te_decide(TeState* s, const unsigned long long* amax_bits, double k) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    te_decide_one(s, amax_bits, k);
+}
+
+__device__ __forceinline__ void te_init_one(TeState* s) {
     s->done = 0;
     s->bad = 0;
     s->iters = 0;
     s->old_change = 1.7976931348623157e308;  // DBL_MAX (compute.cpp:140)
     s->coef = 0.0;
     for (int i = 0; i < 20; ++i) s->change[i] = 0.0;
+}
+
+__global__ void k_te_init(TeState* s) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    te_init_one(s);
+}
+
+// ---- grouped forms over the dense stages of many matrices (a batch) ----
+// Block b of an element-wise launch belongs to job m with blk[m] <= b < blk[m + 1].
+__device__ __forceinline__ int job_of_block(const long* __restrict__ blk, int njobs, long b) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (blk[mid] <= b) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_shift_diag_scale_grouped(const DenseJob* __restrict__ jobs, int njobs, const long* __restrict__ blk) {
+    const int m = job_of_block(blk, njobs, blockIdx.x);
+    const DenseJob& j = jobs[m];
+    const long i = (blockIdx.x - blk[m]) * (long)blockDim.x + threadIdx.x;
+    if (i < j.n) shift_diag_one(j.Z, (int)i, j.ld, j.lambda, j.e, j.err);
+}
+
+__global__ void k_scale_sym_grouped(const DenseJob* __restrict__ jobs, int njobs, const long* __restrict__ blk) {
+    const int m = job_of_block(blk, njobs, blockIdx.x);
+    const DenseJob& j = jobs[m];
+    const long idx = (blockIdx.x - blk[m]) * (long)blockDim.x + threadIdx.x;
+    if (idx < (long)j.n * j.n) scale_sym_one(j.Z, idx, j.n, j.ld, j.e, nullptr, 0);
+}
+
+__global__ void k_unequilibrate_grouped(const DenseJob* __restrict__ jobs, int njobs, const long* __restrict__ blk) {
+    const int m = job_of_block(blk, njobs, blockIdx.x);
+    const DenseJob& j = jobs[m];
+    const long idx = (blockIdx.x - blk[m]) * (long)blockDim.x + threadIdx.x;
+    if (idx < (long)j.n * j.n) scale_sym_from_one(j.add, j.Z, idx, j.n, j.ld, j.e, j.iZ, j.ld);
+}
+
+__global__ void k_te_init_grouped(const DenseJob* __restrict__ jobs, int njobs) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < njobs) te_init_one(jobs[m].te);
+}
+
+__global__ void k_te_decide_grouped(const DenseJob* __restrict__ jobs, int njobs, const double* __restrict__ k) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < njobs) te_decide_one(jobs[m].te, jobs[m].amax, k[m]);
+}
+
+void launch_shift_equilibrate_grouped(const DenseJob* d_jobs, int njobs, const long* d_blk_rows, long nblk_rows,
+                                      const long* d_blk_elems, long nblk_elems, cudaStream_t st) {
+    if (njobs <= 0) return;
+    k_shift_diag_scale_grouped<<<(unsigned)nblk_rows, 256, 0, st>>>(d_jobs, njobs, d_blk_rows);
+    k_scale_sym_grouped<<<(unsigned)nblk_elems, 256, 0, st>>>(d_jobs, njobs, d_blk_elems);
+    count_launch(2);
+}
+
+void launch_unequilibrate_grouped(const DenseJob* d_jobs, int njobs, const long* d_blk_elems, long nblk_elems,
+                                  cudaStream_t st) {
+    if (njobs <= 0) return;
+    k_unequilibrate_grouped<<<(unsigned)nblk_elems, 256, 0, st>>>(d_jobs, njobs, d_blk_elems);
+    count_launch();
+}
+
+void launch_te_init_grouped(const DenseJob* d_jobs, int njobs, cudaStream_t st) {
+    if (njobs <= 0) return;
+    k_te_init_grouped<<<(njobs + 127) / 128, 128, 0, st>>>(d_jobs, njobs);
+    count_launch();
+}
+
+void launch_te_decide_grouped(const DenseJob* d_jobs, int njobs, const double* d_k, cudaStream_t st) {
+    if (njobs <= 0) return;
+    k_te_decide_grouped<<<(njobs + 127) / 128, 128, 0, st>>>(d_jobs, njobs, d_k);
+    count_launch();
 }
 
 void launch_te_init(TeState* s, cudaStream_t st) {

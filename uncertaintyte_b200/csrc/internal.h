@@ -20,6 +20,7 @@ enum : int {
     ERRBIT_NONFINITE = 4,   // NaN / Inf produced
     ERRBIT_SORT_CAP = 8,    // a segment was too long to sort (order left nondeterministic)
     ERRBIT_TIMEOUT = 16,    // a bounded device wait ran out (tensor-core pipeline)
+    ERRBIT_PAIR_CAP = 32,   // more Schur observation pairs than the pair list holds (nothing scattered)
 };
 
 constexpr int kCamParams = 9;
@@ -102,6 +103,7 @@ struct SceneDev {
     int* blk_cnt;         // num_cams^2: pair counts, then scatter cursors, per camera-pair block
     int* blk_ptr;         // num_cams^2 + 1: pair list offsets per block
     unsigned long long* pairs;  // (o << 32 | o') per block, sorted inside a block
+    long pair_cap;        // capacity of `pairs` (entries)
     int* long_list;       // [count, ids...] of blocks with more than 1024 pairs
     int long_cap;         // capacity of long_list ids
     int* nz_list;         // [count, cursor, ids...] of the non-empty camera-pair blocks
@@ -216,6 +218,9 @@ struct SpdTaskMatrix {
 // matrix's own order kept, merged by fractional position so that all matrices
 // progress together; task.x = type + 8 * matrix index.
 std::vector<int4> spd_tasks_grouped_list(const std::vector<int>& ns);
+// Shared-memory attributes of the tile-task kernels (current device; call it
+// outside any stream capture).
+void prepare_task_kernels();
 // One persistent launch over the list (d_mats / d_tasks in device memory; ctl:
 // 2 ints, zeroed by the caller in stream order, as is every matrix's state).
 int chol_inverse_tasks_grouped(const SpdTaskMatrix* d_mats, const int4* d_tasks, int ntasks, int* ctl,
@@ -240,6 +245,27 @@ struct TeState {
 void launch_te_decide(TeState* s, const unsigned long long* amax, double k, cudaStream_t st);
 // Reset the state (not done, no iteration, old change = DBL_MAX).
 void launch_te_init(TeState* s, cudaStream_t st);
+// Grouped dense-stage kernels over many matrices (a batch). Element-wise
+// launches: block b belongs to job m with blk[m] <= b < blk[m + 1] (blk: njobs
+// + 1 longs; 256 threads per block over the job's rows, or n^2 elements).
+struct DenseJob {
+    double *Z, *iZ, *add, *e;  // Z (in: Schur complement, out: X), iZ (T, then X), add (O = inverse)
+    long ld;
+    int n;
+    double lambda;
+    int* err;
+    TeState* te;
+    const unsigned long long* amax;
+};
+// Z += lambda I and the symmetric equilibration of every job (as launch_shift_equilibrate).
+void launch_shift_equilibrate_grouped(const DenseJob* d_jobs, int njobs, const long* d_blk_rows, long nblk_rows,
+                                      const long* d_blk_elems, long nblk_elems, cudaStream_t st);
+// Z = E add E, iZ = Z for every job (as launch_unequilibrate_from(add, Z, ..., iZ)).
+void launch_unequilibrate_grouped(const DenseJob* d_jobs, int njobs, const long* d_blk_elems, long nblk_elems,
+                                  cudaStream_t st);
+void launch_te_init_grouped(const DenseJob* d_jobs, int njobs, cudaStream_t st);
+// the stop rule of every job with its coefficient d_k[m]
+void launch_te_decide_grouped(const DenseJob* d_jobs, int njobs, const double* d_k, cudaStream_t st);
 // Y <- Y + s->coef * X unless s->done.
 void launch_axpy_te(double* Y, const double* X, const TeState* s, int n, int ld, cudaStream_t st);
 void launch_zero(double* p, size_t n, cudaStream_t st);
@@ -262,6 +288,43 @@ size_t mixed_slice_bytes(int n, int slices);
 // when the driver's tensor-map encoder is unavailable.
 bool mixed_plan(MixedOperand& op, int8_t* buf, int* exps, int n, int slices, bool as_b);
 struct TeState;
+// Operand planning with an explicit output tile width nt (the B boxes' rows):
+// rows padded for both the 128-row A boxes and nt; the slice bytes for it.
+bool mixed_plan_nt(MixedOperand& op, int8_t* buf, int* exps, int n, int slices, bool as_b, int nt);
+size_t mixed_slice_bytes_nt(int n, int slices, int nt);
+// Grouped forms for a batch of matrices (arguments in device memory).
+struct MixedSliceJob {  // k_slice_rows of one matrix
+    const double* A;
+    long lda;
+    int n, S;
+    int8_t* out;
+    int rows_pad, kp;
+    int* exps;
+    double* Y;            // optional Taylor update Y += te->coef * A
+    const TeState* te;
+    const int* skip;      // optional: return when *skip != 0
+};
+struct MixedGemmJob {  // one lower-triangle symmetric product C = P X (mirrored)
+    const CUtensorMap* tA;  // 64-byte aligned maps in device memory
+    const CUtensorMap* tB;
+    int n, kp, rowsA, rowsB;
+    const int* eA;
+    const int* eB;
+    double* C;
+    long ldc;
+    unsigned long long* amax;
+    int* err;
+    const int* skip;
+};
+// block b of the launch slices row b - row_start[m] of job m (row_start: njobs + 1 ints)
+void mixed_slice_grouped(const MixedSliceJob* d_jobs, int njobs, const int* d_row_start, int total_rows,
+                         cudaStream_t st);
+// the lower-triangle 128 x nt tiles of an n x n product, as (job, m0, n0, 0)
+void mixed_lower_tiles(int job, int n, int nt, std::vector<int4>& out);
+// tile widths with a grouped kernel for `slices`: {64, 96} for 5, {128} for 3 and 4
+std::vector<int> mixed_tile_candidates(int slices);
+void mixed_gemm_grouped(int slices, int nt, const MixedGemmJob* d_jobs, const int4* d_tiles, int ntiles,
+                        cudaStream_t st);
 // Y, te (optional): Y += te->coef * A while A is sliced, unless te->done.
 void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st, const int* skip = nullptr,
                  double* Y = nullptr, const TeState* te = nullptr);

@@ -143,13 +143,10 @@ __device__ __forceinline__ double pow2(int e) {
 
 // Y (optional): Y += te->coef * A on the way (the Taylor update iZ += k add of
 // the power being sliced, compute.cpp:64-71), unless te->done.
-__global__ void __launch_bounds__(256) k_slice_rows(const double* __restrict__ A, long lda, int n, int S,
-                                                   int8_t* __restrict__ out, int rows_pad, int kp,
-                                                   int* __restrict__ exps, const int* skip, double* Y,
-                                                   const TeState* te) {
-    if (skip && *skip) return;
-    __shared__ double red[8];
-    const int j = blockIdx.x;
+// Row j of one matrix, all 256 threads of the block (red: 8 shared doubles).
+__device__ __forceinline__ void slice_row(int j, const double* __restrict__ A, long lda, int n, int S,
+                                          int8_t* __restrict__ out, int rows_pad, int kp, int* __restrict__ exps,
+                                          double* Y, const TeState* te, double* red) {
     const double* col = A + (long)j * lda;
     double m = 0.0;
     for (int k = threadIdx.x; k < n; k += 256) m = fmax(m, fabs(col[k]));
@@ -203,15 +200,40 @@ __global__ void __launch_bounds__(256) k_slice_rows(const double* __restrict__ A
     }
 }
 
-template <int NT, int S>
-__global__ void __launch_bounds__(THREADS, 1)
-    k_ozaki_gemm(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int M, int N,
-                 int kp, int rowsA, int rowsB, const int* __restrict__ eA, const int* __restrict__ eB, double* C,
-                 long ldc, unsigned long long* amax, int lower_only, int* err, const int* skip, int mirror) {
-    using Sh = Shape<NT, S>;
+__global__ void __launch_bounds__(256) k_slice_rows(const double* __restrict__ A, long lda, int n, int S,
+                                                   int8_t* __restrict__ out, int rows_pad, int kp,
+                                                   int* __restrict__ exps, const int* skip, double* Y,
+                                                   const TeState* te) {
     if (skip && *skip) return;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * NT;
-    if (lower_only && n0 > m0 + BM - 1) return;
+    __shared__ double red[8];
+    slice_row(blockIdx.x, A, lda, n, S, out, rows_pad, kp, exps, Y, te, red);
+}
+
+// The same over the rows of many matrices (a batch): block b slices row
+// b - row_start[m] of matrix m, row_start[m] <= b < row_start[m + 1].
+__global__ void __launch_bounds__(256) k_slice_rows_grouped(const MixedSliceJob* __restrict__ jobs, int njobs,
+                                                           const int* __restrict__ row_start) {
+    int lo = 0, hi = njobs - 1;
+    const int b = blockIdx.x;
+    while (lo < hi) {  // the last m with row_start[m] <= b
+        const int mid = (lo + hi + 1) >> 1;
+        if (row_start[mid] <= b) lo = mid; else hi = mid - 1;
+    }
+    const MixedSliceJob& jb = jobs[lo];
+    if (jb.skip && *jb.skip) return;
+    __shared__ double red[8];
+    slice_row(b - row_start[lo], jb.A, jb.lda, jb.n, jb.S, jb.out, jb.rows_pad, jb.kp, jb.exps, jb.Y, jb.te, red);
+}
+
+// One 128 x NT output tile at (m0, n0): TMA producer, MMA issuer, epilogue.
+// tA / tB: the operands' tensor maps (kernel parameters, or 64-byte aligned
+// maps in global memory written before the launch: maps_in_global).
+template <int NT, int S>
+__device__ __forceinline__ void ozaki_tile(const CUtensorMap* tA, const CUtensorMap* tB, int m0, int n0, int M, int N,
+                                           int kp, int rowsA, int rowsB, const int* __restrict__ eA,
+                                           const int* __restrict__ eB, double* C, long ldc,
+                                           unsigned long long* amax, int* err, int mirror, bool maps_in_global) {
+    using Sh = Shape<NT, S>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * Sh::STAGE);
@@ -243,6 +265,10 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (warp == 0) {
       if (lane == 0) {
         // TMA producer
+        if (maps_in_global) {  // maps written to global memory by the host: acquire them for the TMA unit
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(tA) : "memory");
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(tB) : "memory");
+        }
         bool ok = true;
         int issued = 0;
         for (int kt = 0; kt < KT && ok; ++kt) {
@@ -255,9 +281,9 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
             uint8_t* st = base + s * Sh::STAGE;
             mbar_expect_tx(full + s, Sh::STAGE);
-            for (int i = 0; i < S; ++i) tma_load_2d(st + i * Sh::A_BOX, &tA, kt * BKB, i * rowsA + m0, full + s);
+            for (int i = 0; i < S; ++i) tma_load_2d(st + i * Sh::A_BOX, tA, kt * BKB, i * rowsA + m0, full + s);
             for (int i = 0; i < S; ++i)
-                tma_load_2d(st + S * Sh::A_BOX + i * Sh::B_BOX, &tB, kt * BKB, i * rowsB + n0, full + s);
+                tma_load_2d(st + S * Sh::A_BOX + i * Sh::B_BOX, tB, kt * BKB, i * rowsB + n0, full + s);
             issued = kt + 1;
         }
         // no copy may be in flight when the CTA exits
@@ -351,6 +377,31 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(Sh::TMEM_COLS));
 }
 
+template <int NT, int S>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_ozaki_gemm(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int M, int N,
+                 int kp, int rowsA, int rowsB, const int* __restrict__ eA, const int* __restrict__ eB, double* C,
+                 long ldc, unsigned long long* amax, int lower_only, int* err, const int* skip, int mirror) {
+    if (skip && *skip) return;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * NT;
+    if (lower_only && n0 > m0 + BM - 1) return;
+    ozaki_tile<NT, S>(&tA, &tB, m0, n0, M, N, kp, rowsA, rowsB, eA, eB, C, ldc, amax, err, mirror, false);
+}
+
+// The products of many matrices (a batch) in one launch: CTA b computes tile
+// tiles[b] = (job, m0, n0) of jobs[job] (lower-triangle tiles only; the result
+// mirrored). The per-element arithmetic is that of k_ozaki_gemm for any tile
+// width, so a batch gives the bytes of one launch per matrix.
+template <int NT, int S>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_ozaki_gemm_grouped(const MixedGemmJob* __restrict__ jobs, const int4* __restrict__ tiles) {
+    const int4 t = tiles[blockIdx.x];
+    const MixedGemmJob& j = jobs[t.x];
+    if (j.skip && *j.skip) return;
+    ozaki_tile<NT, S>(j.tA, j.tB, t.y, t.z, j.n, j.n, j.kp, j.rowsA, j.rowsB, j.eA, j.eB, j.C, j.ldc, j.amax, j.err,
+                      1, true);
+}
+
 // ------------------------------------------------------------------------
 // host side
 // ------------------------------------------------------------------------
@@ -392,11 +443,24 @@ void set_attr_once() {
 }
 }  // namespace
 
+template <int NT, int S>
+void set_attr_grouped_once() {
+    static std::atomic<unsigned long long> done{0};
+    once_per_device(done, [] {
+        return cudaFuncSetAttribute(k_ozaki_gemm_grouped<NT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    Shape<NT, S>::SMEM) == cudaSuccess;
+    });
+}
+
 void prepare_mixed_kernels() {
     set_attr_once<128, 4>();
     set_attr_once<64, 5>();
     set_attr_once<96, 5>();
     set_attr_once<128, 3>();
+    set_attr_grouped_once<128, 4>();
+    set_attr_grouped_once<64, 5>();
+    set_attr_grouped_once<96, 5>();
+    set_attr_grouped_once<128, 3>();
 }
 
 // Output tile width: slices * tile_n <= 512 TMEM columns, so 128 for up to 4
@@ -443,6 +507,61 @@ bool mixed_plan(MixedOperand& op, int8_t* buf, int* exps, int n, int slices, boo
     op.buf = buf;
     op.exps = exps;
     return make_map(&op.map, buf, op.rows * slices, op.kp, as_b ? nt : BM);
+}
+
+static int mixed_rows_nt(int n, int nt) {
+    const int ra = ((n + BM - 1) / BM) * BM, rb = ((n + nt - 1) / nt) * nt;
+    return ra > rb ? ra : rb;
+}
+
+size_t mixed_slice_bytes_nt(int n, int slices, int nt) {
+    const int kp = ((n + BKB - 1) / BKB) * BKB;
+    return (size_t)slices * (size_t)mixed_rows_nt(n, nt) * kp;
+}
+
+bool mixed_plan_nt(MixedOperand& op, int8_t* buf, int* exps, int n, int slices, bool as_b, int nt) {
+    op.n = n;
+    op.slices = slices;
+    op.kp = ((n + BKB - 1) / BKB) * BKB;
+    op.rows = mixed_rows_nt(n, nt);
+    op.buf = buf;
+    op.exps = exps;
+    return make_map(&op.map, buf, op.rows * slices, op.kp, as_b ? nt : BM);
+}
+
+void mixed_slice_grouped(const MixedSliceJob* d_jobs, int njobs, const int* d_row_start, int total_rows,
+                         cudaStream_t st) {
+    if (total_rows <= 0) return;
+    k_slice_rows_grouped<<<total_rows, 256, 0, st>>>(d_jobs, njobs, d_row_start);
+    count_launch();
+}
+
+void mixed_lower_tiles(int job, int n, int nt, std::vector<int4>& out) {
+    const int by_n = (n + BM - 1) / BM, bx_n = (n + nt - 1) / nt;
+    for (int by = 0; by < by_n; ++by) {
+        const int last = (by * BM + BM - 1) / nt;
+        for (int bx = 0; bx <= last && bx < bx_n; ++bx) out.push_back(make_int4(job, by * BM, bx * nt, 0));
+    }
+}
+
+std::vector<int> mixed_tile_candidates(int slices) {
+    if (slices == 5) return {64, 96};
+    return {128};
+}
+
+void mixed_gemm_grouped(int slices, int nt, const MixedGemmJob* d_jobs, const int4* d_tiles, int ntiles,
+                        cudaStream_t st) {
+    if (ntiles <= 0) return;
+    if (slices == 5 && nt == 64) {
+        k_ozaki_gemm_grouped<64, 5><<<ntiles, THREADS, Shape<64, 5>::SMEM, st>>>(d_jobs, d_tiles);
+    } else if (slices == 5) {
+        k_ozaki_gemm_grouped<96, 5><<<ntiles, THREADS, Shape<96, 5>::SMEM, st>>>(d_jobs, d_tiles);
+    } else if (slices == 4) {
+        k_ozaki_gemm_grouped<128, 4><<<ntiles, THREADS, Shape<128, 4>::SMEM, st>>>(d_jobs, d_tiles);
+    } else {
+        k_ozaki_gemm_grouped<128, 3><<<ntiles, THREADS, Shape<128, 3>::SMEM, st>>>(d_jobs, d_tiles);
+    }
+    count_launch();
 }
 
 void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st, const int* skip, double* Y,

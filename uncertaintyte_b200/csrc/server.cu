@@ -21,6 +21,10 @@
 //   so the block scheduler serves their kernels ahead of a large request's
 //   GEMM tiles, and a quarter of the workers take small requests only, so a
 //   burst of large requests cannot hold every slot.
+// * Packing: a worker that starts a small request also takes the other small
+//   requests waiting behind it (up to kMaxPack, within the memory budget) and
+//   runs them as one grouped batch (unc_batch_compute: one launch sequence,
+//   replayed from a CUDA graph when the pack's shape repeats).
 // * Each result depends only on its own inputs (no atomics in the arithmetic,
 //   fixed reduction orders): alone or in a mix, a request gives the same bytes.
 #include <chrono>
@@ -40,6 +44,7 @@ namespace {
 
 constexpr int kMaxBypass = 16;
 constexpr long long kSmallBytes = 1LL << 30;
+constexpr int kMaxPack = 64;  // small requests run together as one grouped batch
 
 using Clock = std::chrono::steady_clock;
 
@@ -65,6 +70,7 @@ struct Request {
 
 struct Worker {
     unc_context* ctx = nullptr;
+    unc_batch* batch = nullptr;  // packs of small requests
     long long committed = 0;  // device bytes held or promised (workspace, or the running request's footprint)
     bool busy = false;
     bool small_only = false;  // reserved for small requests
@@ -96,33 +102,55 @@ long long committed_except(const unc_server* s, const Worker* w) {
     return t;
 }
 
-// Under the lock: the request worker `w` may start now, or nullptr.
-std::shared_ptr<Request> pick(unc_server* s, Worker* w) {
+long long worker_bytes(const Worker* w) {
+    return (w->ctx ? unc_context_device_bytes(w->ctx) : 0) + (w->batch ? unc_batch_device_bytes(w->batch) : 0);
+}
+
+// Under the lock: the requests worker `w` may start now (empty: none). A small
+// request takes the small requests waiting behind it along (a pack) as long as
+// their footprints fit.
+std::vector<std::shared_ptr<Request>> pick(unc_server* s, Worker* w) {
+    std::vector<std::shared_ptr<Request>> pack;
     for (size_t i = 0; i < s->pending.size(); ++i) {
         auto& r = s->pending[i];
         if (w->small_only && !r->small) continue;  // not this worker's kind; no bypass counted
-        const long long mine = std::max(w->committed, r->bytes);
+        long long mine = std::max(w->committed, r->bytes);
         bool fits = committed_except(s, w) + mine <= s->budget;
         if (!fits) {
             // release idle workspaces (not this worker's) and look again
             for (auto& v : s->workers)
-                if (v.get() != w && !v->busy && v->committed > 0 && v->ctx) {
-                    unc_context_release(v->ctx);
+                if (v.get() != w && !v->busy && v->committed > 0) {
+                    if (v->ctx) unc_context_release(v->ctx);
+                    if (v->batch) unc_batch_release(v->batch);
                     v->committed = 0;
                 }
             fits = committed_except(s, w) + mine <= s->budget;
         }
         if (fits) {
-            auto req = r;
             for (size_t j = 0; j < i; ++j)
                 if (!w->small_only || s->pending[j]->small) s->pending[j]->bypassed++;
+            pack.push_back(r);
             s->pending.erase(s->pending.begin() + (long)i);
+            if (pack[0]->small) {
+                long long sum = pack[0]->bytes;
+                for (size_t j = i; j < s->pending.size() && (int)pack.size() < kMaxPack;) {
+                    auto& q = s->pending[j];
+                    if (q->small && committed_except(s, w) + std::max(w->committed, sum + q->bytes) <= s->budget) {
+                        sum += q->bytes;
+                        pack.push_back(q);
+                        s->pending.erase(s->pending.begin() + (long)j);
+                    } else {
+                        ++j;
+                    }
+                }
+                mine = std::max(w->committed, sum);
+            }
             w->committed = mine;
-            return req;
+            return pack;
         }
         if (r->bypassed >= kMaxBypass) break;  // the head waits for memory; nobody overtakes it any more
     }
-    return nullptr;
+    return pack;
 }
 
 void worker_loop(unc_server* s, Worker* w) {
@@ -133,31 +161,70 @@ void worker_loop(unc_server* s, Worker* w) {
     if (w->ctx) unc::context_set_task_ctas(w->ctx, (2 * sms + (int)s->workers.size() - 1) / (int)s->workers.size());
     std::unique_lock<std::mutex> lk(s->mu);
     for (;;) {
-        std::shared_ptr<Request> r;
-        s->cv_work.wait(lk, [&] { return (r = pick(s, w)) != nullptr || (s->stopping && s->pending.empty()); });
-        if (!r) break;
+        std::vector<std::shared_ptr<Request>> pack;
+        s->cv_work.wait(lk, [&] { return !(pack = pick(s, w)).empty() || (s->stopping && s->pending.empty()); });
+        if (pack.empty()) break;
         w->busy = true;
-        s->running++;
+        s->running += (int)pack.size();
         lk.unlock();
-        r->t_start = Clock::now();
-        if (w->ctx) unc_context_set_priority(w->ctx, r->small ? 1 : 0);
-        int rc = w->ctx ? unc_compute(w->ctx, &r->opt, r->num_rows, r->num_cols, r->rows, r->cols, r->vals, r->cam,
-                                      r->pt, &r->st)
-                        : UNC_ERR_CUDA;
-        std::string err = rc != UNC_OK ? unc_last_error() : std::string();
-        r->t_end = Clock::now();
+        const auto t_start = Clock::now();
+        for (auto& r : pack) r->t_start = t_start;
+        std::vector<int> rcs(pack.size(), UNC_ERR_CUDA);
+        std::vector<std::string> errs(pack.size());
+        if (pack.size() == 1) {
+            auto& r = pack[0];
+            if (w->ctx) unc_context_set_priority(w->ctx, r->small ? 1 : 0);
+            rcs[0] = w->ctx ? unc_compute(w->ctx, &r->opt, r->num_rows, r->num_cols, r->rows, r->cols, r->vals,
+                                          r->cam, r->pt, &r->st)
+                            : UNC_ERR_CUDA;
+            if (rcs[0] != UNC_OK) errs[0] = unc_last_error();
+        } else {
+            if (!w->batch && unc_batch_create(s->device, &w->batch) != UNC_OK) w->batch = nullptr;
+            const size_t n = pack.size();
+            std::vector<unc_options> opts(n);
+            std::vector<int> nr(n), nc(n);
+            std::vector<const int*> rows(n), cols(n);
+            std::vector<const double*> vals(n);
+            std::vector<double*> cam(n), pt(n);
+            std::vector<unc_statistic> st(n);
+            for (size_t k = 0; k < n; ++k) {
+                opts[k] = pack[k]->opt;
+                nr[k] = pack[k]->num_rows;
+                nc[k] = pack[k]->num_cols;
+                rows[k] = pack[k]->rows;
+                cols[k] = pack[k]->cols;
+                vals[k] = pack[k]->vals;
+                cam[k] = pack[k]->cam;
+                pt[k] = pack[k]->pt;
+            }
+            int rc = w->batch ? unc_batch_compute(w->batch, (int)n, opts.data(), nr.data(), nc.data(), rows.data(),
+                                                  cols.data(), vals.data(), cam.data(), pt.data(), rcs.data(), st.data())
+                              : UNC_ERR_CUDA;
+            const std::string msg = unc_last_error();
+            for (size_t k = 0; k < n; ++k) {
+                if (rc != UNC_OK) rcs[k] = rc;
+                if (rcs[k] != UNC_OK) errs[k] = rc != UNC_OK ? msg : std::string(unc_status_string(rcs[k]));
+                pack[k]->st = st[k];
+            }
+        }
+        const auto t_end = Clock::now();
         lk.lock();
-        r->status = rc;
-        r->error = err;
-        r->done = true;
+        for (size_t k = 0; k < pack.size(); ++k) {
+            pack[k]->t_end = t_end;
+            pack[k]->status = rcs[k];
+            pack[k]->error = errs[k];
+            pack[k]->done = true;
+        }
         w->busy = false;
-        w->committed = w->ctx ? unc_context_device_bytes(w->ctx) : 0;  // what the workspace now holds
-        s->running--;
-        s->completed++;
+        w->committed = worker_bytes(w);  // what the workspaces now hold
+        s->running -= (int)pack.size();
+        s->completed += (long long)pack.size();
         s->cv_done.notify_all();
         s->cv_work.notify_all();  // memory may have come free for a waiting request
     }
     lk.unlock();
+    if (w->batch) unc_batch_destroy(w->batch);
+    w->batch = nullptr;
     if (w->ctx) unc_context_destroy(w->ctx);
     w->ctx = nullptr;
 }

@@ -86,7 +86,9 @@ EXPORTS = ("unc_options_init", "unc_context_create", "unc_context_destroy", "unc
            "unc_context_set_priority", "unc_jacobian_device", "unc_compute_scene",
            "unc_block_eigen_device", "unc_block_eigen", "unc_jacob_read_header", "unc_jacob_read",
            "unc_jacob_write_binary",
-           "unc_server_create", "unc_server_submit", "unc_server_wait", "unc_server_destroy")
+           "unc_server_create", "unc_server_submit", "unc_server_wait", "unc_server_destroy",
+           "unc_batch_create", "unc_batch_destroy", "unc_batch_compute", "unc_batch_last_timing",
+           "unc_batch_device_bytes", "unc_batch_release")
 
 _lib = None
 
@@ -130,6 +132,14 @@ def lib():
     L.unc_block_eigen.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp]
     L.unc_jacobian_device.argtypes = [C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp]
     L.unc_compute_scene.argtypes = [vp, P(UncOptions), vp, vp, vp, vp, vp, vp, P(UncStatistic)]
+    L.unc_batch_create.argtypes = [C.c_int, P(vp)]
+    L.unc_batch_destroy.argtypes = [vp]
+    L.unc_batch_compute.argtypes = [vp, C.c_int, P(UncOptions), P(C.c_int), P(C.c_int), P(vp), P(vp), P(vp),
+                                    P(vp), P(vp), P(C.c_int), P(UncStatistic)]
+    L.unc_batch_last_timing.argtypes = [vp, P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_int), P(C.c_int)]
+    L.unc_batch_device_bytes.argtypes = [vp]
+    L.unc_batch_device_bytes.restype = C.c_longlong
+    L.unc_batch_release.argtypes = [vp]
     L.unc_server_create.argtypes = [C.c_int, C.c_longlong, C.c_int, P(vp)]
     L.unc_server_submit.argtypes = [vp, P(UncOptions), C.c_int, C.c_int, vp, vp, vp, vp, vp, P(C.c_longlong)]
     L.unc_server_wait.argtypes = [vp, C.c_longlong, C.c_double, P(C.c_int), P(UncStatistic), P(C.c_double),
@@ -348,6 +358,59 @@ class Server:
             lib().unc_server_destroy(self._h)
             self._h = C.c_void_p()
             self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many reconstructions in one grouped launch sequence (unc_batch_compute).
+
+    compute() returns, per Jacobian, (cam, pt, stats, status) with status the
+    scene's own status code (0 = UNC_OK); last_timing() the input-copy,
+    device and output-copy seconds of the last call, the number of grouped
+    scenes and the product tile width."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        _check(lib().unc_batch_create(device, C.byref(self._h)))
+
+    def compute(self, jacs, precision="mixed", algorithm: Optional[int] = None, pt_init=None):
+        n = len(jacs)
+        precs = precision if isinstance(precision, (list, tuple)) else [precision] * n
+        opts = (UncOptions * n)(*[make_options(j, algorithm, p) for j, p in zip(jacs, precs)])
+        arrs = [(np.ascontiguousarray(j.rows, dtype=np.int32), np.ascontiguousarray(j.cols, dtype=np.int32),
+                 np.ascontiguousarray(j.values, dtype=np.float64)) for j in jacs]
+        cams = [np.zeros(j.num_cams * 45) for j in jacs]
+        pts = [np.zeros(j.num_points * 6) if pt_init is None else np.array(pt_init[k], dtype=np.float64)
+               for k, j in enumerate(jacs)]
+        vp = C.c_void_p
+        nr = (C.c_int * n)(*[j.num_rows for j in jacs])
+        nc = (C.c_int * n)(*[j.num_cols for j in jacs])
+        rows = (vp * n)(*[a[0].ctypes.data for a in arrs])
+        cols = (vp * n)(*[a[1].ctypes.data for a in arrs])
+        vals = (vp * n)(*[a[2].ctypes.data for a in arrs])
+        cp = (vp * n)(*[c.ctypes.data for c in cams])
+        pp = (vp * n)(*[p.ctypes.data for p in pts])
+        status = (C.c_int * n)()
+        stats = (UncStatistic * n)()
+        _check(lib().unc_batch_compute(self._h, n, opts, nr, nc, rows, cols, vals, cp, pp, status, stats))
+        return [(cams[k], pts[k], stats[k].as_dict(), status[k]) for k in range(n)]
+
+    def last_timing(self) -> dict:
+        h, d, o = C.c_double(), C.c_double(), C.c_double()
+        g, t = C.c_int(), C.c_int()
+        _check(lib().unc_batch_last_timing(self._h, C.byref(h), C.byref(d), C.byref(o), C.byref(g), C.byref(t)))
+        return {"h2d_s": h.value, "device_s": d.value, "d2h_s": o.value, "grouped_scenes": g.value,
+                "tile_n": t.value}
+
+    def close(self):
+        if self._h:
+            lib().unc_batch_destroy(self._h)
+            self._h = C.c_void_p()
 
     def __del__(self):
         try:
