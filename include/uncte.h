@@ -54,6 +54,16 @@ extern "C" {
 #define UNC_PRECISION_MIXED4 2  /* same with 4 slices (~1e-8 per product, faster) */
 #define UNC_PRECISION_MIXED3 3  /* same with 3 slices (~1e-6 per product) */
 
+/* How the Taylor series of teInverse (compute.cpp:141-160) is evaluated; both
+ * give the reference's polynomial, coefficients and stop decisions.
+ * POWERS: from X^2, X^3, X^4, X^8, X^12 (X^16 past 15 iterations): the stop
+ * rule's max|X^(i+1)| is the largest diagonal entry of the SPD power, a column
+ * dot product of two lower powers, and the sum is formed in blocks of four
+ * coefficients (8 products for up to 15 iterations). SEQUENTIAL: one product
+ * per iteration, the reference's order. */
+#define UNC_TAYLOR_POWERS 0
+#define UNC_TAYLOR_SEQUENTIAL 1
+
 typedef struct unc_context unc_context;
 
 /* Mirrors cov::Options (src/uncertaintyTE/uncertainty.h:52-71) as plain C. */
@@ -67,6 +77,7 @@ typedef struct {
     int pts2fix[3];     /* fixed point ids (TE); only the first two are sorted, as the reference does */
     int has_pts2fix;    /* 0 = no fixed points given */
     int precision;      /* UNC_PRECISION_FP64 / _MIXED / _MIXED4 / _MIXED3 */
+    int taylor_eval;    /* UNC_TAYLOR_POWERS (0, default) / UNC_TAYLOR_SEQUENTIAL */
 } unc_options;
 
 /* Mirrors cov::Statistic (src/uncertaintyTE/uncertainty.h:73-82). Times are
@@ -220,14 +231,15 @@ int unc_server_destroy(unc_server* srv);
  * at once. The inputs of all scenes go to the device in one copy; the sparse
  * stages of the scenes run as parallel branches, the dense stage is grouped
  * (one persistent tile-task kernel inverts every scene's Schur complement,
- * each Taylor-series step is one launch over all scenes' product tiles); the
+ * each step of the Taylor series is one launch over all scenes); the
  * sequence of a batch shape (sizes, fixed points, lambda) is captured in a
  * CUDA graph the second time it is seen and replayed after. The product tile
  * width is chosen by timing the candidates on the first batch of a size class.
  * Each scene's result is bitwise the one unc_compute gives for it alone.
  * Scenes outside the grouped path (the SVD algorithms, UNC_PRECISION_FP64,
- * 9 * num_cams above 3584, Jacobians not in the 24-entries-per-observation
- * layout) are computed with unc_compute in the same call.
+ * UNC_TAYLOR_SEQUENTIAL, 9 * num_cams above 3584, Jacobians not in the
+ * 24-entries-per-observation layout) are computed with unc_compute in the
+ * same call.
  * Per scene i: opts[i], the host CRS arrays and the host outputs as for
  * unc_compute; status[i] receives the scene's own status code; stats (NULL or
  * num_scenes entries) the statistics (time_all: the whole batch's time). The

@@ -25,9 +25,9 @@ def ctx():
     c.close()
 
 
-def _mixed_vs_fp64(jac, ctx, precision="mixed"):
-    c64, p64, s64 = native.compute_covariances(jac, ctx, precision="fp64")
-    cmp_, pmp, smp = native.compute_covariances(jac, ctx, precision=precision)
+def _mixed_vs_fp64(jac, ctx, precision="mixed", taylor="powers"):
+    c64, p64, s64 = native.compute_covariances(jac, ctx, precision="fp64", taylor=taylor)
+    cmp_, pmp, smp = native.compute_covariances(jac, ctx, precision=precision, taylor=taylor)
     assert smp["te_iterations"] == s64["te_iterations"]
     # the stop-rule values come from the products' max |entry|: same ~1e-8..1e-6 agreement
     np.testing.assert_allclose(smp["cycle_change"], s64["cycle_change"], rtol=1e-5)
@@ -46,8 +46,9 @@ def test_mixed_vs_fp64_synthetic(ctx, name):
     assert ec < MIXED_TOL and ep < MIXED_TOL
 
 
-def test_mixed_vs_fp64_daliborka(ctx):
-    ec, ep = _mixed_vs_fp64(golden_jacobian("daliborka"), ctx)
+@pytest.mark.parametrize("taylor", ["powers", "sequential"])
+def test_mixed_vs_fp64_daliborka(ctx, taylor):
+    ec, ep = _mixed_vs_fp64(golden_jacobian("daliborka"), ctx, taylor=taylor)
     assert ec < MIXED_TOL and ep < MIXED_TOL
 
 

@@ -100,6 +100,22 @@ def test_medium_scene_vs_oracle(ctx):
     _parity(scenes.synthetic_jacobian("medium", seed=0), ctx)
 
 
+@pytest.mark.parametrize("name", ["daliborka", "small", "medium"])
+def test_blocked_powers_and_sequential_evaluation(ctx, name):
+    """The Taylor series from blocked powers (the default: X^2, X^3, X^4, X^8,
+    X^12, the stop rule from the powers' diagonal maxima, the sum in blocks of
+    four coefficients) and one product per iteration in the reference's order:
+    the same iteration count, cycle changes and floor-bounded results."""
+    jac = golden_jacobian("daliborka") if name == "daliborka" else scenes.synthetic_jacobian(name, seed=0)
+    cp, pp, sp = native.compute_covariances(jac, ctx, taylor="powers")
+    cs, ps_, ss = native.compute_covariances(jac, ctx, taylor="sequential")
+    assert sp["te_iterations"] == ss["te_iterations"]
+    np.testing.assert_allclose(sp["cycle_change"], ss["cycle_change"], rtol=1e-9)
+    ref = oracle.compute(jac, threads=8)
+    _check_fp64(cp, pp, jac, ref, f"{name} powers:")
+    _check_fp64(cs, ps_, jac, ref, f"{name} sequential:")
+
+
 def test_repeatable(ctx):
     jac = scenes.synthetic_jacobian("small", seed=4)
     a = native.compute_covariances(jac, ctx)

@@ -141,6 +141,12 @@ size_t carve(char* base, const Plan& pl, bool host_io, long long nnz, int nrows,
     b.iZ = c.take<double>(nn);
     b.add = c.take<double>(nn);
     b.tmp = c.take<double>(nn);
+    b.p4 = c.take<double>(nn);
+    b.p8 = c.take<double>(nn);
+    b.p12 = c.take<double>(nn);
+    b.p16 = c.take<double>(nn);
+    b.g = c.take<double>(nn);
+    b.dmax = c.take<unsigned long long>(24);
     b.e = c.take<double>(pl.N);
     b.gjws = c.take<double>(chol_small_doubles(pl.N));
     b.dag_state = c.take<int>(spd_task_state_ints(pl.N));
@@ -448,23 +454,27 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     // Every power X^(i+1) is symmetric: only the lower-triangle tiles of each
     // product are computed (half the flops), then mirrored for the next product.
     // FP64 mode: DMMA products. Mixed modes: int8-sliced tcgen05 products of
-    // the FP64 operands (X sliced once, each new power sliced per product).
+    // the FP64 operands (X sliced once, each new operand sliced per product).
     const bool mixed = o->precision != UNC_PRECISION_FP64;
+    const bool powers = o->taylor_eval != UNC_TAYLOR_SEQUENTIAL;
     const int slices = o->precision == UNC_PRECISION_MIXED4 ? 4 : (o->precision == UNC_PRECISION_MIXED3 ? 3 : 5);
-    MixedOperand opP, opXa, opXb;
+    // slice buffers: X, the A operand of the moment, and (powers) X^4, X^8, X^12, X^16
+    constexpr int kX = 0, kA = 1, k4 = 2, k8 = 3, k12 = 4, k16 = 5;
+    const int nbuf = powers ? 6 : 2;
+    MixedOperand opa[6], opb[6];  // each buffer as the A (128-row boxes) and as the B operand
     size_t mp_need = 0;
     if (mixed) {  // host-side preparation: buffers and tensor maps
         const size_t sb = (mixed_slice_bytes(N, slices) + 255) & ~size_t(255);
-        mp_need = 2 * sb + 2 * sizeof(int) * ((size_t)N + 64) + 256;
+        const size_t eb = (sizeof(int) * ((size_t)N + 64) + 255) & ~size_t(255);
+        mp_need = nbuf * (sb + eb) + 256;
         if (int r = grow_buffer(&ctx->mp, &ctx->mp_bytes, mp_need, mp_need, sm)) return r;
         char* w = (char*)ctx->mp;
-        int8_t* bufX = reinterpret_cast<int8_t*>(w);
-        int8_t* bufP = reinterpret_cast<int8_t*>(w + sb);
-        int* eX = reinterpret_cast<int*>(w + 2 * sb);
-        int* eP = eX + N + 64;
-        if (!mixed_plan(opXa, bufX, eX, N, slices, false) || !mixed_plan(opXb, bufX, eX, N, slices, true) ||
-            !mixed_plan(opP, bufP, eP, N, slices, false))
-            return fail(UNC_ERR_CUDA, "tensor-map encoding failed");
+        for (int q = 0; q < nbuf; ++q) {
+            int8_t* buf = reinterpret_cast<int8_t*>(w + q * sb);
+            int* ex = reinterpret_cast<int*>(w + nbuf * sb + q * eb);
+            if (!mixed_plan(opa[q], buf, ex, N, slices, false) || !mixed_plan(opb[q], buf, ex, N, slices, true))
+                return fail(UNC_ERR_CUDA, "tensor-map encoding failed");
+        }
     }
     const double* X = b.Z;
     size_t npev = 0;
@@ -484,15 +494,30 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     // the power being sliced rides along in the slicing kernel.
     auto product = [&](const double* P, double* out, const int* skip) -> int {
         if (mixed) {
-            if (P != X) mixed_slice(P, ld, opP, sm, skip, b.iZ, b.te);
+            if (P != X) mixed_slice(P, ld, opa[kA], sm, skip, b.iZ, b.te);
             if (int r = prof_mark()) return r;
-            mixed_gemm(P == X ? opXa : opP, opXb, out, ld, b.amax, true, s.err, sm, skip, true);
+            mixed_gemm(P == X ? opa[kX] : opa[kA], opb[kX], out, ld, b.amax, true, s.err, sm, skip, true);
         } else {
             if (int r = prof_mark()) return r;
             gemm_f64_mode(N, N, N, 1.0, P, ld, X, ld, 0.0, out, ld, b.amax, GEMM_LOWER | GEMM_MIRROR, sm, nullptr,
                           0, skip);
         }
         return prof_mark();
+    };
+    // blocked powers: out (+)= A B, A and B powers of X (symmetric, commuting)
+    // given as FP64 matrices and, in mixed mode, as slice buffers ia / ib
+    auto power_product = [&](const double* A, int ia, const double* B, int ib, double* out, bool acc,
+                             const int* skip) -> int {
+        if (int r = prof_mark()) return r;
+        if (mixed)
+            mixed_gemm(opa[ia], opb[ib], out, ld, nullptr, true, s.err, sm, skip, true, acc);
+        else
+            gemm_f64_mode(N, N, N, 1.0, A, ld, B, ld, acc ? 1.0 : 0.0, out, ld, nullptr, GEMM_LOWER | GEMM_MIRROR,
+                          sm, nullptr, 0, skip);
+        return prof_mark();
+    };
+    auto slice = [&](const double* A, int q, const int* skip) {
+        if (mixed) mixed_slice(A, ld, opa[q], sm, skip);
     };
     // The dense stage, a fixed launch sequence for given sizes and buffers:
     // equilibration, the SPD inverse (SDM::inv, ScaledDenseMatrix.cpp:232-279)
@@ -522,19 +547,76 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         double* tmp = b.tmp;
         if (mixed) {
             CK(cudaMemsetAsync(ctx->mp, 0, mp_need, sm));  // slice padding must be zero
-            mixed_slice(X, ld, opXa, sm);
+            mixed_slice(X, ld, opa[kX], sm);
         }
         launch_te_init(b.te, sm);
         const int* skip = &b.te->done;
         CK(cudaMemsetAsync(b.amax, 0, 8, sm));
         if (int r = product(X, add, nullptr)) return r;
-        for (int i = 1; i < 20; ++i) {
+        for (int i = 1; i < 20; ++i) {  // the reference's order: one product per iteration
             const double k = pow(lambda, i) / factorial_i32(i - 1);
             launch_te_decide(b.te, b.amax, k, sm);
             if (!mixed) launch_axpy_te(b.iZ, add, b.te, N, ld, sm);
             CK(cudaMemsetAsync(b.amax, 0, 8, sm));
             if (int r = product(add, tmp, skip)) return r;
             std::swap(add, tmp);
+        }
+        return UNC_OK;
+    };
+    // The blocked-power evaluation (powers.cu): X^2, X^3, X^4, X^8, X^12 and
+    // X^16 (skipped on the device unless the rule passes iteration 15); the
+    // stop rule from their diagonal maxima; iZ = G_0 + sum_q X^(4q) G_q with
+    // the blocks whose coefficients are all zero skipped on the device.
+    PowerSet ps{};
+    ps.M[0] = b.Z;
+    ps.M[1] = b.add;
+    ps.M[2] = b.tmp;
+    ps.M[3] = b.p4;
+    ps.M[4] = b.p8;
+    ps.M[5] = b.p12;
+    ps.M[6] = b.p16;
+    ps.iZ = b.iZ;
+    ps.G = b.g;
+    ps.n = N;
+    ps.ld = ld;
+    ps.dmax = b.dmax;
+    ps.te = b.te;
+    TaylorCoefs kc{};
+    for (int i = 1; i < 20; ++i) kc.k[i - 1] = pow(lambda, i) / factorial_i32(i - 1);
+    auto powers_stage = [&]() -> int {
+        const int* sk = b.te->skip;
+        if (ld != N)  // padding rows of the extra power buffers must stay finite for the product loads
+            for (double* m : {b.p4, b.p8, b.p12, b.p16, b.g})
+                CK(cudaMemset2DAsync(m + N, sizeof(double) * (size_t)ld, 0, sizeof(double) * (size_t)(ld - N), N, sm));
+        if (mixed) {
+            CK(cudaMemsetAsync(ctx->mp, 0, mp_need, sm));  // slice padding must be zero
+            slice(X, kX, nullptr);
+        }
+        launch_te_init(b.te, sm);
+        CK(cudaMemsetAsync(b.dmax, 0, sizeof(unsigned long long) * 24, sm));
+        if (int r = power_product(X, kX, X, kX, b.add, false, nullptr)) return r;  // X^2
+        slice(b.add, kA, nullptr);
+        if (int r = power_product(b.add, kA, X, kX, b.tmp, false, nullptr)) return r;  // X^3
+        slice(b.tmp, kA, nullptr);
+        if (int r = power_product(b.tmp, kA, X, kX, b.p4, false, nullptr)) return r;  // X^4
+        slice(b.p4, k4, nullptr);
+        if (int r = power_product(b.p4, k4, b.p4, k4, b.p8, false, nullptr)) return r;  // X^8
+        slice(b.p8, k8, nullptr);
+        if (int r = power_product(b.p8, k8, b.p4, k4, b.p12, false, nullptr)) return r;  // X^12
+        slice(b.p12, k12, nullptr);
+        launch_power_diag(ps, 2, 16, nullptr, sm);
+        launch_power_decide(b.te, b.dmax, kc, 1, 15, sm);
+        if (int r = power_product(b.p8, k8, b.p8, k8, b.p16, false, sk)) return r;  // X^16
+        slice(b.p16, k16, sk);
+        launch_power_diag(ps, 17, 20, sk, sm);
+        launch_power_decide(b.te, b.dmax, kc, 16, 19, sm);
+        launch_power_combine(ps, 0, b.iZ, nullptr, sm);
+        const double* Pq[5] = {nullptr, b.p4, b.p8, b.p12, b.p16};
+        const int iq[5] = {0, k4, k8, k12, k16};
+        for (int q = 1; q <= 4; ++q) {
+            launch_power_combine(ps, q, b.g, sk + q, sm);
+            slice(b.g, kA, sk + q);
+            if (int r = power_product(b.g, kA, Pq[q], iq[q], b.iZ, true, sk + q)) return r;
         }
         return UNC_OK;
     };
@@ -555,9 +637,13 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         size_t none = 0;
         if (int r = ctx->prof ? inverse_stage() : run_stage(ctx, key, sm, inverse_stage, none)) return r;
         CK(cudaEventRecord(ev[6], sm));
-        key[0] = 2ULL;
+        key[0] = powers ? 3ULL : 2ULL;
         key[7] = ((unsigned long long)o->precision << 56) ^ (unsigned long long)(uintptr_t)ctx->mp;
-        if (int r = ctx->prof ? taylor_stage() : run_stage(ctx, key, sm, taylor_stage, npev)) return r;
+        if (powers) {
+            if (int r = ctx->prof ? powers_stage() : run_stage(ctx, key, sm, powers_stage, npev)) return r;
+        } else {
+            if (int r = ctx->prof ? taylor_stage() : run_stage(ctx, key, sm, taylor_stage, npev)) return r;
+        }
         CK(cudaEventRecord(ev[7], sm));
     }
 
@@ -571,10 +657,16 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     CK(cudaStreamSynchronize(sm));
     CK(cudaGetLastError());
     const int iters = te.iters;
-    // products actually computed: the first one and one per performed iteration
-    npev = std::min(npev, (size_t)2 * (iters + 1));
-    for (size_t i = 0; i + 1 < npev; i += 2) {
-        ctx->prof_seconds += ev_s(ctx->pev[i], ctx->pev[i + 1]);
+    // products actually computed. Sequential: the first one and one per
+    // performed iteration. Powers: X^2..X^12 (5), X^16 unless skipped, one per
+    // non-zero block.
+    std::vector<bool> ran(npev / 2, false);
+    for (size_t q = 0; q < ran.size(); ++q)
+        ran[q] = powers ? (q < 5 || (q == 5 && !te.skip[0]) || (q > 5 && q < 10 && !te.skip[q - 5]))
+                        : q < (size_t)iters + 1;
+    for (size_t q = 0; q < ran.size(); ++q) {
+        if (!ran[q]) continue;
+        ctx->prof_seconds += ev_s(ctx->pev[2 * q], ctx->pev[2 * q + 1]);
         ctx->prof_launches += 1;
         ctx->prof_flops += (double)N * N * (N + 1);  // symmetric product: lower half of 2 N^3
     }
@@ -784,9 +876,11 @@ long long unc_request_bytes(const unc_options* o, int num_rows, int num_cols, co
     long long pairs = 0;
     for (int c : per_pt) pairs += (long long)c * (c - 1) / 2;
     bytes += (pairs * 8 + pairs / 1025 * 4 + 64) * 5 / 4;
-    if (o->precision != UNC_PRECISION_FP64) {
+    if (o->precision != UNC_PRECISION_FP64) {  // slice buffers: 6 (blocked powers) or 2 (sequential)
         const int slices = o->precision == UNC_PRECISION_MIXED4 ? 4 : (o->precision == UNC_PRECISION_MIXED3 ? 3 : 5);
-        bytes += 2 * (long long)((mixed_slice_bytes(pl.N, slices) + 255) & ~size_t(255)) + 8LL * (pl.N + 64) + 256;
+        const long long nbuf = o->taylor_eval == UNC_TAYLOR_SEQUENTIAL ? 2 : 6;
+        bytes += nbuf * ((long long)((mixed_slice_bytes(pl.N, slices) + 255) & ~size_t(255)) +
+                         (long long)((4 * ((size_t)pl.N + 64) + 255) & ~size_t(255))) + 256;
     }
     return bytes;
 }

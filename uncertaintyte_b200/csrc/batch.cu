@@ -11,8 +11,9 @@
 //     scene as parallel branches of one launch sequence;
 //   * the dense stage grouped across scenes: one persistent tile-task kernel
 //     runs the SPD inverses of all scenes from one interleaved work list, and
-//     every Taylor-series step (stop rule, slicing, int8 tensor-core product)
-//     is one launch over the tiles / rows of all scenes;
+//     every step of the blocked-power Taylor evaluation (powers.cu: slicing,
+//     int8 tensor-core products, diagonal maxima, stop rule, coefficient
+//     blocks) is one launch over the tiles / rows / columns of all scenes;
 //   * the camera and point outputs again as parallel branches.
 //
 // The sequence for a given batch shape (sizes, fixed points, lambda, buffer
@@ -25,8 +26,8 @@
 // unc_compute gives for it alone.
 //
 // Scenes the grouped path does not cover (the SVD algorithms, the FP64
-// precision, N = 9 cameras above 3584) are computed one after another with
-// unc_compute in the same call.
+// precision, the sequential Taylor evaluation, N = 9 cameras above 3584) are
+// computed one after another with unc_compute in the same call.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -57,7 +58,7 @@ int bfail(int code, const std::string& msg) {
 
 constexpr int kBranches = 8;      // parallel streams for the per-scene stages
 constexpr int kGraphs = 4;        // batch-shape graphs kept
-constexpr int kTaylorIters = 19;  // iterations launched after the first product (compute.cpp:145)
+constexpr int kTaylorIters = 19;  // Taylor iterations at most (compute.cpp:145)
 
 struct Scene {
     int idx;  // position in the caller's arrays
@@ -76,8 +77,8 @@ struct Scene {
     double* out_cam;
     double* out_pt;
     size_t in_off[3], out_off[2];  // byte offsets in the staging areas
-    int8_t *bufX, *bufP;
-    int *eX, *eP;
+    int8_t* buf[6];  // slices of X, of the A operand of the moment, of X^4, X^8, X^12, X^16
+    int* ex[6];      // their row exponents
 };
 
 struct Layout {
@@ -161,6 +162,48 @@ int lower_tile_count(int n, int nt) {
     return (int)t.size();
 }
 
+constexpr int kMaps = 9;        // per scene: X (A, B), A operand (A), X^4 (A, B), X^8 (A, B), X^12 (B), X^16 (B)
+constexpr int kSliceSets = 11;  // X, X^2, X^3, X^4, X^8, X^12, X^16, G_1..G_4
+constexpr int kGemmSets = 10;   // X^2, X^3, X^4, X^8, X^12, X^16, X^4 G_1 .. X^16 G_4
+
+// Device addresses of the descriptor region, in lay_out's order.
+struct Desc {
+    SpdTaskMatrix* mats;
+    int4* tasks;
+    CUtensorMap* maps;
+    DenseJob* dense;
+    long* blk_rows;
+    long* blk_elems;
+    long* blk_cols;
+    MixedSliceJob* slice;  // kSliceSets sets of n jobs
+    int* row_start;
+    MixedGemmJob* gemm;    // kGemmSets sets of n jobs
+    int4* tiles;
+    PowerSet* powers;
+    double* kpow;          // 19 coefficients per scene
+};
+
+// With measure: advance that carver (sizes only); else lay out at base.
+Desc desc_at(char* base, size_t n, size_t ntasks, size_t ntiles, Carver* measure) {
+    Carver own{base};
+    Carver& c = measure ? *measure : own;
+    Desc d;
+    d.mats = c.take<SpdTaskMatrix>(n);
+    d.tasks = c.take<int4>(ntasks);
+    d.maps = c.take<CUtensorMap>(kMaps * n);
+    d.dense = c.take<DenseJob>(n);
+    d.blk_rows = c.take<long>(n + 1);
+    d.blk_elems = c.take<long>(n + 1);
+    d.blk_cols = c.take<long>(n + 1);
+    d.slice = c.take<MixedSliceJob>(kSliceSets * n);
+    d.row_start = c.take<int>(n + 1);
+    d.gemm = c.take<MixedGemmJob>(kGemmSets * n);
+    d.tiles = c.take<int4>(ntiles);
+    d.powers = c.take<PowerSet>(n);
+    d.kpow = c.take<double>(19 * n);
+    return d;
+}
+
 // Lay out the device workspace of a group for tile width nt (base == nullptr:
 // sizes only). Fills the per-scene pointers.
 void lay_out(char* base, std::vector<Scene>& sc, int slices, int nt, Layout& L, size_t ntasks, size_t ntiles) {
@@ -196,16 +239,16 @@ void lay_out(char* base, std::vector<Scene>& sc, int slices, int nt, Layout& L, 
     L.mixed_off = c.off;
     for (auto& s : sc) {
         const size_t sb = mixed_slice_bytes_nt(s.pl.N, slices, nt);
-        s.bufX = c.take<int8_t>(sb);
-        s.bufP = c.take<int8_t>(sb);
-        s.eX = c.take<int>((size_t)s.pl.N + 64);
-        s.eP = c.take<int>((size_t)s.pl.N + 64);
+        for (int q = 0; q < 6; ++q) s.buf[q] = c.take<int8_t>(sb);
+        for (int q = 0; q < 6; ++q) s.ex[q] = c.take<int>((size_t)s.pl.N + 64);
     }
     c.off = (c.off + 255) & ~size_t(255);
     L.mixed_bytes = c.off - L.mixed_off;
-    // zero at the start of the dense stage: tile-task counters of every scene, control words
+    // zero at the start of the dense stage: tile-task counters of every scene,
+    // the powers' diagonal maxima, control words (last)
     L.zero_off = c.off;
     for (auto& s : sc) s.b.dag_state = c.take<int>(spd_task_state_ints(s.pl.N));
+    for (auto& s : sc) s.b.dmax = c.take<unsigned long long>(24);
     c.take<int>(4);
     c.off = (c.off + 255) & ~size_t(255);
     L.zero_bytes = c.off - L.zero_off;
@@ -225,53 +268,10 @@ void lay_out(char* base, std::vector<Scene>& sc, int slices, int nt, Layout& L, 
     }
     // descriptors (host-filled, one upload)
     L.desc_off = c.off;
-    const size_t n = sc.size();
-    c.take<SpdTaskMatrix>(n);
-    c.take<int4>(ntasks);
-    c.take<CUtensorMap>(3 * n);
-    c.take<DenseJob>(n);
-    c.take<long>(n + 1);
-    c.take<long>(n + 1);
-    c.take<MixedSliceJob>(3 * n);
-    c.take<int>(n + 1);
-    c.take<MixedGemmJob>(3 * n);
-    c.take<int4>(ntiles);
-    c.take<double>((size_t)kTaylorIters * n);
+    desc_at(nullptr, sc.size(), ntasks, ntiles, &c);
     c.off = (c.off + 255) & ~size_t(255);
     L.desc_bytes = c.off - L.desc_off;
     L.total = c.off + 256;
-}
-
-// Device addresses of the descriptor region, in lay_out's order.
-struct Desc {
-    SpdTaskMatrix* mats;
-    int4* tasks;
-    CUtensorMap* maps;
-    DenseJob* dense;
-    long* blk_rows;
-    long* blk_elems;
-    MixedSliceJob* slice;  // [X | P odd | P even]
-    int* row_start;
-    MixedGemmJob* gemm;    // [first | odd | even]
-    int4* tiles;
-    double* kvals;
-};
-
-Desc desc_at(char* base, size_t n, size_t ntasks, size_t ntiles) {
-    Carver c{base};
-    Desc d;
-    d.mats = c.take<SpdTaskMatrix>(n);
-    d.tasks = c.take<int4>(ntasks);
-    d.maps = c.take<CUtensorMap>(3 * n);
-    d.dense = c.take<DenseJob>(n);
-    d.blk_rows = c.take<long>(n + 1);
-    d.blk_elems = c.take<long>(n + 1);
-    d.slice = c.take<MixedSliceJob>(3 * n);
-    d.row_start = c.take<int>(n + 1);
-    d.gemm = c.take<MixedGemmJob>(3 * n);
-    d.tiles = c.take<int4>(ntiles);
-    d.kvals = c.take<double>((size_t)kTaylorIters * n);
-    return d;
 }
 
 struct GroupRun {
@@ -279,7 +279,7 @@ struct GroupRun {
     int slices = 5, nt = 96;
     Layout L;
     size_t ntasks = 0, ntiles = 0;
-    long nblk_rows = 0, nblk_elems = 0;
+    long nblk_rows = 0, nblk_elems = 0, nblk_cols = 0;
     int total_rows = 0;
     Desc dd{};  // device descriptors
     char* dbase = nullptr;
@@ -300,6 +300,11 @@ int launch_group(unc_batch* b, GroupRun& g, cudaEvent_t taylor0, cudaEvent_t tay
         if (int r = sparse_stage(&s.opt, s.pl, s.nnz, s.in_rows, s.in_cols, s.in_vals, s.b, fx, nullptr, br,
                                  &s.pair_buf, &s.pair_bytes, s.pairs_cap))
             return r;
+        const int N = s.pl.N, ld = s.pl.ld;
+        if (ld != N)  // padding rows of the extra power buffers must stay finite for the product loads
+            for (double* m : {s.b.p4, s.b.p8, s.b.p12, s.b.p16, s.b.g})
+                BCK(cudaMemset2DAsync(m + N, sizeof(double) * (size_t)ld, 0, sizeof(double) * (size_t)(ld - N), N,
+                                      br));
     }
     for (int k = 0; k < kBranches; ++k) {
         BCK(cudaEventRecord(b->join[k], b->branch[k]));
@@ -313,16 +318,36 @@ int launch_group(unc_batch* b, GroupRun& g, cudaEvent_t taylor0, cudaEvent_t tay
     if (int r = chol_inverse_tasks_grouped(g.dd.mats, g.dd.tasks, (int)g.ntasks, ctl, sm, device_sms())) return r;
     launch_unequilibrate_grouped(g.dd.dense, n, g.dd.blk_elems, g.nblk_elems, sm);  // X in Z, iZ = X
     if (taylor0) BCK(cudaEventRecord(taylor0, sm));
-    mixed_slice_grouped(g.dd.slice, n, g.dd.row_start, g.total_rows, sm);  // X
+    // the Taylor series from blocked powers (powers.cu), every step over all scenes
+    auto slice = [&](int set) {
+        mixed_slice_grouped(g.dd.slice + (size_t)set * n, n, g.dd.row_start, g.total_rows, sm);
+    };
+    auto gemm = [&](int set) {
+        mixed_gemm_grouped(g.slices, g.nt, g.dd.gemm + (size_t)set * n, g.dd.tiles, (int)g.ntiles, sm);
+    };
+    slice(0);  // X
     launch_te_init_grouped(g.dd.dense, n, sm);
-    BCK(cudaMemsetAsync(g.dbase + g.L.amax_off, 0, g.L.amax_bytes, sm));
-    mixed_gemm_grouped(g.slices, g.nt, g.dd.gemm, g.dd.tiles, (int)g.ntiles, sm);  // X X -> add
-    for (int it = 1; it <= kTaylorIters; ++it) {
-        const int par = 1 + ((it - 1) & 1);  // odd iterations: add -> tmp, even: tmp -> add
-        launch_te_decide_grouped(g.dd.dense, n, g.dd.kvals + (size_t)(it - 1) * n, sm);
-        BCK(cudaMemsetAsync(g.dbase + g.L.amax_off, 0, g.L.amax_bytes, sm));
-        mixed_slice_grouped(g.dd.slice + (size_t)par * n, n, g.dd.row_start, g.total_rows, sm);
-        mixed_gemm_grouped(g.slices, g.nt, g.dd.gemm + (size_t)par * n, g.dd.tiles, (int)g.ntiles, sm);
+    gemm(0);  // X^2
+    slice(1);
+    gemm(1);  // X^3
+    slice(2);
+    gemm(2);  // X^4
+    slice(3);
+    gemm(3);  // X^8
+    slice(4);
+    gemm(4);  // X^12
+    slice(5);
+    launch_power_diag_grouped(g.dd.powers, n, g.dd.blk_cols, g.nblk_cols, 2, 16, false, sm);
+    launch_power_decide_grouped(g.dd.powers, n, g.dd.kpow, 1, 15, sm);
+    gemm(5);  // X^16 (skipped per scene)
+    slice(6);
+    launch_power_diag_grouped(g.dd.powers, n, g.dd.blk_cols, g.nblk_cols, 17, 20, true, sm);
+    launch_power_decide_grouped(g.dd.powers, n, g.dd.kpow, 16, 19, sm);
+    launch_power_combine_grouped(g.dd.powers, n, g.dd.blk_elems, g.nblk_elems, 0, sm);  // iZ = G_0
+    for (int q = 1; q <= 4; ++q) {  // iZ += X^(4q) G_q
+        launch_power_combine_grouped(g.dd.powers, n, g.dd.blk_elems, g.nblk_elems, q, sm);
+        slice(6 + q);
+        gemm(5 + q);
     }
     if (taylor1) BCK(cudaEventRecord(taylor1, sm));
     // outputs (compute.cpp:168-183, 370-455)
@@ -381,56 +406,94 @@ int prepare_group(unc_batch* b, GroupRun& g, int nt) {
     }
     g.hbase = (char*)b->host;
     // descriptors
-    g.dd = desc_at(g.dbase + g.L.desc_off, n, g.ntasks, g.ntiles);
+    g.dd = desc_at(g.dbase + g.L.desc_off, n, g.ntasks, g.ntiles, nullptr);
     BCK(cudaStreamSynchronize(sm));  // the staging area is reused
     char* hd = g.hbase + g.h_desc;
-    const Desc hdd = desc_at(hd, n, g.ntasks, g.ntiles);
+    const Desc hdd = desc_at(hd, n, g.ntasks, g.ntiles, nullptr);
     memset(hd, 0, g.L.desc_bytes);
-    long br = 0, be = 0;
+    long br = 0, be = 0, bc = 0;
     int rs = 0;
     for (int i = 0; i < n; ++i) {
         Scene& s = g.sc[i];
         const int N = s.pl.N;
         const long ld = s.pl.ld;
-        hdd.mats[i] = SpdTaskMatrix{s.b.Z, s.b.iZ, s.b.add, ld, N, (N / 64 + (N % 64 != 0)) *
-                                                                        (N / 64 + (N % 64 != 0) + 1) / 2,
-                                    s.b.dag_state, s.b.s.err};
-        MixedOperand xa, xb, p;
-        if (!mixed_plan_nt(xa, s.bufX, s.eX, N, g.slices, false, nt) ||
-            !mixed_plan_nt(xb, s.bufX, s.eX, N, g.slices, true, nt) ||
-            !mixed_plan_nt(p, s.bufP, s.eP, N, g.slices, false, nt))
-            return bfail(UNC_ERR_CUDA, "tensor-map encoding failed");
-        hdd.maps[3 * i] = xa.map;
-        hdd.maps[3 * i + 1] = xb.map;
-        hdd.maps[3 * i + 2] = p.map;
+        const int nt64 = (N + 63) / 64;
+        hdd.mats[i] = SpdTaskMatrix{s.b.Z, s.b.iZ, s.b.add, ld, N, nt64 * (nt64 + 1) / 2, s.b.dag_state, s.b.s.err};
+        // tensor maps: X (A, B), A operand (A), X^4 (A, B), X^8 (A, B), X^12 (B), X^16 (B)
+        const int mbuf[kMaps] = {0, 0, 1, 2, 2, 3, 3, 4, 5};
+        const bool mb[kMaps] = {false, true, false, false, true, false, true, true, true};
+        MixedOperand op[kMaps];
+        for (int m = 0; m < kMaps; ++m) {
+            if (!mixed_plan_nt(op[m], s.buf[mbuf[m]], s.ex[mbuf[m]], N, g.slices, mb[m], nt))
+                return bfail(UNC_ERR_CUDA, "tensor-map encoding failed");
+            hdd.maps[kMaps * i + m] = op[m].map;
+        }
+        const int rows = op[0].rows, kp = op[0].kp;
         hdd.dense[i] = DenseJob{s.b.Z, s.b.iZ, s.b.add, s.b.e, ld, N, s.lambda, s.b.s.err, s.b.te, s.b.amax};
         hdd.blk_rows[i] = br;
         hdd.blk_elems[i] = be;
+        hdd.blk_cols[i] = bc;
         br += (N + 255) / 256;
         be += ((long)N * N + 255) / 256;
+        bc += N;
         hdd.row_start[i] = rs;
         rs += N;
-        // slicing: X (no update), then the power of odd / even iterations with the Taylor update
-        hdd.slice[i] = MixedSliceJob{s.b.Z, ld, N, g.slices, s.bufX, xa.rows, xa.kp, s.eX, nullptr, nullptr, nullptr};
-        hdd.slice[n + i] = MixedSliceJob{s.b.add, ld, N, g.slices, s.bufP, p.rows, p.kp, s.eP, s.b.iZ, s.b.te,
-                                         &s.b.te->done};
-        hdd.slice[2 * n + i] = MixedSliceJob{s.b.tmp, ld, N, g.slices, s.bufP, p.rows, p.kp, s.eP, s.b.iZ, s.b.te,
-                                             &s.b.te->done};
-        const CUtensorMap* dm = g.dd.maps + 3 * i;
-        hdd.gemm[i] = MixedGemmJob{dm, dm + 1, N, xa.kp, xa.rows, xb.rows, s.eX, s.eX, s.b.add, ld, s.b.amax,
-                                   s.b.s.err, nullptr};
-        hdd.gemm[n + i] = MixedGemmJob{dm + 2, dm + 1, N, p.kp, p.rows, xb.rows, s.eP, s.eX, s.b.tmp, ld, s.b.amax,
-                                       s.b.s.err, &s.b.te->done};
-        hdd.gemm[2 * n + i] = MixedGemmJob{dm + 2, dm + 1, N, p.kp, p.rows, xb.rows, s.eP, s.eX, s.b.add, ld,
-                                           s.b.amax, s.b.s.err, &s.b.te->done};
+        // slicing sets (powers.cu's order): X, X^2, X^3, X^4, X^8, X^12, X^16, G_1..G_4
+        const int* sk = s.b.te->skip;
+        struct SliceDef {
+            const double* src;
+            int buf;
+            const int* skip;
+        };
+        const SliceDef sd[kSliceSets] = {{s.b.Z, 0, nullptr},  {s.b.add, 1, nullptr}, {s.b.tmp, 1, nullptr},
+                                         {s.b.p4, 2, nullptr}, {s.b.p8, 3, nullptr},  {s.b.p12, 4, nullptr},
+                                         {s.b.p16, 5, sk},     {s.b.g, 1, sk + 1},    {s.b.g, 1, sk + 2},
+                                         {s.b.g, 1, sk + 3},   {s.b.g, 1, sk + 4}};
+        for (int q = 0; q < kSliceSets; ++q)
+            hdd.slice[(size_t)q * n + i] = MixedSliceJob{sd[q].src, ld, N, g.slices, s.buf[sd[q].buf], rows, kp,
+                                                         s.ex[sd[q].buf], nullptr, nullptr, sd[q].skip};
+        // products: A map, B map, A / B exponent buffers, output, accumulate, skip
+        const CUtensorMap* dm = g.dd.maps + kMaps * i;
+        struct GemmDef {
+            int a, b, ea, eb;
+            double* C;
+            int acc;
+            const int* skip;
+        };
+        const GemmDef gd[kGemmSets] = {{0, 1, 0, 0, s.b.add, 0, nullptr}, {2, 1, 1, 0, s.b.tmp, 0, nullptr},
+                                       {2, 1, 1, 0, s.b.p4, 0, nullptr},  {3, 4, 2, 2, s.b.p8, 0, nullptr},
+                                       {5, 4, 3, 2, s.b.p12, 0, nullptr}, {5, 6, 3, 3, s.b.p16, 0, sk},
+                                       {2, 4, 1, 2, s.b.iZ, 1, sk + 1},   {2, 6, 1, 3, s.b.iZ, 1, sk + 2},
+                                       {2, 7, 1, 4, s.b.iZ, 1, sk + 3},   {2, 8, 1, 5, s.b.iZ, 1, sk + 4}};
+        for (int q = 0; q < kGemmSets; ++q)
+            hdd.gemm[(size_t)q * n + i] = MixedGemmJob{dm + gd[q].a,   dm + gd[q].b,   N,          kp, rows, rows,
+                                                       s.ex[gd[q].ea], s.ex[gd[q].eb], gd[q].C,    ld, nullptr,
+                                                       s.b.s.err,      gd[q].skip,     gd[q].acc};
+        PowerSet ps{};
+        ps.M[0] = s.b.Z;
+        ps.M[1] = s.b.add;
+        ps.M[2] = s.b.tmp;
+        ps.M[3] = s.b.p4;
+        ps.M[4] = s.b.p8;
+        ps.M[5] = s.b.p12;
+        ps.M[6] = s.b.p16;
+        ps.iZ = s.b.iZ;
+        ps.G = s.b.g;
+        ps.n = N;
+        ps.ld = ld;
+        ps.dmax = s.b.dmax;
+        ps.te = s.b.te;
+        hdd.powers[i] = ps;
         for (int it = 1; it <= kTaylorIters; ++it)
-            hdd.kvals[(size_t)(it - 1) * n + i] = pow(s.lambda, it) / factorial_i32(it - 1);
+            hdd.kpow[19L * i + it - 1] = pow(s.lambda, it) / factorial_i32(it - 1);
     }
     hdd.blk_rows[n] = br;
     hdd.blk_elems[n] = be;
+    hdd.blk_cols[n] = bc;
     hdd.row_start[n] = rs;
     g.nblk_rows = br;
     g.nblk_elems = be;
+    g.nblk_cols = bc;
     g.total_rows = rs;
     memcpy(hdd.tasks, tasks.data(), sizeof(int4) * tasks.size());
     memcpy(hdd.tiles, tiles.data(), sizeof(int4) * tiles.size());
@@ -671,7 +734,7 @@ int unc_batch_compute(unc_batch* b, int num_scenes, const unc_options* opts, con
             continue;
         }
         if (o->algorithm != UNC_TAYLOR_EXPANSION || o->precision == UNC_PRECISION_FP64 ||
-            !spd_tasks_apply(9 * o->num_cams)) {
+            o->taylor_eval == UNC_TAYLOR_SEQUENTIAL || !spd_tasks_apply(9 * o->num_cams)) {
             single.push_back(i);
             continue;
         }

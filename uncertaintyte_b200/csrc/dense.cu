@@ -565,6 +565,8 @@ __device__ __forceinline__ void te_init_one(TeState* s) {
     s->old_change = 1.7976931348623157e308;  // DBL_MAX (compute.cpp:140)
     s->coef = 0.0;
     for (int i = 0; i < 20; ++i) s->change[i] = 0.0;
+    for (int i = 0; i < 20; ++i) s->c[i] = 0.0;
+    for (int i = 0; i < 8; ++i) s->skip[i] = 0;
 }
 
 __global__ void k_te_init(TeState* s) {

@@ -239,12 +239,55 @@ struct TeState {
     double old_change;      // previous |k * max|add||
     double coef;            // k of the current iteration (read by the axpy)
     double change[20];      // cycle_change record
+    // blocked-power evaluation (powers.cu): the series' coefficients c[0] = 1,
+    // c[i] = k_i for the performed iterations, 0 after; skip[0]: X^16 is not
+    // needed, skip[q] (q = 1..4): the block X^(4q) G_q is zero
+    double c[20];
+    int skip[8];
 };
 // One thread: change = |k * max(amax, DBL_MIN)|; stop when change < 1e-5 or
 // change > old_change, else record it and publish k for the axpy.
 void launch_te_decide(TeState* s, const unsigned long long* amax, double k, cudaStream_t st);
 // Reset the state (not done, no iteration, old change = DBL_MAX).
 void launch_te_init(TeState* s, cudaStream_t st);
+// ---------------- powers.cu ----------------
+// The Taylor series iZ = X + sum_{i=1..m} k_i X^(i+1) (compute.cpp:141-160)
+// evaluated from the powers X^2, X^3, X^4, X^8, X^12 (X^16 when m >= 15):
+// the stop rule's max|X^j| is the largest diagonal entry of the SPD power X^j,
+// the dot product of columns of two lower powers; the sum is formed in blocks
+// iZ = G_0 + X^4 G_1 + X^8 G_2 + X^12 G_3 + X^16 G_4, G_q = sum_r c_(4q+r) X^(r+1).
+// 8 products for m <= 15 instead of m + 1.
+struct PowerSet {
+    double* M[7];  // X, X^2, X^3, X^4, X^8, X^12, X^16
+    double *iZ, *G;
+    int n;
+    long ld;
+    unsigned long long* dmax;  // 21 words: max diag of X^j, j = 0..20 (bits of a non-negative double)
+    TeState* te;
+};
+// k[i - 1] = lambda^i / factorial(i - 1), i = 1..19 (host values)
+struct TaylorCoefs {
+    double k[19];
+};
+// The powers' diagonal maxima for j in [jlo, jhi] (2..16 or 17..20), unless *skip.
+void launch_power_diag(const PowerSet& ps, int jlo, int jhi, const int* skip, cudaStream_t st);
+// The stop rule over iterations [ilo, ihi] from the diagonal maxima (a
+// non-finite one marks the state bad); the coefficients c[i] of the performed
+// iterations; after ilo..15 the X^16 skip word, after ..19 the block skip words.
+void launch_power_decide(TeState* te, const unsigned long long* dmax, const TaylorCoefs& k, int ilo, int ihi,
+                         cudaStream_t st);
+// out = c[4q] X + c[4q+1] X^2 + c[4q+2] X^3 + c[4q+3] X^4 (q = 0: into iZ), unless skipped.
+void launch_power_combine(const PowerSet& ps, int q, double* out, const int* skip, cudaStream_t st);
+// Grouped forms over many matrices (a batch): one block per column (diag) or
+// per 256 elements (combine) of set m with blk[m] <= b < blk[m + 1].
+void launch_power_diag_grouped(const PowerSet* d_sets, int nsets, const long* d_blk_cols, long nblk, int jlo,
+                               int jhi, bool skip_if_done_early, cudaStream_t st);
+// d_k: 19 coefficients per set (set-major)
+void launch_power_decide_grouped(const PowerSet* d_sets, int nsets, const double* d_k, int ilo, int ihi,
+                                 cudaStream_t st);
+void launch_power_combine_grouped(const PowerSet* d_sets, int nsets, const long* d_blk_elems, long nblk, int q,
+                                  cudaStream_t st);
+
 // Grouped dense-stage kernels over many matrices (a batch). Element-wise
 // launches: block b belongs to job m with blk[m] <= b < blk[m + 1] (blk: njobs
 // + 1 longs; 256 threads per block over the job's rows, or n^2 elements).
@@ -315,6 +358,7 @@ struct MixedGemmJob {  // one lower-triangle symmetric product C = P X (mirrored
     unsigned long long* amax;
     int* err;
     const int* skip;
+    int accumulate;  // C += P X
 };
 // block b of the launch slices row b - row_start[m] of job m (row_start: njobs + 1 ints)
 void mixed_slice_grouped(const MixedSliceJob* d_jobs, int njobs, const int* d_row_start, int total_rows,
@@ -331,8 +375,10 @@ void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st, co
 // C = P * X from the slices of P (a) and X (b); lower_only: tiles on/below the
 // diagonal; mirror: the result's lower triangle is also written transposed
 // into the upper one (a symmetric product needs no separate mirror pass).
+// accumulate: C += P X (C symmetric, with mirror) instead of C = P X.
 void mixed_gemm(const MixedOperand& a, const MixedOperand& b, double* C, int ldc, unsigned long long* amax,
-                bool lower_only, int* err, cudaStream_t st, const int* skip = nullptr, bool mirror = false);
+                bool lower_only, int* err, cudaStream_t st, const int* skip = nullptr, bool mirror = false,
+                bool accumulate = false);
 
 // ---------------- svd.cu ----------------
 // Scratch of the PSD pseudo-inverse (n x ld matrices and p x n blocks).

@@ -232,7 +232,8 @@ template <int NT, int S>
 __device__ __forceinline__ void ozaki_tile(const CUtensorMap* tA, const CUtensorMap* tB, int m0, int n0, int M, int N,
                                            int kp, int rowsA, int rowsB, const int* __restrict__ eA,
                                            const int* __restrict__ eB, double* C, long ldc,
-                                           unsigned long long* amax, int* err, int mirror, bool maps_in_global) {
+                                           unsigned long long* amax, int* err, int mirror, bool maps_in_global,
+                                           int accumulate) {
     using Sh = Shape<NT, S>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -352,9 +353,11 @@ __device__ __forceinline__ void ozaki_tile(const CUtensorMap* tA, const CUtensor
                 for (int j = 0; j < 16; ++j) {
                     const int col = n0 + c0 + j;
                     if (col < N) {
-                        const double x = v[j] * pow2(er + eB[col]);
+                        double x = v[j] * pow2(er + eB[col]);
                         // mirror: the lower triangle is written at (row, col) and at
                         // (col, row); nothing above the diagonal is written directly
+                        // accumulate: C += P X (C symmetric: its lower element is read)
+                        if (accumulate && (!mirror || row >= col)) x += C[row + (long)col * ldc];
                         if (!mirror || row >= col) {
                             C[row + (long)col * ldc] = x;
                             const double ax = fabs(x);
@@ -381,11 +384,13 @@ template <int NT, int S>
 __global__ void __launch_bounds__(THREADS, 1)
     k_ozaki_gemm(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int M, int N,
                  int kp, int rowsA, int rowsB, const int* __restrict__ eA, const int* __restrict__ eB, double* C,
-                 long ldc, unsigned long long* amax, int lower_only, int* err, const int* skip, int mirror) {
+                 long ldc, unsigned long long* amax, int lower_only, int* err, const int* skip, int mirror,
+                 int accumulate) {
     if (skip && *skip) return;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * NT;
     if (lower_only && n0 > m0 + BM - 1) return;
-    ozaki_tile<NT, S>(&tA, &tB, m0, n0, M, N, kp, rowsA, rowsB, eA, eB, C, ldc, amax, err, mirror, false);
+    ozaki_tile<NT, S>(&tA, &tB, m0, n0, M, N, kp, rowsA, rowsB, eA, eB, C, ldc, amax, err, mirror, false,
+                      accumulate);
 }
 
 // The products of many matrices (a batch) in one launch: CTA b computes tile
@@ -399,7 +404,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     const MixedGemmJob& j = jobs[t.x];
     if (j.skip && *j.skip) return;
     ozaki_tile<NT, S>(j.tA, j.tB, t.y, t.z, j.n, j.n, j.kp, j.rowsA, j.rowsB, j.eA, j.eB, j.C, j.ldc, j.amax, j.err,
-                      1, true);
+                      1, true, j.accumulate);
 }
 
 // ------------------------------------------------------------------------
@@ -571,32 +576,36 @@ void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st, co
 }
 
 void mixed_gemm(const MixedOperand& a, const MixedOperand& b, double* C, int ldc, unsigned long long* amax,
-                bool lower_only, int* err, cudaStream_t st, const int* skip, bool mirror) {
+                bool lower_only, int* err, cudaStream_t st, const int* skip, bool mirror, bool accumulate) {
     const int n = a.n;
     if (a.slices == 4) {
         set_attr_once<128, 4>();
         dim3 grid((n + 127) / 128, (n + BM - 1) / BM);
         k_ozaki_gemm<128, 4><<<grid, THREADS, Shape<128, 4>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
                                                                          a.exps, b.exps, C, ldc, amax,
-                                                                         lower_only ? 1 : 0, err, skip, mirror ? 1 : 0);
+                                                                         lower_only ? 1 : 0, err, skip, mirror ? 1 : 0,
+                                                                         accumulate ? 1 : 0);
     } else if (a.slices == 5 && mixed_tile_n(5, n) == 64) {
         set_attr_once<64, 5>();
         dim3 grid((n + 63) / 64, (n + BM - 1) / BM);
         k_ozaki_gemm<64, 5><<<grid, THREADS, Shape<64, 5>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
                                                                        a.exps, b.exps, C, ldc, amax,
-                                                                       lower_only ? 1 : 0, err, skip, mirror ? 1 : 0);
+                                                                       lower_only ? 1 : 0, err, skip, mirror ? 1 : 0,
+                                                                         accumulate ? 1 : 0);
     } else if (a.slices == 5) {
         set_attr_once<96, 5>();
         dim3 grid((n + 95) / 96, (n + BM - 1) / BM);
         k_ozaki_gemm<96, 5><<<grid, THREADS, Shape<96, 5>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
                                                                        a.exps, b.exps, C, ldc, amax,
-                                                                       lower_only ? 1 : 0, err, skip, mirror ? 1 : 0);
+                                                                       lower_only ? 1 : 0, err, skip, mirror ? 1 : 0,
+                                                                         accumulate ? 1 : 0);
     } else {
         set_attr_once<128, 3>();
         dim3 grid((n + 127) / 128, (n + BM - 1) / BM);
         k_ozaki_gemm<128, 3><<<grid, THREADS, Shape<128, 3>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
                                                                          a.exps, b.exps, C, ldc, amax,
-                                                                         lower_only ? 1 : 0, err, skip, mirror ? 1 : 0);
+                                                                         lower_only ? 1 : 0, err, skip, mirror ? 1 : 0,
+                                                                         accumulate ? 1 : 0);
     }
     count_launch();
 }

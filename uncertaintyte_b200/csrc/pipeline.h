@@ -16,6 +16,8 @@ struct Buffers {
     double *cam_out, *pt_out;
     SceneDev s;
     double *Z, *iZ, *add, *tmp, *e, *gjws, *sig;
+    double *p4, *p8, *p12, *p16, *g;   // blocked-power Taylor evaluation: X^4, X^8, X^12, X^16, G_q
+    unsigned long long* dmax;          // 24 words: the powers' diagonal maxima
     int* dag_state;  // counters of the tile-task inverse
     unsigned long long* amax;
     TeState* te;

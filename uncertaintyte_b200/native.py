@@ -45,6 +45,7 @@ class UncOptions(C.Structure):
         ("pts2fix", C.c_int * 3),
         ("has_pts2fix", C.c_int),
         ("precision", C.c_int),
+        ("taylor_eval", C.c_int),
     ]
 
 
@@ -168,8 +169,11 @@ def _ptr(a: np.ndarray) -> int:
     return a.ctypes.data
 
 
+TAYLOR_EVAL = {"powers": 0, "sequential": 1}
+
+
 def make_options(jac: Jacobian, algorithm: Optional[int] = None, precision: str = "fp64",
-                 lam: Optional[float] = None) -> UncOptions:
+                 lam: Optional[float] = None, taylor: str = "powers") -> UncOptions:
     o = UncOptions()
     lib().unc_options_init(C.byref(o), jac.num_cams, jac.cam_params, jac.num_points, jac.num_obs)
     o.algorithm = jac.algorithm if algorithm is None else algorithm
@@ -180,6 +184,7 @@ def make_options(jac: Jacobian, algorithm: Optional[int] = None, precision: str 
         o.pts2fix[:] = [int(x) for x in jac.pts2fix]
         o.has_pts2fix = 1
     o.precision = PRECISION[precision]
+    o.taylor_eval = TAYLOR_EVAL[taylor]
     return o
 
 
@@ -256,9 +261,11 @@ class Context:
 
 
 def compute_covariances(jac: Jacobian, ctx: Optional[Context] = None, algorithm: Optional[int] = None,
-                        precision: str = "fp64", cam_init=None, pt_init=None):
-    """computeCovariances on host arrays: returns (cam (C*45,), pt (P*6,), stats dict)."""
-    o = make_options(jac, algorithm, precision)
+                        precision: str = "fp64", cam_init=None, pt_init=None, taylor: str = "powers"):
+    """computeCovariances on host arrays: returns (cam (C*45,), pt (P*6,), stats dict).
+    taylor: "powers" (blocked powers, the default) or "sequential" (one product
+    per Taylor iteration, the reference's order)."""
+    o = make_options(jac, algorithm, precision, taylor=taylor)
     cam = np.zeros(jac.num_cams * 45) if cam_init is None else np.array(cam_init, dtype=np.float64)
     pt = np.zeros(jac.num_points * 6) if pt_init is None else np.array(pt_init, dtype=np.float64)
     rows = np.ascontiguousarray(jac.rows, dtype=np.int32)
