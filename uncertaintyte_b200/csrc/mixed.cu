@@ -380,15 +380,50 @@ __device__ __forceinline__ void ozaki_tile(const CUtensorMap* tA, const CUtensor
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(Sh::TMEM_COLS));
 }
 
+// Lower-triangle tile t of an n x n product in grouped order: row blocks in
+// groups of gm, each group walked column by column (the rows of a column whose
+// lower tiles reach it), so that the CTAs running together share the B tiles
+// of a few columns and the A tiles of gm row blocks in L2 instead of streaming
+// B once per row block. O(columns) integer steps per CTA.
+__device__ __forceinline__ void grouped_lower_tile(int t, int n, int nt, int gm, int& by, int& bx) {
+    const int by_n = (n + BM - 1) / BM, bx_n = (n + nt - 1) / nt;
+    by = bx = 0;
+    for (int r0 = 0; r0 < by_n; r0 += gm) {
+        const int r1 = min(r0 + gm, by_n) - 1;
+        const int cols = min((r1 * BM + BM - 1) / nt + 1, bx_n);
+        for (int c = 0; c < cols; ++c) {
+            const int need = c * nt - (BM - 1);  // by * BM + BM - 1 >= c * nt
+            const int lo = max(r0, need > 0 ? (need + BM - 1) / BM : 0);
+            const int cnt = r1 - lo + 1;
+            if (t < cnt) {
+                by = lo + t;
+                bx = c;
+                return;
+            }
+            t -= cnt;
+        }
+    }
+}
+
 template <int NT, int S>
 __global__ void __launch_bounds__(THREADS, 1)
     k_ozaki_gemm(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int M, int N,
                  int kp, int rowsA, int rowsB, const int* __restrict__ eA, const int* __restrict__ eB, double* C,
                  long ldc, unsigned long long* amax, int lower_only, int* err, const int* skip, int mirror,
-                 int accumulate) {
+                 int accumulate, int group_m) {
     if (skip && *skip) return;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * NT;
-    if (lower_only && n0 > m0 + BM - 1) return;
+    int m0, n0;
+    if (group_m > 0) {  // 1-D grid over exactly the lower tiles, grouped order
+        __shared__ int s_tile[2];
+        if (threadIdx.x == 0) grouped_lower_tile(blockIdx.x, N, NT, group_m, s_tile[0], s_tile[1]);
+        __syncthreads();
+        m0 = s_tile[0] * BM;
+        n0 = s_tile[1] * NT;
+    } else {
+        m0 = blockIdx.y * BM;
+        n0 = blockIdx.x * NT;
+        if (lower_only && n0 > m0 + BM - 1) return;
+    }
     ozaki_tile<NT, S>(&tA, &tB, m0, n0, M, N, kp, rowsA, rowsB, eA, eB, C, ldc, amax, err, mirror, false,
                       accumulate);
 }
@@ -575,38 +610,37 @@ void mixed_slice(const double* A, int lda, MixedOperand& op, cudaStream_t st, co
     count_launch();
 }
 
+// Row blocks per group of the grouped tile order: used when one operand's
+// slices exceed about 3/4 of L2 (the B operand would be re-streamed from HBM
+// for every row block); small products keep the 2-D grid.
+static int group_rows_for(int n, int slices) {
+    const double b_bytes = (double)slices * n * (double)n;
+    return b_bytes > 96.0 * (1 << 20) ? 8 : 0;
+}
+
+template <int NT, int S>
+static void launch_ozaki(const MixedOperand& a, const MixedOperand& b, double* C, int ldc, unsigned long long* amax,
+                         bool lower_only, int* err, cudaStream_t st, const int* skip, bool mirror, bool accumulate) {
+    set_attr_once<NT, S>();
+    const int n = a.n;
+    const int gm = lower_only ? group_rows_for(n, S) : 0;
+    dim3 grid = gm > 0 ? dim3((unsigned)lower_tiles(n, NT), 1) : dim3((n + NT - 1) / NT, (n + BM - 1) / BM);
+    k_ozaki_gemm<NT, S><<<grid, THREADS, Shape<NT, S>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows, a.exps,
+                                                                   b.exps, C, ldc, amax, lower_only ? 1 : 0, err,
+                                                                   skip, mirror ? 1 : 0, accumulate ? 1 : 0, gm);
+}
+
 void mixed_gemm(const MixedOperand& a, const MixedOperand& b, double* C, int ldc, unsigned long long* amax,
                 bool lower_only, int* err, cudaStream_t st, const int* skip, bool mirror, bool accumulate) {
     const int n = a.n;
-    if (a.slices == 4) {
-        set_attr_once<128, 4>();
-        dim3 grid((n + 127) / 128, (n + BM - 1) / BM);
-        k_ozaki_gemm<128, 4><<<grid, THREADS, Shape<128, 4>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
-                                                                         a.exps, b.exps, C, ldc, amax,
-                                                                         lower_only ? 1 : 0, err, skip, mirror ? 1 : 0,
-                                                                         accumulate ? 1 : 0);
-    } else if (a.slices == 5 && mixed_tile_n(5, n) == 64) {
-        set_attr_once<64, 5>();
-        dim3 grid((n + 63) / 64, (n + BM - 1) / BM);
-        k_ozaki_gemm<64, 5><<<grid, THREADS, Shape<64, 5>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
-                                                                       a.exps, b.exps, C, ldc, amax,
-                                                                       lower_only ? 1 : 0, err, skip, mirror ? 1 : 0,
-                                                                         accumulate ? 1 : 0);
-    } else if (a.slices == 5) {
-        set_attr_once<96, 5>();
-        dim3 grid((n + 95) / 96, (n + BM - 1) / BM);
-        k_ozaki_gemm<96, 5><<<grid, THREADS, Shape<96, 5>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
-                                                                       a.exps, b.exps, C, ldc, amax,
-                                                                       lower_only ? 1 : 0, err, skip, mirror ? 1 : 0,
-                                                                         accumulate ? 1 : 0);
-    } else {
-        set_attr_once<128, 3>();
-        dim3 grid((n + 127) / 128, (n + BM - 1) / BM);
-        k_ozaki_gemm<128, 3><<<grid, THREADS, Shape<128, 3>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows,
-                                                                         a.exps, b.exps, C, ldc, amax,
-                                                                         lower_only ? 1 : 0, err, skip, mirror ? 1 : 0,
-                                                                         accumulate ? 1 : 0);
-    }
+    if (a.slices == 4)
+        launch_ozaki<128, 4>(a, b, C, ldc, amax, lower_only, err, st, skip, mirror, accumulate);
+    else if (a.slices == 5 && mixed_tile_n(5, n) == 64)
+        launch_ozaki<64, 5>(a, b, C, ldc, amax, lower_only, err, st, skip, mirror, accumulate);
+    else if (a.slices == 5)
+        launch_ozaki<96, 5>(a, b, C, ldc, amax, lower_only, err, st, skip, mirror, accumulate);
+    else
+        launch_ozaki<128, 3>(a, b, C, ldc, amax, lower_only, err, st, skip, mirror, accumulate);
     count_launch();
 }
 
