@@ -51,7 +51,7 @@ def block_rel_err(a, b, width):
     return float(r.max()) if r.size else 0.0
 
 
-def fp64_floor(jac, ref_lu, threads=8):
+def fp64_floor(jac, ref_lu, threads=8, **kw):
     """How far two correct FP64 computations of this scene lie apart.
 
     Z + lambda*I is ill-conditioned (the gauge is fixed only by lambda), so
@@ -65,12 +65,12 @@ def fp64_floor(jac, ref_lu, threads=8):
 
     import oracle
     det = {}
-    chol = oracle.compute(jac, threads=threads, route="cholesky")
+    chol = oracle.compute(jac, threads=threads, route="cholesky", **kw)
     det["cholesky"] = (block_rel_err(chol["cam"], ref_lu["cam"], 45), block_rel_err(chol["pt"], ref_lu["pt"], 6))
     for seed in (1, 2):
         j2 = copy.copy(jac)
         r = np.random.default_rng(seed).uniform(-1.0, 1.0, jac.values.size)
         j2.values = jac.values * (1.0 + 2.0 ** -52 * r)
-        o = oracle.compute(j2, threads=threads)
+        o = oracle.compute(j2, threads=threads, **kw)
         det[f"ulp{seed}"] = (block_rel_err(o["cam"], ref_lu["cam"], 45), block_rel_err(o["pt"], ref_lu["pt"], 6))
     return max(v[0] for v in det.values()), max(v[1] for v in det.values()), det, chol

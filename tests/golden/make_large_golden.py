@@ -10,21 +10,25 @@ fingerprint of the scene (so that a test notices a generator change).
 
 Both dense-inverse routes are run: "lu" (the reference's equilibrated
 dgetrf/dgetri) and "cholesky" (the Jacobi-equilibrated Cholesky inverse that
-the CUDA path also uses). How far the two routes lie apart is the FP64 floor
-of this ill-conditioned problem, which the GPU test uses as its bar.
+the CUDA path also uses), and the LU route on the Jacobian with every value
+moved by at most one ulp (two seeds, "ulp1" / "ulp2", the perturbation of
+tests/conftest.py fp64_floor). How far these lie apart is the FP64 floor of
+this ill-conditioned problem, which the GPU test uses as its bar.
 
 The oracle's point stage runs with its per-point observation index
 (faithful_point_scan=False): the reference's O(points x observations) row scan
 (compute.cpp:393) would visit ~1.75e12 rows here; the index visits the same
 rows of each point in the same order.
 
-    python tests/golden/make_large_golden.py [--threads N]
+    python tests/golden/make_large_golden.py [--threads N] [--only-ulp]
 
-writes tests/golden/large_sample.npz.
+writes tests/golden/large_sample.npz (--only-ulp: adds the perturbed runs to
+an existing file).
 """
 from __future__ import annotations
 
 import argparse
+import copy
 import hashlib
 import os
 import sys
@@ -60,22 +64,33 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--threads", type=int, default=os.cpu_count() or 1)
     ap.add_argument("--out", default=os.path.join(HERE, "large_sample.npz"))
+    ap.add_argument("--only-ulp", action="store_true")
     a = ap.parse_args()
     jac = scenes.synthetic_jacobian("large", seed=0)
     cams, pts = sample_indices(jac)
     out = {"fingerprint": scene_fingerprint(jac), "cams": cams, "pts": pts,
            "pts2fix": np.asarray(jac.pts2fix, dtype=np.int32)}
-    for route in ("lu", "cholesky"):
+    runs = [("lu", "lu", None), ("cholesky", "cholesky", None), ("ulp1", "lu", 1), ("ulp2", "lu", 2)]
+    if a.only_ulp:
+        old = np.load(a.out)
+        out.update({k: old[k] for k in old.files})
+        runs = runs[2:]
+    for name, route, seed in runs:
         t0 = time.perf_counter()
-        r = oracle.compute(jac, threads=a.threads, faithful_point_scan=False, route=route)
+        j = jac
+        if seed is not None:  # every value moved by at most one ulp
+            j = copy.copy(jac)
+            r = np.random.default_rng(seed).uniform(-1.0, 1.0, jac.values.size)
+            j.values = jac.values * (1.0 + 2.0 ** -52 * r)
+        r = oracle.compute(j, threads=a.threads, faithful_point_scan=False, route=route)
         st = r["stats"]
-        print(f"{route}: {time.perf_counter() - t0:.1f} s, {st.te_iterations} iterations", flush=True)
-        out[f"{route}_cam"] = r["cam"].reshape(-1, 45)[cams]
-        out[f"{route}_pt"] = r["pt"].reshape(-1, 6)[pts]
-        out[f"{route}_iters"] = np.int32(st.te_iterations)
-        out[f"{route}_cycle_change"] = np.array(st.cycle_change[: st.te_iterations])
-        out[f"{route}_lambda"] = np.float64(st.lam)
-        out[f"{route}_fixed"] = np.array(list(st.fixed_pts), dtype=np.int32)
+        print(f"{name}: {time.perf_counter() - t0:.1f} s, {st.te_iterations} iterations", flush=True)
+        out[f"{name}_cam"] = r["cam"].reshape(-1, 45)[cams]
+        out[f"{name}_pt"] = r["pt"].reshape(-1, 6)[pts]
+        out[f"{name}_iters"] = np.int32(st.te_iterations)
+        out[f"{name}_cycle_change"] = np.array(st.cycle_change[: st.te_iterations])
+        out[f"{name}_lambda"] = np.float64(st.lam)
+        out[f"{name}_fixed"] = np.array(list(st.fixed_pts), dtype=np.int32)
     np.savez_compressed(a.out, **out)
     print("wrote", a.out)
 

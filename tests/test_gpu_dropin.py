@@ -82,7 +82,7 @@ def test_cpp_gauge_choice_and_accessors(prog):
     Uncertainty; its accessors decompose every block on the GPU."""
     exe, d = prog
     sc = scenes.make_scene("small", seed=3)
-    jac = scenes.scene_jacobian(sc, with_fixed=False)
+    jac = scenes.scene_jacobian(sc)  # the file names fixed points (the first two calls need them)
     path = str(d / "small.jacob")
     jacob.save_jacob(path, jac)
     pts = str(d / "small_pts.bin")

@@ -35,8 +35,8 @@ def ctx():
     c.close()
 
 
-def _check_fp64(cam, pt, jac, ref, label=""):
-    fc, fp, det, chol = fp64_floor(jac, ref)
+def _check_fp64(cam, pt, jac, ref, label="", **kw):
+    fc, fp, det, chol = fp64_floor(jac, ref, **kw)
     bar_c, bar_p = max(FP64_BAR, FLOOR_MULT * fc), max(FP64_BAR, FLOOR_MULT * fp)
     ec, ep = block_rel_err(cam, ref["cam"], 45), block_rel_err(pt, ref["pt"], 6)
     hc, hp = block_rel_err(cam, chol["cam"], 45), block_rel_err(pt, chol["pt"], 6)
@@ -87,7 +87,7 @@ def test_cube_vs_oracle_and_tail_rule(ctx):
     assert np.all(pt[11] == 0)
     assert np.all(pt[12] == 7.0) and np.all(pt[14] == 7.0)
     np.testing.assert_array_equal(ref["pt"].reshape(-1, 6)[[11, 12, 14]], pt[[11, 12, 14]])
-    _check_fp64(cam, pt.reshape(-1), jac, ref, "cube:")
+    _check_fp64(cam, pt.reshape(-1), jac, ref, "cube:", pt_init=sentinel)
 
 
 @pytest.mark.parametrize("seed", [0, 1])
