@@ -70,6 +70,8 @@ def _args():
     ap.add_argument("--precision", choices=["fp64", "mixed", "mixed4", "mixed3"], default="mixed")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--solve-only", action="store_true",
+                    help="time the solves of the main precision only and print a reduced line (for profilers)")
     ap.add_argument("--scenes", type=int, default=256, help="batch: number of scenes")
     ap.add_argument("--requests", type=int, default=200, help="serve: requests per precision")
     ap.add_argument("--rate", type=float, default=10.0, help="serve: Poisson arrival rate (requests/s)")
@@ -227,20 +229,22 @@ def measured_peaks():
 def stage_rooflines(stats, num_cams: int, num_points: int, num_obs: int):
     """HBM rooflines of the assembly and Schur stages from their CUDA-event
     times and the algorithmic bytes per unit: assembly reads 296 B and writes
-    216 B per observation (J values, columns and row pointers in; W out) plus
-    72 B per point (V) and 648 B per camera (U); the Schur scatter reads W
-    (216 B per observation) and V^-1 (72 B per point) and writes Z once
+    432 B per observation (J values, columns and row pointers in; W and Y out)
+    plus 72 B per point (V) and 648 B per camera (U); the Schur stage reads W
+    and Y (432 B per observation) and U (648 B per camera) and writes Z once
     (8 N^2 B, N = 9 cameras)."""
     peak, src, _ = measured_peaks()
     N = 9 * num_cams
-    asm_b = 512.0 * num_obs + 72.0 * num_points + 648.0 * num_cams
+    asm_b = 728.0 * num_obs + 72.0 * num_points + 648.0 * num_cams
     asm_t = sum(stats[k] for k in ("time_create_j", "time_fix_j", "time_norm_j", "time_multiply_jj"))
-    sch_b = 216.0 * num_obs + 72.0 * num_points + 8.0 * N * N
+    sch_b = 432.0 * num_obs + 648.0 * num_cams + 8.0 * N * N
     sch_t = stats["time_compose_z"]
     out = {}
     for name, b, t, what in (("roofline_assembly", asm_b, asm_t, "validation, index, J^T J blocks, column norms, "
-                              "point blocks and inverses, W/Y and the self terms, zeroing of the dense buffers"),
-                             ("roofline_schur", sch_b, sch_t, "pair list, pair products scattered into Z, mirror")):
+                              "point blocks and inverses, W and Y records, zeroing of the dense work buffers"),
+                             ("roofline_schur", sch_b, sch_t, "zeroing of Z, then one CTA per camera column: "
+                                                                "partner lists, run masks, block sums in registers, "
+                                                                "both triangles written")):
         ach = b / t / 1e9 if t > 0 else None
         out[name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                      "frac": ach / peak if ach else None, "algorithmic_bytes": b, "seconds": t,
@@ -402,14 +406,6 @@ def _mixed_tile_n(n: int, slices: int) -> int:
     return 64 if w64 * 80 < w96 * 112 else 96
 
 
-def _mixed_issued_ops(n: int, slices: int) -> float:
-    """int8 multiply-adds x 2 issued by one lower-triangle mixed product."""
-    nt = _mixed_tile_n(n, slices)
-    kp = (n + 63) // 64 * 64
-    pairs = slices * (slices + 1) // 2
-    return 2.0 * pairs * _lower_tiles(n, nt) * 128 * nt * kp
-
-
 def run_ours(a):
     import ctypes as C
 
@@ -477,7 +473,10 @@ def run_ours(a):
         if ws > 1:
             dist.barrier()
         launches = native.kernel_launches() - l0
-        prof = ctx.profile(reset=True) if profile else None
+        prof = None
+        if profile:
+            i8 = ctx.profile_int8()  # read before the reset
+            prof = ctx.profile(reset=True) + (i8,)
         ctx.set_profiling(False)
         t = max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in evs) * 1e-3, dev)
         return t, st, launches, prof
@@ -488,6 +487,15 @@ def run_ours(a):
     t_main, stats, launches, _ = timed(opts, a.steps, a.warmup, profile=False, clocks=clocks)
     clk = clocks.stop()
     cam_main, pt_main = d_cam.cpu().numpy().copy(), d_pt.cpu().numpy().copy()
+    if a.solve_only:  # the solves alone (launch lists and kernel captures); no side measurements
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": ws * a.steps / t_main, "unit": UNIT, "n_gpus": ws,
+                              "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * t_main / a.steps,
+                              "mode": "solve-only", "config": {"workload": WORKLOADS[a.workload], "precision": prec},
+                              "gpu_launches": launches, "clocks": clk}))
+        if ws > 1:
+            dist.destroy_process_group()
+        return
     value = replica_throughput(ws, a.steps, t_main)
     # the product kernel's own time for the roofline: a separate profiled pass
     # (CUDA events around every product; the dense stages then run without graphs)
@@ -514,7 +522,7 @@ def run_ours(a):
                 "mixed_vs_fp64_max_rel_err": {"camera_9x9": blk(cam_main, c64, 45),
                                               "point_3x3": blk(pt_main, p64, 6), "bar": 1e-6}}
         if rank == 0 and prof64 is not None and prof64[1] > 0:
-            n_prod, prod_s, prod_flops = prof64
+            n_prod, prod_s, prod_flops, _ = prof64
             nd = min(16384, max(4096, N // 8 * 8))
             peak64 = _fp64_peak_tflops(torch, dev, n=nd, reps=3)
             ach = prod_flops / prod_s / 1e12
@@ -601,7 +609,7 @@ def run_ours(a):
     # roofline of the dominant kernel (the Taylor-series product)
     roof = None
     if rank == 0 and prof is not None and prof[1] > 0:
-        n_prod, prod_s, prod_flops = prof
+        n_prod, prod_s, prod_flops, prod_i8 = prof
         if prec == "fp64":
             peak = _fp64_peak_tflops(torch, dev)
             achieved = prod_flops / prod_s / 1e12
@@ -612,11 +620,13 @@ def run_ours(a):
                     "launches_timed": n_prod, "flops_per_launch": prod_flops / n_prod}
         else:
             slices = {"mixed": 5, "mixed4": 4, "mixed3": 3}[prec]
-            ops = _mixed_issued_ops(N, slices) * n_prod
+            ops = prod_i8  # issued by the library's slice schedule, product by product
             achieved = ops / prod_s / 1e12
             peak = _int8_peak_tops(torch, dev)
-            roof = {"bound": "tensor", "kernel": f"k_ozaki_gemm (tcgen05 kind::i8, TMA, {slices} slices, "
-                                                 f"128x{_mixed_tile_n(N, slices)} lower tiles)",
+            roof = {"bound": "tensor", "kernel": f"k_ozaki_gemm (tcgen05 kind::i8, TMA, {slices} slices for X^2..X^4 "
+                                                 f"and X^4 G_1, fewer for the higher powers and blocks; "
+                                                 f"128x{_mixed_tile_n(N, slices)} lower tiles at {slices} slices, "
+                                                 f"128x128 below)",
                     "achieved": achieved, "peak": peak, "unit": "TOP/s int8",
                     "frac": (achieved / peak) if peak else None,
                     "traffic": _traffic_from_profile("ozaki", a.workload),

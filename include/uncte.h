@@ -129,6 +129,9 @@ int unc_compute_device(unc_context* ctx, const unc_options* opt, int num_rows, i
 int unc_context_set_profiling(unc_context* ctx, int enable);
 int unc_context_profile(unc_context* ctx, long long* launches, double* seconds, double* flops,
                         int reset);
+/* Mixed modes: the int8 multiply-adds x 2 those products issued (tile padding
+ * included; each product with its own slice count). Read it before a reset. */
+int unc_context_profile_int8(unc_context* ctx, double* int8_ops);
 
 /* Device bytes unc_compute_device would use for this problem (admission). */
 long long unc_workspace_bytes(const unc_options* opt, int num_rows, int num_cols);

@@ -53,8 +53,6 @@ struct unc_context {
     cudaStream_t stream = nullptr;
     void* ws = nullptr;
     size_t ws_bytes = 0;
-    void* tup = nullptr;  // Schur observation pairs (sized at run time)
-    size_t tup_bytes = 0;
     void* mp = nullptr;   // int8 slice planes of the mixed-precision products
     size_t mp_bytes = 0;
     void* jac = nullptr;  // unc_compute_scene: scene inputs, the generated CRS Jacobian, outputs
@@ -74,7 +72,7 @@ struct unc_context {
     bool prof = false;
     std::vector<cudaEvent_t> pev;
     long long prof_launches = 0;
-    double prof_seconds = 0, prof_flops = 0;
+    double prof_seconds = 0, prof_flops = 0, prof_int8_ops = 0;
 };
 
 namespace unc {
@@ -123,7 +121,7 @@ size_t carve(char* base, const Plan& pl, bool host_io, long long nnz, int nrows,
     s.pt_ptr = c.take<int>((size_t)pl.P + 1);
     s.pt_obs = c.take<int>(pl.nobs);
     s.cursor = c.take<int>((size_t)pl.C + pl.P + 1);
-    s.scan_tmp = c.take<int>(scan_tmp_ints(std::max(std::max(pl.C, pl.P), pl.C * pl.C)));
+    s.scan_tmp = c.take<int>(scan_tmp_ints(std::max(pl.C, pl.P)));
     s.s_cam = c.take<double>((size_t)pl.C * 9);
     s.s_pt = c.take<double>((size_t)pl.P * 3);
     s.Vraw = c.take<double>((size_t)pl.P * 6);
@@ -131,8 +129,7 @@ size_t carve(char* base, const Plan& pl, bool host_io, long long nnz, int nrows,
     s.Ws = c.take<double>((size_t)pl.nobs * 27);
     s.Ys = c.take<double>((size_t)pl.nobs * 27);
     s.cam_part = c.take<double>(45 * camera_tile_slots(pl.C, pl.nobs));
-    s.blk_cnt = c.take<int>((size_t)pl.C * pl.C);
-    s.blk_ptr = c.take<int>((size_t)pl.C * pl.C + 1);
+    s.Ucam = c.take<double>(81 * (size_t)pl.C);
     s.err = c.take<int>(4);
     b.amax = c.take<unsigned long long>(4);
     b.te = c.take<TeState>(1);
@@ -213,29 +210,6 @@ bool is_svd(const unc_options* o) {
     return o->algorithm == UNC_SVD_QR_ITERATION || o->algorithm == UNC_SVD_DEVIDE_AND_CONQUER;
 }
 
-size_t schur_pair_bytes(int C, long long npairs) {
-    const size_t long_cap = (size_t)npairs / 1025 + 1;
-    const size_t nz_ints = schur_list_ints(C, (long)npairs);
-    return (size_t)npairs * 8 + (long_cap + 1 + nz_ints) * sizeof(int) + 64;
-}
-
-long long schur_pairs_bound(const unc_options* o, int num_rows, long long nnz, const int* cols) {
-    const int C = o->num_cams, P = o->num_points, nobs = num_rows / 2;
-    const long long cam_off = 9LL * C;
-    std::vector<int> m(P > 0 ? P : 1, 0);
-    for (int ob = 0; ob < nobs; ++ob) {
-        const long long k = 24LL * ob + 9;  // the point column the device reads (k_validate_obs)
-        if (k >= nnz) break;
-        const long long c = cols[k];
-        if (c < cam_off) continue;
-        const long long pt = (c - cam_off) / 3;
-        if (pt < P) ++m[pt];
-    }
-    long long pairs = 0;
-    for (int v : m) pairs += (long long)v * (v - 1);
-    return pairs;
-}
-
 double auto_lambda(int N) { return pow(10, -1.2653 * log10((double)N) - 2.9415); }
 
 int32_t factorial_i32(int n) {
@@ -256,8 +230,7 @@ Plan make_plan(const unc_options* o, int num_rows) {
 }
 
 int sparse_stage(const unc_options* o, const Plan& pl, long long nnz, const int* rows, const int* cols,
-                 const double* vals, Buffers& b, int fx[3], cudaEvent_t* ev, cudaStream_t sm, void** pair_buf,
-                 size_t* pair_bytes, long long pairs_cap) {
+                 const double* vals, Buffers& b, int fx[3], cudaEvent_t* ev, cudaStream_t sm) {
     SceneDev& s = b.s;
     s.nnz = (long)nnz;
     s.num_cams = pl.C;
@@ -285,37 +258,16 @@ int sparse_stage(const unc_options* o, const Plan& pl, long long nnz, const int*
     if (int r = mark(1)) return r;
     launch_build_index(s, sm);
     if (int r = mark(2)) return r;
-    // zero the dense buffers once (padding rows must stay finite for the GEMM loads)
-    CK(cudaMemsetAsync(b.Z, 0, (size_t)((char*)(b.tmp + (size_t)ld * N) - (char*)b.Z), sm));
-    launch_camera_blocks(s, b.Z, ld, sm);
+    // zero the dense work buffers once (padding rows must stay finite for the GEMM loads)
+    CK(cudaMemsetAsync(b.iZ, 0, (size_t)((char*)(b.tmp + (size_t)ld * N) - (char*)b.iZ), sm));
+    launch_camera_blocks(s, sm);
     launch_point_blocks(s, sm);
     if (int r = mark(3)) return r;
     launch_obs_blocks(s, sm);
-    launch_schur_count(s, sm);
-    long long npairs = pairs_cap;
-    if (pairs_cap < 0) {
-        int dev_pairs = 0;
-        CK(cudaMemcpyAsync(&dev_pairs, s.blk_ptr + (size_t)pl.C * pl.C, sizeof(int), cudaMemcpyDeviceToHost, sm));
-        if (int r = mark(4)) return r;
-        CK(cudaStreamSynchronize(sm));
-        if (dev_pairs < 0) return fail(UNC_ERR_TOO_LARGE, "more than 2^31 co-visible observation pairs");
-        npairs = dev_pairs;
-        const size_t need = schur_pair_bytes(pl.C, npairs);
-        // headroom for the next scene
-        if (int r = grow_buffer(pair_buf, pair_bytes, need, need + need / 4, sm)) return r;
-    } else {
-        if (int r = mark(4)) return r;
-        if (*pair_bytes < schur_pair_bytes(pl.C, npairs)) return fail(UNC_ERR_INVALID_ARG, "pair list too small");
-    }
-    const size_t long_cap = (size_t)npairs / 1025 + 1;
-    s.pairs = reinterpret_cast<unsigned long long*>(*pair_buf);
-    s.pair_cap = (long)npairs;
-    s.long_list = reinterpret_cast<int*>(s.pairs + npairs + 1);
-    s.long_cap = (int)long_cap;
-    s.nz_list = s.long_list + long_cap + 1;
-    launch_camera_self(s, b.Z, ld, sm);
-    launch_schur(s, b.Z, ld, sm);
-    launch_mirror_upper(b.Z, N, ld, sm);
+    if (int r = mark(4)) return r;
+    CK(cudaMemsetAsync(b.Z, 0, sizeof(double) * (size_t)ld * N, sm));
+    if (launch_schur_columns(s, b.Z, ld, sm) != UNC_OK)
+        return fail(UNC_ERR_TOO_LARGE, "more cameras than the Schur stage supports");
     if (int r = mark(5)) return r;
     return UNC_OK;
 }
@@ -407,7 +359,7 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     int fx[3];
     const int N = pl.N, ld = pl.ld;
     cudaEvent_t* ev = ctx->ev;
-    if (int r = sparse_stage(o, pl, nnz, rows, cols, vals, b, fx, ev, sm, &ctx->tup, &ctx->tup_bytes, -1)) return r;
+    if (int r = sparse_stage(o, pl, nnz, rows, cols, vals, b, fx, ev, sm)) return r;
 
     PinvInfo pinfo{};
     if (pl.svd_schur) {
@@ -462,6 +414,7 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     constexpr int kX = 0, kA = 1, k4 = 2, k8 = 3, k12 = 4, k16 = 5;
     const int nbuf = powers ? 6 : 2;
     MixedOperand opa[6], opb[6];  // each buffer as the A (128-row boxes) and as the B operand
+    MixedOperand opa_k[6][6], opb_k[6][6];  // [buffer][k]: its first k slices
     size_t mp_need = 0;
     if (mixed) {  // host-side preparation: buffers and tensor maps
         const size_t sb = (mixed_slice_bytes(N, slices) + 255) & ~size_t(255);
@@ -474,6 +427,18 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
             int* ex = reinterpret_cast<int*>(w + nbuf * sb + q * eb);
             if (!mixed_plan(opa[q], buf, ex, N, slices, false) || !mixed_plan(opb[q], buf, ex, N, slices, true))
                 return fail(UNC_ERR_CUDA, "tensor-map encoding failed");
+        }
+        // the same buffers with fewer slices (power_product_slices)
+        for (int q = 0; q < nbuf; ++q)
+            for (int k = 2; k < slices; ++k) {
+                bool ok_a = false, ok_b = false;
+                opa_k[q][k] = mixed_fewer_slices(opa[q], k, false, &ok_a);
+                opb_k[q][k] = mixed_fewer_slices(opb[q], k, true, &ok_b);
+                if (!ok_a || !ok_b) return fail(UNC_ERR_CUDA, "tensor-map encoding failed");
+            }
+        for (int q = 0; q < nbuf; ++q) {
+            opa_k[q][slices] = opa[q];
+            opb_k[q][slices] = opb[q];
         }
     }
     const double* X = b.Z;
@@ -505,13 +470,15 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         return prof_mark();
     };
     // blocked powers: out (+)= A B, A and B powers of X (symmetric, commuting)
-    // given as FP64 matrices and, in mixed mode, as slice buffers ia / ib
-    auto power_product = [&](const double* A, int ia, const double* B, int ib, double* out, bool acc,
+    // given as FP64 matrices and, in mixed mode, as slice buffers ia / ib;
+    // q: the product's index in power_product_slices
+    auto power_product = [&](int q, const double* A, int ia, const double* B, int ib, double* out, bool acc,
                              const int* skip) -> int {
         if (int r = prof_mark()) return r;
-        if (mixed)
-            mixed_gemm(opa[ia], opb[ib], out, ld, nullptr, true, s.err, sm, skip, true, acc);
-        else
+        if (mixed) {
+            const int k = power_product_slices(q, slices);
+            mixed_gemm(opa_k[ia][k], opb_k[ib][k], out, ld, nullptr, true, s.err, sm, skip, true, acc);
+        } else
             gemm_f64_mode(N, N, N, 1.0, A, ld, B, ld, acc ? 1.0 : 0.0, out, ld, nullptr, GEMM_LOWER | GEMM_MIRROR,
                           sm, nullptr, 0, skip);
         return prof_mark();
@@ -594,19 +561,19 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         }
         launch_te_init(b.te, sm);
         CK(cudaMemsetAsync(b.dmax, 0, sizeof(unsigned long long) * 24, sm));
-        if (int r = power_product(X, kX, X, kX, b.add, false, nullptr)) return r;  // X^2
+        if (int r = power_product(0, X, kX, X, kX, b.add, false, nullptr)) return r;  // X^2
         slice(b.add, kA, nullptr);
-        if (int r = power_product(b.add, kA, X, kX, b.tmp, false, nullptr)) return r;  // X^3
+        if (int r = power_product(1, b.add, kA, X, kX, b.tmp, false, nullptr)) return r;  // X^3
         slice(b.tmp, kA, nullptr);
-        if (int r = power_product(b.tmp, kA, X, kX, b.p4, false, nullptr)) return r;  // X^4
+        if (int r = power_product(2, b.tmp, kA, X, kX, b.p4, false, nullptr)) return r;  // X^4
         slice(b.p4, k4, nullptr);
-        if (int r = power_product(b.p4, k4, b.p4, k4, b.p8, false, nullptr)) return r;  // X^8
+        if (int r = power_product(3, b.p4, k4, b.p4, k4, b.p8, false, nullptr)) return r;  // X^8
         slice(b.p8, k8, nullptr);
-        if (int r = power_product(b.p8, k8, b.p4, k4, b.p12, false, nullptr)) return r;  // X^12
+        if (int r = power_product(4, b.p8, k8, b.p4, k4, b.p12, false, nullptr)) return r;  // X^12
         slice(b.p12, k12, nullptr);
         launch_power_diag(ps, 2, 16, nullptr, sm);
         launch_power_decide(b.te, b.dmax, kc, 1, 15, sm);
-        if (int r = power_product(b.p8, k8, b.p8, k8, b.p16, false, sk)) return r;  // X^16
+        if (int r = power_product(5, b.p8, k8, b.p8, k8, b.p16, false, sk)) return r;  // X^16
         slice(b.p16, k16, sk);
         launch_power_diag(ps, 17, 20, sk, sm);
         launch_power_decide(b.te, b.dmax, kc, 16, 19, sm);
@@ -616,7 +583,7 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         for (int q = 1; q <= 4; ++q) {
             launch_power_combine(ps, q, b.g, sk + q, sm);
             slice(b.g, kA, sk + q);
-            if (int r = power_product(b.g, kA, Pq[q], iq[q], b.iZ, true, sk + q)) return r;
+            if (int r = power_product(5 + q, b.g, kA, Pq[q], iq[q], b.iZ, true, sk + q)) return r;
         }
         return UNC_OK;
     };
@@ -669,6 +636,7 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         ctx->prof_seconds += ev_s(ctx->pev[2 * q], ctx->pev[2 * q + 1]);
         ctx->prof_launches += 1;
         ctx->prof_flops += (double)N * N * (N + 1);  // symmetric product: lower half of 2 N^3
+        if (mixed) ctx->prof_int8_ops += mixed_issued_ops(N, powers ? power_product_slices((int)q, slices) : slices);
     }
     if (st) {
         st->lambda = lambda;
@@ -693,6 +661,8 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         return fail(UNC_ERR_SINGULAR, "non-positive pivot or non-finite value while inverting Z + lambda*I");
     if (err & ERRBIT_TIMEOUT)
         return fail(UNC_ERR_CUDA, "a bounded device wait ran out (tensor-core pipeline or tile-task inverse)");
+    if (err & ERRBIT_SCHUR_CAP)
+        return fail(UNC_ERR_TOO_LARGE, "an observation shares its point with more observations than the Schur stage holds");
     if (te.bad) return fail(UNC_ERR_SINGULAR, "non-finite Taylor-series power");
     return UNC_OK;
 }
@@ -796,7 +766,14 @@ int unc_context_profile(unc_context* c, long long* launches, double* seconds, do
         c->prof_launches = 0;
         c->prof_seconds = 0;
         c->prof_flops = 0;
+        c->prof_int8_ops = 0;
     }
+    return UNC_OK;
+}
+
+int unc_context_profile_int8(unc_context* c, double* int8_ops) {
+    if (!c || !int8_ops) return fail(UNC_ERR_INVALID_ARG, "ctx or int8_ops is NULL");
+    *int8_ops = c->prof_int8_ops;
     return UNC_OK;
 }
 
@@ -817,9 +794,9 @@ int unc_context_release(unc_context* c) {
     if (!c) return fail(UNC_ERR_INVALID_ARG, "ctx is NULL");
     cudaSetDevice(c->device);
     drop_graphs(c);  // they name the buffers freed below
-    void** bufs[4] = {&c->ws, &c->tup, &c->mp, &c->jac};
-    size_t* sizes[4] = {&c->ws_bytes, &c->tup_bytes, &c->mp_bytes, &c->jac_bytes};
-    for (int i = 0; i < 4; ++i) {
+    void** bufs[3] = {&c->ws, &c->mp, &c->jac};
+    size_t* sizes[3] = {&c->ws_bytes, &c->mp_bytes, &c->jac_bytes};
+    for (int i = 0; i < 3; ++i) {
         if (*bufs[i]) cudaFreeAsync(*bufs[i], c->stream);
         *bufs[i] = nullptr;
         *sizes[i] = 0;
@@ -848,7 +825,7 @@ int unc_context_set_priority(unc_context* c, int high) {
 
 long long unc_context_device_bytes(const unc_context* c) {
     if (!c) return -1;
-    return (long long)(c->ws_bytes + c->tup_bytes + c->mp_bytes + c->jac_bytes);
+    return (long long)(c->ws_bytes + c->mp_bytes + c->jac_bytes);
 }
 
 long long unc_request_bytes(const unc_options* o, int num_rows, int num_cols, const int* rows, const int* cols) {
@@ -860,22 +837,6 @@ long long unc_request_bytes(const unc_options* o, int num_rows, int num_cols, co
     Plan pl = make_plan(o, num_rows);
     Buffers b;
     long long bytes = (long long)carve(nullptr, pl, true, nnz, num_rows, b);
-    // Schur pair list: observation pairs that share a point (counted per point
-    // from the first point column of each observation row), with headroom
-    std::vector<int> per_pt(pl.P > 0 ? pl.P : 1, 0);
-    const int cam_cols = 9 * pl.C;
-    for (int ob = 0; ob < nobs; ++ob) {
-        const int r0 = rows[2 * ob], r1 = rows[2 * ob + 1];
-        for (int k = r0; k < r1; ++k)
-            if (cols[k] >= cam_cols) {
-                const int p = (cols[k] - cam_cols) / 3;
-                if (p >= 0 && p < pl.P) ++per_pt[p];
-                break;
-            }
-    }
-    long long pairs = 0;
-    for (int c : per_pt) pairs += (long long)c * (c - 1) / 2;
-    bytes += (pairs * 8 + pairs / 1025 * 4 + 64) * 5 / 4;
     if (o->precision != UNC_PRECISION_FP64) {  // slice buffers: 6 (blocked powers) or 2 (sequential)
         const int slices = o->precision == UNC_PRECISION_MIXED4 ? 4 : (o->precision == UNC_PRECISION_MIXED3 ? 3 : 5);
         const long long nbuf = o->taylor_eval == UNC_TAYLOR_SEQUENTIAL ? 2 : 6;

@@ -429,11 +429,12 @@ __global__ void __launch_bounds__(kObsTile) k_camera_gram_tiles(int num_cams, co
 }
 
 // One warp per camera: U = sum of the camera's tile partials, column norms
-// s = sqrt(diag U), scaled block U/(s s) written into the diagonal block of Z
-// (both triangles). J <- J diag(1/s) skips s == 0 (ScaledSparseMatrix.cpp:352-356).
+// s = sqrt(diag U), scaled block U/(s s) written as a full 9 x 9 block
+// (column-major, 81 per camera). J <- J diag(1/s) skips s == 0
+// (ScaledSparseMatrix.cpp:352-356).
 __global__ void __launch_bounds__(128) k_camera_gram_reduce(int num_cams, const int* __restrict__ cam_ptr,
                                                             const double* __restrict__ part,
-                                                            double* __restrict__ s_cam, double* Z, long ldz) {
+                                                            double* __restrict__ s_cam, double* __restrict__ U) {
     __shared__ double sh[4][45];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cam = blockIdx.x * 4 + w;
@@ -456,20 +457,19 @@ __global__ void __launch_bounds__(128) k_camera_gram_reduce(int num_cams, const 
         double v = u[el];
         if (sj != 0) v *= 1.0 / sj;
         if (sk != 0) v *= 1.0 / sk;
-        const long r = 9L * cam + j, c = 9L * cam + k;
-        Z[r + c * ldz] = v;
-        Z[c + r * ldz] = v;
+        U[81L * cam + j + 9 * k] = v;
+        U[81L * cam + k + 9 * j] = v;
     }
 }
 
 size_t camera_tile_part_doubles(int num_cams, int num_obs) { return 45 * camera_tile_slots(num_cams, num_obs); }
 
-void launch_camera_blocks(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
+void launch_camera_blocks(const SceneDev& s, cudaStream_t st) {
     if (s.num_cams == 0) return;
     const unsigned slots = (unsigned)camera_tile_slots(s.num_cams, s.num_obs);
     k_camera_gram_tiles<<<slots, kObsTile, 0, st>>>(s.num_cams, s.J, s.cam_ptr, s.cam_obs, s.cam_part);
-    k_camera_gram_reduce<<<(s.num_cams + 3) / 4, 128, 0, st>>>(s.num_cams, s.cam_ptr, s.cam_part, s.s_cam, Z,
-                                                                ldz);
+    k_camera_gram_reduce<<<(s.num_cams + 3) / 4, 128, 0, st>>>(s.num_cams, s.cam_ptr, s.cam_part, s.s_cam,
+                                                                s.Ucam);
     count_launch(2);
 }
 
@@ -524,18 +524,16 @@ void launch_point_blocks(const SceneDev& s, cudaStream_t st) {
 }
 
 // W_o = Jc^T Jp scaled by the column norms and Y_o = W_o iV_p (the
-// camera-point block of Y = W * iV, compute.cpp:108), one camera tile per CTA,
-// fused with the tile's share of the Schur self terms sum_o Y_o W_o^T of the
-// camera's diagonal block. One thread per observation computes its two 9 x 3
-// blocks into shared memory (odd record stride 27: conflict-free); warps then
-// write whole 216-byte records, and thread (el, g) sums upper-triangle element
-// el of Y_o W_o^T over the tile's observations g, g + 5, ...
+// camera-point block of Y = W * iV, compute.cpp:108), one camera tile per CTA.
+// One thread per observation computes its two 9 x 3 blocks into shared memory
+// (odd record stride 27: conflict-free); warps then write whole 216-byte
+// records.
 constexpr size_t kObsTileSmem = 2ul * kObsTile * 27 * sizeof(double);  // 110,592 bytes
 
 __global__ void __launch_bounds__(kObsTile) k_camera_obs_tiles(
     int num_cams, const double* __restrict__ J, const int* __restrict__ cam_ptr, const int* __restrict__ cam_obs,
     const int* __restrict__ obs_pt, const double* __restrict__ s_cam, const double* __restrict__ s_pt,
-    const double* __restrict__ iVs, double* __restrict__ Ws, double* __restrict__ Ys, double* __restrict__ part) {
+    const double* __restrict__ iVs, double* __restrict__ Ws, double* __restrict__ Ys) {
     extern __shared__ double smem[];
     double* sw = smem;                   // [kObsTile][27] W_o
     double* sy = smem + kObsTile * 27;   // [kObsTile][27] Y_o
@@ -588,26 +586,6 @@ __global__ void __launch_bounds__(kObsTile) k_camera_obs_tiles(
             Ws[27 * o + lane] = sw[27 * i + lane];
             Ys[27 * o + lane] = sy[27 * i + lane];
         }
-    double acc = 0.0;
-    const int el = t % 45, g = t / 45;
-    if (t < 45 * kTileGroups) {
-        int j, k;
-        ut9_inv(el, j, k);
-        for (int i = g; i < n; i += kTileGroups) {
-            const double* y = sy + 27 * i + 3 * j;
-            const double* w = sw + 27 * i + 3 * k;
-            acc += y[0] * w[0] + y[1] * w[1] + y[2] * w[2];
-        }
-    }
-    __syncthreads();  // the tile is consumed: its first 225 doubles take the group sums
-    if (t < 45 * kTileGroups) smem[45 * g + el] = acc;
-    __syncthreads();
-    if (t < 45) {
-        double v = smem[t];
-#pragma unroll
-        for (int q = 1; q < kTileGroups; ++q) v += smem[45 * q + t];
-        part[45L * blockIdx.x + t] = v;
-    }
 }
 
 void launch_obs_blocks(const SceneDev& s, cudaStream_t st) {
@@ -615,330 +593,19 @@ void launch_obs_blocks(const SceneDev& s, cudaStream_t st) {
     prepare_assembly_kernels();
     const unsigned slots = (unsigned)camera_tile_slots(s.num_cams, s.num_obs);
     k_camera_obs_tiles<<<slots, kObsTile, kObsTileSmem, st>>>(s.num_cams, s.J, s.cam_ptr, s.cam_obs, s.obs_pt,
-                                                              s.s_cam, s.s_pt, s.iVs, s.Ws, s.Ys, s.cam_part);
+                                                              s.s_cam, s.s_pt, s.iVs, s.Ws, s.Ys);
     count_launch();
-}
-
-// Self terms of the Schur complement, Z(c, c) -= sum over observations o of
-// camera c of Y_o W_o^T (= W_o iV_p W_o^T, symmetric): one warp per camera adds
-// the camera's tile partials in slot order. Only the upper triangle of the
-// diagonal block is updated (it is mirrored later).
-__global__ void __launch_bounds__(128) k_camera_self_reduce(int num_cams, const int* __restrict__ cam_ptr,
-                                                            const double* __restrict__ part, double* Z,
-                                                            long ldz) {
-    const int cam = blockIdx.x * 4 + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (cam >= num_cams) return;
-    const int k0 = tile_base(cam_ptr, cam), k1 = tile_base(cam_ptr, cam + 1);
-    for (int el = lane; el < 45; el += 32) {
-        double v = 0.0;
-        for (int k = k0; k < k1; ++k) v += part[45L * k + el];
-        int j, k;
-        ut9_inv(el, j, k);
-        Z[(9L * cam + j) + (9L * cam + k) * ldz] -= v;
-    }
-}
-
-void launch_camera_self(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
-    if (s.num_cams == 0) return;
-    k_camera_self_reduce<<<(s.num_cams + 3) / 4, 128, 0, st>>>(s.num_cams, s.cam_ptr, s.cam_part, Z, ldz);
-    count_launch();
-}
-
-// Deterministic Schur scatter: Z(c, c') -= sum over points p seen by both
-// cameras of Y_o W_o'^T, for c <= c' (upper block triangle).
-//
-//  1. k_pair_enum (count / scatter): one warp per point lists its ordered
-//     observation pairs (o, o') with camera(o) <= camera(o'); pairs are
-//     counted per camera-pair block and scattered into a block-grouped list.
-//  2. k_list_blocks collects the non-empty blocks (any order: it only
-//     distributes work).
-//  3. the pairs of each block are sorted by (o, o') (warp rank sort, or a
-//     block bitonic sort for long lists), which fixes the summation order.
-//  4. k_schur_blocks: one warp per non-empty block reduces its pairs in
-//     registers and writes the block of Z once. No floating-point atomics:
-//     results are bitwise repeatable.
-template <bool kScatter>
-__global__ void __launch_bounds__(128) k_pair_enum(int num_points, int num_cams, const int* __restrict__ pt_ptr,
-                                                   const int* __restrict__ pt_obs, const int* __restrict__ obs_cam,
-                                                   int* cnt_or_cursor, unsigned long long* __restrict__ pairs,
-                                                   long cap) {
-    const int p = blockIdx.x * 4 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (p >= num_points) return;
-    const int b = pt_ptr[p], m = pt_ptr[p + 1] - b;
-    const long mm = (long)m * m;
-    for (long idx = lane; idx < mm; idx += 32) {
-        const int i = (int)(idx / m), k = (int)(idx - (long)i * m);
-        if (i == k) continue;  // self pairs are reduced per camera (k_camera_obs_tiles)
-        const int oa = pt_obs[b + i], ob = pt_obs[b + k];
-        const int ca = obs_cam[oa], cb = obs_cam[ob];
-        if (ca > cb) continue;
-        const long key = (long)ca * num_cams + cb;
-        if (kScatter) {
-            const int pos = atomicAdd(cnt_or_cursor + key, 1);
-            if (pos < cap) pairs[pos] = ((unsigned long long)(unsigned)oa << 32) | (unsigned)ob;
-        } else {
-            atomicAdd(cnt_or_cursor + key, 1);
-        }
-    }
-}
-
-// nz[0] = number of non-empty blocks, nz[1] = work cursor of k_schur_blocks,
-// nz[2 ...] = their ids (warp-aggregated appends).
-__global__ void k_list_blocks(long nblk, const int* __restrict__ blk_ptr, int* nz) {
-    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = k < nblk && blk_ptr[k + 1] > blk_ptr[k];
-    const unsigned mask = __ballot_sync(0xffffffffu, live);
-    if (!mask) return;
-    const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(nz, __popc(mask));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (live) nz[2 + base + __popc(mask & ((1u << lane) - 1))] = (int)k;
-}
-
-constexpr int kPairWarpCap = 1024;
-constexpr int kSortWarps = 4;
-// One warp per listed block (grid-stride over the list), rank sort through
-// shared memory. long_list[0] counts the blocks with more than kPairWarpCap
-// pairs; their ids follow (capacity long_cap) and are sorted by
-// k_sort_pairs_block.
-__global__ void __launch_bounds__(32 * kSortWarps) k_sort_pairs_warp(const int* __restrict__ nz,
-                                                                    const int* __restrict__ ptr,
-                                                                    unsigned long long* data, int* long_list,
-                                                                    int long_cap) {
-    __shared__ unsigned long long sh[kSortWarps][kPairWarpCap];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nlist = nz[0];
-    unsigned long long* s = sh[w];
-    for (int t = blockIdx.x * kSortWarps + w; t < nlist; t += gridDim.x * kSortWarps) {
-        const int seg = nz[2 + t];
-        const int b = ptr[seg], n = ptr[seg + 1] - b;
-        if (n <= 1) continue;
-        if (n > kPairWarpCap) {
-            if (lane == 0) {
-                const int i = atomicAdd(long_list, 1);
-                if (i < long_cap) long_list[1 + i] = seg;
-            }
-            continue;
-        }
-        for (int i = lane; i < n; i += 32) s[i] = data[b + i];
-        __syncwarp();
-        for (int i = lane; i < n; i += 32) {
-            const unsigned long long v = s[i];
-            int r = 0;
-            for (int j = 0; j < n; ++j) r += s[j] < v;
-            data[b + r] = v;
-        }
-        __syncwarp();
-    }
-}
-
-constexpr int kPairBlockCap = 8192;
-__global__ void k_sort_pairs_block(const int* __restrict__ ptr, unsigned long long* data,
-                                   const int* __restrict__ long_list, int long_cap, int* err) {
-    extern __shared__ unsigned long long sb[];
-    const int nlong = min(long_list[0], long_cap);
-    if (blockIdx.x == 0 && threadIdx.x == 0 && long_list[0] > long_cap) atomicOr(err, ERRBIT_SORT_CAP);
-    for (int t = blockIdx.x; t < nlong; t += gridDim.x) {
-        const int seg = long_list[1 + t];
-        const int b = ptr[seg], n = ptr[seg + 1] - b;
-        if (n > kPairBlockCap) {
-            if (threadIdx.x == 0) atomicOr(err, ERRBIT_SORT_CAP);
-            continue;
-        }
-        int m = 1;
-        while (m < n) m <<= 1;
-        for (int i = threadIdx.x; i < m; i += blockDim.x) sb[i] = i < n ? data[b + i] : ~0ull;
-        __syncthreads();
-        for (int k = 2; k <= m; k <<= 1)
-            for (int j = k >> 1; j > 0; j >>= 1) {
-                for (int i = threadIdx.x; i < m; i += blockDim.x) {
-                    int l = i ^ j;
-                    if (l > i) {
-                        bool up = (i & k) == 0;
-                        unsigned long long x = sb[i], y = sb[l];
-                        if ((x > y) == up) {
-                            sb[i] = y;
-                            sb[l] = x;
-                        }
-                    }
-                }
-                __syncthreads();
-            }
-        for (int i = threadIdx.x; i < n; i += blockDim.x) data[b + i] = sb[i];
-        __syncthreads();
-    }
-}
-
-// One warp per non-empty camera-pair block, persistent: warps take list
-// entries from the cursor nz[1] (the assignment of blocks to warps varies
-// from run to run; each block's arithmetic does not). A block's pairs are
-// walked in their sorted order, 8 at a time: lanes 0..26 load Y_o and W_o' as
-// two coalesced 216-byte records and element (r, q) = sum_m Y_o(r, m) W_o'(q, m)
-// takes its operands by shuffle. Lane l owns elements l, l + 32, l + 64 of the
-// 9 x 9 block (column-major: r = el % 9, q = el / 9); every element is summed
-// in pair order, so the result is bitwise repeatable.
-constexpr int kSchurWarps = 8;
-__global__ void __launch_bounds__(32 * kSchurWarps) k_schur_blocks(int num_cams, const int* __restrict__ blk_ptr,
-                                                                   int* nz,
-                                                                   const unsigned long long* __restrict__ pairs,
-                                                                   const double* __restrict__ Ws,
-                                                                   const double* __restrict__ Ys, double* Z,
-                                                                   long ldz) {
-    const int lane = threadIdx.x & 31;
-    const int nlist = *(volatile int*)nz;
-    int rr[3], qq[3];
-#pragma unroll
-    for (int u = 0; u < 3; ++u) {
-        const int el = min(lane + 32 * u, 80);
-        rr[u] = 3 * (el % 9);
-        qq[u] = 3 * (el / 9);
-    }
-    const bool has2 = lane + 64 < 81;
-    while (true) {
-        int t = 0;
-        if (lane == 0) t = atomicAdd(nz + 1, 1);
-        t = __shfl_sync(0xffffffffu, t, 0);
-        if (t >= nlist) break;
-        const int blk = nz[2 + t];
-        const int b = blk_ptr[blk], e = blk_ptr[blk + 1];
-        double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-        for (int i0 = b; i0 < e; i0 += 32) {
-            const int cnt = min(32, e - i0);
-            const unsigned long long mine = lane < cnt ? __ldg(pairs + i0 + lane) : 0ull;
-            for (int j0 = 0; j0 < cnt; j0 += 8) {
-                double yv[8], wv[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const unsigned long long pr = __shfl_sync(0xffffffffu, mine, j0 + u);
-                    const bool ok = j0 + u < cnt && lane < 27;
-                    yv[u] = ok ? __ldg(Ys + 27L * (long)(pr >> 32) + lane) : 0.0;
-                    wv[u] = ok ? __ldg(Ws + 27L * (long)(pr & 0xffffffffu) + lane) : 0.0;
-                }
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    double d0 = 0.0, d1 = 0.0, d2 = 0.0;
-#pragma unroll
-                    for (int m = 0; m < 3; ++m) {
-                        d0 += __shfl_sync(0xffffffffu, yv[u], rr[0] + m) * __shfl_sync(0xffffffffu, wv[u], qq[0] + m);
-                        d1 += __shfl_sync(0xffffffffu, yv[u], rr[1] + m) * __shfl_sync(0xffffffffu, wv[u], qq[1] + m);
-                        d2 += __shfl_sync(0xffffffffu, yv[u], rr[2] + m) * __shfl_sync(0xffffffffu, wv[u], qq[2] + m);
-                    }
-                    acc0 += d0;
-                    acc1 += d1;
-                    acc2 += d2;
-                }
-            }
-        }
-        const int ca = blk / num_cams, cb = blk - ca * num_cams;
-#pragma unroll
-        for (int u = 0; u < 3; ++u) {
-            if (u == 2 && !has2) break;
-            const double v = u == 0 ? acc0 : (u == 1 ? acc1 : acc2);
-            const int r = rr[u] / 3, q = qq[u] / 3;
-            double* z = Z + (9L * ca + r) + (9L * cb + q) * ldz;
-            if (ca == cb) {
-                if (r <= q) *z -= v;  // the diagonal block holds U and the self terms already
-            } else {
-                *z = -v;
-            }
-        }
-    }
-}
-
-size_t schur_blocks(int num_cams) { return (size_t)num_cams * num_cams; }
-
-void launch_schur_count(const SceneDev& s, cudaStream_t st) {
-    const long nblk = (long)s.num_cams * s.num_cams;
-    cudaMemsetAsync(s.blk_cnt, 0, sizeof(int) * (size_t)nblk, st);
-    if (s.num_points > 0) {
-        k_pair_enum<false><<<(s.num_points + 3) / 4, 128, 0, st>>>(s.num_points, s.num_cams, s.pt_ptr, s.pt_obs,
-                                                                   s.obs_cam, s.blk_cnt, nullptr, 0);
-        count_launch();
-    }
-    exclusive_scan(s.blk_cnt, s.blk_ptr, (int)nblk, s.scan_tmp, st);
 }
 
 void prepare_assembly_kernels() {
+    prepare_schur_columns();
     static std::atomic<unsigned long long> attr{0};
     once_per_device(attr, [] {
-        return cudaFuncSetAttribute(k_sort_pairs_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(kPairBlockCap * sizeof(unsigned long long))) == cudaSuccess &&
-               cudaFuncSetAttribute(k_camera_obs_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        return cudaFuncSetAttribute(k_camera_obs_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kObsTileSmem) == cudaSuccess &&
                cudaFuncSetAttribute(k_camera_obs_tiles, cudaFuncAttributePreferredSharedMemoryCarveout,
                                     (int)cudaSharedmemCarveoutMaxShared) == cudaSuccess;
     });
-}
-
-// ints of the non-empty block list for a scene with npairs pairs
-size_t schur_list_ints(int num_cams, long npairs) {
-    const long upper = (long)num_cams * (num_cams + 1) / 2;
-    return (size_t)std::min(upper, npairs) + 2;
-}
-
-// A pair list sized from a host-side count (a captured launch sequence cannot
-// read the device count back) that the device count exceeds: the error bit is
-// set and every block is emptied, so that nothing reads or writes past the list.
-__global__ void k_pair_capacity(int* blk_ptr, long nblk, long cap, int* err) {
-    __shared__ int over;
-    if (threadIdx.x == 0) {
-        over = blk_ptr[nblk] > cap;
-        if (over) atomicOr(err, ERRBIT_PAIR_CAP);
-    }
-    __syncthreads();  // every thread has the decision before any entry is cleared
-    if (!over) return;
-    for (long k = threadIdx.x; k <= nblk; k += blockDim.x) blk_ptr[k] = 0;
-}
-
-void launch_schur(const SceneDev& s, double* Z, int ldz, cudaStream_t st) {
-    const long nblk = (long)s.num_cams * s.num_cams;
-    if (nblk == 0) return;
-    k_pair_capacity<<<1, 256, 0, st>>>(s.blk_ptr, nblk, s.pair_cap, s.err);
-    count_launch();
-    cudaMemcpyAsync(s.blk_cnt, s.blk_ptr, sizeof(int) * (size_t)nblk, cudaMemcpyDeviceToDevice, st);
-    if (s.num_points > 0) {
-        k_pair_enum<true><<<(s.num_points + 3) / 4, 128, 0, st>>>(s.num_points, s.num_cams, s.pt_ptr, s.pt_obs,
-                                                                  s.obs_cam, s.blk_cnt, s.pairs, s.pair_cap);
-        count_launch();
-    }
-    cudaMemsetAsync(s.long_list, 0, sizeof(int), st);
-    cudaMemsetAsync(s.nz_list, 0, 2 * sizeof(int), st);
-    k_list_blocks<<<(unsigned)((nblk + 255) / 256), 256, 0, st>>>(nblk, s.blk_ptr, s.nz_list);
-    const unsigned sms = (unsigned)device_sms();
-    k_sort_pairs_warp<<<sms * 8, 32 * kSortWarps, 0, st>>>(s.nz_list, s.blk_ptr, s.pairs, s.long_list, s.long_cap);
-    prepare_assembly_kernels();
-    k_sort_pairs_block<<<sms, 1024, kPairBlockCap * sizeof(unsigned long long), st>>>(
-        s.blk_ptr, s.pairs, s.long_list, s.long_cap, s.err);
-    k_schur_blocks<<<sms * 8, 32 * kSchurWarps, 0, st>>>(s.num_cams, s.blk_ptr, s.nz_list, s.pairs, s.Ws, s.Ys, Z,
-                                                          ldz);
-    count_launch(4);
-}
-
-// Copy the strict upper triangle onto the lower one (32x32 tiles via smem).
-__global__ void k_mirror_upper(double* Z, int n, long ld) {
-    __shared__ double t[32][33];
-    int bi = blockIdx.y, bj = blockIdx.x;  // tile row, tile col
-    if (bi > bj) return;
-    int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
-    for (int r = ty; r < 32; r += 8) {
-        int i = bi * 32 + r, j = bj * 32 + tx;
-        t[r][tx] = (i < n && j < n) ? Z[i + (long)j * ld] : 0.0;
-    }
-    __syncthreads();
-    // write element (j, i) = upper (i, j) for i < j
-    for (int r = ty; r < 32; r += 8) {
-        int j = bj * 32 + r, i = bi * 32 + tx;  // target row j, col i
-        if (i < n && j < n && i < j) Z[j + (long)i * ld] = t[tx][r];
-    }
-}
-
-void launch_mirror_upper(double* Z, int n, int ldz, cudaStream_t st) {
-    if (n == 0) return;
-    dim3 g((n + 31) / 32, (n + 31) / 32);
-    k_mirror_upper<<<g, dim3(32, 8), 0, st>>>(Z, n, ldz);
-    count_launch();
 }
 
 // Unscaled blocks for the J^T J export: U (9x9 per camera, column-major

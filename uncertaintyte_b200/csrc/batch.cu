@@ -65,12 +65,9 @@ struct Scene {
     unc_options opt;
     Plan pl;
     long long nnz;
-    long long pairs_cap;
     int fx[3];
     double lambda;
     Buffers b;
-    void* pair_buf;
-    size_t pair_bytes;
     int* in_rows;
     int* in_cols;
     double* in_vals;
@@ -162,7 +159,9 @@ int lower_tile_count(int n, int nt) {
     return (int)t.size();
 }
 
-constexpr int kMaps = 9;        // per scene: X (A, B), A operand (A), X^4 (A, B), X^8 (A, B), X^12 (B), X^16 (B)
+// per scene: X (A, B), A operand (A), X^4 (A, B), X^8 (A, B), X^12 (B), X^16 (B), and X^4, X^8, X^12, X^16
+// as B operands of 128-column tiles (the products with fewer slices than the group's)
+constexpr int kMaps = 13;
 constexpr int kSliceSets = 11;  // X, X^2, X^3, X^4, X^8, X^12, X^16, G_1..G_4
 constexpr int kGemmSets = 10;   // X^2, X^3, X^4, X^8, X^12, X^16, X^4 G_1 .. X^16 G_4
 
@@ -232,8 +231,6 @@ void lay_out(char* base, std::vector<Scene>& sc, int slices, int nt, Layout& L, 
         const size_t need = carve(nullptr, s.pl, false, 0, s.pl.nobs * 2, s.b);
         char* at = c.take<char>(need);
         carve(base ? at : nullptr, s.pl, false, 0, s.pl.nobs * 2, s.b);
-        s.pair_bytes = schur_pair_bytes(s.pl.C, s.pairs_cap);
-        s.pair_buf = c.take<char>(s.pair_bytes);
     }
     c.off = (c.off + 255) & ~size_t(255);
     L.mixed_off = c.off;
@@ -279,6 +276,7 @@ struct GroupRun {
     int slices = 5, nt = 96;
     Layout L;
     size_t ntasks = 0, ntiles = 0;
+    size_t ntiles_nt = 0, ntiles_128 = 0;  // tiles of width nt, then (nt != 128) of width 128
     long nblk_rows = 0, nblk_elems = 0, nblk_cols = 0;
     int total_rows = 0;
     Desc dd{};  // device descriptors
@@ -297,8 +295,7 @@ int launch_group(unc_batch* b, GroupRun& g, cudaEvent_t taylor0, cudaEvent_t tay
         Scene& s = g.sc[i];
         cudaStream_t br = b->branch[i % kBranches];
         int fx[3];
-        if (int r = sparse_stage(&s.opt, s.pl, s.nnz, s.in_rows, s.in_cols, s.in_vals, s.b, fx, nullptr, br,
-                                 &s.pair_buf, &s.pair_bytes, s.pairs_cap))
+        if (int r = sparse_stage(&s.opt, s.pl, s.nnz, s.in_rows, s.in_cols, s.in_vals, s.b, fx, nullptr, br))
             return r;
         const int N = s.pl.N, ld = s.pl.ld;
         if (ld != N)  // padding rows of the extra power buffers must stay finite for the product loads
@@ -322,8 +319,13 @@ int launch_group(unc_batch* b, GroupRun& g, cudaEvent_t taylor0, cudaEvent_t tay
     auto slice = [&](int set) {
         mixed_slice_grouped(g.dd.slice + (size_t)set * n, n, g.dd.row_start, g.total_rows, sm);
     };
-    auto gemm = [&](int set) {
-        mixed_gemm_grouped(g.slices, g.nt, g.dd.gemm + (size_t)set * n, g.dd.tiles, (int)g.ntiles, sm);
+    auto gemm = [&](int set) {  // product `set` with its slices (power_product_slices)
+        const int k = power_product_slices(set, g.slices);
+        if (k == g.slices || g.nt == 128)
+            mixed_gemm_grouped(k, g.nt, g.dd.gemm + (size_t)set * n, g.dd.tiles, (int)g.ntiles_nt, sm);
+        else
+            mixed_gemm_grouped(k, 128, g.dd.gemm + (size_t)set * n, g.dd.tiles + g.ntiles_nt, (int)g.ntiles_128,
+                               sm);
     };
     slice(0);  // X
     launch_te_init_grouped(g.dd.dense, n, sm);
@@ -376,6 +378,10 @@ int prepare_group(unc_batch* b, GroupRun& g, int nt) {
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return ns[a] > ns[c]; });
     std::vector<int4> tiles;
     for (int i : order) mixed_lower_tiles(i, ns[i], nt, tiles);
+    g.ntiles_nt = tiles.size();
+    if (nt != 128)
+        for (int i : order) mixed_lower_tiles(i, ns[i], 128, tiles);
+    g.ntiles_128 = tiles.size() - g.ntiles_nt;
     g.ntiles = tiles.size();
     lay_out(nullptr, g.sc, g.slices, nt, g.L, g.ntasks, g.ntiles);
     cudaStream_t sm = b->stream;
@@ -419,13 +425,15 @@ int prepare_group(unc_batch* b, GroupRun& g, int nt) {
         const long ld = s.pl.ld;
         const int nt64 = (N + 63) / 64;
         hdd.mats[i] = SpdTaskMatrix{s.b.Z, s.b.iZ, s.b.add, ld, N, nt64 * (nt64 + 1) / 2, s.b.dag_state, s.b.s.err};
-        // tensor maps: X (A, B), A operand (A), X^4 (A, B), X^8 (A, B), X^12 (B), X^16 (B)
-        const int mbuf[kMaps] = {0, 0, 1, 2, 2, 3, 3, 4, 5};
-        const bool mb[kMaps] = {false, true, false, false, true, false, true, true, true};
+        // tensor maps: X (A, B), A operand (A), X^4 (A, B), X^8 (A, B), X^12 (B), X^16 (B); then
+        // X^4, X^8, X^12, X^16 as B operands with 128-row boxes (same buffers and plane stride)
+        const int mbuf[kMaps] = {0, 0, 1, 2, 2, 3, 3, 4, 5, 2, 3, 4, 5};
+        const bool mb[kMaps] = {false, true, false, false, true, false, true, true, true, true, true, true, true};
         MixedOperand op[kMaps];
         for (int m = 0; m < kMaps; ++m) {
-            if (!mixed_plan_nt(op[m], s.buf[mbuf[m]], s.ex[mbuf[m]], N, g.slices, mb[m], nt))
-                return bfail(UNC_ERR_CUDA, "tensor-map encoding failed");
+            bool ok = mixed_plan_nt(op[m], s.buf[mbuf[m]], s.ex[mbuf[m]], N, g.slices, mb[m], nt);
+            if (ok && m >= 9) op[m] = mixed_fewer_slices(op[m], 2, true, &ok);  // 128-row boxes
+            if (!ok) return bfail(UNC_ERR_CUDA, "tensor-map encoding failed");
             hdd.maps[kMaps * i + m] = op[m].map;
         }
         const int rows = op[0].rows, kp = op[0].kp;
@@ -455,20 +463,25 @@ int prepare_group(unc_batch* b, GroupRun& g, int nt) {
         // products: A map, B map, A / B exponent buffers, output, accumulate, skip
         const CUtensorMap* dm = g.dd.maps + kMaps * i;
         struct GemmDef {
-            int a, b, ea, eb;
+            int a, b, b128, ea, eb;  // b128: the B map with 128-row boxes (-1: always full slices)
             double* C;
             int acc;
             const int* skip;
         };
-        const GemmDef gd[kGemmSets] = {{0, 1, 0, 0, s.b.add, 0, nullptr}, {2, 1, 1, 0, s.b.tmp, 0, nullptr},
-                                       {2, 1, 1, 0, s.b.p4, 0, nullptr},  {3, 4, 2, 2, s.b.p8, 0, nullptr},
-                                       {5, 4, 3, 2, s.b.p12, 0, nullptr}, {5, 6, 3, 3, s.b.p16, 0, sk},
-                                       {2, 4, 1, 2, s.b.iZ, 1, sk + 1},   {2, 6, 1, 3, s.b.iZ, 1, sk + 2},
-                                       {2, 7, 1, 4, s.b.iZ, 1, sk + 3},   {2, 8, 1, 5, s.b.iZ, 1, sk + 4}};
-        for (int q = 0; q < kGemmSets; ++q)
-            hdd.gemm[(size_t)q * n + i] = MixedGemmJob{dm + gd[q].a,   dm + gd[q].b,   N,          kp, rows, rows,
+        const GemmDef gd[kGemmSets] = {
+            {0, 1, -1, 0, 0, s.b.add, 0, nullptr}, {2, 1, -1, 1, 0, s.b.tmp, 0, nullptr},
+            {2, 1, -1, 1, 0, s.b.p4, 0, nullptr},  {3, 4, 9, 2, 2, s.b.p8, 0, nullptr},
+            {5, 4, 9, 3, 2, s.b.p12, 0, nullptr},  {5, 6, 10, 3, 3, s.b.p16, 0, sk},
+            {2, 4, 9, 1, 2, s.b.iZ, 1, sk + 1},    {2, 6, 10, 1, 3, s.b.iZ, 1, sk + 2},
+            {2, 7, 11, 1, 4, s.b.iZ, 1, sk + 3},   {2, 8, 12, 1, 5, s.b.iZ, 1, sk + 4}};
+        for (int q = 0; q < kGemmSets; ++q) {
+            const bool narrow = power_product_slices(q, g.slices) != g.slices && nt != 128;
+            const int bm = narrow ? gd[q].b128 : gd[q].b;
+            if (bm < 0) return bfail(UNC_ERR_UNSUPPORTED, "slice schedule and map table disagree");
+            hdd.gemm[(size_t)q * n + i] = MixedGemmJob{dm + gd[q].a,   dm + bm,        N,          kp, rows, rows,
                                                        s.ex[gd[q].ea], s.ex[gd[q].eb], gd[q].C,    ld, nullptr,
                                                        s.b.s.err,      gd[q].skip,     gd[q].acc};
+        }
         PowerSet ps{};
         ps.M[0] = s.b.Z;
         ps.M[1] = s.b.add;
@@ -508,7 +521,7 @@ std::vector<unsigned long long> shape_key(const unc_batch* b, const GroupRun& g)
         unsigned long long lam;
         memcpy(&lam, &s.lambda, 8);
         k.insert(k.end(), {(unsigned long long)s.pl.C, (unsigned long long)s.pl.P, (unsigned long long)s.pl.nobs,
-                           (unsigned long long)s.nnz, (unsigned long long)s.pairs_cap,
+                           (unsigned long long)s.nnz,
                            (unsigned long long)(unsigned)s.fx[0] << 32 | (unsigned)s.fx[1],
                            (unsigned long long)(unsigned)s.fx[2], lam});
     }
@@ -628,7 +641,8 @@ int run_group(unc_batch* b, GroupRun& g, const int* const* rows, const int* cons
         int rc = UNC_OK;
         if (err & ERRBIT_LAYOUT) rc = UNC_ERR_LAYOUT;
         else if (err & (ERRBIT_SINGULAR | ERRBIT_NONFINITE)) rc = UNC_ERR_SINGULAR;
-        else if (err & (ERRBIT_TIMEOUT | ERRBIT_PAIR_CAP)) rc = UNC_ERR_CUDA;
+        else if (err & ERRBIT_TIMEOUT) rc = UNC_ERR_CUDA;
+        else if (err & ERRBIT_SCHUR_CAP) rc = UNC_ERR_TOO_LARGE;
         else if (te.bad) rc = UNC_ERR_SINGULAR;
         status[s.idx] = rc;
         if (stats) {
@@ -743,7 +757,6 @@ int unc_batch_compute(unc_batch* b, int num_scenes, const unc_options* opts, con
         s.opt = *o;
         s.pl = make_plan(o, num_rows[i]);
         s.nnz = nnz;
-        s.pairs_cap = schur_pairs_bound(o, num_rows[i], nnz, cols[i]);
         s.fx[0] = o->pts2fix[0];
         s.fx[1] = o->pts2fix[1];
         s.fx[2] = o->pts2fix[2];

@@ -24,24 +24,27 @@ constexpr int BK = 16, STAGES = 4, GEMM_THREADS = 256;
 constexpr int LDB_S = BK + 4;  // Bs[n][k]: 20 doubles per n row (conflict-free fragment reads)
 
 // Output tile BM x BN computed by 8 warps of WM x WN (FM x FN fragments of
-// the 8 x 8 DMMA result). Shared-memory rows are padded by 8 doubles so the
-// fragment reads of a warp hit distinct banks.
+// the 8 x 8 DMMA result). Shared-memory rows of A (and of the transposed B)
+// are padded by 4 doubles: a fragment read takes rows kk + t (t = 0..3) at 8
+// doubles apart in bank space (row pitch = 8 mod 32 banks), so each half-warp
+// hits 16 distinct bank pairs; cp.async rows stay 16-byte aligned.
 template <int BM_, int BN_, int WM_, int WN_>
 struct GemmCfg {
     static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_;
     static constexpr int WARPS_M = BM / WM;
     static_assert((BM / WM) * (BN / WN) == GEMM_THREADS / 32, "8 warps per CTA");
     static constexpr int FM = WM / 8, FN = WN / 8;
-    static constexpr int LDA_S = BM + 8;   // As[k][m]
-    static constexpr int LDBT_S = BN + 8;  // Bs[k][n] (transposed B)
+    static constexpr int LDA_S = BM + 4;   // As[k][m]
+    static constexpr int LDBT_S = BN + 4;  // Bs[k][n] (transposed B)
+    static_assert((2 * LDA_S) % 32 == 8 && (2 * LDBT_S) % 32 == 8, "conflict-free fragment rows");
     static constexpr int A_STAGE = BK * LDA_S;
     static constexpr int B_STAGE = (BN * LDB_S > BK * LDBT_S) ? BN * LDB_S : BK * LDBT_S;
     static constexpr size_t SMEM = sizeof(double) * (size_t)STAGES * (A_STAGE + B_STAGE);
     static constexpr int A_CHUNKS = BM * BK / 2 / GEMM_THREADS;  // 16-byte copies per thread
     static constexpr int B_CHUNKS = BN * BK / 2 / GEMM_THREADS;
 };
-using CfgBig = GemmCfg<128, 128, 32, 64>;   // 1 CTA per SM (151 KB shared)
-using CfgSmall = GemmCfg<64, 64, 16, 32>;   // small outputs: 4x the CTAs (78 KB shared)
+using CfgBig = GemmCfg<128, 128, 32, 64>;   // 1 CTA per SM (150 KB shared)
+using CfgSmall = GemmCfg<64, 64, 16, 32>;   // small outputs: 4x the CTAs (76 KB shared)
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
     unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));

@@ -20,7 +20,7 @@ enum : int {
     ERRBIT_NONFINITE = 4,   // NaN / Inf produced
     ERRBIT_SORT_CAP = 8,    // a segment was too long to sort (order left nondeterministic)
     ERRBIT_TIMEOUT = 16,    // a bounded device wait ran out (tensor-core pipeline)
-    ERRBIT_PAIR_CAP = 32,   // more Schur observation pairs than the pair list holds (nothing scattered)
+    ERRBIT_SCHUR_CAP = 32,  // an observation has more Schur partners than one chunk holds (Z incomplete)
 };
 
 constexpr int kCamParams = 9;
@@ -100,33 +100,25 @@ struct SceneDev {
     double* Ws;           // 27*num_obs scaled W_o = (J_c^T J_p)/(s s), 9x3 row-major
     double* Ys;           // 27*num_obs Y_o = W_o * iV_p, 9x3 row-major
     double* cam_part;     // 45 * camera_tile_slots(): per-tile partial sums of the camera blocks
-    int* blk_cnt;         // num_cams^2: pair counts, then scatter cursors, per camera-pair block
-    int* blk_ptr;         // num_cams^2 + 1: pair list offsets per block
-    unsigned long long* pairs;  // (o << 32 | o') per block, sorted inside a block
-    long pair_cap;        // capacity of `pairs` (entries)
-    int* long_list;       // [count, ids...] of blocks with more than 1024 pairs
-    int long_cap;         // capacity of long_list ids
-    int* nz_list;         // [count, cursor, ids...] of the non-empty camera-pair blocks
+    double* Ucam;         // 81*num_cams scaled camera blocks U (9 x 9, column-major)
     int* err;             // device error bits
 };
 
 void launch_validate_obs(const SceneDev& s, cudaStream_t st);
 // Camera observations are processed in tiles of 256; slots = C + num_obs/256 + 1.
 size_t camera_tile_slots(int num_cams, int num_obs);
-// ints of the non-empty camera-pair block list for npairs pairs
-size_t schur_list_ints(int num_cams, long npairs);
 void launch_build_index(SceneDev& s, cudaStream_t st);
-// U blocks (scaled) written to the diagonal blocks of Z (ldz), column norms.
-void launch_camera_blocks(const SceneDev& s, double* Z, int ldz, cudaStream_t st);
+// U blocks (scaled) into s.Ucam, column norms into s.s_cam.
+void launch_camera_blocks(const SceneDev& s, cudaStream_t st);
 void launch_point_blocks(const SceneDev& s, cudaStream_t st);
 void launch_obs_blocks(const SceneDev& s, cudaStream_t st);
-// Schur scatter: pair counts per camera-pair block (total = blk_ptr[C*C]),
-// then Z(c,c') -= sum_p Y_o W_o'^T (upper camera-block triangle); mirror after.
-void launch_schur_count(const SceneDev& s, cudaStream_t st);
-// Self terms Z(c,c) -= sum_o Y_o W_o^T (upper triangle of the diagonal blocks).
-void launch_camera_self(const SceneDev& s, double* Z, int ldz, cudaStream_t st);
-void launch_schur(const SceneDev& s, double* Z, int ldz, cudaStream_t st);
-void launch_mirror_upper(double* Z, int n, int ldz, cudaStream_t st);
+// The Schur complement Z = U - W V^-1 W^T (schur.cu) over a zeroed Z: the
+// diagonal blocks from s.Ucam, every co-visible camera-pair block written in
+// both triangles, bitwise symmetric. UNC_ERR_TOO_LARGE above kSchurMaxCams.
+constexpr int kSchurMaxCams = 5120;  // above the dense path's limit (9 C <= 46000)
+int launch_schur_columns(const SceneDev& s, double* Z, int ldz, cudaStream_t st);
+size_t schur_columns_smem(int num_cams);
+void prepare_schur_columns();  // kernel attributes (before any stream capture)
 // Generic 9/12-entry-row repack for the J^T J export (camera-only rows allowed).
 void launch_repack_generic(int num_obs, int cam_off, const int* rows, const int* cols,
                            const double* vals, double* J, int* obs_cam, int* obs_pt, int* err,
@@ -265,6 +257,22 @@ struct PowerSet {
     unsigned long long* dmax;  // 21 words: max diag of X^j, j = 0..20 (bits of a non-negative double)
     TeState* te;
 };
+// Slices of the int8-sliced products of the blocked-power evaluation (mixed
+// modes with S slices). Product q: 0..5 = X^2, X^3, X^4, X^8, X^12, X^16;
+// 6..9 = X^4 G_1, X^8 G_2, X^12 G_3, X^16 G_4. Z is positive semi-definite,
+// so the eigenvalues of X = (Z + lambda I)^-1 are at most 1/lambda and the
+// series term lambda^i / (i-1)! X^(i+1) = X (lambda X)^i / (i-1)! has norm at
+// most ||X|| / (i-1)! (32-bit factorial). G_2 (terms 8..11) therefore adds at
+// most 2.3e-4 ||X||, G_3 3e-8 and G_4 1e-8 (the factorial wraps there): their
+// products keep the absolute error of the full-slice ones with 2 and 3 slices
+// (7 bits each) fewer. X^8, X^12 and X^16 feed only those blocks and the stop
+// rule's diagonal maxima (relative error ~2^-28 with one slice fewer). The
+// digits are rounded greedily, so the first k slices of an operand are its
+// k-slice form: the same slice buffers serve every count.
+inline int power_product_slices(int q, int S) {
+    const int drop = (q >= 3 && q <= 5) ? 1 : (q == 7 ? 2 : (q >= 8 ? 3 : 0));
+    return S - drop < 2 ? (S < 2 ? S : 2) : S - drop;
+}
 // k[i - 1] = lambda^i / factorial(i - 1), i = 1..19 (host values)
 struct TaylorCoefs {
     double k[19];
@@ -326,6 +334,9 @@ struct MixedOperand {
     int n, slices, rows, kp;
 };
 int mixed_tile_n(int slices, int n);
+// int8 multiply-adds x 2 that one lower-triangle product of n x n operands
+// issues with `slices` slices (tile padding included).
+double mixed_issued_ops(int n, int slices);
 size_t mixed_slice_bytes(int n, int slices);
 // Prepare the operand over buf/exps (as_b: box rows of the B operand). False
 // when the driver's tensor-map encoder is unavailable.
@@ -335,6 +346,11 @@ struct TeState;
 // rows padded for both the 128-row A boxes and nt; the slice bytes for it.
 bool mixed_plan_nt(MixedOperand& op, int8_t* buf, int* exps, int n, int slices, bool as_b, int nt);
 size_t mixed_slice_bytes_nt(int n, int slices, int nt);
+// The same sliced operand used with its first `slices` slices only (the digits
+// are greedy, so they are the operand's representation with fewer slices):
+// same buffer and plane stride; as_b: a B map with that slice count's tile
+// width. *ok: false when the tensor map could not be encoded.
+MixedOperand mixed_fewer_slices(const MixedOperand& op, int slices, bool as_b, bool* ok);
 // Grouped forms for a batch of matrices (arguments in device memory).
 struct MixedSliceJob {  // k_slice_rows of one matrix
     const double* A;

@@ -107,13 +107,24 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
+// 16 consecutive 32-bit TMEM columns of this warp's 32 lanes; the values may
+// be used only after tmem_wait_ld.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int (&r)[16]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+
+// After tmem_wait_ld: ties the 16 registers to this point of the program, so
+// that no use of them is scheduled before the wait.
+__device__ __forceinline__ void tmem_fence_regs(int (&r)[16]) {
+    asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]),
+                 "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]),
+                 "+r"(r[14]), "+r"(r[15]));
 }
 
 template <int NT, int S>
@@ -337,16 +348,29 @@ __device__ __forceinline__ void ozaki_tile(const CUtensorMap* tA, const CUtensor
     double mx = 0.0;
     if (ok) {
         for (int c0 = 0; c0 < NT; c0 += 16) {
+            // all levels' accumulators of these 16 columns in one round trip
+            int r[S][16];
+#pragma unroll
+            for (int l = 0; l < S; ++l) tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(l * NT + c0), r[l]);
+            // accumulate: the previous values of C, loaded together before any store of
+            // this chunk (reads are of the lower triangle, mirrored stores go above it)
+            double prev[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int col = n0 + c0 + j;
+                prev[j] = accumulate && row < M && col < N && (!mirror || row >= col) ? C[row + (long)col * ldc] : 0.0;
+            }
+            tmem_wait_ld();
+#pragma unroll
+            for (int l = 0; l < S; ++l) tmem_fence_regs(r[l]);
             double v[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j) v[j] = 0.0;
 #pragma unroll
             for (int l = S - 1; l >= 0; --l) {  // small levels first
-                int r[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(l * NT + c0), r);
                 const double w = ldexp(1.0, -7 * (l + 2));
 #pragma unroll
-                for (int j = 0; j < 16; ++j) v[j] += (double)r[j] * w;
+                for (int j = 0; j < 16; ++j) v[j] += (double)r[l][j] * w;
             }
             if (row < M) {
 #pragma unroll
@@ -357,7 +381,7 @@ __device__ __forceinline__ void ozaki_tile(const CUtensorMap* tA, const CUtensor
                         // mirror: the lower triangle is written at (row, col) and at
                         // (col, row); nothing above the diagonal is written directly
                         // accumulate: C += P X (C symmetric: its lower element is read)
-                        if (accumulate && (!mirror || row >= col)) x += C[row + (long)col * ldc];
+                        if (accumulate && (!mirror || row >= col)) x += prev[j];
                         if (!mirror || row >= col) {
                             C[row + (long)col * ldc] = x;
                             const double ax = fabs(x);
@@ -497,10 +521,12 @@ void prepare_mixed_kernels() {
     set_attr_once<64, 5>();
     set_attr_once<96, 5>();
     set_attr_once<128, 3>();
+    set_attr_once<128, 2>();
     set_attr_grouped_once<128, 4>();
     set_attr_grouped_once<64, 5>();
     set_attr_grouped_once<96, 5>();
     set_attr_grouped_once<128, 3>();
+    set_attr_grouped_once<128, 2>();
 }
 
 // Output tile width: slices * tile_n <= 512 TMEM columns, so 128 for up to 4
@@ -525,6 +551,12 @@ int mixed_tile_n(int slices, int n) {
     constexpr int kSMs = 148;
     const long w96 = (lower_tiles(n, 96) + kSMs - 1) / kSMs, w64 = (lower_tiles(n, 64) + kSMs - 1) / kSMs;
     return w64 * (64 + 16) < w96 * (96 + 16) ? 64 : 96;
+}
+
+double mixed_issued_ops(int n, int slices) {
+    const int nt = mixed_tile_n(slices, n);
+    const double kp = (double)(((n + BKB - 1) / BKB) * BKB);
+    return 2.0 * (slices * (slices + 1) / 2) * (double)lower_tiles(n, nt) * BM * nt * kp;
 }
 
 static int mixed_rows(int n, int slices) {
@@ -569,6 +601,14 @@ bool mixed_plan_nt(MixedOperand& op, int8_t* buf, int* exps, int n, int slices, 
     return make_map(&op.map, buf, op.rows * slices, op.kp, as_b ? nt : BM);
 }
 
+MixedOperand mixed_fewer_slices(const MixedOperand& op, int slices, bool as_b, bool* ok) {
+    MixedOperand r = op;
+    r.slices = slices;
+    if (as_b) *ok = make_map(&r.map, op.buf, op.rows * op.slices, op.kp, mixed_tile_n(slices, op.n));
+    else *ok = true;  // A boxes are 128 rows whatever the slice count
+    return r;
+}
+
 void mixed_slice_grouped(const MixedSliceJob* d_jobs, int njobs, const int* d_row_start, int total_rows,
                          cudaStream_t st) {
     if (total_rows <= 0) return;
@@ -598,8 +638,10 @@ void mixed_gemm_grouped(int slices, int nt, const MixedGemmJob* d_jobs, const in
         k_ozaki_gemm_grouped<96, 5><<<ntiles, THREADS, Shape<96, 5>::SMEM, st>>>(d_jobs, d_tiles);
     } else if (slices == 4) {
         k_ozaki_gemm_grouped<128, 4><<<ntiles, THREADS, Shape<128, 4>::SMEM, st>>>(d_jobs, d_tiles);
-    } else {
+    } else if (slices == 3) {
         k_ozaki_gemm_grouped<128, 3><<<ntiles, THREADS, Shape<128, 3>::SMEM, st>>>(d_jobs, d_tiles);
+    } else {
+        k_ozaki_gemm_grouped<128, 2><<<ntiles, THREADS, Shape<128, 2>::SMEM, st>>>(d_jobs, d_tiles);
     }
     count_launch();
 }
@@ -639,8 +681,10 @@ void mixed_gemm(const MixedOperand& a, const MixedOperand& b, double* C, int ldc
         launch_ozaki<64, 5>(a, b, C, ldc, amax, lower_only, err, st, skip, mirror, accumulate);
     else if (a.slices == 5)
         launch_ozaki<96, 5>(a, b, C, ldc, amax, lower_only, err, st, skip, mirror, accumulate);
-    else
+    else if (a.slices == 3)
         launch_ozaki<128, 3>(a, b, C, ldc, amax, lower_only, err, st, skip, mirror, accumulate);
+    else
+        launch_ozaki<128, 2>(a, b, C, ldc, amax, lower_only, err, st, skip, mirror, accumulate);
     count_launch();
 }
 

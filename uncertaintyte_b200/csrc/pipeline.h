@@ -33,28 +33,15 @@ bool is_svd(const unc_options* o);
 // Grow-only device buffer allocated in stream order on sm.
 int grow_buffer(void** p, size_t* have, size_t need, size_t want, cudaStream_t sm);
 
-// Bytes of the Schur pair list (pairs, long-block list, non-empty block list)
-// for a scene of C cameras and npairs co-visible observation pairs.
-size_t schur_pair_bytes(int C, long long npairs);
-// An upper bound of the co-visible observation pairs the device will list for
-// this Jacobian (host arrays): sum over points of m (m - 1) with m the
-// observations whose point column names the point (fixed points and invalid
-// observations are dropped on the device, which only lowers the count).
-long long schur_pairs_bound(const unc_options* o, int num_rows, long long nnz, const int* cols);
-
 // The sparse stages of computeCovariances on stream sm (compute.cpp:73-118,
 // 283-368): observation validation (fixPts), the observation index, J^T J
-// blocks and column norms, point blocks and their inverses, W/Y and the self
-// terms, and the scaled Schur complement Z = U - W V^-1 W^T, mirrored.
+// blocks and column norms, point blocks and their inverses, W/Y, and the
+// scaled Schur complement Z = U - W V^-1 W^T (both triangles). No host round
+// trip: the stage can be captured in a graph.
 // fx receives the fixed points as the reference orders them. ev: 6 events
 // recorded at the stage boundaries, or nullptr.
-// Pair list: with pairs_cap >= 0 the caller provides *pair_buf holding
-// schur_pair_bytes(C, pairs_cap) bytes (a host-side bound: no read-back, the
-// stage can be captured in a graph); otherwise the device count is read back
-// and *pair_buf grown with grow_buffer on sm.
 int sparse_stage(const unc_options* o, const Plan& pl, long long nnz, const int* rows, const int* cols,
-                 const double* vals, Buffers& b, int fx[3], cudaEvent_t* ev, cudaStream_t sm, void** pair_buf,
-                 size_t* pair_bytes, long long pairs_cap);
+                 const double* vals, Buffers& b, int fx[3], cudaEvent_t* ev, cudaStream_t sm);
 
 // The camera outputs (removeScaleJ4Z, compute.cpp:168-183) from iZ and the
 // point covariances (compute.cpp:370-455, 517-527) into cam_out / pt_out.

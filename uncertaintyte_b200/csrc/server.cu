@@ -12,8 +12,8 @@
 //   (different streams), the host-side waits of one request block only its
 //   worker.
 // * Admission by device-memory footprint (unc_request_bytes: the dense Schur
-//   complement and its inverse buffers, the block storage, the pair list, the
-//   int8 slices): the sum over running requests and idle workspaces stays
+//   complement and its inverse buffers, the block storage, the int8
+//   slices): the sum over running requests and idle workspaces stays
 //   within `max_device_bytes`. Idle workspaces are released when that makes a
 //   request fit. Later requests may start ahead of a waiting one (backfill) at
 //   most kMaxBypass times, so large requests are not starved.

@@ -79,7 +79,7 @@ class UncStatistic(C.Structure):
 
 # every symbol declared in include/uncte.h
 EXPORTS = ("unc_options_init", "unc_context_create", "unc_context_destroy", "unc_compute",
-           "unc_context_set_profiling", "unc_context_profile",
+           "unc_context_set_profiling", "unc_context_profile", "unc_context_profile_int8",
            "unc_compute_device", "unc_workspace_bytes", "unc_dense_inverse_device",
            "unc_dense_inverse_noalloc", "unc_spd_task_list", "unc_spd_inverse_tasks_bounded", "unc_pinv_psd_device", "unc_jtj_crs",
            "unc_gemm_f64_device", "unc_gemm_mixed_device", "unc_status_string", "unc_last_error",
@@ -113,6 +113,7 @@ def lib():
                                      P(UncStatistic), vp]
     L.unc_context_set_profiling.argtypes = [vp, C.c_int]
     L.unc_context_profile.argtypes = [vp, P(C.c_longlong), P(C.c_double), P(C.c_double), C.c_int]
+    L.unc_context_profile_int8.argtypes = [vp, P(C.c_double)]
     L.unc_workspace_bytes.argtypes = [P(UncOptions), C.c_int, C.c_int]
     L.unc_workspace_bytes.restype = C.c_longlong
     L.unc_dense_inverse_device.argtypes = [vp, C.c_int, C.c_int, vp]
@@ -252,6 +253,12 @@ class Context:
         n, s, f = C.c_longlong(), C.c_double(), C.c_double()
         _check(lib().unc_context_profile(self._h, C.byref(n), C.byref(s), C.byref(f), int(reset)))
         return n.value, s.value, f.value
+
+    def profile_int8(self) -> float:
+        """int8 multiply-adds x 2 issued by the profiled products (mixed modes), since the last reset."""
+        v = C.c_double()
+        _check(lib().unc_context_profile_int8(self._h, C.byref(v)))
+        return v.value
 
     def __enter__(self):
         return self
