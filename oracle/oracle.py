@@ -34,6 +34,7 @@ class OracleOptions(C.Structure):
         ("threads", C.c_int),
         ("inverse_route", C.c_int),
         ("z_perturb", C.c_double),
+        ("z_perturb_terms", C.c_double),
         ("skip_dense", C.c_int),
     ]
 
@@ -102,13 +103,14 @@ def _p(a, t):
 
 def compute(jac, algorithm=2, lam=-1.0, epsilon=1e-10, svd_remove_n=-1, faithful_point_scan=False,
             threads=0, debug=False, cam_init=None, pt_init=None, route="lu", z_perturb=0.0,
-            skip_dense=False):
+            z_perturb_terms=0.0, skip_dense=False):
     """Run the oracle on a Jacobian (uncertaintyte_b200.jacob.Jacobian-like object).
 
     route: "lu" (the reference's ScaledDenseMatrix::inv) or "cholesky" (the
     Jacobi-equilibrated Cholesky inverse, the CUDA path's route) for the dense
     inverse of the Taylor path. z_perturb: relative rounding-level perturbation
-    of the Schur complement (see uncte_oracle.h), 0 for none. skip_dense:
+    of the Schur complement (see uncte_oracle.h), 0 for none; z_perturb_terms:
+    the same at the size of the Schur complement's terms. skip_dense:
     timing samples only (the dense inverse and Taylor loop are skipped, the
     outputs are meaningless). Returns dict(cam, pt, stats[, Z, iZ, d])."""
     o = OracleOptions()
@@ -125,6 +127,7 @@ def compute(jac, algorithm=2, lam=-1.0, epsilon=1e-10, svd_remove_n=-1, faithful
     o.threads = threads
     o.inverse_route = {"lu": 0, "cholesky": 1}[route]
     o.z_perturb = z_perturb
+    o.z_perturb_terms = z_perturb_terms
     o.skip_dense = int(bool(skip_dense))
     ncam = jac.num_cams * jac.cam_params * (jac.cam_params + 1) // 2
     cam = np.zeros(ncam) if cam_init is None else np.array(cam_init, dtype=np.float64)

@@ -820,6 +820,26 @@ extern "C" int oracle_compute(const oracle_options* opt, int nrows, int ncols, c
                 if (r != c) Z[c + (size_t)r * N] = Z[r + (size_t)c * N];
             }
     }
+    if (opt->z_perturb_terms != 0) {
+        /* rounding error of U - Y W^T at the size of its terms (test infrastructure) */
+        auto r_of = [](int r, int c, uint64_t salt) {
+            uint64_t h = (((uint64_t)r << 32 | (uint32_t)c) ^ salt) * 0x9E3779B97F4A7C15ull;
+            h ^= h >> 29;
+            h *= 0xBF58476D1CE4E5B9ull;
+            h ^= h >> 32;
+            return (double)(h >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+        };
+        const double z = opt->z_perturb_terms;
+        for (int i = 0; i < N; ++i) {
+            for (int k = U.row[i]; k < U.row[i + 1]; ++k)
+                if (U.col[k] <= i) Z[i + (size_t)U.col[k] * N] += z * r_of(i, U.col[k], 0x5555) * std::fabs(U.val[k]);
+            for (int k = YWt.row[i]; k < YWt.row[i + 1]; ++k)
+                if (YWt.col[k] <= i)
+                    Z[i + (size_t)YWt.col[k] * N] += z * r_of(i, YWt.col[k], 0xAAAA) * std::fabs(YWt.val[k]);
+        }
+        for (int c = 0; c < N; ++c)
+            for (int r = c + 1; r < N; ++r) Z[c + (size_t)r * N] = Z[r + (size_t)c * N];
+    }
     if (dbg_Z) std::copy(Z.begin(), Z.end(), dbg_Z);
     if (dbg_d) std::copy(d.begin(), d.begin() + N, dbg_d);
 

@@ -36,6 +36,12 @@ typedef struct {
                                  symmetric. At z_perturb = 2^-53 this measures how far the results move
                                  under a rounding-level change of Z (cond(Z + lambda*I) * eps): the
                                  floor below which two correct FP64 implementations cannot agree. */
+    double z_perturb_terms;   /* 0: none. Otherwise every entry Z_ij of the Schur complement moves by
+                                 z_perturb_terms * r * (|U_ij| + |(Y W^T)_ij|), r in [-1, 1) from a fixed
+                                 hash of (row, col), symmetric: the rounding error of Z = U - Y W^T at the
+                                 size of its terms (what another summation order of the Schur complement
+                                 amounts to), where the relative form above stays at the size of the
+                                 result and misses the cancellation. */
     int skip_dense;           /* timing samples only: 1 skips the dense inverse and the Taylor loop (iZ is
                                  left as Z + lambda*I), so every sparse stage runs at full size but the
                                  outputs are meaningless. 0 for results. */

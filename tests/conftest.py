@@ -59,8 +59,10 @@ def fp64_floor(jac, ref_lu, threads=8, **kw):
     oracle: the Cholesky inverse route against the LU route (same Z), and the
     LU route on the Jacobian with every value moved by at most one ulp (two
     seeds): rounding-level input noise, which is what a different summation
-    order in the assembly amounts to. Returns (camera floor, point floor,
-    details)."""
+    order in the assembly amounts to; and the LU route with the Schur
+    complement Z = U - Y W^T moved by one ulp of the size of its terms (the
+    rounding of another summation order of Z itself). Returns (camera floor,
+    point floor, details)."""
     import copy
 
     import oracle
@@ -73,4 +75,6 @@ def fp64_floor(jac, ref_lu, threads=8, **kw):
         j2.values = jac.values * (1.0 + 2.0 ** -52 * r)
         o = oracle.compute(j2, threads=threads, **kw)
         det[f"ulp{seed}"] = (block_rel_err(o["cam"], ref_lu["cam"], 45), block_rel_err(o["pt"], ref_lu["pt"], 6))
+    o = oracle.compute(jac, threads=threads, z_perturb_terms=2.0 ** -52, **kw)
+    det["terms"] = (block_rel_err(o["cam"], ref_lu["cam"], 45), block_rel_err(o["pt"], ref_lu["pt"], 6))
     return max(v[0] for v in det.values()), max(v[1] for v in det.values()), det, chol

@@ -11,8 +11,10 @@ fingerprint of the scene (so that a test notices a generator change).
 Both dense-inverse routes are run: "lu" (the reference's equilibrated
 dgetrf/dgetri) and "cholesky" (the Jacobi-equilibrated Cholesky inverse that
 the CUDA path also uses), and the LU route on the Jacobian with every value
-moved by at most one ulp (two seeds, "ulp1" / "ulp2", the perturbation of
-tests/conftest.py fp64_floor). How far these lie apart is the FP64 floor of
+moved by at most one ulp (two seeds, "ulp1" / "ulp2"), and the LU route with
+the Schur complement moved at the size of its terms ("terms": the rounding of
+Z = U - Y W^T in another summation order), the perturbations of
+tests/conftest.py fp64_floor. How far these lie apart is the FP64 floor of
 this ill-conditioned problem, which the GPU test uses as its bar.
 
 The oracle's point stage runs with its per-point observation index
@@ -20,10 +22,10 @@ The oracle's point stage runs with its per-point observation index
 (compute.cpp:393) would visit ~1.75e12 rows here; the index visits the same
 rows of each point in the same order.
 
-    python tests/golden/make_large_golden.py [--threads N] [--only-ulp]
+    python tests/golden/make_large_golden.py [--threads N] [--only-ulp | --only-terms]
 
-writes tests/golden/large_sample.npz (--only-ulp: adds the perturbed runs to
-an existing file).
+writes tests/golden/large_sample.npz (--only-ulp, --only-terms: add those
+perturbed runs to an existing file).
 """
 from __future__ import annotations
 
@@ -65,24 +67,28 @@ def main():
     ap.add_argument("--threads", type=int, default=os.cpu_count() or 1)
     ap.add_argument("--out", default=os.path.join(HERE, "large_sample.npz"))
     ap.add_argument("--only-ulp", action="store_true")
+    ap.add_argument("--only-terms", action="store_true")
     a = ap.parse_args()
     jac = scenes.synthetic_jacobian("large", seed=0)
     cams, pts = sample_indices(jac)
     out = {"fingerprint": scene_fingerprint(jac), "cams": cams, "pts": pts,
            "pts2fix": np.asarray(jac.pts2fix, dtype=np.int32)}
-    runs = [("lu", "lu", None), ("cholesky", "cholesky", None), ("ulp1", "lu", 1), ("ulp2", "lu", 2)]
-    if a.only_ulp:
+    runs = [("lu", "lu", None), ("cholesky", "cholesky", None), ("ulp1", "lu", 1), ("ulp2", "lu", 2),
+            ("terms", "lu", "terms")]
+    if a.only_ulp or a.only_terms:
         old = np.load(a.out)
         out.update({k: old[k] for k in old.files})
-        runs = runs[2:]
+        runs = runs[2:4] if a.only_ulp else runs[4:]
     for name, route, seed in runs:
         t0 = time.perf_counter()
-        j = jac
-        if seed is not None:  # every value moved by at most one ulp
+        j, zt = jac, 0.0
+        if seed == "terms":  # the Schur complement moved at the size of its terms
+            zt = 2.0 ** -52
+        elif seed is not None:  # every value moved by at most one ulp
             j = copy.copy(jac)
             r = np.random.default_rng(seed).uniform(-1.0, 1.0, jac.values.size)
             j.values = jac.values * (1.0 + 2.0 ** -52 * r)
-        r = oracle.compute(j, threads=a.threads, faithful_point_scan=False, route=route)
+        r = oracle.compute(j, threads=a.threads, faithful_point_scan=False, route=route, z_perturb_terms=zt)
         st = r["stats"]
         print(f"{name}: {time.perf_counter() - t0:.1f} s, {st.te_iterations} iterations", flush=True)
         out[f"{name}_cam"] = r["cam"].reshape(-1, 45)[cams]

@@ -7,8 +7,9 @@ so its output is committed as a sample (tests/golden/large_sample.npz: every
 tests/golden/make_large_golden.py on the same seeded scene). Bars, per camera
 9x9 and point 3x3 block (relative Frobenius error):
   * FP64 GPU vs the oracle's LU and Cholesky routes: max(1e-9, FLOOR_MULT x the
-    floor), the floor being how far the Cholesky route and the LU route on the
-    Jacobian moved by one ulp (two seeds) lie from the LU route, as in
+    floor), the floor being how far the Cholesky route, the LU route on the
+    Jacobian moved by one ulp (two seeds) and the LU route with the Schur
+    complement moved at the size of its terms lie from the LU route, as in
     test_gpu_parity.py;
   * mixed precision vs the FP64 oracle (sample) and vs the FP64 GPU path (all
     blocks): 1e-6, the accuracy target of the mixed path;
@@ -61,7 +62,7 @@ def test_large_statistics_match_the_oracle(large):
 def test_large_fp64_vs_oracle_sample(large):
     g, jac, (c64, p64, s64), _ = large
     # the floor: the Cholesky route and the one-ulp perturbed Jacobians against the LU route
-    others = [k for k in ("cholesky", "ulp1", "ulp2") if f"{k}_cam" in g.files]
+    others = [k for k in ("cholesky", "ulp1", "ulp2", "terms") if f"{k}_cam" in g.files]
     fc = max(block_rel_err(g[f"{k}_cam"], g["lu_cam"], 45) for k in others)
     fp = max(block_rel_err(g[f"{k}_pt"], g["lu_pt"], 6) for k in others)
     bar_c, bar_p = max(FP64_BAR, FLOOR_MULT * fc), max(FP64_BAR, FLOOR_MULT * fp)
