@@ -35,6 +35,7 @@ class OracleOptions(C.Structure):
         ("inverse_route", C.c_int),
         ("z_perturb", C.c_double),
         ("z_perturb_terms", C.c_double),
+        ("swap_products", C.c_int),
         ("skip_dense", C.c_int),
     ]
 
@@ -85,7 +86,7 @@ def lib():
         L.oracle_dense_inv.restype = C.c_int
         L.oracle_te_inverse.argtypes = [C.c_int, P(C.c_double), C.c_double, P(OracleStats)]
         L.oracle_te_inverse.restype = C.c_int
-        L.oracle_te_inverse_route.argtypes = [C.c_int, P(C.c_double), C.c_double, C.c_int, P(OracleStats)]
+        L.oracle_te_inverse_route.argtypes = [C.c_int, P(C.c_double), C.c_double, C.c_int, P(OracleStats), C.c_int]
         L.oracle_te_inverse_route.restype = C.c_int
         L.oracle_dense_inv_cholesky.argtypes = [C.c_int, P(C.c_double)]
         L.oracle_dense_inv_cholesky.restype = C.c_int
@@ -103,14 +104,16 @@ def _p(a, t):
 
 def compute(jac, algorithm=2, lam=-1.0, epsilon=1e-10, svd_remove_n=-1, faithful_point_scan=False,
             threads=0, debug=False, cam_init=None, pt_init=None, route="lu", z_perturb=0.0,
-            z_perturb_terms=0.0, skip_dense=False):
+            z_perturb_terms=0.0, swap_products=False, skip_dense=False):
     """Run the oracle on a Jacobian (uncertaintyte_b200.jacob.Jacobian-like object).
 
     route: "lu" (the reference's ScaledDenseMatrix::inv) or "cholesky" (the
     Jacobi-equilibrated Cholesky inverse, the CUDA path's route) for the dense
     inverse of the Taylor path. z_perturb: relative rounding-level perturbation
     of the Schur complement (see uncte_oracle.h), 0 for none; z_perturb_terms:
-    the same at the size of the Schur complement's terms. skip_dense:
+    the same at the size of the Schur complement's terms; swap_products: the
+    Taylor products as X * add instead of add * X (same series, other
+    rounding). skip_dense:
     timing samples only (the dense inverse and Taylor loop are skipped, the
     outputs are meaningless). Returns dict(cam, pt, stats[, Z, iZ, d])."""
     o = OracleOptions()
@@ -125,9 +128,10 @@ def compute(jac, algorithm=2, lam=-1.0, epsilon=1e-10, svd_remove_n=-1, faithful
         o.has_pts2fix = 1
     o.faithful_point_scan = int(bool(faithful_point_scan))
     o.threads = threads
-    o.inverse_route = {"lu": 0, "cholesky": 1}[route]
+    o.inverse_route = {"lu": 0, "cholesky": 1, "recursive": 2}[route]
     o.z_perturb = z_perturb
     o.z_perturb_terms = z_perturb_terms
+    o.swap_products = int(bool(swap_products))
     o.skip_dense = int(bool(skip_dense))
     ncam = jac.num_cams * jac.cam_params * (jac.cam_params + 1) // 2
     cam = np.zeros(ncam) if cam_init is None else np.array(cam_init, dtype=np.float64)
@@ -187,7 +191,7 @@ def te_inverse(Z, lam, route="lu"):
     n = Z.shape[0]
     F = np.array(Z, dtype=np.float64, order="F")
     st = OracleStats()
-    lib().oracle_te_inverse_route(n, _p(F, C.c_double), lam, {"lu": 0, "cholesky": 1}[route], C.byref(st))
+    lib().oracle_te_inverse_route(n, _p(F, C.c_double), lam, {"lu": 0, "cholesky": 1}[route], C.byref(st), 0)
     return F, st
 
 

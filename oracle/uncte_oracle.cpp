@@ -300,15 +300,83 @@ int oracle_dense_inv_cholesky(int n, double* A) {
     return info;
 }
 
-/* teInverse: compute.cpp:121-166 (iZupdate :64-71, operator*= :314-353). */
-int oracle_te_inverse(int n, double* Z, double lambda, oracle_stats* st) {
-    return oracle_te_inverse_route(n, Z, lambda, 0, st);
+/* Route 2 (test infrastructure): the CUDA path's recursive form of the same
+ * Cholesky inverse, restated with BLAS. On halves [r0, m) [m, r1) (m a multiple
+ * of 64): L11 and T11 = L11^-1 by recursion, L21 = A21 T11^T, A22 -= L21 L21^T,
+ * X = L21 T11, T22 by recursion, T21 = -T22 X; 64 x 64 leaves by dpotrf and a
+ * forward substitution for T; then A^-1 = T^T T. */
+static void rec_chol(double* A, double* T, double* W, int n, int r0, int r1, int* info) {
+    const int len = r1 - r0;
+    if (*info) return;
+    if (len <= 64) {
+        double* a = A + r0 + (size_t)r0 * n;
+        int inf = 0;
+        scipy_dpotrf_("L", &len, a, &n, &inf);
+        if (inf) { *info = r0 + inf; return; }
+        double* t = T + r0 + (size_t)r0 * n;
+        for (int c = 0; c < len; ++c)
+            for (int r = 0; r < len; ++r) t[r + (size_t)c * n] = 0.0;
+        for (int c = 0; c < len; ++c) {  /* column c of L^-1: L x = e_c */
+            for (int r = c; r < len; ++r) {
+                double sum = r == c ? 1.0 : 0.0;
+                for (int k = c; k < r; ++k) sum -= a[r + (size_t)k * n] * t[k + (size_t)c * n];
+                t[r + (size_t)c * n] = sum / a[r + (size_t)r * n];
+            }
+        }
+        return;
+    }
+    int m = r0 + ((len / 2 + 63) / 64) * 64;
+    if (m >= r1) m = r1 - 64;
+    const int h1 = m - r0, h2 = r1 - m;
+    rec_chol(A, T, W, n, r0, m, info);
+    const double one = 1.0, zero = 0.0, mone = -1.0;
+    double* A21 = A + m + (size_t)r0 * n;
+    const double* T11 = T + r0 + (size_t)r0 * n;
+    scipy_dgemm_("N", "T", &h2, &h1, &h1, &one, A21, &n, T11, &n, &zero, W, &n);           /* L21 */
+    scipy_dgemm_("N", "T", &h2, &h2, &h1, &mone, W, &n, W, &n, &one, A + m + (size_t)m * n, &n);
+    scipy_dgemm_("N", "N", &h2, &h1, &h1, &one, W, &n, T11, &n, &zero, A21, &n);          /* X */
+    rec_chol(A, T, W, n, m, r1, info);
+    scipy_dgemm_("N", "N", &h2, &h1, &h2, &mone, T + m + (size_t)m * n, &n, A21, &n, &zero, T + m + (size_t)r0 * n, &n);
 }
 
-int oracle_te_inverse_route(int n, double* Z, double lambda, int route, oracle_stats* st) {
+int oracle_dense_inv_recursive(int n, double* A) {
+    std::vector<double> e(n);
+    for (int i = 0; i < n; ++i) {
+        const double d = A[i + (size_t)i * n];
+        if (!(d > 0)) return i + 1;
+        e[i] = 1.0 / std::sqrt(d);
+    }
+#pragma omp parallel for
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < n; ++r) A[r + (size_t)c * n] *= e[r] * e[c];
+    std::vector<double> T((size_t)n * n, 0.0), W((size_t)n * n, 0.0);
+    int info = 0;
+    rec_chol(A, T.data(), W.data(), n, 0, n, &info);
+    if (info) return info;
+    for (int c = 0; c < n; ++c)  /* T is lower triangular: clear what the recursion left above */
+        for (int r = 0; r < c; ++r) T[r + (size_t)c * n] = 0.0;
+    const double one = 1.0, zero = 0.0;
+    scipy_dgemm_("T", "N", &n, &n, &n, &one, T.data(), &n, T.data(), &n, &zero, A, &n);
+#pragma omp parallel for
+    for (int c = 0; c < n; ++c)
+        for (int r = c; r < n; ++r) {
+            const double v = A[r + (size_t)c * n] * e[r] * e[c];
+            A[r + (size_t)c * n] = v;
+            A[c + (size_t)r * n] = v;
+        }
+    return 0;
+}
+
+/* teInverse: compute.cpp:121-166 (iZupdate :64-71, operator*= :314-353). */
+int oracle_te_inverse(int n, double* Z, double lambda, oracle_stats* st) {
+    return oracle_te_inverse_route(n, Z, lambda, 0, st, 0);
+}
+
+int oracle_te_inverse_route(int n, double* Z, double lambda, int route, oracle_stats* st, int swap) {
     auto t0 = Clock::now();
     for (int i = 0; i < n; ++i) Z[i + (size_t)i * n] += lambda;
-    int info = route == 1 ? oracle_dense_inv_cholesky(n, Z) : oracle_dense_inv(n, Z);
+    int info = route == 1 ? oracle_dense_inv_cholesky(n, Z)
+                          : (route == 2 ? oracle_dense_inv_recursive(n, Z) : oracle_dense_inv(n, Z));
     auto t1 = Clock::now();
     const size_t nn = (size_t)n * n;
     std::vector<double> X(Z, Z + nn), add(nn), tmp(nn);
@@ -324,7 +392,10 @@ int oracle_te_inverse_route(int n, double* Z, double lambda, int route, oracle_s
         iters++;
 #pragma omp parallel for
         for (size_t e = 0; e < nn; ++e) Z[e] = Z[e] + k * add[e];
-        gemm_nn(n, add.data(), X.data(), tmp.data());
+        if (swap)
+            gemm_nn(n, X.data(), add.data(), tmp.data());
+        else
+            gemm_nn(n, add.data(), X.data(), tmp.data());
         add.swap(tmp);
     }
     auto t2 = Clock::now();
@@ -850,7 +921,7 @@ extern "C" int oracle_compute(const oracle_options* opt, int nrows, int ncols, c
         for (int i = 0; i < N; ++i) Z[i + (size_t)i * N] += lambda;  /* timing sample: no inverse */
         st->lambda = lambda;
     } else {
-        oracle_te_inverse_route(N, Z.data(), lambda, opt->inverse_route, st);
+        oracle_te_inverse_route(N, Z.data(), lambda, opt->inverse_route, st, opt->swap_products);
     }
     if (dbg_iZ) std::copy(Z.begin(), Z.end(), dbg_iZ);
 

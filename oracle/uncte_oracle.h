@@ -42,6 +42,9 @@ typedef struct {
                                  size of its terms (what another summation order of the Schur complement
                                  amounts to), where the relative form above stays at the size of the
                                  result and misses the cancellation. */
+    int swap_products;        /* 0: Taylor products add * X (the reference's order); 1: X * add. The powers of
+                                 X commute, so both are the same series; their rounding differs (another
+                                 correct FP64 evaluation, for the parity floor). */
     int skip_dense;           /* timing samples only: 1 skips the dense inverse and the Taylor loop (iZ is
                                  left as Z + lambda*I), so every sparse stage runs at full size but the
                                  outputs are meaningless. 0 for results. */
@@ -93,7 +96,7 @@ int oracle_te_inverse(int n, double* Z, double lambda, oracle_stats* st);
 int oracle_dense_inv_cholesky(int n, double* A);
 
 /* oracle_te_inverse with the inverse route chosen (0 LU, 1 Cholesky). */
-int oracle_te_inverse_route(int n, double* Z, double lambda, int route, oracle_stats* st);
+int oracle_te_inverse_route(int n, double* Z, double lambda, int route, oracle_stats* st, int swap_products);
 
 /* One dense product of the Taylor loop (operator*=, ScaledDenseMatrix.cpp:314-353:
  * row and column scaling of A, dgemm, unscaling): C = A * B, all n*n

@@ -18,7 +18,13 @@
 //     three lanes per term (each a band of three rows of the 9 x 9 block); the
 //     partial sums are added in a fixed order and the block is stored
 //     (subtracted from U on the diagonal, read back and updated for the second
-//     and later chunks).
+//     and later chunks). The self terms Y_o' W_o'^T of the diagonal block (one
+//     per observation of cb, as many as all other terms of a typical block
+//     together) are summed first by all warps over contiguous ranges and added
+//     in warp order.
+// Scenes with few cameras split every column over several CTAs (camera ca's
+// block to CTA (cb - ca) mod parts, in every chunk), so that the grid covers
+// the SMs.
 // No floating-point atomics, no device-to-host round trip: the result is
 // bitwise repeatable and the stage can be captured in a graph. A camera that
 // observes a point more than once gives more than one term per (slot,
@@ -28,14 +34,15 @@
 namespace unc {
 namespace {
 
-constexpr int kSzThreads = 384;       // 12 warps
+constexpr int kSzThreads = 256;       // 8 warps (registers for three steps of records in flight)
 constexpr int kSzWarps = kSzThreads / 32;
 constexpr int kSzChunk = 2048;        // owner observations per chunk, at most
-constexpr int kSzParts = 16384;       // partner list slots per chunk, at most
-constexpr int kSzMaskWords = 16384;   // run-mask words (also the list-slot owners and the camera scan)
+constexpr int kSzParts = 12288;       // partner list slots per chunk, at most
+constexpr int kSzMaskWords = 11776;   // run-mask words (also the list-slot owners and the camera scan)
 constexpr int kSzGroups = 10;         // terms per step of sz_block10 (three lanes each)
 constexpr int kSzSegCap = 512;        // run entries staged per warp at a time
 constexpr unsigned short kNoSlot = 0xFFFF;
+constexpr unsigned short kSelf = 0xFFFE;  // list-slot camera of the owner observation itself
 
 static_assert(kSzMaskWords >= kSchurMaxCams, "the camera scan reuses the mask words");
 static_assert(kSzMaskWords * 2 >= kSzParts, "the list-slot owners (16-bit) reuse the mask words");
@@ -52,24 +59,51 @@ struct SzShared {
     unsigned short* slot_of;      // [C] slot of a camera, kNoSlot when none
     unsigned short* cam_of_slot;  // [C]
     int* tmp;             // [kSzWarps + 4] scan scratch and broadcast words
+    double* self;         // [81] the chunk's self terms of the diagonal block (column-major)
+    double* red;          // [kSzWarps][81 + 81 * kSzGroups] per-warp block sums and group partials
     unsigned* runbuf;     // [kSzWarps][kSzSegCap] staged run entries, one buffer per warp
     int* sb;              // [kSzChunk] start of each observation's point list (aliases runbuf)
     unsigned short* seg;  // [kSzParts] observation of each list slot (aliases mask)
 };
 
+// Shared-memory layout (byte offsets; every array starts 16-byte aligned).
+struct SzOffsets {
+    size_t mask, off, own, part_o, tmp, self, red, runbuf, part_c, slot_of, cam_of_slot, total;
+};
+__host__ __device__ constexpr size_t sz_align(size_t x) { return (x + 15) & ~size_t(15); }
+__host__ __device__ inline SzOffsets sz_offsets(int C) {
+    SzOffsets o{};
+    o.mask = 0;
+    o.off = sz_align(o.mask + sizeof(unsigned) * kSzMaskWords);
+    o.own = sz_align(o.off + sizeof(int) * (kSzChunk + 1));
+    o.part_o = sz_align(o.own + sizeof(int) * kSzChunk);
+    o.tmp = sz_align(o.part_o + sizeof(int) * kSzParts);
+    o.self = sz_align(o.tmp + sizeof(int) * (kSzWarps + 4));
+    o.red = sz_align(o.self + sizeof(double) * 81);
+    o.runbuf = sz_align(o.red + sizeof(double) * kSzWarps * 81 * (1 + kSzGroups));
+    o.part_c = sz_align(o.runbuf + sizeof(unsigned) * kSzWarps * kSzSegCap);
+    o.slot_of = sz_align(o.part_c + sizeof(unsigned short) * kSzParts);
+    o.cam_of_slot = sz_align(o.slot_of + sizeof(unsigned short) * (size_t)C);
+    o.total = sz_align(o.cam_of_slot + sizeof(unsigned short) * (size_t)C);
+    return o;
+}
+
 __device__ __forceinline__ SzShared sz_layout(char* base, int C) {
+    const SzOffsets o = sz_offsets(C);
     SzShared s;
-    s.mask = reinterpret_cast<unsigned*>(base);
-    s.off = reinterpret_cast<int*>(s.mask + kSzMaskWords);
-    s.own = s.off + kSzChunk + 1;
-    s.part_o = s.own + kSzChunk;
-    s.tmp = s.part_o + kSzParts;
-    s.runbuf = reinterpret_cast<unsigned*>(s.tmp + kSzWarps + 4);
+    s.mask = reinterpret_cast<unsigned*>(base + o.mask);
+    s.off = reinterpret_cast<int*>(base + o.off);
+    s.own = reinterpret_cast<int*>(base + o.own);
+    s.part_o = reinterpret_cast<int*>(base + o.part_o);
+    s.tmp = reinterpret_cast<int*>(base + o.tmp);
+    s.self = reinterpret_cast<double*>(base + o.self);
+    s.red = reinterpret_cast<double*>(base + o.red);
+    s.runbuf = reinterpret_cast<unsigned*>(base + o.runbuf);
+    s.part_c = reinterpret_cast<unsigned short*>(base + o.part_c);
+    s.slot_of = reinterpret_cast<unsigned short*>(base + o.slot_of);
+    s.cam_of_slot = reinterpret_cast<unsigned short*>(base + o.cam_of_slot);
     s.sb = reinterpret_cast<int*>(s.runbuf);
     s.seg = reinterpret_cast<unsigned short*>(s.mask);
-    s.part_c = reinterpret_cast<unsigned short*>(s.runbuf + kSzWarps * kSzSegCap);
-    s.slot_of = s.part_c + kSzParts;
-    s.cam_of_slot = s.slot_of + C;
     return s;
 }
 
@@ -109,44 +143,36 @@ __device__ int sz_scan(int* a, int n, int* tmp) {
     return total;
 }
 
-// One block, ten terms per step: lanes 3g .. 3g+2 (g = 0..9) take the g-th
-// term of the step, lane band r3 = lane % 3 owns rows 3 r3 .. 3 r3 + 2 of the
-// 9 x 9 block and all nine columns. A lane loads its three rows of both
-// records (P = Y_o, partner; O = W_o', owner) and receives the other two
-// bands of O from its group's lanes by shuffles; its columns are kept in
-// rotated band order (band (r3 + k) mod 3 in slot k), so the accumulator
-// indices are compile-time. The run (the observations marked for this slot,
-// in index order, each with its partner entry) is staged in a per-warp
-// buffer, segment by segment; the records of the next step are loaded while
-// the current one is summed. The ten partial sums are added in a fixed tree
-// order (g + 1, g + 2, g + 4, g + 8). Warp-level.
-__device__ void sz_block10(const SzShared& sh, unsigned* buf, int s, int ca, int cb, int W, int u, bool store,
-                           const double* __restrict__ Ws, const double* __restrict__ Ys,
-                           const double* __restrict__ U, double* Z, long ldz) {
-    const int lane = threadIdx.x & 31;
-    const int g = lane / 3;          // term group 0..9 (10: lanes 30, 31, idle)
-    const int r3 = lane - 3 * g;     // row band
-    const bool act = g < kSzGroups;
-    const unsigned* mk = sh.mask + (size_t)s * W;
+// Ten terms per step: lanes 3g .. 3g+2 (g = 0..9) take the g-th term of a
+// step, lane band r3 = lane % 3 owns rows 3 r3 .. 3 r3 + 2 of the 9 x 9 block
+// and all nine columns. A lane loads its three rows of both records (P = Y_o,
+// partner; O = W_o', owner) and receives the other two bands of O from its
+// group's lanes by shuffles; its columns are kept in rotated band order (band
+// (r3 + k) mod 3 in slot k), so the accumulator indices are compile-time. The
+// records of the next two steps are in flight while a step is summed.
+struct SzSteps {
+    int lane, g, r3;
+    bool act;
     double acc[3][3][3];  // [row a][band slot k][row of the band bb]
+
+    __device__ explicit SzSteps(int lane_) : lane(lane_), g(lane_ / 3), r3(lane_ - 3 * (lane_ / 3)) {
+        act = g < kSzGroups;
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
+        for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int k = 0; k < 3; ++k)
+            for (int k = 0; k < 3; ++k)
 #pragma unroll
-            for (int b = 0; b < 3; ++b) acc[a][k][b] = 0.0;
-    auto fetch = [&](int e, int nseg, double (&p)[9], double (&q)[9]) {
-        unsigned v = 0xFFFFFFFFu;
-        if (act && e < nseg) v = buf[e];
-        const bool ok = v != 0xFFFFFFFFu;
-        const int o = ok ? sh.part_o[v & 0xFFFFu] : 0, o2 = ok ? sh.own[v >> 16] : 0;
+                for (int b = 0; b < 3; ++b) acc[a][k][b] = 0.0;
+    }
+    __device__ void load(int o, int o2, bool ok, const double* __restrict__ Ws, const double* __restrict__ Ys,
+                         double (&p)[9], double (&q)[9]) const {
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
             p[k] = ok ? __ldg(Ys + 27L * o + 9 * r3 + k) : 0.0;
             q[k] = ok ? __ldg(Ws + 27L * o2 + 9 * r3 + k) : 0.0;
         }
-    };
-    auto sum_step = [&](const double (&p)[9], const double (&q)[9]) {
+    }
+    __device__ void sum(const double (&p)[9], const double (&q)[9]) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             double ob[9];
@@ -164,7 +190,59 @@ __device__ void sz_block10(const SzShared& sh, unsigned* buf, int s, int ca, int
                     acc[a][k][b] = v;
                 }
         }
-    };
+    }
+    // steps over entries 0 .. n-1; fetch(e, p, q) loads entry e (or zeros past n)
+    template <class F>
+    __device__ void run(int n, F&& fetch) {
+        double p0[9], q0[9], p1[9], q1[9], p2[9], q2[9];
+        fetch(g, p0, q0);
+        fetch(kSzGroups + g, p1, q1);
+        for (int base = 0; base < n; base += 3 * kSzGroups) {
+            fetch(base + 2 * kSzGroups + g, p2, q2);
+            sum(p0, q0);
+            if (base + kSzGroups >= n) break;
+            fetch(base + 3 * kSzGroups + g, p0, q0);
+            sum(p1, q1);
+            if (base + 2 * kSzGroups >= n) break;
+            fetch(base + 4 * kSzGroups + g, p1, q1);
+            sum(p2, q2);
+        }
+    }
+    // the ten partial blocks added in group order into red[0..80] (column-major
+    // element r + 9 q), through the warp's buffer red[81 .. 81 + 810)
+    __device__ void reduce(double* red) const {
+        double* part = red + 81;
+        if (act) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+#pragma unroll
+                    for (int b = 0; b < 3; ++b)
+                        part[81 * g + (3 * r3 + a) + 9 * (3 * ((r3 + k) % 3) + b)] = acc[a][k][b];
+        }
+        __syncwarp();
+        for (int e = lane; e < 81; e += 32) {
+            double v = part[e];
+#pragma unroll
+            for (int q = 1; q < kSzGroups; ++q) v += part[81 * q + e];
+            red[e] = v;
+        }
+        __syncwarp();
+    }
+};
+
+// One block: the terms of slot s (camera ca <= cb) over the chunk, pass u (the
+// (u+1)-th partner of camera ca of each marked observation), then the block
+// stored in both triangles (the diagonal: U minus the terms and the self
+// terms). The run is staged in the warp's buffer segment by segment.
+// Warp-level.
+__device__ void sz_block10(const SzShared& sh, unsigned* buf, double* red, int s, int ca, int cb, int W, int u,
+                           bool store, const double* __restrict__ Ws, const double* __restrict__ Ys,
+                           const double* __restrict__ U, double* Z, long ldz) {
+    const int lane = threadIdx.x & 31;
+    const unsigned* mk = sh.mask + (size_t)s * W;
+    SzSteps st(lane);
     for (int wi = 0; wi < W;) {
         // stage a segment of the run: the marked observations j in order (32
         // mask words per step, a prefix scan of their bit counts gives every
@@ -200,53 +278,58 @@ __device__ void sz_block10(const SzShared& sh, unsigned* buf, int s, int ca, int
             buf[e] = t < t1 ? ((unsigned)t | ((unsigned)j << 16)) : 0xFFFFFFFFu;
         }
         __syncwarp();
-        double pa[9], qa[9], pb[9], qb[9];
-        fetch(g, nseg, pa, qa);
-        for (int base = 0; base < nseg; base += 2 * kSzGroups) {
-            fetch(base + kSzGroups + g, nseg, pb, qb);
-            sum_step(pa, qa);
-            fetch(base + 2 * kSzGroups + g, nseg, pa, qa);
-            if (base + kSzGroups < nseg) sum_step(pb, qb);
-        }
+        st.run(nseg, [&](int e, double (&p)[9], double (&q)[9]) {
+            unsigned v = 0xFFFFFFFFu;
+            if (st.act && e < nseg) v = buf[e];
+            const bool ok = v != 0xFFFFFFFFu;
+            st.load(ok ? sh.part_o[v & 0xFFFFu] : 0, ok ? sh.own[v >> 16] : 0, ok, Ws, Ys, p, q);
+        });
         __syncwarp();  // the buffer is refilled next
     }
-    // the ten partial sums into group 0, in a fixed tree order
-#pragma unroll
-    for (int d = 1; d < 16; d <<= 1) {
-        const bool take = (g % (2 * d)) == 0 && g + d < kSzGroups;
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-#pragma unroll
-                for (int b = 0; b < 3; ++b) {
-                    const double v = __shfl_sync(0xffffffffu, acc[a][k][b], lane + 3 * d);
-                    if (take) acc[a][k][b] += v;
-                }
+    st.reduce(red);
+    for (int e = lane; e < 81; e += 32) {
+        const int r = e % 9, q = e / 9;
+        const double t = ca == cb && u == 0 ? red[e] + sh.self[e] : red[e];
+        if (ca < cb) {
+            const long row = 9L * ca + r, col = 9L * cb + q;
+            double* up = Z + row + col * ldz;
+            const double v = store ? -t : *up - t;
+            *up = v;
+            Z[col + row * ldz] = v;
+        } else if (r <= q) {  // the diagonal block: U minus the terms, kept symmetric
+            const long row = 9L * cb + r, col = 9L * cb + q;
+            double* up = Z + row + col * ldz;
+            const double v = (store ? U[81L * cb + e] : *up) - t;
+            *up = v;
+            Z[col + row * ldz] = v;
+        }
     }
-    if (g != 0) return;
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) {
-                const int r = 3 * r3 + a, q = 3 * ((r3 + k) % 3) + b;
-                const double t = acc[a][k][b];
-                if (ca < cb) {
-                    const long row = 9L * ca + r, col = 9L * cb + q;
-                    double* up = Z + row + col * ldz;
-                    const double v = store ? -t : *up - t;
-                    *up = v;
-                    Z[col + row * ldz] = v;
-                } else if (r <= q) {  // the diagonal block: U minus the terms, kept symmetric
-                    const long row = 9L * cb + r, col = 9L * cb + q;
-                    double* up = Z + row + col * ldz;
-                    const double v = (store ? U[81L * cb + r + 9 * q] : *up) - t;
-                    *up = v;
-                    Z[col + row * ldz] = v;
-                }
-            }
+    __syncwarp();  // red is reused by the next block
+}
+
+// The self terms sum_o' Y_o' W_o'^T of the chunk's observations into sh.self:
+// warp w sums observations [w len / warps, (w+1) len / warps) ten per step,
+// its partial goes to scratch[w] (81 doubles), and the partials are added in
+// warp order. Block-level.
+__device__ void sz_self(const SzShared& sh, int len, double* scratch, double* red, const double* __restrict__ Ws,
+                        const double* __restrict__ Ys) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j0 = (int)((long)warp * len / kSzWarps), j1 = (int)((long)(warp + 1) * len / kSzWarps);
+    SzSteps st(lane);
+    st.run(j1 - j0, [&](int e, double (&p)[9], double (&q)[9]) {
+        const bool ok = st.act && e < j1 - j0;
+        const int o = ok ? sh.own[j0 + e] : 0;
+        st.load(o, o, ok, Ws, Ys, p, q);
+    });
+    st.reduce(red);
+    for (int e = lane; e < 81; e += 32) scratch[81 * warp + e] = red[e];
+    __syncthreads();
+    if (threadIdx.x < 81) {
+        double v = scratch[threadIdx.x];
+        for (int w = 1; w < kSzWarps; ++w) v += scratch[81 * w + threadIdx.x];
+        sh.self[threadIdx.x] = v;
+    }
+    __syncthreads();
 }
 
 // The terms of the partners of rank u (their camera's (u+1)-th observation of
@@ -280,10 +363,11 @@ __global__ void __launch_bounds__(kSzThreads, 1)
     k_schur_columns(int C, const int* __restrict__ cam_ptr, const int* __restrict__ cam_obs,
                     const int* __restrict__ obs_pt, const int* __restrict__ pt_ptr, const int* __restrict__ pt_obs,
                     const int* __restrict__ obs_cam, const double* __restrict__ Ws, const double* __restrict__ Ys,
-                    const double* __restrict__ U, double* Z, long ldz, int* err) {
+                    const double* __restrict__ U, double* Z, long ldz, int* err, int parts) {
     extern __shared__ __align__(16) char sz_smem[];
     const SzShared sh = sz_layout(sz_smem, C);
-    const int cb = C - 1 - (int)blockIdx.x;  // the most partners (cameras <= cb) first
+    const int cb = C - 1 - (int)(blockIdx.x / parts);  // the most partners (cameras <= cb) first
+    const int part = (int)(blockIdx.x % parts);        // this CTA's share of the column's slots
     const int base = cam_ptr[cb], n = cam_ptr[cb + 1] - base;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (n == 0) {  // no observations: the diagonal block is U alone
@@ -352,12 +436,14 @@ __global__ void __launch_bounds__(kSzThreads, 1)
             for (int q = 0; q < 8; ++q) {
                 const int k = i + q * kSzThreads;
                 if (k < E) {
+                    const bool self = o[q] == sh.own[sh.seg[k]];
                     sh.part_o[k] = o[q];
-                    sh.part_c[k] = (unsigned short)c[q];
-                    if (c[q] <= cb) sh.slot_of[c[q]] = 0;
+                    sh.part_c[k] = self ? kSelf : (unsigned short)c[q];
+                    if (!self && c[q] <= cb) sh.slot_of[c[q]] = 0;
                 }
             }
         }
+        if (tid == 0) sh.slot_of[cb] = 0;  // the diagonal block always has a slot (its self terms)
         __syncthreads();
         int K = 0, W = 0;
         for (;;) {
@@ -373,6 +459,7 @@ __global__ void __launch_bounds__(kSzThreads, 1)
             __syncthreads();
             for (int i = tid; i < sh.off[len]; i += kSzThreads)
                 if (sh.part_c[i] <= cb) sh.slot_of[sh.part_c[i]] = 0;
+            if (tid == 0) sh.slot_of[cb] = 0;
             __syncthreads();
         }
         {
@@ -385,16 +472,22 @@ __global__ void __launch_bounds__(kSzThreads, 1)
                 }
         }
         __syncthreads();
+        if (part == 0)  // before the masks (its scratch is their words)
+            sz_self(sh, len, reinterpret_cast<double*>(sh.mask), sh.red + warp * 81 * (1 + kSzGroups), Ws, Ys);
         for (int u = 0;; ++u) {
             const bool more = sz_masks(sh, cb, len, K, W, u);
             if (tid == 0) sh.tmp[kSzWarps + 1] = 0;  // slot cursor: warps take slots as they finish
             __syncthreads();
-            for (;;) {
-                int s = 0;
-                if (lane == 0) s = atomicAdd(sh.tmp + kSzWarps + 1, 1);
-                s = __shfl_sync(0xffffffffu, s, 0);
-                if (s >= K) break;
-                sz_block10(sh, sh.runbuf + warp * kSzSegCap, s, sh.cam_of_slot[s], cb, W, u, j0 == 0 && u == 0,
+            for (;;) {  // this CTA's blocks: cameras ca with (cb - ca) mod parts == part, the same in
+                        // every chunk (slot numbers are not), so no block is updated by two CTAs
+                int q = 0;
+                if (lane == 0) q = atomicAdd(sh.tmp + kSzWarps + 1, 1);
+                q = __shfl_sync(0xffffffffu, q, 0);
+                const int s = K - 1 - q;
+                if (s < 0) break;
+                if ((cb - sh.cam_of_slot[s]) % parts != part) continue;
+                sz_block10(sh, sh.runbuf + warp * kSzSegCap, sh.red + warp * 81 * (1 + kSzGroups), s,
+                           sh.cam_of_slot[s], cb, W, u, j0 == 0 && u == 0,
                            Ws, Ys, U, Z, ldz);
             }
             __syncthreads();
@@ -408,11 +501,7 @@ __global__ void __launch_bounds__(kSzThreads, 1)
 
 }  // namespace
 
-size_t schur_columns_smem(int C) {
-    return (size_t)kSzMaskWords * 4 + (size_t)(kSzChunk + 1) * 4 + (size_t)kSzChunk * 4 + (size_t)kSzParts * 4 +
-           (size_t)(kSzWarps + 4) * 4 + (size_t)kSzWarps * kSzSegCap * 4 + (size_t)kSzParts * 2 +
-           2 * (size_t)C * 2 + 16;
-}
+size_t schur_columns_smem(int C) { return sz_offsets(C).total; }
 
 void prepare_schur_columns() {
     static std::atomic<unsigned long long> attr{0};
@@ -428,8 +517,10 @@ int launch_schur_columns(const SceneDev& s, double* Z, int ldz, cudaStream_t st)
     if (C > kSchurMaxCams) return UNC_ERR_TOO_LARGE;
     const size_t smem = schur_columns_smem(C);
     prepare_schur_columns();
-    k_schur_columns<<<C, kSzThreads, smem, st>>>(C, s.cam_ptr, s.cam_obs, s.obs_pt, s.pt_ptr, s.pt_obs, s.obs_cam,
-                                                 s.Ws, s.Ys, s.Ucam, Z, ldz, s.err);
+    // few cameras: split every column so that the grid covers about two waves of SMs
+    const int parts = std::max(1, std::min(8, (2 * device_sms() + C - 1) / C));
+    k_schur_columns<<<C * parts, kSzThreads, smem, st>>>(C, s.cam_ptr, s.cam_obs, s.obs_pt, s.pt_ptr, s.pt_obs, s.obs_cam,
+                                                 s.Ws, s.Ys, s.Ucam, Z, ldz, s.err, parts);
     count_launch();
     return UNC_OK;
 }
