@@ -1,7 +1,7 @@
 // dense.cu - FP64 dense kernels for the inverse of the camera Schur
 // complement (sm_100a):
 //   * gemm_f64      : C = alpha*A*B + beta*C on DMMA (mma.sync m8n8k4 f64),
-//                     4-stage cp.async pipeline, optional fused max|C| for the
+//                     3-stage cp.async pipeline of 32-deep K tiles, optional fused max|C| for the
 //                     Taylor stop rule (ScaledDenseMatrix.cpp:207-216,314-353),
 //                     lower-tile and triangular-operand (k range per tile) modes.
 //   * chol_inverse  : SPD inverse by recursive Cholesky that forms T = L^{-1}
@@ -20,8 +20,8 @@ namespace unc {
 // GEMM
 // ------------------------------------------------------------------------
 namespace {
-constexpr int BK = 16, STAGES = 4, GEMM_THREADS = 256;
-constexpr int LDB_S = BK + 4;  // Bs[n][k]: 20 doubles per n row (conflict-free fragment reads)
+constexpr int BK = 32, STAGES = 3, GEMM_THREADS = 256;  // 32-deep K stages: half the barriers of 16
+constexpr int LDB_S = BK + 4;  // Bs[n][k]: 36 doubles per n row (8 mod 32 banks: conflict-free fragment reads)
 
 // Output tile BM x BN computed by 8 warps of WM x WN (FM x FN fragments of
 // the 8 x 8 DMMA result). Shared-memory rows of A (and of the transposed B)
@@ -43,8 +43,8 @@ struct GemmCfg {
     static constexpr int A_CHUNKS = BM * BK / 2 / GEMM_THREADS;  // 16-byte copies per thread
     static constexpr int B_CHUNKS = BN * BK / 2 / GEMM_THREADS;
 };
-using CfgBig = GemmCfg<128, 128, 32, 64>;   // 1 CTA per SM (150 KB shared)
-using CfgSmall = GemmCfg<64, 64, 16, 32>;   // small outputs: 4x the CTAs (76 KB shared)
+using CfgBig = GemmCfg<128, 128, 32, 64>;   // 1 CTA per SM (212 KB shared)
+using CfgSmall = GemmCfg<64, 64, 16, 32>;   // small outputs: 4x the CTAs (108 KB shared, 2 per SM)
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
     unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -96,7 +96,7 @@ __device__ __forceinline__ void load_tiles(double* As, double* Bs, const double*
 #pragma unroll
         for (int q = 0; q < Cfg::B_CHUNKS; ++q) {
             int idx = tid + q * GEMM_THREADS;
-            int n = idx >> 3, k2 = (idx & 7) * 2;
+            int n = idx / (BK / 2), k2 = (idx % (BK / 2)) * 2;
             bool p = (n0 + n < N) && (k0 + k2 < K);
             const double* src = p ? B + (k0 + k2) + (long)(n0 + n) * ldb : B;
             cp_async16(Bs + n * LDB_S + k2, src, p);
