@@ -526,8 +526,8 @@ void launch_point_blocks(const SceneDev& s, cudaStream_t st) {
 // W_o = Jc^T Jp scaled by the column norms and Y_o = W_o iV_p (the
 // camera-point block of Y = W * iV, compute.cpp:108), one camera tile per CTA.
 // One thread per observation computes its two 9 x 3 blocks into shared memory
-// (odd record stride 27: conflict-free); warps then write whole 216-byte
-// records.
+// (odd record stride 27: conflict-free); the block then writes them out as
+// 216-byte records, consecutive threads on consecutive elements.
 constexpr size_t kObsTileSmem = 2ul * kObsTile * 27 * sizeof(double);  // 110,592 bytes
 
 __global__ void __launch_bounds__(kObsTile) k_camera_obs_tiles(
@@ -579,13 +579,14 @@ __global__ void __launch_bounds__(kObsTile) k_camera_obs_tiles(
         }
     }
     __syncthreads();
-    const int warp = t >> 5, lane = t & 31;
-    if (lane < 27)
-        for (int i = warp; i < n; i += kObsTile / 32) {
-            const long o = so[i];
-            Ws[27 * o + lane] = sw[27 * i + lane];
-            Ys[27 * o + lane] = sy[27 * i + lane];
-        }
+    // write-out over the flattened (record, element) index: consecutive threads take consecutive
+    // elements of a record and then the next record, so every store instruction covers 256 bytes
+    for (int idx = t; idx < n * 27; idx += kObsTile) {
+        const int i = idx / 27, e = idx - 27 * i;
+        const long o = so[i];
+        Ws[27 * o + e] = sw[idx];
+        Ys[27 * o + e] = sy[idx];
+    }
 }
 
 void launch_obs_blocks(const SceneDev& s, cudaStream_t st) {
