@@ -57,7 +57,21 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+// Accumulation. By default the products accumulate in the MMA's own C
+// operand over the whole k range. With GEMM_SHORT_ACC they accumulate there
+// over two 8 x 8 x 4 steps only (k = 8), starting from zero, and those partial
+// sums are added to the running sums with ordinary FP64 additions (IEEE
+// round to nearest): accumulating in the C operand over the thousands of
+// steps of a long dot product carried a one-sided rounding into the SPD
+// inverse's Cholesky pivots (the last ones are ~lambda, formed by cancellation
+// from O(1) entries, and set the inverse's largest, gauge, components), so the
+// products that feed pivots (L21 = A21 T11^T and A22 -= L21 L21^T) take it.
+__device__ __forceinline__ void dmma0(double& t0, double& t1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%4,%4};\n"
+                 : "=d"(t0), "=d"(t1)
+                 : "d"(a), "d"(b), "d"(0.0));
+}
+__device__ __forceinline__ void dmma_acc(double& d0, double& d1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                  : "+d"(d0), "+d"(d1)
                  : "d"(a), "d"(b));
@@ -104,7 +118,7 @@ __device__ __forceinline__ void load_tiles(double* As, double* Bs, const double*
     }
 }
 
-template <class Cfg, bool kTransB>
+template <class Cfg, bool kTransB, bool kShortAcc>
 __global__ void __launch_bounds__(GEMM_THREADS, (Cfg::BM == 128 ? 1 : 2))
     k_gemm_f64(int M, int N, int K, double alpha, const double* __restrict__ A, long lda,
                const double* __restrict__ B, long ldb, double beta, double* C, long ldc,
@@ -162,18 +176,51 @@ __global__ void __launch_bounds__(GEMM_THREADS, (Cfg::BM == 128 ? 1 : 2))
         const double* as = As + (kt % STAGES) * Cfg::A_STAGE;
         const double* bs = Bs + (kt % STAGES) * Cfg::B_STAGE;
         if (!wact) continue;  // this warp's sub-tile lies outside C
+        if (kShortAcc) {
+#pragma unroll 1
+            for (int kk = 0; kk < BK; kk += 8) {  // two 4-deep steps: a partial sum from zero, then added
+                double af[2][FM], bf[2][FN];
 #pragma unroll
-        for (int kk = 0; kk < BK; kk += 4) {
-            double af[FM], bf[FN];
+                for (int h = 0; h < 2; ++h) {
 #pragma unroll
-            for (int i = 0; i < FM; ++i) af[i] = as[(kk + t) * Cfg::LDA_S + wm + i * 8 + g];
+                    for (int i = 0; i < FM; ++i) af[h][i] = as[(kk + 4 * h + t) * Cfg::LDA_S + wm + i * 8 + g];
 #pragma unroll
-            for (int j = 0; j < FN; ++j)
-                bf[j] = kTransB ? bs[(kk + t) * Cfg::LDBT_S + wn + j * 8 + g] : bs[(wn + j * 8 + g) * LDB_S + kk + t];
+                    for (int j = 0; j < FN; ++j)
+                        bf[h][j] = kTransB ? bs[(kk + 4 * h + t) * Cfg::LDBT_S + wn + j * 8 + g]
+                                           : bs[(wn + j * 8 + g) * LDB_S + kk + 4 * h + t];
+                }
+                constexpr int FH = FN >= 8 ? FN / 2 : FN;  // fragments per group (register pressure)
 #pragma unroll
-            for (int i = 0; i < FM; ++i)
+                for (int i = 0; i < FM; ++i)  // FH partial sums at a time, then added
 #pragma unroll
-                for (int j = 0; j < FN; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+                    for (int j0 = 0; j0 < FN; j0 += FH) {
+                        double p[FH][2];
+#pragma unroll
+                        for (int j = 0; j < FH; ++j) dmma0(p[j][0], p[j][1], af[0][i], bf[0][j0 + j]);
+#pragma unroll
+                        for (int j = 0; j < FH; ++j) dmma_acc(p[j][0], p[j][1], af[1][i], bf[1][j0 + j]);
+#pragma unroll
+                        for (int j = 0; j < FH; ++j) {
+                            acc[i][j0 + j][0] += p[j][0];
+                            acc[i][j0 + j][1] += p[j][1];
+                        }
+                    }
+            }
+        } else {
+#pragma unroll
+            for (int kk = 0; kk < BK; kk += 4) {
+                double af[FM], bf[FN];
+#pragma unroll
+                for (int i = 0; i < FM; ++i) af[i] = as[(kk + t) * Cfg::LDA_S + wm + i * 8 + g];
+#pragma unroll
+                for (int j = 0; j < FN; ++j)
+                    bf[j] = kTransB ? bs[(kk + t) * Cfg::LDBT_S + wn + j * 8 + g]
+                                    : bs[(wn + j * 8 + g) * LDB_S + kk + t];
+#pragma unroll
+                for (int i = 0; i < FM; ++i)
+#pragma unroll
+                    for (int j = 0; j < FN; ++j) dmma_acc(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+            }
         }
     }
     cp_async_wait<0>();
@@ -268,9 +315,13 @@ template <class Cfg>
 void gemm_attr() {
     static std::atomic<unsigned long long> attr{0};
     once_per_device(attr, [] {
-        return cudaFuncSetAttribute(k_gemm_f64<Cfg, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        return cudaFuncSetAttribute(k_gemm_f64<Cfg, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)Cfg::SMEM) == cudaSuccess &&
-               cudaFuncSetAttribute(k_gemm_f64<Cfg, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+               cudaFuncSetAttribute(k_gemm_f64<Cfg, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)Cfg::SMEM) == cudaSuccess &&
+               cudaFuncSetAttribute(k_gemm_f64<Cfg, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)Cfg::SMEM) == cudaSuccess &&
+               cudaFuncSetAttribute(k_gemm_f64<Cfg, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)Cfg::SMEM) == cudaSuccess;
     });
 }
@@ -295,12 +346,11 @@ void launch_gemm(int M, int N, int K, double alpha, const double* A, int lda, co
     }
     double* part = splits > 1 ? ws : nullptr;
     grid.z = splits;
-    if (mode & GEMM_TRANS_B)
-        k_gemm_f64<Cfg, true><<<grid, GEMM_THREADS, Cfg::SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
-                                                                     ldc, amax, mode, part, skip);
-    else
-        k_gemm_f64<Cfg, false><<<grid, GEMM_THREADS, Cfg::SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
-                                                                      ldc, amax, mode, part, skip);
+    const bool tb = (mode & GEMM_TRANS_B) != 0, sa = (mode & GEMM_SHORT_ACC) != 0;
+    auto kern = tb ? (sa ? k_gemm_f64<Cfg, true, true> : k_gemm_f64<Cfg, true, false>)
+                   : (sa ? k_gemm_f64<Cfg, false, true> : k_gemm_f64<Cfg, false, false>);
+    kern<<<grid, GEMM_THREADS, Cfg::SMEM, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, amax, mode, part,
+                                                skip);
     count_launch();
     if (part) {
         const long total = (long)M * N;
@@ -427,10 +477,10 @@ void chol_rec(double* A, int lda, double* T, double* W, double* ws, size_t wsd, 
     chol_rec(A, lda, T, W, ws, wsd, r0, m, err, st);
     double* A21 = A + m + (long)r0 * lda;
     const double* T11 = T + r0 + (long)r0 * lda;
-    gemm_f64_mode(h2, h1, h1, 1.0, A21, lda, T11, lda, 0.0, W, lda, nullptr, GEMM_TRANS_B | GEMM_KHI_N, st, ws,
-                  wsd);
+    gemm_f64_mode(h2, h1, h1, 1.0, A21, lda, T11, lda, 0.0, W, lda, nullptr,
+                  GEMM_TRANS_B | GEMM_KHI_N | GEMM_SHORT_ACC, st, ws, wsd);
     gemm_f64_mode(h2, h2, h1, -1.0, W, lda, W, lda, 1.0, A + m + (long)m * lda, lda, nullptr,
-                  GEMM_TRANS_B | GEMM_LOWER, st, ws, wsd);
+                  GEMM_TRANS_B | GEMM_LOWER | GEMM_SHORT_ACC, st, ws, wsd);
     gemm_f64_mode(h2, h1, h1, 1.0, W, lda, T11, lda, 0.0, A21, lda, nullptr, GEMM_KLO_N, st, ws, wsd);
     chol_rec(A, lda, T, W, ws, wsd, m, r1, err, st);
     gemm_f64_mode(h2, h1, h2, -1.0, T + m + (long)m * lda, lda, A21, lda, 0.0, T + m + (long)r0 * lda, lda,

@@ -150,6 +150,8 @@ enum : int {
     GEMM_KHI_M = 16,
     GEMM_KHI_N = 32,
     GEMM_MIRROR = 64,  // symmetric C: write the lower triangle at (i, j) and (j, i), nothing above it directly
+    GEMM_SHORT_ACC = 128,  // partial sums over k = 8 from zero, added with ordinary FP64 additions (the
+                           // products that feed Cholesky pivots: see k_gemm_f64)
 };
 // ws (ws_doubles): optional scratch that enables split-K for outputs with
 // fewer tiles than SMs (partials summed in a fixed order by a second kernel).
