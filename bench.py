@@ -32,6 +32,7 @@ N GPUs run N independent replicas (scaling "weak"); value = N*K / max time.
 from __future__ import annotations
 
 import argparse
+import collections
 import json
 import os
 import re
@@ -795,7 +796,7 @@ def run_batch(a):
             "grouped": {"scenes_per_s_end_to_end": n / t_b, "seconds_end_to_end": t_b,
                         "device_seconds": t_dev, "scenes_per_s_device": n / t_dev if t_dev > 0 else None,
                         "h2d_seconds": float(np.median(h2d)), "d2h_seconds": float(np.median(d2h)),
-                        "grouped_scenes": tuned["grouped_scenes"], "tile_n_autotuned": tuned["tile_n"],
+                        "grouped_scenes": tuned["grouped_scenes"], "tile_n": tuned["tile_n"],
                         "gpu_launches_per_batch": int(launches),
                         "per_scene_completion_ms": 1e3 * t_b,
                         "note": "every scene of a batch completes with the batch (one launch sequence)"},
@@ -862,7 +863,9 @@ def serve_stream(local, requests, rate, pool, inflight, seed, precisions=("mixed
         if sampler:
             sampler.start()
             sampler.mark(True)
-        ids, late = [], 0
+        # results are collected as they finish (a request's host arrays live until
+        # then; 10k distinct scenes do not fit in host memory together)
+        outstanding, out, late = collections.deque(), [], 0
         h2d = d2h = 0
         t0 = time.perf_counter()
         due = t0
@@ -874,10 +877,18 @@ def serve_stream(local, requests, rate, pool, inflight, seed, precisions=("mixed
                 time.sleep(wait)
             elif wait < -0.05:
                 late += 1
-            ids.append(srv.submit(j, precision=prec))
+            outstanding.append((srv.submit(j, precision=prec), j.num_cams))
             h2d += j.values.nbytes + j.cols.nbytes + j.rows.nbytes
             d2h += 8 * (45 * j.num_cams + 6 * j.num_points)
-        out = [srv.wait(i) for i in ids]
+            del j
+            while outstanding:
+                r = srv.poll(outstanding[0][0]) if len(outstanding) <= 256 else srv.wait(outstanding[0][0])
+                if r is None:
+                    break
+                out.append((r[3], r[4], outstanding.popleft()[1]))
+        while outstanding:
+            r = srv.wait(outstanding[0][0])
+            out.append((r[3], r[4], outstanding.popleft()[1]))
         t1 = time.perf_counter()
         if stream:
             stream.close()
@@ -885,8 +896,14 @@ def serve_stream(local, requests, rate, pool, inflight, seed, precisions=("mixed
             sampler.mark(False)
             clk = sampler.stop()
         srv.close()
-        lat, que = [o[3] for o in out], [o[4] for o in out]
+        lat, que, cams = [o[0] for o in out], [o[1] for o in out], np.array([o[2] for o in out])
+        by_cams = {}
+        for lo, hi in ((8, 100), (100, 400), (400, 1000), (1000, 3001)):
+            sel = [x for x, c in zip(lat, cams) if lo <= c < hi]
+            if sel:
+                by_cams[f"cams {lo}-{hi - 1}"] = {"requests": len(sel), **_dist_ms(sel)}
         res[prec] = {"latency_ms": _dist_ms(lat), "queue_ms": _dist_ms(que),
+                     "latency_ms_by_cams": by_cams,
                      "throughput_req_s": requests / (t1 - t0), "seconds": t1 - t0,
                      "submitted_late": late}
     out = {"requests": requests, "rate_req_s": rate, "inflight": inflight,

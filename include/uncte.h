@@ -264,6 +264,10 @@ int unc_batch_last_timing(const unc_batch* batch, double* h2d_s, double* device_
  * next call allocates again). */
 long long unc_batch_device_bytes(const unc_batch* batch);
 int unc_batch_release(unc_batch* batch);
+/* Product tile width of the 5-slice grouped products: 0 (default) picks 64 or
+ * 96 by a cost model of the tiles on the SMs; 64 or 96 force it. Results do
+ * not depend on it (bitwise). */
+int unc_batch_set_tile_width(unc_batch* batch, int tile_n);
 
 /* SDM::inv (src/uncertaintyTE/ScaledDenseMatrix.cpp:232-279) for a
  * symmetric positive-definite n x n matrix in device memory (column-major,
@@ -343,6 +347,14 @@ int unc_gemm_f64_device(int M, int N, int K, double alpha, const double* d_A, in
  * Scratch is allocated per call. */
 int unc_gemm_mixed_device(int n, const double* d_P, const double* d_X, int ld, double* d_C, int slices,
                           void* stream);
+/* A = T^T T (n x n, column-major, leading dimension ld for both) for a lower
+ * triangular T (zero above the diagonal) on the tensor cores: the columns of
+ * T split into 7 int8 slices, lower 128 x 64 tiles whose k loops start at the
+ * tile's first nonzero row, the result written in both triangles (per term an
+ * error of about 2^-50 of the two columns' maxima, zero-mean). The last product of the mixed
+ * modes' SPD inverse above N = 3584 (A^{-1} = L^{-T} L^{-1}). Scratch is
+ * allocated per call. */
+int unc_gram_lower_mixed_device(int n, const double* d_T, int ld, double* d_A, void* stream);
 
 /* Human-readable name of a status code, and the last error message of the
  * calling thread (empty when none). */

@@ -4,10 +4,10 @@ A batch runs the sparse stages of its scenes as parallel branches, the dense
 stage grouped across scenes (one persistent tile-task inverse over every
 scene's tasks, one launch per Taylor step over all product tiles), is
 captured in a CUDA graph when its shape repeats, and picks its product tile
-width by timing. None of that may change a single bit of any scene's result:
-each scene must equal unc_compute on that scene alone, bitwise, on the first
-call (direct, with the tile-width trials), the second (captured) and the third
-(replayed)."""
+width by a cost model. None of that may change a single bit of any scene's
+result: each scene must equal unc_compute on that scene alone, bitwise, on the
+first call (direct), the second (captured) and the third (replayed), and with
+either tile width forced."""
 import numpy as np
 import pytest
 
@@ -28,17 +28,19 @@ def _alone(jacs, precision):
     return out
 
 
-def test_batch_bitwise_equal_to_per_scene_path_over_three_calls():
+def test_batch_bitwise_equal_to_per_scene_path_over_calls_and_tile_widths():
     jacs = _scenes()
     precs = ["mixed"] * len(jacs)
     precs[3] = "mixed4"   # a second grouped slice count
     precs[5] = "fp64"     # outside the grouped path: computed per scene in the same call
     ref = _alone(jacs, precs)
     b = native.Batch()
-    for call in range(3):
+    for call, width in enumerate([0, 0, 0, 64, 96]):
+        b.set_tile_width(width)
         got = b.compute(jacs, precision=precs)
         t = b.last_timing()
         assert t["grouped_scenes"] == len(jacs) - 1
+        assert t["tile_n"] in (64, 96) and (width == 0 or t["tile_n"] == width)
         for k, ((c0, p0, s0), (c1, p1, s1, status)) in enumerate(zip(ref, got)):
             assert status == 0, (call, k, status)
             np.testing.assert_array_equal(c0, c1, err_msg=f"call {call} scene {k}")

@@ -74,3 +74,47 @@ def test_mixed_gemm_vs_torch(n, slices, tol):
     ref = (P @ X).T  # column-major C read row-major by torch
     rel = ((C - ref).norm() / ref.norm()).item()
     assert rel < tol, rel
+
+
+def _lower_factor_inverse(n, seed, cond):
+    """T = L^-1 of a Jacobi-equilibrated SPD matrix with eigenvalues spread over `cond`."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    Q, _ = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g))
+    ev = torch.logspace(0, -float(np.log10(cond)), n, dtype=torch.float64, device="cuda")
+    A = (Q * ev) @ Q.T
+    d = A.diagonal().rsqrt()
+    A = A * d[:, None] * d[None, :]
+    L = torch.linalg.cholesky(A)
+    return torch.linalg.solve_triangular(L, torch.eye(n, dtype=torch.float64, device="cuda"), upper=False)
+
+
+@pytest.mark.parametrize("n,kind", [(1, "rand"), (70, "rand"), (130, "rand"), (1000, "factor"),
+                                    (3701, "factor"), (4100, "rand")])
+def test_mixed_gram_lower_vs_torch(n, kind):
+    """A = T^T T of a lower-triangular T from 7 int8 slices (the mixed inverse's last
+    product), against torch FP64. The slicing's error per term is about 2^-50 of
+    the product of the two columns' maxima and zero-mean: every element within
+    2e-11 of that scale, and the diagonal (sums of squares, where a dropped
+    squared digit would add up with one sign over K) without a bias: the mean
+    signed error of the diagonal over its scale below 1e-12."""
+    import torch
+    if kind == "rand":
+        g = torch.Generator(device="cuda").manual_seed(n)
+        T = torch.tril(torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g))
+    else:
+        T = _lower_factor_inverse(n, n, 1e8)
+    M = T.T.contiguous()  # memory of the column-major T
+    A = torch.full((n, n), float("nan"), dtype=torch.float64, device="cuda")
+    native.gram_lower_mixed_device(n, M.data_ptr(), n, A.data_ptr())
+    torch.cuda.synchronize()
+    ref = T.T @ T
+    m = T.abs().amax(dim=0)  # column maxima of T
+    scale = m[:, None] * m[None, :]
+    err = ((A - ref).abs() / scale).max().item()
+    bias = ((A - ref).diagonal() / scale.diagonal()).mean().item()
+    assert torch.isfinite(A).all()
+    assert torch.equal(A, A.T)  # both triangles written, bitwise symmetric
+    assert err < 2e-11, err
+    assert abs(bias) < 1e-12, bias
+

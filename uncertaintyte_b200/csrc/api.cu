@@ -495,6 +495,11 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     // k = lambda^i / factorial(i-1) is evaluated here (32-bit factorial wrap).
     // moderate sizes: the tile-task inverse (one persistent kernel); larger: the recursive form
     const bool tasks = spd_tasks_apply(N);
+    // mixed modes, recursive inverse: its last product T^T T on the int8 path, in the
+    // first two slice buffers (free until the Taylor stage) and the first exponent array
+    const size_t slice_region = mixed ? (size_t)nbuf * ((mixed_slice_bytes(N, slices) + 255) & ~size_t(255)) : 0;
+    const bool gram = mixed && !tasks && mixed_gram_bytes(N) <= slice_region;
+    int* gram_exps = mixed ? opa[kX].exps : nullptr;
     if (tasks)
         if (int r = spd_tasks_prepare(N)) return fail(r, "tile-task inverse: cannot upload the task list");
     auto inverse_stage = [&]() -> int {
@@ -503,6 +508,14 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
             if (int r = chol_inverse_tasks(b.Z, N, ld, b.iZ, b.add, b.dag_state, s.err, sm, ctx->task_ctas))
                 return r;
             launch_unequilibrate_from(b.add, b.Z, N, ld, b.e, b.iZ, sm);  // X in Z, iZ = X
+        } else if (gram) {
+            // mixed: T = L^{-1} in FP64 (its products feed the pivots), A^{-1} = T^T T
+            // from int8 slices of T on the tensor cores
+            chol_lower_inverse(b.Z, N, ld, b.iZ, b.add, b.tmp, s.err, sm);
+            CK(cudaMemsetAsync(ctx->mp, 0, mixed_gram_bytes(N), sm));  // slice padding must be zero
+            if (!mixed_gram_lower_tri(b.iZ, N, ld, reinterpret_cast<int8_t*>(ctx->mp), gram_exps, b.Z, ld, s.err, sm))
+                return fail(UNC_ERR_CUDA, "tensor-map encoding failed");
+            launch_unequilibrate(b.Z, N, ld, b.e, b.iZ, sm);  // X in Z, iZ = X
         } else {
             chol_inverse(b.Z, N, ld, b.iZ, b.add, b.tmp, b.gjws, s.err, sm);
             launch_unequilibrate(b.Z, N, ld, b.e, b.iZ, sm);  // X in Z, iZ = X
@@ -1228,6 +1241,31 @@ int unc_gemm_mixed_device(int n, const double* d_P, const double* d_X, int ld, d
         mixed_gemm(a, b, d_C, ld, nullptr, false, err, sm);
         ce = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, sm);
     }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(sm);
+    cudaFree(ws);
+    if (ce != cudaSuccess) return fail(UNC_ERR_CUDA, cudaGetErrorString(ce));
+    if (h_err & ERRBIT_TIMEOUT) return fail(UNC_ERR_CUDA, "tensor-core pipeline wait timed out");
+    return UNC_OK;
+}
+
+int unc_gram_lower_mixed_device(int n, const double* d_T, int ld, double* d_A, void* stream) {
+    g_last_error.clear();
+    if (n <= 0 || !d_T || !d_A || ld < n) return fail(UNC_ERR_INVALID_ARG, "bad mixed Gram arguments");
+    cudaStream_t sm = (cudaStream_t)stream;
+    const size_t sb = mixed_gram_bytes(n);
+    const size_t total = sb + sizeof(int) * ((size_t)n + 64) + 256;
+    char* ws = nullptr;
+    CK(cudaMalloc(&ws, total));
+    int* ex = reinterpret_cast<int*>(ws + sb);
+    int* err = ex + n + 64;
+    int h_err = 0;
+    cudaError_t ce = cudaMemsetAsync(ws, 0, total, sm);
+    if (ce == cudaSuccess && !mixed_gram_lower_tri(d_T, n, ld, reinterpret_cast<int8_t*>(ws), ex, d_A, ld, err, sm)) {
+        cudaStreamSynchronize(sm);
+        cudaFree(ws);
+        return fail(UNC_ERR_CUDA, "tensor-map encoding failed");
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, sm);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(sm);
     cudaFree(ws);
     if (ce != cudaSuccess) return fail(UNC_ERR_CUDA, cudaGetErrorString(ce));

@@ -18,9 +18,9 @@
 //
 // The sequence for a given batch shape (sizes, fixed points, lambda, buffer
 // addresses) is captured in a CUDA graph the second time the shape is seen and
-// replayed from then on. The product's tile width is chosen by timing the
-// candidates on the first batch of a size class (an autotuner, cached per size
-// class); the products' per-element arithmetic does not depend on it.
+// replayed from then on. The product's tile width (64 or 96 for 5 slices)
+// comes from a cost model of the group's tiles on the SMs; the products'
+// per-element arithmetic does not depend on it.
 // Every grouped kernel performs, per element, exactly the arithmetic of its
 // per-scene counterpart, so each scene's result is bitwise the one
 // unc_compute gives for it alone.
@@ -100,17 +100,17 @@ struct unc_batch {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t branch[kBranches] = {};
-    cudaEvent_t fork = nullptr, join[kBranches] = {}, ev[6] = {};
+    cudaEvent_t fork = nullptr, join[kBranches] = {}, ev[4] = {};
     void* ws = nullptr;
     size_t ws_bytes = 0;
     void* host = nullptr;  // pinned staging: inputs, outputs, descriptors, status words
     size_t host_bytes = 0;
     std::vector<Graph> graphs;
     std::vector<std::vector<unsigned long long>> seen;
-    std::map<std::pair<int, int>, int> tile_choice;  // (slices, size class) -> tile width
     unc_context* single = nullptr;                  // scenes outside the grouped path
     double t_h2d = 0, t_dev = 0, t_d2h = 0;
     int grouped = 0, tile_n = 0;
+    int force_nt = 0;  // unc_batch_set_tile_width: 0 = cost model
 };
 
 namespace {
@@ -151,12 +151,6 @@ void parallel_copy(const std::vector<Copy>& jobs) {
 
 int slices_of(int precision) {
     return precision == UNC_PRECISION_MIXED4 ? 4 : (precision == UNC_PRECISION_MIXED3 ? 3 : 5);
-}
-
-int lower_tile_count(int n, int nt) {
-    std::vector<int4> t;
-    mixed_lower_tiles(0, n, nt, t);
-    return (int)t.size();
 }
 
 // per scene: X (A, B), A operand (A), X^4 (A, B), X^8 (A, B), X^12 (B), X^16 (B), and X^4, X^8, X^12, X^16
@@ -286,7 +280,7 @@ struct GroupRun {
 };
 
 // The launch sequence of a group on b->stream (captured or direct).
-int launch_group(unc_batch* b, GroupRun& g, cudaEvent_t taylor0, cudaEvent_t taylor1) {
+int launch_group(unc_batch* b, GroupRun& g) {
     cudaStream_t sm = b->stream;
     const int n = (int)g.sc.size();
     BCK(cudaEventRecord(b->fork, sm));
@@ -314,7 +308,6 @@ int launch_group(unc_batch* b, GroupRun& g, cudaEvent_t taylor0, cudaEvent_t tay
     int* ctl = reinterpret_cast<int*>(g.dbase + g.L.zero_off + g.L.zero_bytes - 256);
     if (int r = chol_inverse_tasks_grouped(g.dd.mats, g.dd.tasks, (int)g.ntasks, ctl, sm, device_sms())) return r;
     launch_unequilibrate_grouped(g.dd.dense, n, g.dd.blk_elems, g.nblk_elems, sm);  // X in Z, iZ = X
-    if (taylor0) BCK(cudaEventRecord(taylor0, sm));
     // the Taylor series from blocked powers (powers.cu), every step over all scenes
     auto slice = [&](int set) {
         mixed_slice_grouped(g.dd.slice + (size_t)set * n, n, g.dd.row_start, g.total_rows, sm);
@@ -351,7 +344,6 @@ int launch_group(unc_batch* b, GroupRun& g, cudaEvent_t taylor0, cudaEvent_t tay
         slice(6 + q);
         gemm(5 + q);
     }
-    if (taylor1) BCK(cudaEventRecord(taylor1, sm));
     // outputs (compute.cpp:168-183, 370-455)
     BCK(cudaEventRecord(b->fork, sm));
     for (int k = 0; k < kBranches; ++k) BCK(cudaStreamWaitEvent(b->branch[k], b->fork, 0));
@@ -403,12 +395,15 @@ int prepare_group(unc_batch* b, GroupRun& g, int nt) {
     g.h_stat = g.h_desc + g.L.desc_bytes;
     const size_t hneed = g.h_stat + g.L.stat_bytes + 256;
     if (b->host_bytes < hneed) {
+        // grown by half again at least: freeing pinned memory waits for the whole
+        // device (every other stream's work), so a serving worker should rarely do it
+        const size_t want = std::max(hneed, b->host_bytes + b->host_bytes / 2);
         BCK(cudaStreamSynchronize(sm));
         if (b->host) cudaFreeHost(b->host);
         b->host = nullptr;
         b->host_bytes = 0;
-        BCK(cudaMallocHost(&b->host, hneed));
-        b->host_bytes = hneed;
+        BCK(cudaMallocHost(&b->host, want));
+        b->host_bytes = want;
     }
     g.hbase = (char*)b->host;
     // descriptors
@@ -530,8 +525,7 @@ std::vector<unsigned long long> shape_key(const unc_batch* b, const GroupRun& g)
 
 // Run the device part of a group: from the graph of its shape when there is
 // one, else directly (and capture it when the shape was seen before).
-int run_device(unc_batch* b, GroupRun& g, cudaEvent_t taylor0, cudaEvent_t taylor1) {
-    if (taylor0) return launch_group(b, g, taylor0, taylor1);  // timed runs (the autotuner) are not captured
+int run_device(unc_batch* b, GroupRun& g) {
     const auto key = shape_key(b, g);
     for (auto& gr : b->graphs)
         if (gr.key == key) {
@@ -543,7 +537,7 @@ int run_device(unc_batch* b, GroupRun& g, cudaEvent_t taylor0, cudaEvent_t taylo
     if (!again) {
         if (b->seen.size() >= 16) b->seen.erase(b->seen.begin());
         b->seen.push_back(key);
-        return launch_group(b, g, nullptr, nullptr);
+        return launch_group(b, g);
     }
     const long long l0 = g_thread_launches;
     cudaGraph_t graph = nullptr;
@@ -551,7 +545,7 @@ int run_device(unc_batch* b, GroupRun& g, cudaEvent_t taylor0, cudaEvent_t taylo
     bool ok = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
     int rc = UNC_OK;
     if (ok) {
-        rc = launch_group(b, g, nullptr, nullptr);
+        rc = launch_group(b, g);
         ok = cudaStreamEndCapture(b->stream, &graph) == cudaSuccess && rc == UNC_OK && graph;
     }
     if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
@@ -562,7 +556,7 @@ int run_device(unc_batch* b, GroupRun& g, cudaEvent_t taylor0, cudaEvent_t taylo
     if (!ok) {
         cudaGetLastError();
         if (exec) cudaGraphExecDestroy(exec);
-        return launch_group(b, g, nullptr, nullptr);
+        return launch_group(b, g);
     }
     if (b->graphs.size() >= (size_t)kGraphs) {
         cudaGraphExecDestroy(b->graphs.front().exec);
@@ -578,20 +572,14 @@ int run_group(unc_batch* b, GroupRun& g, const int* const* rows, const int* cons
               const double* const* values, double* const* cam_unc, double* const* pt_unc, int* status,
               unc_statistic* stats) {
     cudaStream_t sm = b->stream;
-    // tile width: the size class's cached choice, else time every candidate
-    const std::vector<int> cand = mixed_tile_candidates(g.slices);
-    long tiles96 = 0;
-    for (const Scene& s : g.sc) tiles96 += lower_tile_count(s.pl.N, 96);
-    const int size_class = (int)std::lround(2.0 * std::log2((double)std::max(1L, tiles96)));
-    const auto ck = std::make_pair(g.slices, size_class);
-    auto hit = b->tile_choice.find(ck);
-    // every candidate computes the same bytes; the last one run leaves the results
-    const std::vector<int> trials = hit != b->tile_choice.end() ? std::vector<int>{hit->second} : cand;
-    float best_ms = 0;
-    int best = trials[0];
-    for (size_t t = 0; t < trials.size(); ++t) {
-        if (int r = prepare_group(b, g, trials[t])) return r;
-        // inputs: pack and copy (one transfer)
+    // tile width by the cost model over all the group's tiles (deterministic:
+    // no timed trial runs, so a serving worker never solves a pack twice)
+    std::vector<int> ns;
+    for (const Scene& s : g.sc) ns.push_back(s.pl.N);
+    const int nt = g.slices == 5 && b->force_nt ? b->force_nt : mixed_group_tile_n(g.slices, ns);
+    if (int r = prepare_group(b, g, nt)) return r;
+    // inputs: pack and copy (one transfer)
+    {
         std::vector<Copy> cp;
         for (const Scene& s : g.sc) {
             cp.push_back({g.hbase + g.h_in + s.in_off[0], rows[s.idx], sizeof(int) * ((size_t)s.pl.nobs * 2 + 1)});
@@ -599,27 +587,17 @@ int run_group(unc_batch* b, GroupRun& g, const int* const* rows, const int* cons
             cp.push_back({g.hbase + g.h_in + s.in_off[2], values[s.idx], sizeof(double) * (size_t)s.nnz});
         }
         parallel_copy(cp);
-        BCK(cudaEventRecord(b->ev[0], sm));
-        BCK(cudaMemcpyAsync(g.dbase, g.hbase + g.h_in, g.L.in_bytes, cudaMemcpyHostToDevice, sm));
-        BCK(cudaEventRecord(b->ev[1], sm));
-        const bool timed = trials.size() > 1;
-        if (int r = run_device(b, g, timed ? b->ev[4] : nullptr, timed ? b->ev[5] : nullptr)) return r;
-        BCK(cudaEventRecord(b->ev[2], sm));
-        BCK(cudaMemcpyAsync(g.hbase + g.h_out, g.dbase + g.L.in_bytes, g.L.out_bytes, cudaMemcpyDeviceToHost, sm));
-        BCK(cudaMemcpyAsync(g.hbase + g.h_stat, g.dbase + g.L.stat_off, g.L.stat_bytes, cudaMemcpyDeviceToHost, sm));
-        BCK(cudaEventRecord(b->ev[3], sm));
-        BCK(cudaStreamSynchronize(sm));
-        BCK(cudaGetLastError());
-        if (timed) {
-            float ms = 0;
-            cudaEventElapsedTime(&ms, b->ev[4], b->ev[5]);
-            if (t == 0 || ms < best_ms) {
-                best_ms = ms;
-                best = trials[t];
-            }
-        }
     }
-    if (hit == b->tile_choice.end()) b->tile_choice[ck] = best;
+    BCK(cudaEventRecord(b->ev[0], sm));
+    BCK(cudaMemcpyAsync(g.dbase, g.hbase + g.h_in, g.L.in_bytes, cudaMemcpyHostToDevice, sm));
+    BCK(cudaEventRecord(b->ev[1], sm));
+    if (int r = run_device(b, g)) return r;
+    BCK(cudaEventRecord(b->ev[2], sm));
+    BCK(cudaMemcpyAsync(g.hbase + g.h_out, g.dbase + g.L.in_bytes, g.L.out_bytes, cudaMemcpyDeviceToHost, sm));
+    BCK(cudaMemcpyAsync(g.hbase + g.h_stat, g.dbase + g.L.stat_off, g.L.stat_bytes, cudaMemcpyDeviceToHost, sm));
+    BCK(cudaEventRecord(b->ev[3], sm));
+    BCK(cudaStreamSynchronize(sm));
+    BCK(cudaGetLastError());
     float ms = 0;
     cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
     b->t_h2d += ms * 1e-3;
@@ -690,7 +668,7 @@ int unc_batch_create(int device, unc_batch** out) {
     for (int k = 0; k < kBranches && e == cudaSuccess; ++k) e = cudaStreamCreateWithFlags(&b->branch[k], cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     for (int k = 0; k < kBranches && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming);
-    for (int k = 0; k < 6 && e == cudaSuccess; ++k) e = cudaEventCreate(&b->ev[k]);
+    for (int k = 0; k < 4 && e == cudaSuccess; ++k) e = cudaEventCreate(&b->ev[k]);
     if (e != cudaSuccess) {
         g_last_error = std::string("unc_batch_create: ") + cudaGetErrorString(e);
         unc_batch_destroy(b);
@@ -709,7 +687,7 @@ int unc_batch_destroy(unc_batch* b) {
     if (b->ws) cudaFree(b->ws);
     if (b->host) cudaFreeHost(b->host);
     if (b->single) unc_context_destroy(b->single);
-    for (int k = 0; k < 6; ++k)
+    for (int k = 0; k < 4; ++k)
         if (b->ev[k]) cudaEventDestroy(b->ev[k]);
     for (int k = 0; k < kBranches; ++k) {
         if (b->join[k]) cudaEventDestroy(b->join[k]);
@@ -791,10 +769,21 @@ int unc_batch_release(unc_batch* b) {
     for (auto& g : b->graphs) cudaGraphExecDestroy(g.exec);
     b->graphs.clear();
     b->seen.clear();
-    if (b->ws) BCK(cudaFree(b->ws));
+    // stream-ordered free: a cudaFree would wait for every other stream's work
+    // (a serving process releases idle workspaces while others compute)
+    if (b->ws) BCK(cudaFreeAsync(b->ws, b->stream));
     b->ws = nullptr;
     b->ws_bytes = 0;
+    BCK(cudaStreamSynchronize(b->stream));
     if (b->single) unc_context_release(b->single);
+    return UNC_OK;
+}
+
+int unc_batch_set_tile_width(unc_batch* b, int tile_n) {
+    if (!b) return bfail(UNC_ERR_INVALID_ARG, "batch is NULL");
+    if (tile_n != 0 && tile_n != 64 && tile_n != 96)
+        return bfail(UNC_ERR_INVALID_ARG, "tile_n must be 0 (cost model), 64 or 96");
+    b->force_nt = tile_n;
     return UNC_OK;
 }
 

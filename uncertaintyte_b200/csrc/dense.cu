@@ -488,11 +488,15 @@ void chol_rec(double* A, int lda, double* T, double* W, double* ws, size_t wsd, 
 }
 }  // namespace
 
+void chol_lower_inverse(double* A, int n, int lda, double* T, double* W, double* ws, int* err, cudaStream_t st) {
+    chol_rec(A, lda, T, W, ws, (size_t)n * lda, 0, n, err, st);
+}
+
 void chol_inverse(double* A, int n, int lda, double* T, double* W, double* Tt, double* small, int* err,
                   cudaStream_t st) {
     (void)small;
     // Tt is free until the final product: split-K partial sums of the recursion
-    chol_rec(A, lda, T, W, Tt, (size_t)n * lda, 0, n, err, st);
+    chol_lower_inverse(A, n, lda, T, W, Tt, err, st);
     // A^{-1} = T^T T: lower tiles, k >= the tile's first row (T lower triangular), then mirror
     dim3 g((n + 31) / 32, (n + 31) / 32);
     k_transpose<<<g, dim3(32, 8), 0, st>>>(T, lda, n, Tt, lda);

@@ -172,6 +172,9 @@ void gemm_f64_tri(int M, int N, int K, double alpha, const double* A, int lda, c
 size_t chol_small_doubles(int n);
 void chol_inverse(double* A, int n, int lda, double* T, double* W, double* Tt, double* small, int* err,
                   cudaStream_t st);
+// The recursion of chol_inverse alone: T = L^{-1} (lower triangle; T zero on
+// entry), A overwritten; ws: n x lda doubles of split-K scratch.
+void chol_lower_inverse(double* A, int n, int lda, double* T, double* W, double* ws, int* err, cudaStream_t st);
 // A <- A + lambda*I and symmetric Jacobi equilibration: A_s = E A E, E = diag(A_ii)^-1/2.
 void launch_shift_equilibrate(double* A, int n, int lda, double lambda, double* e, int* err,
                               cudaStream_t st);
@@ -383,8 +386,16 @@ void mixed_slice_grouped(const MixedSliceJob* d_jobs, int njobs, const int* d_ro
                          cudaStream_t st);
 // the lower-triangle 128 x nt tiles of an n x n product, as (job, m0, n0, 0)
 void mixed_lower_tiles(int job, int n, int nt, std::vector<int4>& out);
-// tile widths with a grouped kernel for `slices`: {64, 96} for 5, {128} for 3 and 4
-std::vector<int> mixed_tile_candidates(int slices);
+// tile width of a grouped product over scenes of sizes ns: 128 for up to 4
+// slices; for 5, 64 or 96 by the single-scene cost model over all the tiles
+int mixed_group_tile_n(int slices, const std::vector<int>& ns);
+// A = T^T T (lower tiles, mirrored) for lower-triangular n x n T from
+// kGramSlices int8 slices of T's columns; buf holds mixed_gram_bytes(n) bytes
+// whose padding is zero, exps n + 64 ints. false: tensor-map encoding failed.
+constexpr int kGramSlices = 7;
+size_t mixed_gram_bytes(int n);
+bool mixed_gram_lower_tri(const double* T, int n, int ld, int8_t* buf, int* exps, double* A, int lda, int* err,
+                          cudaStream_t st);
 void mixed_gemm_grouped(int slices, int nt, const MixedGemmJob* d_jobs, const int4* d_tiles, int ntiles,
                         cudaStream_t st);
 // Y, te (optional): Y += te->coef * A while A is sliced, unless te->done.

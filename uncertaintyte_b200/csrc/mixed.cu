@@ -27,6 +27,11 @@
 // accumulators with tcgen05.ld and write FP64. Every mbarrier wait has an
 // iteration limit after which the kernel records ERRBIT_TIMEOUT and unwinds
 // (TMEM is always freed).
+#include <algorithm>
+#include <functional>
+#include <queue>
+#include <vector>
+
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -135,7 +140,10 @@ struct Shape {
     static constexpr int LEVELS = S;                       // L = 2 .. S+1
     static constexpr int GROUP = 256 / NT;                 // B slices per MMA (N <= 256)
     static constexpr int TMEM_COLS = LEVELS * NT <= 256 ? (LEVELS * NT <= 128 ? 128 : 256) : 512;
-    static constexpr int SMEM = STAGES * STAGE + 1024 /*align*/ + 256 /*barriers*/;
+    // three pipeline stages where they fit in the 227 KB of shared memory, else two
+    static constexpr int NSTAGE = STAGES * STAGE + 1280 <= 232448 ? STAGES : 2;
+    static constexpr int SMEM = NSTAGE * STAGE + 1024 /*align*/ + 256 /*barriers*/;
+    static_assert(SMEM <= 232448, "one CTA's shared memory is at most 227 KB");
     static_assert(LEVELS * NT <= 512, "TMEM holds at most 512 accumulator columns");
 };
 
@@ -244,13 +252,13 @@ __device__ __forceinline__ void ozaki_tile(const CUtensorMap* tA, const CUtensor
                                            int kp, int rowsA, int rowsB, const int* __restrict__ eA,
                                            const int* __restrict__ eB, double* C, long ldc,
                                            unsigned long long* amax, int* err, int mirror, bool maps_in_global,
-                                           int accumulate) {
+                                           int accumulate, int klo = 0) {
     using Sh = Shape<NT, S>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * Sh::STAGE);
-    uint64_t* empty = full + STAGES;
-    uint64_t* done = empty + STAGES;
+    uint64_t* full = reinterpret_cast<uint64_t*>(base + Sh::NSTAGE * Sh::STAGE);
+    uint64_t* empty = full + Sh::NSTAGE;
+    uint64_t* done = empty + Sh::NSTAGE;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
@@ -260,7 +268,7 @@ __device__ __forceinline__ void ozaki_tile(const CUtensorMap* tA, const CUtensor
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
     }
     if (tid == 32) {
-        for (int s = 0; s < STAGES; ++s) {
+        for (int s = 0; s < Sh::NSTAGE; ++s) {
             mbar_init(full + s, 1);
             mbar_init(empty + s, 1);
         }
@@ -273,6 +281,10 @@ __device__ __forceinline__ void ozaki_tile(const CUtensorMap* tA, const CUtensor
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = *tmem_slot;
     const int KT = kp / BKB;
+    // klo: both operands are the columns of one lower-triangular matrix T (C = T^T T),
+    // column r being zero above row r, so no term of this tile has k < max(m0, n0)
+    const int kt0 = klo ? (m0 > n0 ? m0 : n0) / BKB : 0;
+    const int kt1 = KT;
 
     if (warp == 0) {
       if (lane == 0) {
@@ -283,32 +295,33 @@ __device__ __forceinline__ void ozaki_tile(const CUtensorMap* tA, const CUtensor
         }
         bool ok = true;
         int issued = 0;
-        for (int kt = 0; kt < KT && ok; ++kt) {
-            const int s = kt % STAGES;
-            const unsigned ph = (unsigned)(kt / STAGES) & 1u;
-            if (kt >= STAGES && !mbar_wait(empty + s, ph ^ 1u)) {
+        for (int kt = kt0; kt < kt1 && ok; ++kt) {
+            const int i = kt - kt0;  // pipeline step
+            const int s = i % Sh::NSTAGE;
+            const unsigned ph = (unsigned)(i / Sh::NSTAGE) & 1u;
+            if (i >= Sh::NSTAGE && !mbar_wait(empty + s, ph ^ 1u)) {
                 atomicOr(err, ERRBIT_TIMEOUT);
                 ok = false;
                 break;
             }
             uint8_t* st = base + s * Sh::STAGE;
             mbar_expect_tx(full + s, Sh::STAGE);
-            for (int i = 0; i < S; ++i) tma_load_2d(st + i * Sh::A_BOX, tA, kt * BKB, i * rowsA + m0, full + s);
-            for (int i = 0; i < S; ++i)
-                tma_load_2d(st + S * Sh::A_BOX + i * Sh::B_BOX, tB, kt * BKB, i * rowsB + n0, full + s);
-            issued = kt + 1;
+            for (int q = 0; q < S; ++q) tma_load_2d(st + q * Sh::A_BOX, tA, kt * BKB, q * rowsA + m0, full + s);
+            for (int q = 0; q < S; ++q)
+                tma_load_2d(st + S * Sh::A_BOX + q * Sh::B_BOX, tB, kt * BKB, q * rowsB + n0, full + s);
+            issued = i + 1;
         }
         // no copy may be in flight when the CTA exits
-        for (int kt = issued - STAGES < 0 ? 0 : issued - STAGES; kt < issued; ++kt)
-            if (!mbar_wait(full + kt % STAGES, (unsigned)(kt / STAGES) & 1u)) atomicOr(err, ERRBIT_TIMEOUT);
+        for (int i = issued - Sh::NSTAGE < 0 ? 0 : issued - Sh::NSTAGE; i < issued; ++i)
+            if (!mbar_wait(full + i % Sh::NSTAGE, (unsigned)(i / Sh::NSTAGE) & 1u)) atomicOr(err, ERRBIT_TIMEOUT);
       }
       __syncwarp();
     } else if (warp == 1) {
       if (lane == 0) {
         // MMA issuer
-        for (int kt = 0; kt < KT; ++kt) {
-            const int s = kt % STAGES;
-            if (!mbar_wait(full + s, (unsigned)(kt / STAGES) & 1u)) {
+        for (int i = 0; i < kt1 - kt0; ++i) {
+            const int s = i % Sh::NSTAGE;
+            if (!mbar_wait(full + s, (unsigned)(i / Sh::NSTAGE) & 1u)) {
                 atomicOr(err, ERRBIT_TIMEOUT);
                 break;
             }
@@ -328,7 +341,7 @@ __device__ __forceinline__ void ozaki_tile(const CUtensorMap* tA, const CUtensor
                         const int l = sa + sb0 - 2;
                         const uint64_t b = desc_sw64(st + S * Sh::A_BOX + (sb0 - 1) * Sh::B_BOX + kk * 32);
                         // the first A slice of the first K step opens every level
-                        mma_i8(tmem + (uint32_t)(l * NT), a, b, idesc_i8(g * NT), kt > 0 || kk > 0 || sa > 1);
+                        mma_i8(tmem + (uint32_t)(l * NT), a, b, idesc_i8(g * NT), i > 0 || kk > 0 || sa > 1);
                     }
                 }
             }
@@ -434,7 +447,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     k_ozaki_gemm(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int M, int N,
                  int kp, int rowsA, int rowsB, const int* __restrict__ eA, const int* __restrict__ eB, double* C,
                  long ldc, unsigned long long* amax, int lower_only, int* err, const int* skip, int mirror,
-                 int accumulate, int group_m) {
+                 int accumulate, int group_m, int klo) {
     if (skip && *skip) return;
     int m0, n0;
     if (group_m > 0) {  // 1-D grid over exactly the lower tiles, grouped order
@@ -449,7 +462,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (lower_only && n0 > m0 + BM - 1) return;
     }
     ozaki_tile<NT, S>(&tA, &tB, m0, n0, M, N, kp, rowsA, rowsB, eA, eB, C, ldc, amax, err, mirror, false,
-                      accumulate);
+                      accumulate, klo);
 }
 
 // The products of many matrices (a batch) in one launch: CTA b computes tile
@@ -522,6 +535,7 @@ void prepare_mixed_kernels() {
     set_attr_once<96, 5>();
     set_attr_once<128, 3>();
     set_attr_once<128, 2>();
+    set_attr_once<64, kGramSlices>();
     set_attr_grouped_once<128, 4>();
     set_attr_grouped_once<64, 5>();
     set_attr_grouped_once<96, 5>();
@@ -624,9 +638,35 @@ void mixed_lower_tiles(int job, int n, int nt, std::vector<int4>& out) {
     }
 }
 
-std::vector<int> mixed_tile_candidates(int slices) {
-    if (slices == 5) return {64, 96};
-    return {128};
+// The single-scene cost model over a group's tiles: each tile costs its
+// K-steps x (tile_n + 16); tiles go, longest first (the grouped launch's
+// order), to whichever of the 148 SMs frees first; the width with the
+// shorter makespan wins (ties: 96, fewer tiles).
+int mixed_group_tile_n(int slices, const std::vector<int>& ns) {
+    if (slices <= 4) return 128;
+    constexpr int kSMs = 148;
+    double span_of[2] = {0, 0};
+    const int widths[2] = {96, 64};
+    for (int w = 0; w < 2; ++w) {
+        const int nt = widths[w];
+        std::vector<double> cost;
+        for (int n : ns) {
+            const double c = (double)((n + BKB - 1) / BKB) * (nt + 16);
+            cost.insert(cost.end(), (size_t)lower_tiles(n, nt), c);
+        }
+        std::sort(cost.begin(), cost.end(), std::greater<double>());
+        std::priority_queue<double, std::vector<double>, std::greater<double>> sm;
+        for (int i = 0; i < kSMs; ++i) sm.push(0.0);
+        double span = 0;
+        for (double c : cost) {
+            const double t = sm.top() + c;
+            sm.pop();
+            sm.push(t);
+            span = std::max(span, t);
+        }
+        span_of[w] = span;
+    }
+    return span_of[1] < span_of[0] ? 64 : 96;
 }
 
 void mixed_gemm_grouped(int slices, int nt, const MixedGemmJob* d_jobs, const int4* d_tiles, int ntiles,
@@ -662,14 +702,16 @@ static int group_rows_for(int n, int slices) {
 
 template <int NT, int S>
 static void launch_ozaki(const MixedOperand& a, const MixedOperand& b, double* C, int ldc, unsigned long long* amax,
-                         bool lower_only, int* err, cudaStream_t st, const int* skip, bool mirror, bool accumulate) {
+                         bool lower_only, int* err, cudaStream_t st, const int* skip, bool mirror, bool accumulate,
+                         bool klo = false) {
     set_attr_once<NT, S>();
     const int n = a.n;
     const int gm = lower_only ? group_rows_for(n, S) : 0;
     dim3 grid = gm > 0 ? dim3((unsigned)lower_tiles(n, NT), 1) : dim3((n + NT - 1) / NT, (n + BM - 1) / BM);
     k_ozaki_gemm<NT, S><<<grid, THREADS, Shape<NT, S>::SMEM, st>>>(a.map, b.map, n, n, a.kp, a.rows, b.rows, a.exps,
                                                                    b.exps, C, ldc, amax, lower_only ? 1 : 0, err,
-                                                                   skip, mirror ? 1 : 0, accumulate ? 1 : 0, gm);
+                                                                   skip, mirror ? 1 : 0, accumulate ? 1 : 0, gm,
+                                                                   klo ? 1 : 0);
 }
 
 void mixed_gemm(const MixedOperand& a, const MixedOperand& b, double* C, int ldc, unsigned long long* amax,
@@ -686,6 +728,27 @@ void mixed_gemm(const MixedOperand& a, const MixedOperand& b, double* C, int ldc
     else
         launch_ozaki<128, 2>(a, b, C, ldc, amax, lower_only, err, st, skip, mirror, accumulate);
     count_launch();
+}
+
+
+size_t mixed_gram_bytes(int n) {
+    return (mixed_slice_bytes_nt(n, kGramSlices, 64) + 255) & ~size_t(255);
+}
+
+// A = T^T T for lower-triangular T (the last product of the SPD inverse,
+// A^{-1} = L^{-T} L^{-1}): the columns of T sliced into kGramSlices int8
+// planes, lower 128 x 64 tiles, each tile's K loop from max(m0, n0) (the rows
+// above are zero in both of its columns), the result mirrored. buf: the
+// slice planes (mixed_gram_bytes(n)); its K and row padding must be zero.
+bool mixed_gram_lower_tri(const double* T, int n, int ld, int8_t* buf, int* exps, double* A, int lda, int* err,
+                          cudaStream_t st) {
+    MixedOperand a, b;
+    if (!mixed_plan_nt(a, buf, exps, n, kGramSlices, false, 64) || !mixed_plan_nt(b, buf, exps, n, kGramSlices, true, 64))
+        return false;
+    mixed_slice(T, ld, a, st);
+    launch_ozaki<64, kGramSlices>(a, b, A, lda, nullptr, true, err, st, nullptr, true, false, true);
+    count_launch();
+    return true;
 }
 
 }  // namespace unc

@@ -73,6 +73,7 @@ struct Worker {
     unc_batch* batch = nullptr;  // packs of small requests
     long long committed = 0;  // device bytes held or promised (workspace, or the running request's footprint)
     bool busy = false;
+    bool releasing = false;   // another worker is freeing this one's workspaces
     bool small_only = false;  // reserved for small requests
     std::thread th;
 };
@@ -108,23 +109,32 @@ long long worker_bytes(const Worker* w) {
 
 // Under the lock: the requests worker `w` may start now (empty: none). A small
 // request takes the small requests waiting behind it along (a pack) as long as
-// their footprints fit.
-std::vector<std::shared_ptr<Request>> pick(unc_server* s, Worker* w) {
+// their footprints fit. Idle workers whose workspaces must go to make room are
+// returned in `release` (marked, their bytes no longer counted): the caller
+// frees them after unlocking, before its own allocations, so that no CUDA call
+// runs under the lock.
+std::vector<std::shared_ptr<Request>> pick(unc_server* s, Worker* w, std::vector<Worker*>& release) {
     std::vector<std::shared_ptr<Request>> pack;
+    release.clear();
+    if (w->releasing) return pack;
     for (size_t i = 0; i < s->pending.size(); ++i) {
         auto& r = s->pending[i];
         if (w->small_only && !r->small) continue;  // not this worker's kind; no bypass counted
         long long mine = std::max(w->committed, r->bytes);
         bool fits = committed_except(s, w) + mine <= s->budget;
         if (!fits) {
-            // release idle workspaces (not this worker's) and look again
+            // count idle workspaces (not this worker's) as released and look again
+            long long idle = 0;
             for (auto& v : s->workers)
-                if (v.get() != w && !v->busy && v->committed > 0) {
-                    if (v->ctx) unc_context_release(v->ctx);
-                    if (v->batch) unc_batch_release(v->batch);
-                    v->committed = 0;
-                }
-            fits = committed_except(s, w) + mine <= s->budget;
+                if (v.get() != w && !v->busy && !v->releasing) idle += v->committed;
+            fits = committed_except(s, w) - idle + mine <= s->budget;
+            if (fits)
+                for (auto& v : s->workers)
+                    if (v.get() != w && !v->busy && !v->releasing && v->committed > 0) {
+                        v->releasing = true;
+                        v->committed = 0;
+                        release.push_back(v.get());
+                    }
         }
         if (fits) {
             for (size_t j = 0; j < i; ++j)
@@ -160,13 +170,27 @@ void worker_loop(unc_server* s, Worker* w) {
     const int sms = unc::device_sms();
     if (w->ctx) unc::context_set_task_ctas(w->ctx, (2 * sms + (int)s->workers.size() - 1) / (int)s->workers.size());
     std::unique_lock<std::mutex> lk(s->mu);
+    std::vector<Worker*> release;
     for (;;) {
         std::vector<std::shared_ptr<Request>> pack;
-        s->cv_work.wait(lk, [&] { return !(pack = pick(s, w)).empty() || (s->stopping && s->pending.empty()); });
+        s->cv_work.wait(lk, [&] {
+            return !(pack = pick(s, w, release)).empty() || (s->stopping && s->pending.empty() && !w->releasing);
+        });
         if (pack.empty()) break;
         w->busy = true;
         s->running += (int)pack.size();
         lk.unlock();
+        if (!release.empty()) {
+            // the idle workers picked for release wait (releasing) until this is done
+            for (Worker* v : release) {
+                if (v->ctx) unc_context_release(v->ctx);
+                if (v->batch) unc_batch_release(v->batch);
+            }
+            lk.lock();
+            for (Worker* v : release) v->releasing = false;
+            s->cv_work.notify_all();
+            lk.unlock();
+        }
         const auto t_start = Clock::now();
         for (auto& r : pack) r->t_start = t_start;
         std::vector<int> rcs(pack.size(), UNC_ERR_CUDA);

@@ -18,6 +18,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libuncte.so")
 
 UNC_OK = 0
+UNC_ERR_TIMEOUT = -9  # unc_server_wait: the request is still running
 TAYLOR_EXPANSION = 2
 SVD_QR_ITERATION = 0
 SVD_SCHUR = 3  # extension: SVD pseudo-inverse of the camera Schur complement
@@ -82,14 +83,15 @@ EXPORTS = ("unc_options_init", "unc_context_create", "unc_context_destroy", "unc
            "unc_context_set_profiling", "unc_context_profile", "unc_context_profile_int8",
            "unc_compute_device", "unc_workspace_bytes", "unc_dense_inverse_device",
            "unc_dense_inverse_noalloc", "unc_spd_task_list", "unc_spd_inverse_tasks_bounded", "unc_pinv_psd_device", "unc_jtj_crs",
-           "unc_gemm_f64_device", "unc_gemm_mixed_device", "unc_status_string", "unc_last_error",
+           "unc_gemm_f64_device", "unc_gemm_mixed_device", "unc_gram_lower_mixed_device", "unc_status_string",
+           "unc_last_error",
            "unc_kernel_launches", "unc_request_bytes", "unc_context_device_bytes", "unc_context_release",
            "unc_context_set_priority", "unc_jacobian_device", "unc_compute_scene",
            "unc_block_eigen_device", "unc_block_eigen", "unc_jacob_read_header", "unc_jacob_read",
            "unc_jacob_write_binary",
            "unc_server_create", "unc_server_submit", "unc_server_wait", "unc_server_destroy",
            "unc_batch_create", "unc_batch_destroy", "unc_batch_compute", "unc_batch_last_timing",
-           "unc_batch_device_bytes", "unc_batch_release")
+           "unc_batch_device_bytes", "unc_batch_release", "unc_batch_set_tile_width")
 
 _lib = None
 
@@ -142,6 +144,7 @@ def lib():
     L.unc_batch_device_bytes.argtypes = [vp]
     L.unc_batch_device_bytes.restype = C.c_longlong
     L.unc_batch_release.argtypes = [vp]
+    L.unc_batch_set_tile_width.argtypes = [vp, C.c_int]
     L.unc_server_create.argtypes = [C.c_int, C.c_longlong, C.c_int, P(vp)]
     L.unc_server_submit.argtypes = [vp, P(UncOptions), C.c_int, C.c_int, vp, vp, vp, vp, vp, P(C.c_longlong)]
     L.unc_server_wait.argtypes = [vp, C.c_longlong, C.c_double, P(C.c_int), P(UncStatistic), P(C.c_double),
@@ -152,6 +155,7 @@ def lib():
     L.unc_gemm_f64_device.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, vp, C.c_int, vp, C.c_int,
                                       C.c_double, vp, C.c_int, vp]
     L.unc_gemm_mixed_device.argtypes = [C.c_int, vp, vp, C.c_int, vp, C.c_int, vp]
+    L.unc_gram_lower_mixed_device.argtypes = [C.c_int, vp, C.c_int, vp, vp]
     L.unc_status_string.argtypes = [C.c_int]
     L.unc_status_string.restype = C.c_char_p
     L.unc_last_error.restype = C.c_char_p
@@ -367,6 +371,19 @@ class Server:
         _check(status.value)
         return cam, pt, st.as_dict(), lat.value, que.value
 
+    def poll(self, rid: int):
+        """wait() without blocking: None while request rid still runs."""
+        status = C.c_int()
+        st = UncStatistic()
+        lat, que = C.c_double(), C.c_double()
+        rc = lib().unc_server_wait(self._h, rid, 0.0, C.byref(status), C.byref(st), C.byref(lat), C.byref(que))
+        if rc == UNC_ERR_TIMEOUT:
+            return None
+        _check(rc)
+        _, _, _, _, cam, pt = self._live.pop(rid)
+        _check(status.value)
+        return cam, pt, st.as_dict(), lat.value, que.value
+
     def close(self):
         if self._h:
             lib().unc_server_destroy(self._h)
@@ -420,6 +437,10 @@ class Batch:
         _check(lib().unc_batch_last_timing(self._h, C.byref(h), C.byref(d), C.byref(o), C.byref(g), C.byref(t)))
         return {"h2d_s": h.value, "device_s": d.value, "d2h_s": o.value, "grouped_scenes": g.value,
                 "tile_n": t.value}
+
+    def set_tile_width(self, tile_n: int):
+        """5-slice product tile width: 0 = cost model, 64 or 96 forced."""
+        _check(lib().unc_batch_set_tile_width(self._h, tile_n))
 
     def close(self):
         if self._h:
@@ -510,6 +531,11 @@ def gemm_f64_device(M, N, K, alpha, d_A, lda, d_B, ldb, beta, d_C, ldc, stream: 
 def gemm_mixed_device(n, d_P, d_X, ld, d_C, slices=4, stream: int = 0) -> None:
     """C = P X for symmetric P, X on the int8-sliced tensor-core product."""
     _check(lib().unc_gemm_mixed_device(n, d_P, d_X, ld, d_C, slices, stream or None))
+
+
+def gram_lower_mixed_device(n, d_T, ld, d_A, stream: int = 0) -> None:
+    """A = T^T T for lower-triangular T on the int8-sliced tensor-core product (7 slices)."""
+    _check(lib().unc_gram_lower_mixed_device(n, d_T, ld, d_A, stream or None))
 
 
 def kernel_launches() -> int:
