@@ -97,14 +97,18 @@ def _right_jacobian(aa: np.ndarray) -> np.ndarray:
 
 def observation_blocks(cams: np.ndarray, points: np.ndarray, obs_cam: np.ndarray,
                        obs_pt: np.ndarray):
-    """Analytic Jacobian blocks: returns (Jc (n,2,9), Jp (n,2,3))."""
-    aa = cams[obs_cam, 0:3]
+    """Analytic Jacobian blocks: returns (Jc (n,2,9), Jp (n,2,3)).
+
+    The rotation and its right Jacobian are formed once per camera and
+    gathered per observation (each matrix is computed on its own, so the
+    values do not depend on how many are formed together)."""
     Cc = cams[obs_cam, 3:6]
     f = cams[obs_cam, 6]
     k1 = cams[obs_cam, 7]
     k2 = cams[obs_cam, 8]
     X = points[obs_pt]
-    R = _aa_to_rot(aa)
+    R = _aa_to_rot(cams[:, 0:3])[obs_cam]
+    Jr = _right_jacobian(cams[:, 0:3])[obs_cam]
     pC = X - Cc
     p = np.einsum("nij,nj->ni", R, pC)
     xp, yp, z = p[:, 0] / p[:, 2], p[:, 1] / p[:, 2], p[:, 2]
@@ -124,7 +128,7 @@ def observation_blocks(cams: np.ndarray, points: np.ndarray, obs_cam: np.ndarray
     dUdp = M @ Q  # (n,2,3)
     Jp = dUdp @ R  # d/dX
     Jc = np.empty((len(f), 2, 9))
-    Jc[:, :, 0:3] = -dUdp @ R @ _skew(pC) @ _right_jacobian(aa)
+    Jc[:, :, 0:3] = -dUdp @ R @ _skew(pC) @ Jr
     Jc[:, :, 3:6] = -Jp
     Jc[:, 0, 6], Jc[:, 1, 6] = xp * d, yp * d
     Jc[:, 0, 7], Jc[:, 1, 7] = f * xp * r2, f * yp * r2
