@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "../../include/uncte.h"
@@ -57,6 +58,11 @@ struct unc_context {
     size_t mp_bytes = 0;
     void* jac = nullptr;  // unc_compute_scene: scene inputs, the generated CRS Jacobian, outputs
     size_t jac_bytes = 0;
+    // pinned staging ring for copies of ordinary (pageable) host memory
+    // (allocated at the first such copy, freed with the context)
+    char* stage = nullptr;
+    cudaEvent_t stage_ev[16] = {};
+    bool stage_used[16] = {};
     cudaEvent_t ev[12] = {};
     int priority = 0;  // of `stream` (0: the default priority)
     int sm_count = 148;  // of `device`
@@ -171,6 +177,96 @@ int grow_buffer(void** p, size_t* have, size_t need, size_t want, cudaStream_t s
 
 int ensure_ws(unc_context* ctx, size_t bytes, cudaStream_t sm) {
     return grow_buffer(&ctx->ws, &ctx->ws_bytes, bytes, bytes, sm);
+}
+
+// Copies between the caller's host arrays and the device. A copy from page-
+// locked (pinned or registered) memory goes to the copy engine directly. A
+// copy of ordinary pageable memory of kStageMin bytes or more is staged: host
+// threads copy kStageChunk pieces into a pinned ring owned by the context and
+// each piece is sent from there as soon as it is in, so that the host copies
+// run side by side and overlap the transfers (the driver's own path for
+// pageable memory is one host thread through small bounce buffers). Each ring
+// slot belongs to one thread during a call and is reused only after the
+// transfer recorded on its event has completed.
+constexpr int kStageSlots = 16;
+constexpr size_t kStageChunk = 4u << 20;
+constexpr size_t kStageMin = 8u << 20;
+
+struct HostCopy {
+    void* dst;
+    const void* src;
+    size_t bytes;
+};
+
+bool is_pageable(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered;
+}
+
+int ensure_stage(unc_context* ctx) {
+    if (ctx->stage) return UNC_OK;
+    CK(cudaHostAlloc((void**)&ctx->stage, kStageSlots * kStageChunk, cudaHostAllocDefault));
+    for (int i = 0; i < kStageSlots; ++i) {
+        CK(cudaEventCreateWithFlags(&ctx->stage_ev[i], cudaEventDisableTiming));
+        ctx->stage_used[i] = false;
+    }
+    return UNC_OK;
+}
+
+// to_device: host -> device (returns once every piece is queued on sm);
+// otherwise device -> host (returns once every piece has arrived in host memory).
+int copy_host(unc_context* ctx, const std::vector<HostCopy>& jobs, bool to_device, cudaStream_t sm) {
+    const cudaMemcpyKind kind = to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+    struct Piece {
+        char* dst;
+        const char* src;
+        size_t n;
+    };
+    std::vector<Piece> pieces;
+    for (const HostCopy& j : jobs) {
+        if (!j.bytes) continue;
+        const void* host = to_device ? j.src : j.dst;
+        if (j.bytes < kStageMin || !is_pageable(host)) {
+            CK(cudaMemcpyAsync(j.dst, j.src, j.bytes, kind, sm));
+            continue;
+        }
+        for (size_t o = 0; o < j.bytes; o += kStageChunk)
+            pieces.push_back({(char*)j.dst + o, (const char*)j.src + o, std::min(kStageChunk, j.bytes - o)});
+    }
+    if (pieces.empty()) return UNC_OK;
+    if (int r = ensure_stage(ctx)) return r;
+    const int hw = (int)std::max(2u, std::thread::hardware_concurrency());
+    const int nt = std::max(1, std::min({kStageSlots / 2, (int)pieces.size(), hw / 2}));
+    std::vector<cudaError_t> failed(nt, cudaSuccess);
+    auto run = [&](int t) {
+        cudaError_t& e = failed[t];
+        if ((e = cudaSetDevice(ctx->device)) != cudaSuccess) return;
+        for (size_t c = t, m = 0; c < pieces.size(); c += nt, ++m) {
+            const int slot = t + nt * (int)(m & 1);  // two slots per thread, alternating
+            char* buf = ctx->stage + (size_t)slot * kStageChunk;
+            if (ctx->stage_used[slot] && (e = cudaEventSynchronize(ctx->stage_ev[slot])) != cudaSuccess) return;
+            const Piece& p = pieces[c];
+            if (to_device) memcpy(buf, p.src, p.n);
+            e = to_device ? cudaMemcpyAsync(p.dst, buf, p.n, kind, sm) : cudaMemcpyAsync(buf, p.src, p.n, kind, sm);
+            if (e != cudaSuccess || (e = cudaEventRecord(ctx->stage_ev[slot], sm)) != cudaSuccess) return;
+            ctx->stage_used[slot] = true;
+            if (!to_device) {
+                if ((e = cudaEventSynchronize(ctx->stage_ev[slot])) != cudaSuccess) return;
+                memcpy(p.dst, buf, p.n);
+            }
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; ++t) th.emplace_back(run, t);
+    run(0);
+    for (auto& x : th) x.join();
+    for (cudaError_t e : failed)
+        if (e != cudaSuccess) return fail(UNC_ERR_CUDA, std::string("staged host copy: ") + cudaGetErrorString(e));
+    return UNC_OK;
 }
 
 int check_options(const unc_options* o, int num_rows, int num_cols) {
@@ -798,6 +894,9 @@ int unc_context_destroy(unc_context* c) {
     for (cudaEvent_t e : c->pev) cudaEventDestroy(e);
     for (int i = 0; i < 12; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    for (int i = 0; i < kStageSlots; ++i)
+        if (c->stage_ev[i]) cudaEventDestroy(c->stage_ev[i]);
+    if (c->stage) cudaFreeHost(c->stage);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return UNC_OK;
@@ -948,17 +1047,23 @@ int unc_compute(unc_context* ctx, const unc_options* o, int num_rows, int num_co
         memset(st, 0, sizeof(*st));
         st->device_bytes = (long long)bytes;
     }
-    CK(cudaMemcpyAsync(b.rows, rows, sizeof(int) * ((size_t)num_rows + 1), cudaMemcpyHostToDevice, sm));
-    CK(cudaMemcpyAsync(b.cols, cols, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, sm));
-    CK(cudaMemcpyAsync(b.vals, values, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice, sm));
+    rc = copy_host(ctx,
+                   {{b.rows, rows, sizeof(int) * ((size_t)num_rows + 1)},
+                    {b.cols, cols, sizeof(int) * (size_t)nnz},
+                    {b.vals, values, sizeof(double) * (size_t)nnz}},
+                   true, sm);
+    if (rc) return rc;
     rc = run_pipeline(ctx, o, num_rows, nnz, b.rows, b.cols, b.vals, b.cam_out, b.pt_out, b, pl, st, sm);
     if (rc) return rc;
-    CK(cudaMemcpyAsync(cam_unc, b.cam_out, sizeof(double) * 45 * (size_t)pl.C, cudaMemcpyDeviceToHost, sm));
     // Points: slots [0, 6(P-3)) are written (zeroed or computed); of the last
     // three points only the non-fixed ones are written (compute.cpp:511,526).
     // The SVD on Z fixes no point: every slot is written.
     size_t head = pl.svd_schur ? (size_t)pl.P : (pl.P > 3 ? (size_t)(pl.P - 3) : 0);
-    if (head) CK(cudaMemcpyAsync(pt_unc, b.pt_out, sizeof(double) * 6 * head, cudaMemcpyDeviceToHost, sm));
+    rc = copy_host(ctx,
+                   {{cam_unc, b.cam_out, sizeof(double) * 45 * (size_t)pl.C},
+                    {pt_unc, b.pt_out, sizeof(double) * 6 * head}},
+                   false, sm);
+    if (rc) return rc;
     for (int p = (int)head; p < pl.P; ++p) {
         if (p == b.s.fix[0] || p == b.s.fix[1] || p == b.s.fix[2]) continue;
         CK(cudaMemcpyAsync(pt_unc + 6L * p, b.pt_out + 6L * p, sizeof(double) * 6, cudaMemcpyDeviceToHost, sm));

@@ -105,6 +105,11 @@ struct unc_batch {
     size_t ws_bytes = 0;
     void* host = nullptr;  // pinned staging: inputs, outputs, descriptors, status words
     size_t host_bytes = 0;
+    // outgrown staging areas, freed with the batch: cudaFreeHost waits for the
+    // whole device (every other stream's work), so a serving worker never calls
+    // it while other requests compute; the sizes grow by half at least, so the
+    // retired areas hold at most twice the current one
+    std::vector<void*> host_retired;
     std::vector<Graph> graphs;
     std::vector<std::vector<unsigned long long>> seen;
     unc_context* single = nullptr;                  // scenes outside the grouped path
@@ -395,11 +400,10 @@ int prepare_group(unc_batch* b, GroupRun& g, int nt) {
     g.h_stat = g.h_desc + g.L.desc_bytes;
     const size_t hneed = g.h_stat + g.L.stat_bytes + 256;
     if (b->host_bytes < hneed) {
-        // grown by half again at least: freeing pinned memory waits for the whole
-        // device (every other stream's work), so a serving worker should rarely do it
+        // grown by half again at least; the old area is retired (freed with the batch)
         const size_t want = std::max(hneed, b->host_bytes + b->host_bytes / 2);
         BCK(cudaStreamSynchronize(sm));
-        if (b->host) cudaFreeHost(b->host);
+        if (b->host) b->host_retired.push_back(b->host);
         b->host = nullptr;
         b->host_bytes = 0;
         BCK(cudaMallocHost(&b->host, want));
@@ -686,6 +690,7 @@ int unc_batch_destroy(unc_batch* b) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
     if (b->ws) cudaFree(b->ws);
     if (b->host) cudaFreeHost(b->host);
+    for (void* h : b->host_retired) cudaFreeHost(h);
     if (b->single) unc_context_destroy(b->single);
     for (int k = 0; k < 4; ++k)
         if (b->ev[k]) cudaEventDestroy(b->ev[k]);

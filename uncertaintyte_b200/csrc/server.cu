@@ -14,8 +14,11 @@
 // * Admission by device-memory footprint (unc_request_bytes: the dense Schur
 //   complement and its inverse buffers, the block storage, the int8
 //   slices): the sum over running requests and idle workspaces stays
-//   within `max_device_bytes`. Idle workspaces are released when that makes a
-//   request fit. Later requests may start ahead of a waiting one (backfill) at
+//   within `max_device_bytes`. A worker holds two workspaces (its context's,
+//   grown by single requests, and its batch's, grown by packs), and both are
+//   counted: a run grows one of them while the other keeps its memory, unless
+//   the worker frees it first to make room. Idle workers' workspaces are
+//   released when that makes a request fit. Later requests may start ahead of a waiting one (backfill) at
 //   most kMaxBypass times, so large requests are not starved.
 // * Small requests (footprint <= kSmallBytes) run on high-priority streams,
 //   so the block scheduler serves their kernels ahead of a large request's
@@ -72,6 +75,10 @@ struct Worker {
     unc_context* ctx = nullptr;
     unc_batch* batch = nullptr;  // packs of small requests
     long long committed = 0;  // device bytes held or promised (workspace, or the running request's footprint)
+    // What the two workspaces hold between runs: a single request grows the
+    // context's, a pack the batch's, and each keeps its memory after the run.
+    long long ctx_held = 0, batch_held = 0;
+    bool drop_ctx = false, drop_batch = false;  // free that workspace before the next run (room for it)
     bool busy = false;
     bool releasing = false;   // another worker is freeing this one's workspaces
     bool small_only = false;  // reserved for small requests
@@ -103,8 +110,12 @@ long long committed_except(const unc_server* s, const Worker* w) {
     return t;
 }
 
-long long worker_bytes(const Worker* w) {
-    return (w->ctx ? unc_context_device_bytes(w->ctx) : 0) + (w->batch ? unc_batch_device_bytes(w->batch) : 0);
+// Device bytes worker w holds while it runs `need` bytes of work as a single
+// request (pack false: the context's workspace grows to it) or as a pack (the
+// batch's grows), with the other workspace kept or freed first (drop_other).
+long long holds(const Worker* w, long long need, bool pack, bool drop_other) {
+    const long long same = pack ? w->batch_held : w->ctx_held, other = pack ? w->ctx_held : w->batch_held;
+    return std::max(same, need) + (drop_other ? 0 : other);
 }
 
 // Under the lock: the requests worker `w` may start now (empty: none). A small
@@ -120,32 +131,42 @@ std::vector<std::shared_ptr<Request>> pick(unc_server* s, Worker* w, std::vector
     for (size_t i = 0; i < s->pending.size(); ++i) {
         auto& r = s->pending[i];
         if (w->small_only && !r->small) continue;  // not this worker's kind; no bypass counted
-        long long mine = std::max(w->committed, r->bytes);
-        bool fits = committed_except(s, w) + mine <= s->budget;
+        // as a single request: this worker's batch workspace stays, unless freeing it makes room
+        const long long others = committed_except(s, w);
+        bool drop = false;
+        bool fits = others + holds(w, r->bytes, false, false) <= s->budget;
+        if (!fits && others + holds(w, r->bytes, false, true) <= s->budget) fits = drop = true;
         if (!fits) {
             // count idle workspaces (not this worker's) as released and look again
             long long idle = 0;
             for (auto& v : s->workers)
                 if (v.get() != w && !v->busy && !v->releasing) idle += v->committed;
-            fits = committed_except(s, w) - idle + mine <= s->budget;
-            if (fits)
+            fits = others - idle + holds(w, r->bytes, false, true) <= s->budget;
+            if (fits) {
+                drop = others - idle + holds(w, r->bytes, false, false) > s->budget;
                 for (auto& v : s->workers)
                     if (v.get() != w && !v->busy && !v->releasing && v->committed > 0) {
                         v->releasing = true;
-                        v->committed = 0;
+                        v->committed = v->ctx_held = v->batch_held = 0;
                         release.push_back(v.get());
                     }
+            }
         }
         if (fits) {
             for (size_t j = 0; j < i; ++j)
                 if (!w->small_only || s->pending[j]->small) s->pending[j]->bypassed++;
             pack.push_back(r);
             s->pending.erase(s->pending.begin() + (long)i);
-            if (pack[0]->small) {
-                long long sum = pack[0]->bytes;
+            long long sum = r->bytes;
+            bool pdrop = false;  // the pack needs this worker's context workspace freed
+            if (r->small) {
                 for (size_t j = i; j < s->pending.size() && (int)pack.size() < kMaxPack;) {
                     auto& q = s->pending[j];
-                    if (q->small && committed_except(s, w) + std::max(w->committed, sum + q->bytes) <= s->budget) {
+                    const long long base = committed_except(s, w);
+                    bool take = q->small && base + holds(w, sum + q->bytes, true, pdrop) <= s->budget;
+                    if (!take && q->small && !pdrop && base + holds(w, sum + q->bytes, true, true) <= s->budget)
+                        take = pdrop = true;
+                    if (take) {
                         sum += q->bytes;
                         pack.push_back(q);
                         s->pending.erase(s->pending.begin() + (long)j);
@@ -153,9 +174,11 @@ std::vector<std::shared_ptr<Request>> pick(unc_server* s, Worker* w, std::vector
                         ++j;
                     }
                 }
-                mine = std::max(w->committed, sum);
             }
-            w->committed = mine;
+            const bool as_pack = pack.size() > 1;
+            w->drop_ctx = as_pack && pdrop;
+            w->drop_batch = !as_pack && drop;
+            w->committed = as_pack ? holds(w, sum, true, pdrop) : holds(w, r->bytes, false, drop);
             return pack;
         }
         if (r->bypassed >= kMaxBypass) break;  // the head waits for memory; nobody overtakes it any more
@@ -191,6 +214,9 @@ void worker_loop(unc_server* s, Worker* w) {
             s->cv_work.notify_all();
             lk.unlock();
         }
+        // this worker's own other workspace, when the admission counted it as freed
+        if (w->drop_ctx && w->ctx) unc_context_release(w->ctx);
+        if (w->drop_batch && w->batch) unc_batch_release(w->batch);
         const auto t_start = Clock::now();
         for (auto& r : pack) r->t_start = t_start;
         std::vector<int> rcs(pack.size(), UNC_ERR_CUDA);
@@ -240,7 +266,11 @@ void worker_loop(unc_server* s, Worker* w) {
             pack[k]->done = true;
         }
         w->busy = false;
-        w->committed = worker_bytes(w);  // what the workspaces now hold
+        // what the workspaces now hold
+        w->ctx_held = w->ctx ? unc_context_device_bytes(w->ctx) : 0;
+        w->batch_held = w->batch ? unc_batch_device_bytes(w->batch) : 0;
+        w->committed = w->ctx_held + w->batch_held;
+        w->drop_ctx = w->drop_batch = false;
         s->running -= (int)pack.size();
         s->completed += (long long)pack.size();
         s->cv_done.notify_all();
