@@ -61,7 +61,7 @@ def test_mixed4_is_faster_and_coarser(ctx):
 
 
 @pytest.mark.parametrize("n,slices,tol", [(1, 4, 1e-6), (70, 4, 1e-5), (200, 4, 1e-5), (1800, 4, 1e-5),
-                                          (1800, 5, 1e-7), (257, 3, 1e-3), (130, 5, 1e-7)])
+                                          (1800, 5, 1e-7), (257, 3, 1e-3), (130, 5, 1e-7), (6000, 5, 1e-7)])
 def test_mixed_gemm_vs_torch(n, slices, tol):
     import torch
     g = torch.Generator(device="cuda").manual_seed(n + slices)

@@ -116,3 +116,27 @@ def test_waiters_survive_concurrent_submits():
     for c, p in got[1:]:
         np.testing.assert_array_equal(c, got[0][0])
         np.testing.assert_array_equal(p, got[0][1])
+
+
+def test_worker_frees_its_other_workspace_for_room():
+    """One worker and a budget that holds the large request plus half of the
+    small ones: the large request grows the worker's context workspace, the
+    small ones queued behind it run as one pack in the batch workspace (the
+    admission counts both, so the worker frees its context workspace first),
+    and the large request submitted again frees the batch workspace. Results
+    equal those of the requests run alone."""
+    big = scenes.scene_jacobian(scenes.make_sized_scene(400, 100, 4, seed=41))
+    smalls = [scenes.scene_jacobian(scenes.make_sized_scene(C, 60, 4, seed=50 + i))
+              for i, C in enumerate([10, 14, 12, 9, 11])]
+    need_big = native.request_bytes(big, precision="mixed")
+    need_small = sum(native.request_bytes(j, precision="mixed") for j in smalls)
+    budget = need_big + need_small // 2
+    ref = _alone([(j, "mixed", None) for j in [big] + smalls])
+    srv = native.Server(max_device_bytes=budget, max_inflight=1)
+    ids = [srv.submit(big, precision="mixed")] + [srv.submit(j, precision="mixed") for j in smalls]
+    got = [srv.wait(i)[:2] for i in ids]
+    got.append(srv.wait(srv.submit(big, precision="mixed"))[:2])
+    srv.close()
+    for (c0, p0), (c1, p1) in zip(ref + ref[:1], got):
+        np.testing.assert_array_equal(c0, c1)
+        np.testing.assert_array_equal(p0, p1)
