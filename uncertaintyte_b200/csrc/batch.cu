@@ -5,8 +5,9 @@
 // compute.cpp:458-540) and is not re-entrant; this is the batched form of that
 // call, with no counterpart there. Per batch:
 //
-//   * inputs of all scenes packed into one pinned staging area and copied to
-//     the device in one transfer; outputs come back the same way;
+//   * inputs of all scenes packed into one pinned staging area by host
+//     threads, each piece sent to the device as soon as it is packed; outputs
+//     come back in one transfer and are unpacked by host threads;
 //   * the sparse stages (validation, J^T J blocks, Schur complement) of every
 //     scene as parallel branches of one launch sequence;
 //   * the dense stage grouped across scenes: one persistent tile-task kernel
@@ -152,6 +153,47 @@ void parallel_copy(const std::vector<Copy>& jobs) {
             for (size_t p = t; p < pieces.size(); p += nt) memcpy(pieces[p].d, pieces[p].s, pieces[p].n);
         });
     for (auto& x : th) x.join();
+}
+
+// The inputs into the pinned staging area and on to the device: the staging
+// area mirrors the device region byte for byte (dev = stage_base -> dev_base),
+// so every thread sends each 8 MB piece as soon as it has copied it, and the
+// host copies overlap the transfers. Small totals: host copies, then one
+// transfer of the whole region.
+cudaError_t parallel_copy_to_device(const std::vector<Copy>& jobs, const char* stage_base, char* dev_base,
+                                    size_t region_bytes, int device, cudaStream_t sm) {
+    const int nt = (int)std::min<size_t>(16, std::max<size_t>(1, std::thread::hardware_concurrency()));
+    size_t total = 0;
+    for (auto& j : jobs) total += j.bytes;
+    if (total < (64u << 20) || nt == 1) {
+        parallel_copy(jobs);
+        return cudaMemcpyAsync(dev_base, stage_base, region_bytes, cudaMemcpyHostToDevice, sm);
+    }
+    struct Piece {
+        char* d;
+        const char* s;
+        size_t n;
+    };
+    std::vector<Piece> pieces;
+    for (auto& j : jobs)
+        for (size_t o = 0; o < j.bytes; o += (8u << 20))
+            pieces.push_back({(char*)j.dst + o, (const char*)j.src + o, std::min<size_t>(8u << 20, j.bytes - o)});
+    std::vector<cudaError_t> err(nt, cudaSuccess);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+        th.emplace_back([&, t] {
+            if ((err[t] = cudaSetDevice(device)) != cudaSuccess) return;
+            for (size_t p = t; p < pieces.size(); p += nt) {
+                memcpy(pieces[p].d, pieces[p].s, pieces[p].n);
+                err[t] = cudaMemcpyAsync(dev_base + (pieces[p].d - stage_base), pieces[p].d, pieces[p].n,
+                                         cudaMemcpyHostToDevice, sm);
+                if (err[t] != cudaSuccess) return;
+            }
+        });
+    for (auto& x : th) x.join();
+    for (cudaError_t e : err)
+        if (e != cudaSuccess) return e;
+    return cudaSuccess;
 }
 
 int slices_of(int precision) {
@@ -582,7 +624,8 @@ int run_group(unc_batch* b, GroupRun& g, const int* const* rows, const int* cons
     for (const Scene& s : g.sc) ns.push_back(s.pl.N);
     const int nt = g.slices == 5 && b->force_nt ? b->force_nt : mixed_group_tile_n(g.slices, ns);
     if (int r = prepare_group(b, g, nt)) return r;
-    // inputs: pack and copy (one transfer)
+    // inputs: packed into the staging area and sent on piece by piece
+    BCK(cudaEventRecord(b->ev[0], sm));
     {
         std::vector<Copy> cp;
         for (const Scene& s : g.sc) {
@@ -590,10 +633,8 @@ int run_group(unc_batch* b, GroupRun& g, const int* const* rows, const int* cons
             cp.push_back({g.hbase + g.h_in + s.in_off[1], cols[s.idx], sizeof(int) * (size_t)s.nnz});
             cp.push_back({g.hbase + g.h_in + s.in_off[2], values[s.idx], sizeof(double) * (size_t)s.nnz});
         }
-        parallel_copy(cp);
+        BCK(parallel_copy_to_device(cp, g.hbase + g.h_in, g.dbase, g.L.in_bytes, b->device, sm));
     }
-    BCK(cudaEventRecord(b->ev[0], sm));
-    BCK(cudaMemcpyAsync(g.dbase, g.hbase + g.h_in, g.L.in_bytes, cudaMemcpyHostToDevice, sm));
     BCK(cudaEventRecord(b->ev[1], sm));
     if (int r = run_device(b, g)) return r;
     BCK(cudaEventRecord(b->ev[2], sm));
