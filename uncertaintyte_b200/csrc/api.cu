@@ -1115,12 +1115,13 @@ int unc_compute_scene(unc_context* ctx, const unc_options* o, const double* cams
     if (int r = grow_buffer(&ctx->jac, &ctx->jac_bytes, bytes, bytes, sm)) return r;
     Carver k{(char*)ctx->jac};
     lay(k, dc, dp, oc, op, drows, dcols, dv, co, po, derr);
-    CK(cudaMemcpyAsync(dc, cams, sizeof(double) * 9 * (size_t)C, cudaMemcpyHostToDevice, sm));
-    if (P) CK(cudaMemcpyAsync(dp, points, sizeof(double) * 3 * (size_t)P, cudaMemcpyHostToDevice, sm));
-    if (nobs) {
-        CK(cudaMemcpyAsync(oc, obs_cam, sizeof(int) * (size_t)nobs, cudaMemcpyHostToDevice, sm));
-        CK(cudaMemcpyAsync(op, obs_pt, sizeof(int) * (size_t)nobs, cudaMemcpyHostToDevice, sm));
-    }
+    rc = copy_host(ctx,
+                   {{dc, cams, sizeof(double) * 9 * (size_t)C},
+                    {dp, points, sizeof(double) * 3 * (size_t)P},
+                    {oc, obs_cam, sizeof(int) * (size_t)nobs},
+                    {op, obs_pt, sizeof(int) * (size_t)nobs}},
+                   true, sm);
+    if (rc) return rc;
     CK(cudaMemsetAsync(derr, 0, sizeof(int), sm));
     if (launch_scene_jacobian(C, P, nobs, dc, dp, oc, op, drows, dcols, dv, derr, sm) != UNC_OK)
         return fail(UNC_ERR_CUDA, "scene Jacobian launch failed");
@@ -1130,14 +1131,17 @@ int unc_compute_scene(unc_context* ctx, const unc_options* o, const double* cams
     if (h_err & ERRBIT_LAYOUT) return fail(UNC_ERR_INVALID_ARG, "camera or point id out of range");
     rc = unc_compute_device(ctx, o, num_rows, num_cols, drows, dcols, dv, co, po, st, sm);
     if (rc) return rc;
-    CK(cudaMemcpyAsync(cam_unc, co, sizeof(double) * 45 * (size_t)C, cudaMemcpyDeviceToHost, sm));
-    if (is_svd(o) || o->algorithm == UNC_SVD_SCHUR) {  // no fixed point
-        if (P) CK(cudaMemcpyAsync(pt_unc, po, sizeof(double) * 6 * (size_t)P, cudaMemcpyDeviceToHost, sm));
-    } else {  // the fixed points' slots are left as the caller had them (compute.cpp:511,526)
+    const bool no_fix = is_svd(o) || o->algorithm == UNC_SVD_SCHUR;
+    // the fixed points' slots past 6 (P - 3) are left as the caller had them (compute.cpp:511,526)
+    const size_t head = no_fix ? (size_t)P : (P > 3 ? (size_t)(P - 3) : 0);
+    rc = copy_host(ctx,
+                   {{cam_unc, co, sizeof(double) * 45 * (size_t)C},
+                    {pt_unc, po, sizeof(double) * 6 * head}},
+                   false, sm);
+    if (rc) return rc;
+    if (!no_fix) {
         int fx[3] = {o->pts2fix[0], o->pts2fix[1], o->pts2fix[2]};
         std::sort(fx, fx + 2);
-        size_t head = P > 3 ? (size_t)(P - 3) : 0;
-        if (head) CK(cudaMemcpyAsync(pt_unc, po, sizeof(double) * 6 * head, cudaMemcpyDeviceToHost, sm));
         for (int q = (int)head; q < P; ++q) {
             if (q == fx[0] || q == fx[1] || q == fx[2]) continue;
             CK(cudaMemcpyAsync(pt_unc + 6L * q, po + 6L * q, sizeof(double) * 6, cudaMemcpyDeviceToHost, sm));
