@@ -18,8 +18,9 @@
 //   grown by single requests, and its batch's, grown by packs), and both are
 //   counted: a run grows one of them while the other keeps its memory, unless
 //   the worker frees it first to make room. Idle workers' workspaces are
-//   released when that makes a request fit. Later requests may start ahead of a waiting one (backfill) at
-//   most kMaxBypass times, so large requests are not starved.
+//   released when that makes a request fit. Later requests may start ahead
+//   of a waiting one (backfill) at most kMaxBypass times, so large requests
+//   are not starved.
 // * Small requests (footprint <= kSmallBytes) run on high-priority streams,
 //   so the block scheduler serves their kernels ahead of a large request's
 //   GEMM tiles, and a quarter of the workers take small requests only, so a
@@ -156,10 +157,11 @@ std::vector<std::shared_ptr<Request>> pick(unc_server* s, Worker* w, std::vector
             for (size_t j = 0; j < i; ++j)
                 if (!w->small_only || s->pending[j]->small) s->pending[j]->bypassed++;
             pack.push_back(r);
-            s->pending.erase(s->pending.begin() + (long)i);
-            long long sum = r->bytes;
+            s->pending.erase(s->pending.begin() + (long)i);  // `r` refers to the erased slot from here on
+            const Request& head = *pack[0];
+            long long sum = head.bytes;
             bool pdrop = false;  // the pack needs this worker's context workspace freed
-            if (r->small) {
+            if (head.small) {
                 for (size_t j = i; j < s->pending.size() && (int)pack.size() < kMaxPack;) {
                     auto& q = s->pending[j];
                     const long long base = committed_except(s, w);
@@ -178,7 +180,7 @@ std::vector<std::shared_ptr<Request>> pick(unc_server* s, Worker* w, std::vector
             const bool as_pack = pack.size() > 1;
             w->drop_ctx = as_pack && pdrop;
             w->drop_batch = !as_pack && drop;
-            w->committed = as_pack ? holds(w, sum, true, pdrop) : holds(w, r->bytes, false, drop);
+            w->committed = as_pack ? holds(w, sum, true, pdrop) : holds(w, head.bytes, false, drop);
             return pack;
         }
         if (r->bypassed >= kMaxBypass) break;  // the head waits for memory; nobody overtakes it any more
