@@ -42,13 +42,12 @@
 #include <vector>
 
 #include "../../include/uncte.h"
+#include "admission.h"
 #include "internal.h"
 
 namespace {
 
-constexpr int kMaxBypass = 16;
 constexpr long long kSmallBytes = 1LL << 30;
-constexpr int kMaxPack = 64;  // small requests run together as one grouped batch
 
 using Clock = std::chrono::steady_clock;
 
@@ -104,90 +103,6 @@ struct unc_server {
 
 namespace {
 
-long long committed_except(const unc_server* s, const Worker* w) {
-    long long t = 0;
-    for (auto& v : s->workers)
-        if (v.get() != w) t += v->committed;
-    return t;
-}
-
-// Device bytes worker w holds while it runs `need` bytes of work as a single
-// request (pack false: the context's workspace grows to it) or as a pack (the
-// batch's grows), with the other workspace kept or freed first (drop_other).
-long long holds(const Worker* w, long long need, bool pack, bool drop_other) {
-    const long long same = pack ? w->batch_held : w->ctx_held, other = pack ? w->ctx_held : w->batch_held;
-    return std::max(same, need) + (drop_other ? 0 : other);
-}
-
-// Under the lock: the requests worker `w` may start now (empty: none). A small
-// request takes the small requests waiting behind it along (a pack) as long as
-// their footprints fit. Idle workers whose workspaces must go to make room are
-// returned in `release` (marked, their bytes no longer counted): the caller
-// frees them after unlocking, before its own allocations, so that no CUDA call
-// runs under the lock.
-std::vector<std::shared_ptr<Request>> pick(unc_server* s, Worker* w, std::vector<Worker*>& release) {
-    std::vector<std::shared_ptr<Request>> pack;
-    release.clear();
-    if (w->releasing) return pack;
-    for (size_t i = 0; i < s->pending.size(); ++i) {
-        auto& r = s->pending[i];
-        if (w->small_only && !r->small) continue;  // not this worker's kind; no bypass counted
-        // as a single request: this worker's batch workspace stays, unless freeing it makes room
-        const long long others = committed_except(s, w);
-        bool drop = false;
-        bool fits = others + holds(w, r->bytes, false, false) <= s->budget;
-        if (!fits && others + holds(w, r->bytes, false, true) <= s->budget) fits = drop = true;
-        if (!fits) {
-            // count idle workspaces (not this worker's) as released and look again
-            long long idle = 0;
-            for (auto& v : s->workers)
-                if (v.get() != w && !v->busy && !v->releasing) idle += v->committed;
-            fits = others - idle + holds(w, r->bytes, false, true) <= s->budget;
-            if (fits) {
-                drop = others - idle + holds(w, r->bytes, false, false) > s->budget;
-                for (auto& v : s->workers)
-                    if (v.get() != w && !v->busy && !v->releasing && v->committed > 0) {
-                        v->releasing = true;
-                        v->committed = v->ctx_held = v->batch_held = 0;
-                        release.push_back(v.get());
-                    }
-            }
-        }
-        if (fits) {
-            for (size_t j = 0; j < i; ++j)
-                if (!w->small_only || s->pending[j]->small) s->pending[j]->bypassed++;
-            pack.push_back(r);
-            s->pending.erase(s->pending.begin() + (long)i);  // `r` refers to the erased slot from here on
-            const Request& head = *pack[0];
-            long long sum = head.bytes;
-            bool pdrop = false;  // the pack needs this worker's context workspace freed
-            if (head.small) {
-                for (size_t j = i; j < s->pending.size() && (int)pack.size() < kMaxPack;) {
-                    auto& q = s->pending[j];
-                    const long long base = committed_except(s, w);
-                    bool take = q->small && base + holds(w, sum + q->bytes, true, pdrop) <= s->budget;
-                    if (!take && q->small && !pdrop && base + holds(w, sum + q->bytes, true, true) <= s->budget)
-                        take = pdrop = true;
-                    if (take) {
-                        sum += q->bytes;
-                        pack.push_back(q);
-                        s->pending.erase(s->pending.begin() + (long)j);
-                    } else {
-                        ++j;
-                    }
-                }
-            }
-            const bool as_pack = pack.size() > 1;
-            w->drop_ctx = as_pack && pdrop;
-            w->drop_batch = !as_pack && drop;
-            w->committed = as_pack ? holds(w, sum, true, pdrop) : holds(w, head.bytes, false, drop);
-            return pack;
-        }
-        if (r->bypassed >= kMaxBypass) break;  // the head waits for memory; nobody overtakes it any more
-    }
-    return pack;
-}
-
 void worker_loop(unc_server* s, Worker* w) {
     cudaSetDevice(s->device);
     if (unc_context_create(s->device, &w->ctx) != UNC_OK) w->ctx = nullptr;
@@ -199,7 +114,8 @@ void worker_loop(unc_server* s, Worker* w) {
     for (;;) {
         std::vector<std::shared_ptr<Request>> pack;
         s->cv_work.wait(lk, [&] {
-            return !(pack = pick(s, w, release)).empty() || (s->stopping && s->pending.empty() && !w->releasing);
+            return !(pack = unc_admission::pick(s, w, release)).empty() ||
+                   (s->stopping && s->pending.empty() && !w->releasing);
         });
         if (pack.empty()) break;
         w->busy = true;
@@ -268,11 +184,8 @@ void worker_loop(unc_server* s, Worker* w) {
             pack[k]->done = true;
         }
         w->busy = false;
-        // what the workspaces now hold
-        w->ctx_held = w->ctx ? unc_context_device_bytes(w->ctx) : 0;
-        w->batch_held = w->batch ? unc_batch_device_bytes(w->batch) : 0;
-        w->committed = w->ctx_held + w->batch_held;
-        w->drop_ctx = w->drop_batch = false;
+        unc_admission::settle(w, w->ctx ? unc_context_device_bytes(w->ctx) : 0,
+                              w->batch ? unc_batch_device_bytes(w->batch) : 0);
         s->running -= (int)pack.size();
         s->completed += (long long)pack.size();
         s->cv_done.notify_all();
