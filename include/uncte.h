@@ -106,7 +106,10 @@ int unc_context_destroy(unc_context* ctx);
 /* computeCovariances(options, statistic, jacobian, camUnc, ptUnc)
  * (src/uncertaintyTE/compute.h:92-97, compute.cpp:458-540).
  * Host pointers in and out; ctx may be NULL (a temporary context on device 0
- * is created and destroyed). stat may be NULL. */
+ * is created and destroyed). stat may be NULL. Arrays in ordinary (pageable)
+ * host memory of 8 MB or more are copied through a 64 MB pinned ring that the
+ * context allocates at its first such copy and frees when it is destroyed;
+ * pinned or registered arrays are copied directly. */
 int unc_compute(unc_context* ctx, const unc_options* opt, int num_rows, int num_cols,
                 const int* rows, const int* cols, const double* values, double* cam_unc,
                 double* pt_unc, unc_statistic* stat);
