@@ -686,14 +686,9 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
         slice(b.p16, k16, sk);
         launch_power_diag(ps, 17, 20, sk, sm);
         launch_power_decide(b.te, b.dmax, kc, 16, 19, sm);
-        launch_power_combine(ps, 0, b.iZ, nullptr, sm);
-        const double* Pq[5] = {nullptr, b.p4, b.p8, b.p12, b.p16};
-        const int iq[5] = {0, k4, k8, k12, k16};
-        for (int q = 1; q <= 4; ++q) {
-            launch_power_combine(ps, q, b.g, sk + q, sm);
-            slice(b.g, kA, sk + q);
-            if (int r = power_product(5 + q, b.g, kA, Pq[q], iq[q], b.iZ, true, sk + q)) return r;
-        }
+        launch_power_combine(ps, 0, b.iZ, nullptr, sm);  // iZ = G_0
+        // iZ += X^(4q) G_q on the camera blocks, the only part of iZ that is read after
+        launch_taylor_blocks(ps, sm);
         return UNC_OK;
     };
     while (ctx->prof && ctx->pev.size() < 2 * 20 + 2) {  // events exist before any capture

@@ -386,11 +386,8 @@ int launch_group(unc_batch* b, GroupRun& g) {
     launch_power_diag_grouped(g.dd.powers, n, g.dd.blk_cols, g.nblk_cols, 17, 20, true, sm);
     launch_power_decide_grouped(g.dd.powers, n, g.dd.kpow, 16, 19, sm);
     launch_power_combine_grouped(g.dd.powers, n, g.dd.blk_elems, g.nblk_elems, 0, sm);  // iZ = G_0
-    for (int q = 1; q <= 4; ++q) {  // iZ += X^(4q) G_q
-        launch_power_combine_grouped(g.dd.powers, n, g.dd.blk_elems, g.nblk_elems, q, sm);
-        slice(6 + q);
-        gemm(5 + q);
-    }
+    // iZ += X^(4q) G_q on the camera blocks (the per-scene path's device function)
+    launch_taylor_blocks_grouped(g.dd.powers, n, g.dd.blk_cols, g.nblk_cols, sm);
     // outputs (compute.cpp:168-183, 370-455)
     BCK(cudaEventRecord(b->fork, sm));
     for (int k = 0; k < kBranches; ++k) BCK(cudaStreamWaitEvent(b->branch[k], b->fork, 0));

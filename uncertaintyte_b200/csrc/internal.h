@@ -264,7 +264,9 @@ struct PowerSet {
 };
 // Slices of the int8-sliced products of the blocked-power evaluation (mixed
 // modes with S slices). Product q: 0..5 = X^2, X^3, X^4, X^8, X^12, X^16;
-// 6..9 = X^4 G_1, X^8 G_2, X^12 G_3, X^16 G_4. Z is positive semi-definite,
+// 6..9 = X^4 G_1, X^8 G_2, X^12 G_3, X^16 G_4 (counts kept for the int8
+// product entry points; the solves form these four on the camera blocks in
+// FP64, launch_taylor_blocks). Z is positive semi-definite,
 // so the eigenvalues of X = (Z + lambda I)^-1 are at most 1/lambda and the
 // series term lambda^i / (i-1)! X^(i+1) = X (lambda X)^i / (i-1)! has norm at
 // most ||X|| / (i-1)! (32-bit factorial). G_2 (terms 8..11) therefore adds at
@@ -291,6 +293,11 @@ void launch_power_decide(TeState* te, const unsigned long long* dmax, const Tayl
                          cudaStream_t st);
 // out = c[4q] X + c[4q+1] X^2 + c[4q+2] X^3 + c[4q+3] X^4 (q = 0: into iZ), unless skipped.
 void launch_power_combine(const PowerSet& ps, int q, double* out, const int* skip, cudaStream_t st);
+// The 9 x 9 camera blocks of iZ += X^(4q) G_q, q = 1..4 (skipped blocks left out);
+// grouped: over the cameras of every set (d_blk_cols: the sets' column offsets).
+void launch_taylor_blocks(const PowerSet& ps, cudaStream_t st);
+void launch_taylor_blocks_grouped(const PowerSet* d_sets, int nsets, const long* d_blk_cols, long nblk_cols,
+                                  cudaStream_t st);
 // Grouped forms over many matrices (a batch): one block per column (diag) or
 // per 256 elements (combine) of set m with blk[m] <= b < blk[m + 1].
 void launch_power_diag_grouped(const PowerSet* d_sets, int nsets, const long* d_blk_cols, long nblk, int jlo,

@@ -15,9 +15,12 @@
 //       G_q = c_4q X + c_(4q+1) X^2 + c_(4q+2) X^3 + c_(4q+3) X^4,
 //     with c_0 = 1, c_i = k_i for the performed iterations and 0 after; the
 //     blocks whose coefficients are all zero are skipped on the device.
-// Products: X^2, X^3, X^4, X^8, X^12, then one per non-zero block: 8 for the
-// 12..15 iterations of the reference scenes, instead of 13..16. The
-// polynomial, its coefficients and the stop decisions are the reference's;
+// Products: X^2, X^3, X^4, X^8, X^12 (X^16 past 15 iterations): 5 for the
+// 12..15 iterations of the reference scenes, instead of 13..16. The block
+// terms X^(4q) G_q are formed on the 9 x 9 camera blocks of iZ only, the only
+// part of iZ read afterwards (k_taylor_blocks: 81 N multiply-adds per camera
+// and block instead of a full product). The polynomial, its coefficients and
+// the stop decisions are the reference's;
 // the results differ from the one-product-per-iteration order at the
 // rounding level. Every kernel here has a fixed summation order, so the
 // results are bitwise repeatable.
@@ -168,7 +171,107 @@ __global__ void k_power_combine_grouped(const PowerSet* __restrict__ sets, int n
     if (idx < (long)ps.n * ps.n) power_combine_one(ps, q, q == 0 ? ps.iZ : ps.G, idx);
 }
 
+// The camera blocks of iZ += X^(4q) G_q, q = 1..4 (blocks whose skip word is
+// set left out). Only the 9 x 9 diagonal camera blocks of iZ are read after
+// the series (the camera output, compute.cpp:168-183, and the point stage's
+// block-diagonal camera covariance, compute.cpp:422-441), so these products
+// are formed on those blocks only: element (r, c) of camera block b, r >= c,
+// is sum_k G_q(k, r) X^(4q)(k, c) with G_q(k, r) = c_4q X + c_(4q+1) X^2 +
+// c_(4q+2) X^3 + c_(4q+3) X^4 at (k, r) (G_q and the powers are symmetric,
+// so their columns are their rows), added to iZ(r, c) in the order q = 1..4
+// and written at (r, c) and (c, r). One CTA per camera; each thread sums a
+// fixed stride of k, the partial sums are added in a fixed tree and warp
+// order, so the result is bitwise repeatable.
+constexpr int kBlkThreads = 128;
+constexpr int kBlkPairs = 45;  // lower triangle of a 9 x 9 block
+
+__device__ __forceinline__ void taylor_camera_block(const PowerSet& ps, int cam, double (*red)[kBlkPairs],
+                                                    double* val) {
+    const long ld = ps.ld;
+    const int n = ps.n, c0 = 9 * cam, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid < kBlkPairs) {  // iZ holds G_0 here
+        int r = 0, s = tid;
+        while (s > r) s -= ++r;  // tid = r (r + 1) / 2 + s, s <= r
+        val[tid] = ps.iZ[(c0 + r) + (long)(c0 + s) * ld];
+    }
+    for (int q = 1; q <= 4; ++q) {
+        if (ps.te->skip[q]) continue;  // the same word for every thread of the CTA
+        const double* cq = ps.te->c + 4 * q;
+        const double k0 = cq[0], k1 = cq[1], k2 = cq[2], k3 = cq[3];
+        const double* P = ps.M[q + 2];  // X^4, X^8, X^12, X^16
+        double acc[kBlkPairs];
+#pragma unroll
+        for (int p = 0; p < kBlkPairs; ++p) acc[p] = 0.0;
+        for (int k = tid; k < n; k += kBlkThreads) {
+            double g[9], x[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                const long o = k + (long)(c0 + i) * ld;
+                double v = k0 * ps.M[0][o];
+                v += k1 * ps.M[1][o];
+                v += k2 * ps.M[2][o];
+                v += k3 * ps.M[3][o];
+                g[i] = v;
+                x[i] = P[o];
+            }
+#pragma unroll
+            for (int r = 0, p = 0; r < 9; ++r)
+#pragma unroll
+                for (int s = 0; s <= r; ++s, ++p) acc[p] = fma(g[r], x[s], acc[p]);
+        }
+#pragma unroll
+        for (int p = 0; p < kBlkPairs; ++p) {
+            double a = acc[p];
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) a += __shfl_xor_sync(0xffffffffu, a, d);
+            if (lane == 0) red[warp][p] = a;
+        }
+        __syncthreads();
+        if (tid < kBlkPairs) {
+            double t = red[0][tid];
+#pragma unroll
+            for (int w = 1; w < kBlkThreads / 32; ++w) t += red[w][tid];
+            val[tid] += t;
+        }
+        __syncthreads();  // red is reused by the next block
+    }
+    if (tid < kBlkPairs) {
+        int r = 0, s = tid;
+        while (s > r) s -= ++r;
+        ps.iZ[(c0 + r) + (long)(c0 + s) * ld] = val[tid];
+        ps.iZ[(c0 + s) + (long)(c0 + r) * ld] = val[tid];
+    }
+}
+
+__global__ void __launch_bounds__(kBlkThreads) k_taylor_blocks(PowerSet ps) {
+    __shared__ double red[kBlkThreads / 32][kBlkPairs];
+    __shared__ double val[kBlkPairs];
+    taylor_camera_block(ps, blockIdx.x, red, val);
+}
+
+// The same over the cameras of many sets: blk holds the sets' column offsets
+// (multiples of 9), so set m owns the cameras [blk[m] / 9, blk[m + 1] / 9).
+__global__ void __launch_bounds__(kBlkThreads) k_taylor_blocks_grouped(const PowerSet* __restrict__ sets, int nsets,
+                                                                       const long* __restrict__ blk) {
+    const int m = set_of_block(blk, nsets, 9L * blockIdx.x);
+    __shared__ double red[kBlkThreads / 32][kBlkPairs];
+    __shared__ double val[kBlkPairs];
+    taylor_camera_block(sets[m], (int)(blockIdx.x - blk[m] / 9), red, val);
+}
+
 }  // namespace
+
+void launch_taylor_blocks(const PowerSet& ps, cudaStream_t st) {
+    k_taylor_blocks<<<ps.n / 9, kBlkThreads, 0, st>>>(ps);
+    count_launch();
+}
+
+void launch_taylor_blocks_grouped(const PowerSet* d_sets, int nsets, const long* d_blk_cols, long nblk_cols,
+                                  cudaStream_t st) {
+    if (nsets <= 0 || nblk_cols < 9) return;
+    k_taylor_blocks_grouped<<<(unsigned)(nblk_cols / 9), kBlkThreads, 0, st>>>(d_sets, nsets, d_blk_cols);
+    count_launch();
+}
 
 void launch_power_diag(const PowerSet& ps, int jlo, int jhi, const int* skip, cudaStream_t st) {
     if (jlo == 2 && jhi == 16) {
