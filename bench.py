@@ -648,8 +648,8 @@ def run_ours(a):
             ops = prod_i8  # issued by the library's slice schedule, product by product
             achieved = ops / prod_s / 1e12
             peak = _int8_peak_tops(torch, dev)
-            roof = {"bound": "tensor", "kernel": f"k_ozaki_gemm (tcgen05 kind::i8, TMA, {slices} slices for X^2..X^4 "
-                                                 f"and X^4 G_1, fewer for the higher powers and blocks; "
+            roof = {"bound": "tensor", "kernel": f"k_ozaki_gemm (tcgen05 kind::i8, TMA, {slices} slices for X^2..X^4, "
+                                                 f"one fewer for X^8, X^12, X^16; "
                                                  f"128x{_mixed_tile_n(N, slices)} lower tiles at {slices} slices, "
                                                  f"128x128 below)",
                     "achieved": achieved, "peak": peak, "unit": "TOP/s int8",
