@@ -641,8 +641,9 @@ int run_pipeline(unc_context* ctx, const unc_options* o, int num_rows, long long
     };
     // The blocked-power evaluation (powers.cu): X^2, X^3, X^4, X^8, X^12 and
     // X^16 (skipped on the device unless the rule passes iteration 15); the
-    // stop rule from their diagonal maxima; iZ = G_0 + sum_q X^(4q) G_q with
-    // the blocks whose coefficients are all zero skipped on the device.
+    // stop rule from their diagonal maxima; iZ = G_0 + sum_q X^(4q) G_q, the
+    // products on the camera blocks only, with the blocks whose coefficients
+    // are all zero skipped on the device.
     PowerSet ps{};
     ps.M[0] = b.Z;
     ps.M[1] = b.add;

@@ -203,6 +203,8 @@ int slices_of(int precision) {
 // per scene: X (A, B), A operand (A), X^4 (A, B), X^8 (A, B), X^12 (B), X^16 (B), and X^4, X^8, X^12, X^16
 // as B operands of 128-column tiles (the products with fewer slices than the group's)
 constexpr int kMaps = 13;
+// descriptor sets (the last four of each are laid out but not launched: the
+// block terms X^(4q) G_q are formed on the camera blocks, launch_taylor_blocks)
 constexpr int kSliceSets = 11;  // X, X^2, X^3, X^4, X^8, X^12, X^16, G_1..G_4
 constexpr int kGemmSets = 10;   // X^2, X^3, X^4, X^8, X^12, X^16, X^4 G_1 .. X^16 G_4
 
