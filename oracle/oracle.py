@@ -37,6 +37,7 @@ class OracleOptions(C.Structure):
         ("z_perturb_terms", C.c_double),
         ("swap_products", C.c_int),
         ("skip_dense", C.c_int),
+        ("offdiag_nan", C.c_int),
     ]
 
 
@@ -104,7 +105,7 @@ def _p(a, t):
 
 def compute(jac, algorithm=2, lam=-1.0, epsilon=1e-10, svd_remove_n=-1, faithful_point_scan=False,
             threads=0, debug=False, cam_init=None, pt_init=None, route="lu", z_perturb=0.0,
-            z_perturb_terms=0.0, swap_products=False, skip_dense=False):
+            z_perturb_terms=0.0, swap_products=False, skip_dense=False, offdiag_nan=False):
     """Run the oracle on a Jacobian (uncertaintyte_b200.jacob.Jacobian-like object).
 
     route: "lu" (the reference's ScaledDenseMatrix::inv) or "cholesky" (the
@@ -115,7 +116,9 @@ def compute(jac, algorithm=2, lam=-1.0, epsilon=1e-10, svd_remove_n=-1, faithful
     Taylor products as X * add instead of add * X (same series, other
     rounding). skip_dense:
     timing samples only (the dense inverse and Taylor loop are skipped, the
-    outputs are meaningless). Returns dict(cam, pt, stats[, Z, iZ, d])."""
+    outputs are meaningless). offdiag_nan: iZ outside its camera diagonal
+    blocks set to NaN before the outputs (which entries the outputs read).
+    Returns dict(cam, pt, stats[, Z, iZ, d])."""
     o = OracleOptions()
     o.algorithm = algorithm
     o.epsilon = epsilon
@@ -133,6 +136,7 @@ def compute(jac, algorithm=2, lam=-1.0, epsilon=1e-10, svd_remove_n=-1, faithful
     o.z_perturb_terms = z_perturb_terms
     o.swap_products = int(bool(swap_products))
     o.skip_dense = int(bool(skip_dense))
+    o.offdiag_nan = int(bool(offdiag_nan))
     ncam = jac.num_cams * jac.cam_params * (jac.cam_params + 1) // 2
     cam = np.zeros(ncam) if cam_init is None else np.array(cam_init, dtype=np.float64)
     pt = np.zeros(jac.num_points * 6) if pt_init is None else np.array(pt_init, dtype=np.float64)

@@ -26,6 +26,7 @@
 #include <cfloat>
 #include <chrono>
 #include <cmath>
+#include <limits>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -924,6 +925,12 @@ extern "C" int oracle_compute(const oracle_options* opt, int nrows, int ncols, c
         oracle_te_inverse_route(N, Z.data(), lambda, opt->inverse_route, st, opt->swap_products);
     }
     if (dbg_iZ) std::copy(Z.begin(), Z.end(), dbg_iZ);
+    if (opt->offdiag_nan) {
+        const int cp_ = opt->cam_params;
+        for (int c = 0; c < N; ++c)
+            for (int r = 0; r < N; ++r)
+                if (r / cp_ != c / cp_) Z[r + (size_t)c * N] = std::numeric_limits<double>::quiet_NaN();
+    }
 
     auto t7 = Clock::now();
     camera_output(Z.data(), N, d.data(), opt->num_cams, cp, cam_unc);

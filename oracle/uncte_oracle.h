@@ -48,6 +48,11 @@ typedef struct {
     int skip_dense;           /* timing samples only: 1 skips the dense inverse and the Taylor loop (iZ is
                                  left as Z + lambda*I), so every sparse stage runs at full size but the
                                  outputs are meaningless. 0 for results. */
+    int offdiag_nan;          /* 1: every entry of the final iZ outside its cam_params x cam_params diagonal
+                                 camera blocks is set to NaN before the camera and point outputs, which
+                                 shows what the outputs read (compute.cpp:168-183, 422-441): they are
+                                 unchanged, so a solver may form the last Taylor terms on those blocks only.
+                                 0 for results. */
 } oracle_options;
 
 typedef struct {

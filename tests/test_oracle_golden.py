@@ -45,6 +45,18 @@ def test_daliborka_points(daliborka):
     assert block_rel_err(pt, gp, 6) < 1e-5
 
 
+def test_outputs_read_only_the_camera_blocks_of_iz(daliborka):
+    """The reference's outputs depend on the final Taylor-series inverse iZ only
+    through its 9 x 9 diagonal camera blocks (removeScaleJ4Z, compute.cpp:168-183,
+    and the block-diagonal camera covariance of the point stage, compute.cpp:422-441):
+    with every other entry of iZ set to NaN the outputs are bitwise the same. The
+    CUDA path relies on this when it forms the last Taylor terms on those blocks only."""
+    jac, out, g = daliborka
+    masked = oracle.compute(jac, threads=8, offdiag_nan=True)
+    np.testing.assert_array_equal(masked["cam"], out["cam"])
+    np.testing.assert_array_equal(masked["pt"], out["pt"])
+
+
 def test_daliborka_faithful_scan_matches_indexed(daliborka):
     jac, out, g = daliborka
     out2 = oracle.compute(jac, threads=8, faithful_point_scan=True)
