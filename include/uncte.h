@@ -211,7 +211,10 @@ int unc_context_set_priority(unc_context* ctx, int high);
  * max_inflight worker threads, each with its own context (stream and reused
  * workspace), run requests concurrently; a request starts when a worker is
  * free and its unc_request_bytes fit in max_device_bytes (<= 0: 90 % of the
- * free device memory at creation) next to the running ones. The host arrays of
+ * free device memory at creation) next to the running requests and the
+ * workspaces idle workers hold (each worker keeps one for single requests and
+ * one for packs of small requests; idle ones are freed when that makes room).
+ * The host arrays of
  * a request (Jacobian in, covariances out) must stay valid until
  * unc_server_wait has returned its result. Results do not depend on what else
  * runs. Thread-safe. */
